@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Agent-steps/s of the per-step hot path on B200.
+
+Default workload (one GPU): a 3D growing colony snapshot of 10^6 agents in
+[0,400]^3 at packed density (0.15 agents per unit volume), Float32, soft-sphere
+repulsion/adhesion (k=10, a=1, r=1), Euler–Maruyama noise sigma=0.05, volume
+growth with division at v=2 and death probability 1e-4 (divisions occur every
+step), CLVD neighbors with list radius 3.3 and rebuild threshold 0.15,
+dt=0.005.  A "step" is one step! (rule, DE, update!, computeNeighbors!).
+
+  value  : device time (CUDA events on the library's stream, CUDA-graph replay),
+           inputs resident in HBM, L2 flushed between timed steps
+  e2e    : loadToPlatform! + step! + bringFromPlatform! per step through the
+           C ABI, from and to pinned host buffers (host copies included)
+  roofline: the dominant kernel's algorithmic bytes / its event-timed duration
+  cpu_baseline: the CPU checker (C++ restatement of the reference CPU path,
+           CellLinked rebuilt every step, OpenMP over agents) on the same
+           workload, a bounded sample of steps
+
+--gpus N (under torchrun) runs N independent colonies, one per rank (weak
+scaling, no data-path collective); the time is the max over ranks.
+--impl reference times the CPU restatement of the reference path instead.
+"""
+import argparse
+import datetime
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "agent-steps/s at 1M agents 3D; batched & adjoint vs plain, one B200"
+UNIT = "agent-steps/s"
+
+
+def load_package():
+    import importlib.util
+    if "cbm_b200" in sys.modules:
+        return sys.modules["cbm_b200"]
+    pkg = os.path.join(ROOT, "cellbasedmodels.jl_b200")
+    spec = importlib.util.spec_from_file_location(
+        "cbm_b200", os.path.join(pkg, "__init__.py"), submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["cbm_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax = max(smax, float(p[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, p[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def alg_bytes_per_agent(name, s, d, nbar, verlet, fate):
+    """Compulsory HBM bytes per agent of one launch (neighbor-position gathers,
+    which are served from L2, are not counted)."""
+    if name == "k_agent_de":
+        b = 2 * d * s + 2 * s + s  # positions r/w, volume r/w, growth rate
+        b += (4 + 4 * nbar) if verlet else 8  # list count + entries, or own cell range
+        b += d * s if verlet else 0  # displacement check against posOld
+        b += 1 if fate else 0  # fate byte
+        return b
+    if name == "k_verlet_list":
+        return d * s + 4 * nbar + 4  # positions, list entries, count
+    if name == "k_cells_hist":
+        return d * s + 8 + (d * s if verlet else 0)
+    if name == "k_cells_scatter":
+        return 12
+    if name == "k_cells_stable":
+        return 8
+    if name == "k_agent_rule":
+        return 2 * s + 1
+    return None
+
+
+def make_workload(abi, args, rank):
+    from scenarios import packed_colony_3d
+    prec = abi.F64 if args.precision == "f64" else abi.F32
+    kw, state = packed_colony_3d(abi, N=args.n, seed=2 + rank, precision=prec)
+    return kw, state
+
+
+def pinned_state(cbm, cfg, state, capacity):
+    import torch
+    dt = torch.float64 if cfg.precision == cbm._abi.F64 else torch.float32
+    bufs = cbm._abi.StateBuffers(cfg, capacity, 0)
+    for k in list(bufs.arrays):
+        tdt = torch.int64 if k in ("id", "parent") else dt
+        bufs.arrays[k] = torch.zeros(capacity, dtype=tdt, pin_memory=True).numpy()
+    for k, v in state.items():
+        if k in bufs.arrays:
+            bufs.arrays[k][: len(v)] = v
+    return bufs
+
+
+def run_ours(args, rank, world, local_rank):
+    import ctypes as C
+
+    import torch
+    cbm = load_package()
+    abi = cbm._abi
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    kw, state = make_workload(abi, args, rank)
+    cfg = abi.make_config(**kw)
+    ctx = cbm.Context(cfg)
+    ctx.upload(state)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    for _ in range(args.warmup):
+        ctx.step(1, abi.SYNC)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local_rank)
+    clocks.start()
+    total_ms, agent_steps = 0.0, 0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for _ in range(args.steps):
+        n_before = ctx.counters()["N"]
+        e0.record(stream)
+        ctx.step(1, 0)
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        agent_steps += n_before
+        flush.zero_()  # evict L2 (256 MB > 126 MB) between timed steps
+        torch.cuda.synchronize()
+    ctx.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist:
+        t = torch.tensor([total_ms, float(agent_steps)], dtype=torch.float64, device="cuda")
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = t.clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        total_ms_job, agent_steps_job = float(tmax[0]), float(tsum[1])
+    else:
+        total_ms_job, agent_steps_job = total_ms, float(agent_steps)
+    value = agent_steps_job / (total_ms_job / 1e3)
+    ms_per_step = total_ms_job / args.steps
+
+    # per-kernel durations of eager steps (events on the library stream)
+    prof = {}
+    for _ in range(args.profile_steps):
+        for name, ms in ctx.profile_step():
+            prof.setdefault(name, []).append(ms)
+    n_now = ctx.counters()["N"]
+    verlet = cfg.neighbors in (abi.NEIGH_CLVD, abi.NEIGH_VERLET_DISPLACEMENT)
+    nbar = float(np.mean(ctx.neighbors()[0])) if verlet else 0.0
+    s = 8 if cfg.precision == abi.F64 else 4
+    kern = {k: (float(np.mean(v)), float(np.sum(v))) for k, v in prof.items()}
+    top = max(kern, key=lambda k: kern[k][1])
+    hbm, peak_kind = peaks()
+    bpa = alg_bytes_per_agent(top, s, cfg.dims, nbar, verlet, cfg.fate != abi.FATE_NONE)
+    roof = None
+    if bpa is not None:
+        achieved = bpa * n_now / (kern[top][0] / 1e3) / 1e9
+        roof = {"kernel": top, "bound": "hbm", "achieved": round(achieved, 1),
+                "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "traffic": None,
+                "alg_bytes_per_agent": round(bpa, 2), "agents": n_now, "nbar": round(nbar, 2),
+                "avg_ms": round(kern[top][0], 4)}
+    step_share = {k: round(v[1] / sum(x[1] for x in kern.values()), 4) for k, v in kern.items()}
+
+    # end to end through the C ABI with pinned host buffers
+    cap = int(cfg.n_max)
+    snap = ctx.download()
+    host = pinned_state(cbm, cfg, {k: snap[k] for k in ("x", "y", "z", "v", "g", "id", "parent")},
+                        cap)
+    lib = ctx.lib
+    e2e_time, e2e_agents, h2d, d2h = 0.0, 0, 0, 0
+    nstate = snap["N"]
+    t_now, st_now, idm = snap["t"], snap["step"], snap["id_max"]
+    per_agent = 3 * s + 2 * s + 16  # x,y,z,v,g + id,parent
+    for k in range(args.e2e_steps):
+        view = host.view(N=nstate, t=t_now, step=st_now, id_max=idm,
+                         fields=("x", "y", "z", "v", "g", "id", "parent"))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx._check(lib.cbm_upload(ctx.h, C.byref(view)))
+        ctx._check(lib.cbm_step(ctx.h, 1, abi.SYNC))
+        view.capacity = cap
+        ctx._check(lib.cbm_download(ctx.h, C.byref(view), abi.VIEW_COMMITTED))
+        t1 = time.perf_counter()
+        if k > 0:  # the first call also builds the step graph of this parity
+            e2e_time += t1 - t0
+            e2e_agents += nstate
+            h2d += nstate * per_agent
+            d2h += view.N * per_agent
+        nstate, t_now, st_now, idm = view.N, view.t, view.step, view.id_max
+    n_e2e = max(args.e2e_steps - 1, 1)
+    if dist:
+        t = torch.tensor([e2e_time, float(e2e_agents)], dtype=torch.float64, device="cuda")
+        tm = t.clone()
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        ts = t.clone()
+        dist.all_reduce(ts, op=dist.ReduceOp.SUM)
+        e2e_value = float(ts[1]) / float(tm[0])
+    else:
+        e2e_value = e2e_agents / e2e_time
+    launches = ctx.kernels_per_step() * args.steps
+    return dict(value=value, ms_per_step=ms_per_step, roof=roof, share=step_share, kern=kern,
+                clocks=clk, e2e=dict(value=round(e2e_value, 1), unit=UNIT,
+                                     h2d_bytes_per_step=int(h2d / n_e2e),
+                                     d2h_bytes_per_step=int(d2h / n_e2e)),
+                launches=launches, cfg=cfg, state_n=len(state["x"]), kw=kw)
+
+
+def cpu_baseline(args, steps, threads=None):
+    """The CPU checker on the same workload (CellLinked, rebuilt every step)."""
+    cbm = load_package()
+    abi = cbm._abi
+    from _oracle import OracleContext
+    kw, state = make_workload(abi, args, 0)
+    kw = dict(kw, neighbors=abi.NEIGH_CELL_LINKED, precision=abi.F64)
+    cfg = abi.make_config(**kw)
+    threads = threads or os.cpu_count()
+    o = OracleContext(abi, cfg, threads=threads)
+    o.upload(state)
+    agent_steps, wall = 0, 0.0
+    for _ in range(steps):
+        n = o.counters()["N"]
+        t0 = time.perf_counter()
+        o.step(1)
+        wall += time.perf_counter() - t0
+        agent_steps += n
+    return dict(value=agent_steps / wall, unit=UNIT, cores=threads, kind="port",
+                sample=f"{steps} full steps of the {args.n}-agent colony, Float64, "
+                       f"CellLinked(3.3) rebuilt every step, OpenMP over agents")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--profile-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=6)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    workload = (f"3D growing colony snapshot, {args.n} agents in a packed ball in [0,400]^3, "
+                f"{args.precision}, EM sigma 0.05, division at v=2 + death 1e-4 every step, "
+                f"CLVD R_list 3.3 rebuild 0.15, dt 0.005")
+    config = {"workload": workload, "n_agents": args.n, "n_max": int(1.2 * args.n),
+              "neighbors": "CLVD", "l2": "flushed between timed steps (256 MB write)",
+              "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "single GPU"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        steps = args.steps + args.warmup
+        cb = cpu_baseline(args, max(1, min(args.steps, 5)))
+        line = {"metric": METRIC, "value": round(cb["value"], 1), "unit": UNIT,
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(1e3 * args.n / cb["value"], 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config, "impl": "reference",
+                "cpu_baseline": cb,
+                "e2e": {"value": round(cb["value"], 1), "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+                "note": "the reference is Julia and cannot run here; this times its C++ "
+                        "restatement (the CPU checker) on the host cores; "
+                        f"{min(args.steps, 5)} of {steps} requested steps were run"}
+        print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    r = run_ours(args, rank, world, local_rank)
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(args, args.cpu_steps)
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(r["value"], 1), "unit": UNIT,
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(r["ms_per_step"], 4), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
+                "data": "synthetic", "config": config, "roofline": r["roof"],
+                "cpu_baseline": cb, "e2e": r["e2e"], "gpu_launches": r["launches"],
+                "clocks": r["clocks"], "kernel_share": r["share"],
+                "kernel_avg_ms": {k: round(v[0], 4) for k, v in r["kern"].items()}}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,324 @@
+"""ctypes binding of include/cbm_b200.h (libcbm_b200.so).
+
+The structures mirror the C declarations field by field; `Context` wraps one
+cbm_ctx.  There is no fallback: if the shared library or a CUDA device is
+missing, loading or cbm_create fails with an exception.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcbm_b200.so")
+
+# ---- constants (include/cbm_b200.h) ------------------------------------------
+CBM_OK = 0
+CBM_ERR_ARG = 1
+CBM_ERR_CUDA = 2
+CBM_ERR_AGENT_OVERFLOW = 3
+CBM_ERR_NEIGHBOR_OVERFLOW = 4
+CBM_ERR_TIMEOUT = 5
+CBM_ERR_STATE = 6
+CBM_ERR_NOMEM = 7
+ERR_NAMES = {1: "CBM_ERR_ARG", 2: "CBM_ERR_CUDA", 3: "CBM_ERR_AGENT_OVERFLOW",
+             4: "CBM_ERR_NEIGHBOR_OVERFLOW", 5: "CBM_ERR_TIMEOUT", 6: "CBM_ERR_STATE",
+             7: "CBM_ERR_NOMEM"}
+
+F32, F64 = 0, 1
+NEIGH_NONE, NEIGH_FULL, NEIGH_CELL_LINKED, NEIGH_VERLET_DISPLACEMENT, NEIGH_CLVD = 0, 1, 2, 3, 4
+INT_EULER, INT_EM = 0, 1
+FORCE_DIRECT, FORCE_LAGGED = 0, 1
+ATT_FROM_REP, ATT_TO_ATT = 0, 1
+WALLS_NONE, WALLS_REFLECT, WALLS_PUSH = 0, 1, 2
+FATE_NONE, FATE_VOLUME, FATE_ID_PARITY = 0, 1, 2
+MEDIUM_NEAREST, MEDIUM_BILINEAR = 0, 1
+SYNC, NO_GRAPH = 1, 2
+VIEW_COMMITTED, VIEW_NEW = 0, 1
+STAGES = ("agent_rule", "agent_de", "medium_rule", "medium_de", "update", "neighbors")
+
+
+class CbmConfig(C.Structure):
+    _fields_ = [
+        ("dims", C.c_int32), ("precision", C.c_int32), ("n_max", C.c_int64),
+        ("box_lo", C.c_double * 3), ("box_hi", C.c_double * 3), ("dt", C.c_double),
+        ("seed", C.c_uint64), ("community", C.c_uint32), ("neighbors", C.c_int32),
+        ("n_max_neighbors", C.c_int32), ("integrator", C.c_int32),
+        ("cell_edge", C.c_double), ("skin", C.c_double), ("rebuild_threshold", C.c_double),
+        ("sigma", C.c_double), ("force_mode", C.c_int32), ("att_form", C.c_int32),
+        ("k_rep", C.c_double), ("r_rep", C.c_double), ("k_att", C.c_double),
+        ("r_att", C.c_double), ("walls", C.c_int32), ("fate", C.c_int32),
+        ("wall_force", C.c_double), ("wall_range", C.c_double), ("drift_linear", C.c_double),
+        ("growth", C.c_int32), ("medium", C.c_int32), ("v_div", C.c_double),
+        ("div_sep", C.c_double), ("p_death", C.c_double), ("n_medium", C.c_int32 * 3),
+        ("medium_sampling", C.c_int32), ("diff_D", C.c_double), ("decay", C.c_double),
+        ("secretion", C.c_double), ("chemotaxis", C.c_double),
+    ]
+
+
+class CbmStateView(C.Structure):
+    _fields_ = [
+        ("N", C.c_int64), ("capacity", C.c_int64), ("t", C.c_double), ("step", C.c_int64),
+        ("id_max", C.c_int64), ("pos", C.c_void_p * 3), ("v", C.c_void_p), ("g", C.c_void_p),
+        ("f", C.c_void_p * 3), ("id", C.POINTER(C.c_int64)), ("parent", C.POINTER(C.c_int64)),
+        ("medium_c", C.c_void_p), ("medium_grad", C.c_void_p * 3),
+    ]
+
+
+def make_config(**kw):
+    """cbm_config with the reference's defaults; keyword names are the C field names."""
+    cfg = CbmConfig()
+    defaults = dict(dims=3, precision=F64, n_max=0, box_lo=(0.0, 0.0, 0.0),
+                    box_hi=(1.0, 1.0, 1.0), dt=1.0, seed=0, community=0,
+                    neighbors=NEIGH_NONE, n_max_neighbors=32, integrator=INT_EULER,
+                    cell_edge=1.0, skin=1.0, rebuild_threshold=0.0, sigma=0.0,
+                    force_mode=FORCE_DIRECT, att_form=ATT_FROM_REP, k_rep=0.0, r_rep=0.0,
+                    k_att=0.0, r_att=0.0, walls=WALLS_NONE, fate=FATE_NONE, wall_force=0.0,
+                    wall_range=0.0, drift_linear=0.0, growth=0, medium=0, v_div=0.0,
+                    div_sep=0.0, p_death=0.0, n_medium=(1, 1, 1),
+                    medium_sampling=MEDIUM_NEAREST, diff_D=0.0, decay=0.0, secretion=0.0,
+                    chemotaxis=0.0)
+    unknown = set(kw) - set(defaults)
+    if unknown:
+        raise TypeError(f"unknown cbm_config fields: {sorted(unknown)}")
+    defaults.update(kw)
+    for name, val in defaults.items():
+        if name in ("box_lo", "box_hi"):
+            v = list(val) + [0.0] * (3 - len(val))
+            setattr(cfg, name, (C.c_double * 3)(*v[:3]))
+        elif name == "n_medium":
+            v = list(val) + [1] * (3 - len(val))
+            setattr(cfg, name, (C.c_int32 * 3)(*v[:3]))
+        else:
+            setattr(cfg, name, val)
+    return cfg
+
+
+def real_dtype(cfg):
+    return np.float64 if cfg.precision == F64 else np.float32
+
+
+class CbmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Loads libcbm_b200.so once.  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with build.py (nvcc, sm_100a)")
+    lib = C.CDLL(path)
+    vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+    sig = {
+        "cbm_version": (C.c_char_p, []),
+        "cbm_last_error": (C.c_char_p, [vp]),
+        "cbm_create": (C.c_int, [C.POINTER(vp), C.POINTER(CbmConfig)]),
+        "cbm_destroy": (None, [vp]),
+        "cbm_upload": (C.c_int, [vp, C.POINTER(CbmStateView)]),
+        "cbm_download": (C.c_int, [vp, C.POINTER(CbmStateView), i32]),
+        "cbm_step": (C.c_int, [vp, i32, i32]),
+        "cbm_agent_step_rule": (C.c_int, [vp]),
+        "cbm_agent_step_de": (C.c_int, [vp]),
+        "cbm_medium_step_rule": (C.c_int, [vp]),
+        "cbm_medium_step_de": (C.c_int, [vp]),
+        "cbm_update": (C.c_int, [vp]),
+        "cbm_compute_neighbors": (C.c_int, [vp]),
+        "cbm_sync": (C.c_int, [vp]),
+        "cbm_get_counters": (C.c_int, [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64),
+                                       C.POINTER(i64), C.POINTER(i32), C.POINTER(i64)]),
+        "cbm_grid_shape": (C.c_int, [vp, C.POINTER(i32)]),
+        "cbm_get_grid": (C.c_int, [vp, vp, vp, vp, vp]),
+        "cbm_get_neighbors": (C.c_int, [vp, vp, vp, i64]),
+        "cbm_count_neighbors": (C.c_int, [vp, dbl, vp]),
+        "cbm_rng_fill": (C.c_int, [vp, i32, dbl, dbl, i64, i64, vp]),
+        "cbm_stream": (vp, [vp]),
+        "cbm_kernels_per_step": (C.c_int, [vp]),
+        "cbm_profile_step": (C.c_int, [vp, i32, C.POINTER(C.c_float), C.POINTER(C.c_char_p),
+                                       C.POINTER(i32)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class StateBuffers:
+    """Host arrays of one Community plus the cbm_state_view pointing at them."""
+
+    AGENT_REAL = ("x", "y", "z", "v", "g", "fx", "fy", "fz")
+    MEDIUM = ("c", "gx", "gy", "gz")
+
+    def __init__(self, cfg, capacity, n_nodes):
+        dt = real_dtype(cfg)
+        self.cfg = cfg
+        self.capacity = capacity
+        self.arrays = {k: np.zeros(capacity, dt) for k in self.AGENT_REAL}
+        self.arrays["id"] = np.zeros(capacity, np.int64)
+        self.arrays["parent"] = np.zeros(capacity, np.int64)
+        for k in self.MEDIUM:
+            self.arrays[k] = np.zeros(max(n_nodes, 1), dt)
+        self.n_nodes = n_nodes
+
+    def view(self, N=0, t=0.0, step=0, id_max=0, fields=None):
+        a = self.arrays
+        d = self.cfg.dims
+        use = set(fields) if fields is not None else None
+
+        def sel(k):
+            return a[k] if (use is None or k in use) else None
+
+        s = CbmStateView()
+        s.N, s.capacity, s.t, s.step, s.id_max = N, self.capacity, t, step, id_max
+        for i, k in enumerate(("x", "y", "z")):
+            s.pos[i] = _ptr(sel(k)) if i < d else None
+        s.v = _ptr(sel("v"))
+        s.g = _ptr(sel("g"))
+        for i, k in enumerate(("fx", "fy", "fz")):
+            s.f[i] = _ptr(sel(k)) if i < d else None
+        s.id = a["id"].ctypes.data_as(C.POINTER(C.c_int64)) if sel("id") is not None else None
+        s.parent = (a["parent"].ctypes.data_as(C.POINTER(C.c_int64))
+                    if sel("parent") is not None else None)
+        if self.n_nodes:
+            s.medium_c = _ptr(sel("c"))
+            for i, k in enumerate(("gx", "gy", "gz")):
+                s.medium_grad[i] = _ptr(sel(k)) if i < d else None
+        return s
+
+
+def state_from_dict(cfg, state, capacity=None, n_nodes=0):
+    """Packs a dict of arrays (x, y, z, v, g, fx.., id, parent, c, gx..) into buffers."""
+    N = int(state.get("N", len(state["x"])))
+    cap = max(capacity or 0, N, 1)
+    buf = StateBuffers(cfg, cap, n_nodes)
+    present = []
+    for k, arr in state.items():
+        if k in buf.arrays and arr is not None:
+            arr = np.asarray(arr)
+            dst = buf.arrays[k]
+            n = N if k not in StateBuffers.MEDIUM else n_nodes
+            dst[:n] = arr[:n]
+            present.append(k)
+    return buf, N, present
+
+
+class Context:
+    """One cbm_ctx: a Community loaded on the B200 platform."""
+
+    def __init__(self, cfg):
+        self.lib = load_library()
+        self.cfg = cfg
+        h = C.c_void_p()
+        rc = self.lib.cbm_create(C.byref(h), C.byref(cfg))
+        if rc != CBM_OK:
+            raise CbmError(rc, self.lib.cbm_last_error(None).decode())
+        self.h = h
+        self.n_nodes = int(np.prod([cfg.n_medium[d] for d in range(cfg.dims)])) if cfg.medium else 0
+
+    def _check(self, rc):
+        if rc != CBM_OK:
+            raise CbmError(rc, self.lib.cbm_last_error(self.h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cbm_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def upload(self, state, t=0.0, step=0, id_max=0):
+        buf, N, present = state_from_dict(self.cfg, state, n_nodes=self.n_nodes)
+        fields = present + [k for k in ("x", "y", "z") if k in present]
+        view = buf.view(N=N, t=t, step=step, id_max=id_max, fields=fields)
+        self._check(self.lib.cbm_upload(self.h, C.byref(view)))
+
+    def download(self, which=VIEW_COMMITTED, capacity=None):
+        cap = capacity or max(int(self.cfg.n_max), 1)
+        buf = StateBuffers(self.cfg, cap, self.n_nodes)
+        view = buf.view()
+        self._check(self.lib.cbm_download(self.h, C.byref(view), which))
+        N = view.N
+        out = {k: v[:N].copy() for k, v in buf.arrays.items() if k not in StateBuffers.MEDIUM}
+        if self.n_nodes:
+            for k in StateBuffers.MEDIUM:
+                out[k] = buf.arrays[k][: self.n_nodes].copy()
+        out.update(N=N, t=view.t, step=view.step, id_max=view.id_max)
+        return out
+
+    def step(self, n=1, flags=SYNC):
+        return self._check(self.lib.cbm_step(self.h, n, flags))
+
+    def stage(self, name):
+        fn = {"agent_rule": self.lib.cbm_agent_step_rule, "agent_de": self.lib.cbm_agent_step_de,
+              "medium_rule": self.lib.cbm_medium_step_rule, "medium_de": self.lib.cbm_medium_step_de,
+              "update": self.lib.cbm_update, "neighbors": self.lib.cbm_compute_neighbors}[name]
+        return self._check(fn(self.h))
+
+    def sync(self):
+        return self._check(self.lib.cbm_sync(self.h))
+
+    def counters(self):
+        v = [C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64(), C.c_int32(), C.c_int64()]
+        self._check(self.lib.cbm_get_counters(self.h, *[C.byref(x) for x in v]))
+        return dict(N=v[0].value, n_add=v[1].value, n_remove=v[2].value, id_max=v[3].value,
+                    flag=v[4].value, step=v[5].value)
+
+    def grid(self):
+        n3 = (C.c_int32 * 3)()
+        self._check(self.lib.cbm_grid_shape(self.h, n3))
+        nc = int(n3[0]) * int(n3[1]) * int(n3[2])
+        N = self.counters()["N"]
+        agent_cell = np.zeros(max(N, 1), np.int32)
+        agent_list = np.zeros(max(N, 1), np.int32)
+        start = np.zeros(nc, np.int32)
+        count = np.zeros(nc, np.int32)
+        self._check(self.lib.cbm_get_grid(self.h, _ptr(agent_cell), _ptr(start), _ptr(count),
+                                          _ptr(agent_list)))
+        return dict(shape=tuple(int(v) for v in n3), agent_cell=agent_cell[:N], cell_start=start,
+                    cell_count=count, cell_agents=agent_list[:N])
+
+    def neighbors(self):
+        N = self.counters()["N"]
+        M = int(self.cfg.n_max_neighbors)
+        counts = np.zeros(max(N, 1), np.int32)
+        lst = np.zeros(max(N * M, 1), np.int32)
+        self._check(self.lib.cbm_get_neighbors(self.h, _ptr(counts), _ptr(lst), lst.size))
+        return counts[:N], lst[: N * M].reshape(N, M)
+
+    def count_neighbors(self, radius):
+        N = self.counters()["N"]
+        out = np.zeros(max(N, 1), np.int32)
+        self._check(self.lib.cbm_count_neighbors(self.h, float(radius), _ptr(out)))
+        return out[:N]
+
+    def rng_fill(self, kind, a, b, n, step=0):
+        out = np.zeros(max(n, 1), real_dtype(self.cfg))
+        self._check(self.lib.cbm_rng_fill(self.h, kind, float(a), float(b), n, step, _ptr(out)))
+        return out[:n]
+
+    def stream(self):
+        return self.lib.cbm_stream(self.h)
+
+    def kernels_per_step(self):
+        return self.lib.cbm_kernels_per_step(self.h)
+
+    def profile_step(self):
+        """One eager step with per-kernel event timing: [(kernel name, ms)]."""
+        ms = (C.c_float * 64)()
+        names = (C.c_char_p * 64)()
+        n = C.c_int32()
+        self._check(self.lib.cbm_profile_step(self.h, 64, ms, names, C.byref(n)))
+        return [(names[i].decode(), ms[i]) for i in range(min(n.value, 64))]

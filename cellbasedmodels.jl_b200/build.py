@@ -1,0 +1,52 @@
+"""Builds libcbm_b200.so, the sm_100a shared library behind include/cbm_b200.h.
+
+`python build.py` (or `build()` from Python) runs nvcc directly; the library
+is written next to this file so it travels with the source tree.  Flags:
+  -gencode arch=compute_100a,code=sm_100a  B200 only
+  -fmad=false   no FMA contraction: the same rounding as the Julia reference
+                and the CPU checker, which makes results bit-identical
+  -lineinfo     source lines for ncu
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libcbm_b200.so")
+SOURCES = [os.path.join(HERE, "csrc", "cbm_api.cu")]
+DEPS = SOURCES + [
+    os.path.join(HERE, "csrc", "cbm_kernels.cuh"),
+    os.path.join(HERE, "..", "include", "cbm_b200.h"),
+    os.path.join(HERE, "..", "include", "cbm_rng.h"),
+]
+
+
+def nvcc_cmd(extra=()):
+    nvcc = os.environ.get("NVCC", "nvcc")
+    return [
+        nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3",
+        "-fmad=false", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+        "--expt-relaxed-constexpr", *extra, "-o", LIB, *SOURCES,
+    ]
+
+
+def up_to_date():
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(p) <= t for p in DEPS)
+
+
+def build(force=False, verbose=False, extra=()):
+    if not force and up_to_date():
+        return LIB
+    cmd = nvcc_cmd(extra)
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True,
+          extra=("-Xptxas", "-v") if "--ptxas-v" in sys.argv else ())

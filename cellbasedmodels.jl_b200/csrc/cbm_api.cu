@@ -1,0 +1,978 @@
+// cbm_api.cu — host side of the C ABI declared in include/cbm_b200.h.
+//
+// A context owns every device buffer of one Community (capacity n_max) and
+// one CUDA stream.  Agent state that a step both reads and writes is held in
+// two copies selected by step parity (committed "x" and written "x__" of the
+// reference, swapped by update! instead of copied, update.jl:126-158); a full
+// step of each parity is captured once as a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cbm_b200.h"
+#include "cbm_kernels.cuh"
+
+using namespace cbm;
+
+struct cbm_ctx {
+  cbm_config cfg{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  size_t tsize = 4;
+  std::string err;
+  std::vector<void*> allocs;
+
+  // device buffers (typed views are built in params<T>())
+  void* pos[2][3] = {};
+  void* pos_u[3] = {};
+  void* v[2] = {};
+  void* f[2][3] = {};
+  void* g = nullptr;
+  long long* id = nullptr;
+  long long* parent = nullptr;
+  unsigned char* fate = nullptr;
+  int* holes = nullptr;
+  int* blk[4] = {};
+  int* agent_cell = nullptr;
+  int* agent_rank = nullptr;
+  int* cell_count = nullptr;
+  int* cell_start = nullptr;
+  int* cell_tmp = nullptr;
+  int* cell_agents = nullptr;
+  unsigned long long* scan_state = nullptr;
+  int* nbr_n = nullptr;
+  int* nbr_list = nullptr;
+  void* pos_old[3] = {};
+  void* c[2] = {};
+  void* grad[2][3] = {};
+  Counters* ctr = nullptr;
+  int* scratch_int = nullptr;  // n_max ints for inspection calls
+
+  int n_blocks = 0;
+  int n_cells = 1;
+  int n_cells_d[3] = {1, 1, 1};
+  int n_scan_tiles = 0;
+  int n_nodes = 0;
+  bool has_grid = false, has_list = false;
+
+  // host-side bookkeeping
+  bool loaded = false;
+  int parity = 0;
+  bool rule_done = false, de_done = false, mrule_done = false, mde_done = false;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+
+  // per-kernel event timing of eager steps (cbm_profile_step)
+  bool prof = false;
+  struct Mark {
+    const char* name;
+    cudaEvent_t ev[2];
+  };
+  std::vector<Mark> marks;
+  size_t mark_used = 0;
+};
+
+namespace {
+
+std::string g_create_error;
+
+int fail(cbm_ctx* ctx, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = buf;
+  else g_create_error = buf;
+  return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                                \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail(ctx, CBM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));      \
+  } while (0)
+
+int grid_blocks(long long n) { return (int)((n + kTile - 1) / kTile); }
+
+// Brackets one kernel launch with events when profiling an eager step.
+struct Prof {
+  cbm_ctx* c;
+  cbm_ctx::Mark* m = nullptr;
+  Prof(cbm_ctx* ctx, const char* name) : c(ctx) {
+    if (!c->prof) return;
+    if (c->mark_used == c->marks.size()) {
+      cbm_ctx::Mark mk{name, {nullptr, nullptr}};
+      cudaEventCreate(&mk.ev[0]);
+      cudaEventCreate(&mk.ev[1]);
+      c->marks.push_back(mk);
+    }
+    m = &c->marks[c->mark_used++];
+    m->name = name;
+    cudaEventRecord(m->ev[0], c->stream);
+  }
+  ~Prof() {
+    if (m) cudaEventRecord(m->ev[1], c->stream);
+  }
+};
+#define PROF(name) Prof prof_scope_(c, name)
+
+template <typename T>
+Params<T> params(const cbm_ctx* c, int parity) {
+  Params<T> P;
+  memset(&P, 0, sizeof P);
+  const cbm_config& k = c->cfg;
+  const int p = parity, q = parity ^ 1;
+  for (int d = 0; d < 3; ++d) {
+    P.pos_cur[d] = (T*)c->pos[p][d];
+    P.pos_nxt[d] = (T*)c->pos[q][d];
+    P.pos_u[d] = c->pos_u[d] ? (T*)c->pos_u[d] : (T*)c->pos[p][d];
+    P.f_cur[d] = (T*)c->f[p][d];
+    P.f_nxt[d] = (T*)c->f[q][d];
+    P.pos_old[d] = (T*)c->pos_old[d];
+    P.grad_cur[d] = (T*)c->grad[p][d];
+    P.grad_nxt[d] = (T*)c->grad[q][d];
+  }
+  P.v_cur = (T*)c->v[p];
+  P.v_nxt = (T*)c->v[q];
+  P.g = (T*)c->g;
+  P.id = c->id;
+  P.parent = c->parent;
+  P.fate = c->fate;
+  P.holes = c->holes;
+  P.blk_children = c->blk[0];
+  P.blk_deaths = c->blk[1];
+  P.blk_child_off = c->blk[2];
+  P.blk_death_off = c->blk[3];
+  P.agent_cell = c->agent_cell;
+  P.agent_rank = c->agent_rank;
+  P.cell_count = c->cell_count;
+  P.cell_start = c->cell_start;
+  P.cell_tmp = c->cell_tmp;
+  P.cell_agents = c->cell_agents;
+  P.scan_state = c->scan_state;
+  P.nbr_n = c->nbr_n;
+  P.nbr_list = c->nbr_list;
+  P.c_cur = (T*)c->c[p];
+  P.c_nxt = (T*)c->c[q];
+  P.ctr = c->ctr;
+  P.n_max = (int)k.n_max;
+  P.n_blocks = c->n_blocks;
+  P.n_cells = c->n_cells;
+  for (int d = 0; d < 3; ++d) {
+    P.n_cells_d[d] = c->n_cells_d[d];
+    P.n_medium[d] = d < k.dims && k.medium ? k.n_medium[d] : 1;
+    P.box_lo[d] = (T)k.box_lo[d];
+    P.box_hi[d] = (T)k.box_hi[d];
+    // dx = (hi - lo) / NMedium in Float64 (communityStructure.jl:274)
+    P.dx_m[d] = d < k.dims && k.medium ? (T)((k.box_hi[d] - k.box_lo[d]) / (double)k.n_medium[d])
+                                       : (T)1;
+  }
+  P.n_scan_tiles = c->n_scan_tiles;
+  P.n_nodes = c->n_nodes;
+  P.max_nbrs = k.n_max_neighbors;
+  P.parity = parity;
+  P.neighbors = k.neighbors;
+  P.integrator = k.integrator;
+  P.force_mode = k.force_mode;
+  P.att_form = k.att_form;
+  P.walls = k.walls;
+  P.fate_rule = k.fate;
+  P.growth = k.growth;
+  P.medium = k.medium;
+  P.medium_sampling = k.medium_sampling;
+  P.dt = (T)k.dt;
+  P.sqrt_dt = sqrt((T)k.dt);
+  P.sigma = (T)k.sigma;
+  P.edge = (T)(k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT ? k.skin : k.cell_edge);
+  P.skin = (T)k.skin;
+  P.rebuild_thr = k.rebuild_threshold > 0 ? (T)k.rebuild_threshold : (T)k.skin / (T)2;
+  P.k_rep = (T)k.k_rep;
+  P.r_rep = (T)k.r_rep;
+  P.k_att = (T)k.k_att;
+  P.r_att = (T)k.r_att;
+  P.wall_force = (T)k.wall_force;
+  P.wall_range = (T)k.wall_range;
+  P.drift_linear = (T)k.drift_linear;
+  P.v_div = (T)k.v_div;
+  P.div_sep = (T)k.div_sep;
+  P.p_death = (T)k.p_death;
+  P.diff_D = (T)k.diff_D;
+  P.decay = (T)k.decay;
+  P.secretion_amt = (T)k.secretion * (T)k.dt;
+  P.chemotaxis = (T)k.chemotaxis;
+  P.seed = k.seed;
+  P.community = k.community;
+  return P;
+}
+
+// ---- stage launches (enqueue only) -----------------------------------------
+template <typename T, int D>
+void enqueue_medium_rule(cbm_ctx* c, const Params<T>& P) {
+  if (c->cfg.medium && c->cfg.chemotaxis != 0) {
+    PROF("k_medium_grad");
+    k_medium_grad<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
+  }
+}
+
+template <typename T, int D>
+void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P) {
+  const cbm_config& k = c->cfg;
+  bool needed = k.walls == CBM_WALLS_REFLECT || (k.medium && k.secretion != 0) ||
+                k.fate != CBM_FATE_NONE;
+  if (!needed) return;
+  {
+    PROF("k_agent_rule");
+    k_agent_rule<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+  }
+  if (k.fate != CBM_FATE_NONE) {
+    PROF("k_fate_scan");
+    k_fate_scan<T><<<1, 1024, 0, c->stream>>>(P);
+  }
+}
+
+template <typename T, int D>
+void enqueue_agent_de(cbm_ctx* c, const Params<T>& P) {
+  PROF("k_agent_de");
+  k_agent_de<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+}
+
+template <typename T, int D>
+void enqueue_medium_de(cbm_ctx* c, const Params<T>& P) {
+  if (c->cfg.medium) {
+    PROF("k_medium_de");
+    k_medium_de<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
+  }
+}
+
+template <typename T, int D>
+void enqueue_update(cbm_ctx* c, const Params<T>& P) {
+  if (c->cfg.fate != CBM_FATE_NONE) {
+    PROF("k_compact");
+    k_compact<T, D><<<2 * 148, kTile, 0, c->stream>>>(P);
+  }
+  PROF("k_commit");
+  k_commit<T><<<1, 1, 0, c->stream>>>(P);
+}
+
+// computeNeighbors! of the step whose parity is P.parity (reads parity ^ 1)
+template <typename T, int D>
+void enqueue_neighbors(cbm_ctx* c, const Params<T>& P) {
+  if (!c->has_grid) return;
+  {
+    PROF("k_cells_hist");
+    k_cells_hist<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+  }
+  {
+    PROF("k_cells_scan");
+    k_cells_scan<T><<<c->n_scan_tiles, kTile, 0, c->stream>>>(P);
+  }
+  {
+    PROF("k_cells_scatter");
+    k_cells_scatter<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+  }
+  {
+    PROF("k_cells_stable");
+    k_cells_stable<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+  }
+  if (c->has_list) {
+    PROF("k_verlet_list");
+    k_verlet_list<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+  }
+}
+
+int kernels_per_step(const cbm_ctx* c) {
+  const cbm_config& k = c->cfg;
+  int n = 0;
+  if (k.medium && k.chemotaxis != 0) n += 1;
+  if (k.walls == CBM_WALLS_REFLECT || (k.medium && k.secretion != 0) || k.fate != CBM_FATE_NONE) n += 1;
+  if (k.fate != CBM_FATE_NONE) n += 2;  // fate scan, compaction
+  n += 1;                               // agent DE
+  if (k.medium) n += 1;
+  n += 1;                               // commit
+  if (c->has_grid) n += 4 + (c->has_list ? 1 : 0);
+  return n;
+}
+
+template <typename T, int D>
+void enqueue_full_step(cbm_ctx* c, int parity) {
+  Params<T> P = params<T>(c, parity);
+  enqueue_medium_rule<T, D>(c, P);  // reads only committed c: may precede the secretion
+  enqueue_agent_rule<T, D>(c, P);
+  enqueue_agent_de<T, D>(c, P);
+  enqueue_medium_de<T, D>(c, P);
+  enqueue_update<T, D>(c, P);
+  enqueue_neighbors<T, D>(c, P);
+}
+
+// dispatch on (precision, dims)
+template <template <typename, int> class Fn, typename... A>
+void dispatch(cbm_ctx* c, A... a) {
+  if (c->cfg.precision == CBM_F64) {
+    switch (c->cfg.dims) {
+      case 1: Fn<double, 1>::run(c, a...); break;
+      case 2: Fn<double, 2>::run(c, a...); break;
+      default: Fn<double, 3>::run(c, a...); break;
+    }
+  } else {
+    switch (c->cfg.dims) {
+      case 1: Fn<float, 1>::run(c, a...); break;
+      case 2: Fn<float, 2>::run(c, a...); break;
+      default: Fn<float, 3>::run(c, a...); break;
+    }
+  }
+}
+
+template <typename T, int D>
+struct FullStep {
+  static void run(cbm_ctx* c, int parity) { enqueue_full_step<T, D>(c, parity); }
+};
+template <typename T, int D>
+struct StageRule {
+  static void run(cbm_ctx* c) {
+    Params<T> P = params<T>(c, c->parity);
+    if (!c->mrule_done) enqueue_medium_rule<T, D>(c, P);
+    enqueue_agent_rule<T, D>(c, P);
+  }
+};
+template <typename T, int D>
+struct StageDE {
+  static void run(cbm_ctx* c) { enqueue_agent_de<T, D>(c, params<T>(c, c->parity)); }
+};
+template <typename T, int D>
+struct StageMediumRule {
+  static void run(cbm_ctx* c) { enqueue_medium_rule<T, D>(c, params<T>(c, c->parity)); }
+};
+template <typename T, int D>
+struct StageMediumDE {
+  static void run(cbm_ctx* c) { enqueue_medium_de<T, D>(c, params<T>(c, c->parity)); }
+};
+template <typename T, int D>
+struct StageUpdate {
+  static void run(cbm_ctx* c, int copy_agents, int copy_c, int copy_grad, int births) {
+    Params<T> P = params<T>(c, c->parity);
+    if (births) {
+      // the rule's births are written by the DE kernel's placement phase
+      Params<T> B = P;
+      B.births_only = 1;
+      k_agent_de<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(B);
+    }
+    if (copy_agents) k_copy_agents<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+    if (c->cfg.medium && (copy_c || copy_grad))
+      k_copy_medium<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P, copy_c ? 0 : 1);
+    enqueue_update<T, D>(c, P);
+  }
+};
+template <typename T, int D>
+struct StageNeighbors {
+  static void run(cbm_ctx* c) { enqueue_neighbors<T, D>(c, params<T>(c, c->parity ^ 1)); }
+};
+template <typename T, int D>
+struct CountNeighbors {
+  static void run(cbm_ctx* c, double radius, int* out) {
+    k_count_neighbors<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(params<T>(c, c->parity),
+                                                                  (T)radius, out);
+  }
+};
+
+int check_launch(cbm_ctx* c) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(c, CBM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+  return CBM_OK;
+}
+
+void* dalloc(cbm_ctx* c, size_t bytes, bool* ok) {
+  if (!*ok) return nullptr;
+  if (bytes == 0) bytes = 16;
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    *ok = false;
+    return nullptr;
+  }
+  c->allocs.push_back(p);
+  return p;
+}
+
+void free_all(cbm_ctx* c) {
+  for (auto& m : c->marks) {
+    cudaEventDestroy(m.ev[0]);
+    cudaEventDestroy(m.ev[1]);
+  }
+  c->marks.clear();
+  for (int q = 0; q < 2; ++q)
+    if (c->graph[q]) cudaGraphExecDestroy(c->graph[q]);
+  for (void* p : c->allocs) cudaFree(p);
+  c->allocs.clear();
+  if (c->stream) cudaStreamDestroy(c->stream);
+  c->stream = nullptr;
+}
+
+int flags_to_status(int err) {
+  if (err & kErrAgentOverflow) return CBM_ERR_AGENT_OVERFLOW;
+  if (err & kErrNeighborOverflow) return CBM_ERR_NEIGHBOR_OVERFLOW;
+  if (err & kErrTimeout) return CBM_ERR_TIMEOUT;
+  return CBM_OK;
+}
+
+int read_counters(cbm_ctx* c, Counters* h) {
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  CUDA_TRY(c, cudaMemcpy(h, c->ctr, sizeof(Counters), cudaMemcpyDeviceToHost));
+  return CBM_OK;
+}
+
+void reset_stage_flags(cbm_ctx* c) {
+  c->rule_done = c->de_done = c->mrule_done = c->mde_done = false;
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+const char* cbm_version(void) { return "cbm_b200 0.1.0 (sm_100a)"; }
+
+const char* cbm_last_error(const cbm_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
+  if (!out || !cfg) return fail(nullptr, CBM_ERR_ARG, "null argument");
+  *out = nullptr;
+  const cbm_config& k = *cfg;
+  if (k.dims < 1 || k.dims > 3) return fail(nullptr, CBM_ERR_ARG, "dims must be 1, 2 or 3");
+  if (k.precision != CBM_F32 && k.precision != CBM_F64)
+    return fail(nullptr, CBM_ERR_ARG, "precision must be CBM_F32 or CBM_F64");
+  if (k.n_max < 0 || k.n_max >= (1ll << 30))
+    return fail(nullptr, CBM_ERR_ARG, "n_max must be in [0, 2^30)");
+  if (!(k.dt > 0)) return fail(nullptr, CBM_ERR_ARG, "dt must be positive");
+  if (k.neighbors < CBM_NEIGH_NONE || k.neighbors > CBM_NEIGH_CLVD)
+    return fail(nullptr, CBM_ERR_ARG, "unknown neighbor algorithm %d", k.neighbors);
+  if (k.integrator != CBM_INT_EULER && k.integrator != CBM_INT_EM)
+    return fail(nullptr, CBM_ERR_ARG, "unknown integrator %d", k.integrator);
+  for (int d = 0; d < k.dims; ++d)
+    if (!(k.box_hi[d] > k.box_lo[d])) return fail(nullptr, CBM_ERR_ARG, "empty simBox on axis %d", d);
+  const bool grid = k.neighbors == CBM_NEIGH_CELL_LINKED || k.neighbors == CBM_NEIGH_CLVD ||
+                    k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT;
+  const bool list = k.neighbors == CBM_NEIGH_CLVD || k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT;
+  if ((k.neighbors == CBM_NEIGH_CELL_LINKED || k.neighbors == CBM_NEIGH_CLVD) && !(k.cell_edge > 0))
+    return fail(nullptr, CBM_ERR_ARG, "cell_edge must be positive");
+  if (list && !(k.skin > 0)) return fail(nullptr, CBM_ERR_ARG, "skin must be positive");
+  if (list && (k.n_max_neighbors < 1 ||
+               (k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT && k.n_max_neighbors > kVdSortMax)))
+    return fail(nullptr, CBM_ERR_ARG, "n_max_neighbors must be in [1, %d]",
+                k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT ? kVdSortMax : (1 << 20));
+  if (k.fate == CBM_FATE_VOLUME && !k.growth && !(k.p_death > 0) )
+    ;  // a volume rule without growth only kills
+  if (k.medium) {
+    for (int d = 0; d < k.dims; ++d)
+      if (k.n_medium[d] < 1) return fail(nullptr, CBM_ERR_ARG, "n_medium[%d] must be >= 1", d);
+  }
+
+  cbm_ctx* c = new cbm_ctx;
+  c->cfg = k;
+  c->tsize = k.precision == CBM_F64 ? 8 : 4;
+  cudaGetDevice(&c->device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    int rc = fail(nullptr, CBM_ERR_CUDA, "cudaStreamCreate failed (is a CUDA device present?)");
+    delete c;
+    return rc;
+  }
+  const size_t n = (size_t)(k.n_max > 0 ? k.n_max : 1);
+  const size_t S = c->tsize;
+  c->n_blocks = grid_blocks((long long)n);
+  c->has_grid = grid;
+  c->has_list = list;
+  if (grid) {
+    double e = k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT ? k.skin : k.cell_edge;
+    long long nc = 1;
+    for (int d = 0; d < k.dims; ++d) {
+      // nCells_ = ceil((hi - lo) / edge + 2), neighbors.jl:605 (Float64 on the host)
+      double v = ceil((k.box_hi[d] - k.box_lo[d]) / e + 2.0);
+      if (!(v >= 1 && v < 2.0e9)) {
+        int rc = fail(nullptr, CBM_ERR_ARG, "cell grid too large on axis %d", d);
+        free_all(c);
+        delete c;
+        return rc;
+      }
+      c->n_cells_d[d] = (int)v;
+      nc *= (long long)v;
+    }
+    if (nc >= (1ll << 31) - 1) {
+      int rc = fail(nullptr, CBM_ERR_ARG, "cell grid has too many cells (%lld)", nc);
+      free_all(c);
+      delete c;
+      return rc;
+    }
+    c->n_cells = (int)nc;
+    c->n_scan_tiles = (c->n_cells + kScanTile - 1) / kScanTile;
+  }
+  if (k.medium) {
+    long long nn = 1;
+    for (int d = 0; d < k.dims; ++d) nn *= k.n_medium[d];
+    if (nn >= (1ll << 31)) {
+      int rc = fail(nullptr, CBM_ERR_ARG, "medium grid too large");
+      free_all(c);
+      delete c;
+      return rc;
+    }
+    c->n_nodes = (int)nn;
+  }
+
+  bool ok = true;
+  for (int q = 0; q < 2; ++q) {
+    for (int d = 0; d < 3; ++d) {
+      c->pos[q][d] = dalloc(c, n * S, &ok);
+      c->f[q][d] = dalloc(c, n * S, &ok);
+    }
+    c->v[q] = dalloc(c, n * S, &ok);
+  }
+  if (k.walls == CBM_WALLS_REFLECT)
+    for (int d = 0; d < 3; ++d) c->pos_u[d] = dalloc(c, n * S, &ok);
+  c->g = dalloc(c, n * S, &ok);
+  c->id = (long long*)dalloc(c, n * 8, &ok);
+  c->parent = (long long*)dalloc(c, n * 8, &ok);
+  c->fate = (unsigned char*)dalloc(c, n, &ok);
+  c->holes = (int*)dalloc(c, n * 4, &ok);
+  for (int q = 0; q < 4; ++q) c->blk[q] = (int*)dalloc(c, (size_t)c->n_blocks * 4, &ok);
+  c->scratch_int = (int*)dalloc(c, n * 4, &ok);
+  if (grid) {
+    c->agent_cell = (int*)dalloc(c, n * 4, &ok);
+    c->agent_rank = (int*)dalloc(c, n * 4, &ok);
+    c->cell_count = (int*)dalloc(c, (size_t)c->n_cells * 4, &ok);
+    c->cell_start = (int*)dalloc(c, ((size_t)c->n_cells + 1) * 4, &ok);
+    c->cell_tmp = (int*)dalloc(c, n * 4, &ok);
+    c->cell_agents = (int*)dalloc(c, n * 4, &ok);
+    c->scan_state = (unsigned long long*)dalloc(c, (size_t)c->n_scan_tiles * 8, &ok);
+  }
+  if (list) {
+    c->nbr_n = (int*)dalloc(c, n * 4, &ok);
+    c->nbr_list = (int*)dalloc(c, n * (size_t)k.n_max_neighbors * 4, &ok);
+    for (int d = 0; d < 3; ++d) c->pos_old[d] = dalloc(c, n * S, &ok);
+  }
+  if (k.medium) {
+    for (int q = 0; q < 2; ++q) {
+      c->c[q] = dalloc(c, (size_t)c->n_nodes * S, &ok);
+      for (int d = 0; d < 3; ++d) c->grad[q][d] = dalloc(c, (size_t)c->n_nodes * S, &ok);
+    }
+  }
+  c->ctr = (Counters*)dalloc(c, sizeof(Counters), &ok);
+  if (!ok) {
+    int rc = fail(nullptr, CBM_ERR_NOMEM, "device allocation failed for n_max=%lld", (long long)k.n_max);
+    free_all(c);
+    delete c;
+    return rc;
+  }
+  for (void* p : c->allocs) cudaMemsetAsync(p, 0, 0, c->stream);
+  if (grid) {
+    cudaMemsetAsync(c->cell_count, 0, (size_t)c->n_cells * 4, c->stream);
+    cudaMemsetAsync(c->scan_state, 0, (size_t)c->n_scan_tiles * 8, c->stream);
+  }
+  cudaMemsetAsync(c->ctr, 0, sizeof(Counters), c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    int rc = fail(nullptr, CBM_ERR_CUDA, "device initialisation failed");
+    free_all(c);
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return CBM_OK;
+}
+
+void cbm_destroy(cbm_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  free_all(ctx);
+  delete ctx;
+}
+
+int cbm_upload(cbm_ctx* c, const cbm_state_view* h) {
+  if (!c || !h) return fail(c, CBM_ERR_ARG, "null argument");
+  cudaSetDevice(c->device);
+  const cbm_config& k = c->cfg;
+  if (h->N < 0 || h->N > k.n_max)
+    return fail(c, CBM_ERR_ARG, "N=%lld exceeds n_max=%lld", (long long)h->N, (long long)k.n_max);
+  const size_t N = (size_t)h->N, S = c->tsize;
+  for (int d = 0; d < k.dims; ++d)
+    if (N && !h->pos[d]) return fail(c, CBM_ERR_ARG, "pos[%d] is NULL", d);
+  if (k.growth && N && (!h->v || !h->g)) return fail(c, CBM_ERR_ARG, "growth needs v and g");
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  // every buffer starts as zeros past N (loadToPlatform! pads with zeros)
+  for (int q = 0; q < 2; ++q) {
+    for (int d = 0; d < 3; ++d) {
+      CUDA_TRY(c, cudaMemset(c->pos[q][d], 0, (size_t)k.n_max * S));
+      CUDA_TRY(c, cudaMemset(c->f[q][d], 0, (size_t)k.n_max * S));
+    }
+    CUDA_TRY(c, cudaMemset(c->v[q], 0, (size_t)k.n_max * S));
+  }
+  CUDA_TRY(c, cudaMemset(c->g, 0, (size_t)k.n_max * S));
+  CUDA_TRY(c, cudaMemset(c->parent, 0, (size_t)k.n_max * 8));
+  for (int q = 0; q < 2; ++q) {
+    for (int d = 0; d < k.dims; ++d) {
+      if (N) CUDA_TRY(c, cudaMemcpy(c->pos[q][d], h->pos[d], N * S, cudaMemcpyHostToDevice));
+      if (N && h->f[d]) CUDA_TRY(c, cudaMemcpy(c->f[q][d], h->f[d], N * S, cudaMemcpyHostToDevice));
+    }
+    if (N && h->v) CUDA_TRY(c, cudaMemcpy(c->v[q], h->v, N * S, cudaMemcpyHostToDevice));
+  }
+  if (N && h->g) CUDA_TRY(c, cudaMemcpy(c->g, h->g, N * S, cudaMemcpyHostToDevice));
+  {
+    std::vector<long long> ids((size_t)k.n_max > 0 ? (size_t)k.n_max : 1, 0);
+    for (size_t i = 0; i < N; ++i) ids[i] = h->id ? h->id[i] : (long long)i + 1;
+    CUDA_TRY(c, cudaMemcpy(c->id, ids.data(), (size_t)k.n_max * 8, cudaMemcpyHostToDevice));
+    if (N && h->parent) CUDA_TRY(c, cudaMemcpy(c->parent, h->parent, N * 8, cudaMemcpyHostToDevice));
+  }
+  if (k.medium) {
+    const size_t nb = (size_t)c->n_nodes * S;
+    for (int q = 0; q < 2; ++q) {
+      if (h->medium_c) CUDA_TRY(c, cudaMemcpy(c->c[q], h->medium_c, nb, cudaMemcpyHostToDevice));
+      else CUDA_TRY(c, cudaMemset(c->c[q], 0, nb));
+      for (int d = 0; d < 3; ++d) {
+        if (d < k.dims && h->medium_grad[d])
+          CUDA_TRY(c, cudaMemcpy(c->grad[q][d], h->medium_grad[d], nb, cudaMemcpyHostToDevice));
+        else CUDA_TRY(c, cudaMemset(c->grad[q][d], 0, nb));
+      }
+    }
+  }
+  if (c->has_grid) CUDA_TRY(c, cudaMemset(c->cell_count, 0, (size_t)c->n_cells * 4));
+  Counters hc;
+  memset(&hc, 0, sizeof hc);
+  hc.N[0] = hc.N[1] = h->N;
+  hc.step[0] = hc.step[1] = h->step;
+  hc.t[0] = hc.t[1] = h->t;
+  hc.id_max = h->id_max > 0 ? h->id_max : h->N;
+  hc.flag[0] = 0;
+  hc.flag[1] = 1;  // flagRecomputeNeighbors_ = [1] (communityStructure.jl:480)
+  hc.scan_epoch = 1;
+  // keep the epoch monotonic across uploads so stale scan states never match
+  {
+    Counters old;
+    if (cudaMemcpy(&old, c->ctr, sizeof old, cudaMemcpyDeviceToHost) == cudaSuccess)
+      hc.scan_epoch = old.scan_epoch + 1;
+  }
+  CUDA_TRY(c, cudaMemcpy(c->ctr, &hc, sizeof hc, cudaMemcpyHostToDevice));
+  c->parity = 0;
+  reset_stage_flags(c);
+  c->loaded = true;
+  // computeNeighbors! at load (communityStructure.jl:648): end-of-step
+  // convention with parity 1 reads buffers/N of parity 0 and flag[1]
+  dispatch<StageNeighbors>(c);  // uses c->parity ^ 1 = 1
+  int rc = check_launch(c);
+  if (rc) return rc;
+  return cbm_sync(c);
+}
+
+int cbm_download(cbm_ctx* c, cbm_state_view* h, int32_t which) {
+  if (!c || !h) return fail(c, CBM_ERR_ARG, "null argument");
+  if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
+  cudaSetDevice(c->device);
+  Counters hc;
+  int rc = read_counters(c, &hc);
+  if (rc) return rc;
+  const cbm_config& k = c->cfg;
+  const int p = c->parity;
+  const long long N = hc.N[p];
+  if (h->capacity < N)
+    return fail(c, CBM_ERR_ARG, "host capacity %lld < N=%lld", (long long)h->capacity, N);
+  h->N = N;
+  h->t = hc.t[p];
+  h->step = hc.step[p];
+  h->id_max = hc.id_max;
+  const size_t S = c->tsize, nb = (size_t)N * S;
+  const bool nw = which == CBM_VIEW_NEW;
+  const int qa = nw && c->de_done ? p ^ 1 : p;
+  for (int d = 0; d < k.dims; ++d) {
+    const void* src = c->pos[qa][d];
+    if (nw && !c->de_done && c->rule_done && c->pos_u[d]) src = c->pos_u[d];
+    if (h->pos[d] && N) CUDA_TRY(c, cudaMemcpy(h->pos[d], src, nb, cudaMemcpyDeviceToHost));
+    if (h->f[d] && N) CUDA_TRY(c, cudaMemcpy(h->f[d], c->f[qa][d], nb, cudaMemcpyDeviceToHost));
+  }
+  if (h->v && N) CUDA_TRY(c, cudaMemcpy(h->v, c->v[qa], nb, cudaMemcpyDeviceToHost));
+  if (h->g && N) CUDA_TRY(c, cudaMemcpy(h->g, c->g, nb, cudaMemcpyDeviceToHost));
+  if (h->id && N) CUDA_TRY(c, cudaMemcpy(h->id, c->id, (size_t)N * 8, cudaMemcpyDeviceToHost));
+  if (h->parent && N) CUDA_TRY(c, cudaMemcpy(h->parent, c->parent, (size_t)N * 8, cudaMemcpyDeviceToHost));
+  if (k.medium) {
+    const size_t mb = (size_t)c->n_nodes * S;
+    const int qc = nw && c->mde_done ? p ^ 1 : p;
+    const int qg = nw && c->mrule_done ? p ^ 1 : p;
+    if (h->medium_c) CUDA_TRY(c, cudaMemcpy(h->medium_c, c->c[qc], mb, cudaMemcpyDeviceToHost));
+    for (int d = 0; d < k.dims; ++d)
+      if (h->medium_grad[d])
+        CUDA_TRY(c, cudaMemcpy(h->medium_grad[d], c->grad[qg][d], mb, cudaMemcpyDeviceToHost));
+  }
+  return CBM_OK;
+}
+
+int cbm_agent_step_rule(cbm_ctx* c) {
+  if (!c) return CBM_ERR_ARG;
+  if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
+  cudaSetDevice(c->device);
+  dispatch<StageRule>(c);
+  if (c->cfg.medium && c->cfg.chemotaxis != 0) c->mrule_done = true;
+  c->rule_done = true;
+  return check_launch(c);
+}
+
+int cbm_agent_step_de(cbm_ctx* c) {
+  if (!c) return CBM_ERR_ARG;
+  if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
+  cudaSetDevice(c->device);
+  const cbm_config& k = c->cfg;
+  if (!c->rule_done) {
+    if (k.fate != CBM_FATE_NONE) {
+      CUDA_TRY(c, cudaMemsetAsync(c->blk[0], 0, (size_t)c->n_blocks * 4, c->stream));
+      CUDA_TRY(c, cudaMemsetAsync(c->blk[1], 0, (size_t)c->n_blocks * 4, c->stream));
+    }
+    if (k.walls == CBM_WALLS_REFLECT)
+      for (int d = 0; d < k.dims; ++d)
+        CUDA_TRY(c, cudaMemcpyAsync(c->pos_u[d], c->pos[c->parity][d], (size_t)k.n_max * c->tsize,
+                                    cudaMemcpyDeviceToDevice, c->stream));
+  }
+  dispatch<StageDE>(c);
+  c->de_done = true;
+  return check_launch(c);
+}
+
+int cbm_medium_step_rule(cbm_ctx* c) {
+  if (!c) return CBM_ERR_ARG;
+  if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
+  cudaSetDevice(c->device);
+  if (!c->mrule_done) dispatch<StageMediumRule>(c);
+  if (c->cfg.medium && c->cfg.chemotaxis != 0) c->mrule_done = true;
+  return check_launch(c);
+}
+
+int cbm_medium_step_de(cbm_ctx* c) {
+  if (!c) return CBM_ERR_ARG;
+  if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
+  cudaSetDevice(c->device);
+  dispatch<StageMediumDE>(c);
+  if (c->cfg.medium) c->mde_done = true;
+  return check_launch(c);
+}
+
+int cbm_update(cbm_ctx* c) {
+  if (!c) return CBM_ERR_ARG;
+  if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
+  cudaSetDevice(c->device);
+  const cbm_config& k = c->cfg;
+  int births = (!c->de_done && c->rule_done && k.fate != CBM_FATE_NONE) ? 1 : 0;
+  int copy_agents = c->de_done ? 0 : 1;
+  int copy_c = (k.medium && !c->mde_done) ? 1 : 0;
+  int copy_grad = (k.medium && !c->mrule_done) ? 1 : 0;
+  if (!c->rule_done && k.fate != CBM_FATE_NONE) {
+    // no rule this step: no events for the compaction
+    CUDA_TRY(c, cudaMemsetAsync(c->blk[0], 0, (size_t)c->n_blocks * 4, c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(c->blk[1], 0, (size_t)c->n_blocks * 4, c->stream));
+  }
+  dispatch<StageUpdate>(c, copy_agents, copy_c, copy_grad, births);
+  c->parity ^= 1;
+  reset_stage_flags(c);
+  return check_launch(c);
+}
+
+int cbm_compute_neighbors(cbm_ctx* c) {
+  if (!c) return CBM_ERR_ARG;
+  if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
+  cudaSetDevice(c->device);
+  dispatch<StageNeighbors>(c);
+  return check_launch(c);
+}
+
+int cbm_sync(cbm_ctx* c) {
+  if (!c) return CBM_ERR_ARG;
+  cudaSetDevice(c->device);
+  Counters hc;
+  int rc = read_counters(c, &hc);
+  if (rc) return rc;
+  if (hc.err) {
+    int code = flags_to_status(hc.err);
+    int zero = 0;
+    CUDA_TRY(c, cudaMemcpy(&c->ctr->err, &zero, sizeof zero, cudaMemcpyHostToDevice));
+    const char* what = code == CBM_ERR_AGENT_OVERFLOW
+                           ? "agent capacity n_max reached: births were dropped"
+                           : code == CBM_ERR_NEIGHBOR_OVERFLOW
+                                 ? "a Verlet row exceeded n_max_neighbors: list truncated"
+                                 : "a bounded device-side wait gave up";
+    return fail(c, code, "%s (device flags 0x%x)", what, hc.err);
+  }
+  return CBM_OK;
+}
+
+int cbm_step(cbm_ctx* c, int32_t nsteps, int32_t flags) {
+  if (!c) return CBM_ERR_ARG;
+  if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
+  if (nsteps < 0) return fail(c, CBM_ERR_ARG, "nsteps must be >= 0");
+  cudaSetDevice(c->device);
+  if (c->rule_done || c->de_done || c->mrule_done || c->mde_done)
+    return fail(c, CBM_ERR_STATE, "a step is half done through the stage calls; call cbm_update first");
+  const bool use_graph = !(flags & CBM_NO_GRAPH);
+  for (int s = 0; s < nsteps; ++s) {
+    const int p = c->parity;
+    if (use_graph) {
+      if (!c->graph[p]) {
+        cudaGraph_t g = nullptr;
+        CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        dispatch<FullStep>(c, p);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (e != cudaSuccess) return fail(c, CBM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&c->graph[p], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(c, CBM_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+      }
+      CUDA_TRY(c, cudaGraphLaunch(c->graph[p], c->stream));
+    } else {
+      dispatch<FullStep>(c, p);
+      int rc = check_launch(c);
+      if (rc) return rc;
+    }
+    c->parity ^= 1;
+  }
+  if (flags & CBM_SYNC) return cbm_sync(c);
+  return CBM_OK;
+}
+
+int cbm_get_counters(cbm_ctx* c, int64_t* N, int64_t* n_add, int64_t* n_remove, int64_t* id_max,
+                     int32_t* flag_recompute, int64_t* stepc) {
+  if (!c) return CBM_ERR_ARG;
+  cudaSetDevice(c->device);
+  Counters hc;
+  int rc = read_counters(c, &hc);
+  if (rc) return rc;
+  const int p = c->parity;
+  if (N) *N = hc.N[p];
+  if (n_add) *n_add = hc.n_add;
+  if (n_remove) *n_remove = hc.n_remove;
+  if (id_max) *id_max = hc.id_max;
+  // flag of the step in flight, or of the step that just ended
+  if (flag_recompute) *flag_recompute = (c->rule_done || c->de_done) ? hc.flag[p] : hc.flag[p ^ 1];
+  if (stepc) *stepc = hc.step[p];
+  return CBM_OK;
+}
+
+int cbm_grid_shape(cbm_ctx* c, int32_t* n3) {
+  if (!c || !n3) return CBM_ERR_ARG;
+  for (int d = 0; d < 3; ++d) n3[d] = c->n_cells_d[d];
+  return CBM_OK;
+}
+
+int cbm_get_grid(cbm_ctx* c, int32_t* agent_cell, int32_t* cell_start, int32_t* cell_count,
+                 int32_t* cell_agents) {
+  if (!c) return CBM_ERR_ARG;
+  if (!c->has_grid) return fail(c, CBM_ERR_STATE, "this neighbor algorithm has no cell grid");
+  cudaSetDevice(c->device);
+  Counters hc;
+  int rc = read_counters(c, &hc);
+  if (rc) return rc;
+  const long long N = hc.N[c->parity];
+  std::vector<int> start((size_t)c->n_cells + 1);
+  CUDA_TRY(c, cudaMemcpy(start.data(), c->cell_start, start.size() * 4, cudaMemcpyDeviceToHost));
+  for (int q = 0; q < c->n_cells; ++q) {
+    if (cell_start) cell_start[q] = start[q];
+    if (cell_count) cell_count[q] = start[q + 1] - start[q];
+  }
+  if (agent_cell && N) CUDA_TRY(c, cudaMemcpy(agent_cell, c->agent_cell, (size_t)N * 4, cudaMemcpyDeviceToHost));
+  if (cell_agents && N) CUDA_TRY(c, cudaMemcpy(cell_agents, c->cell_agents, (size_t)N * 4, cudaMemcpyDeviceToHost));
+  return CBM_OK;
+}
+
+int cbm_get_neighbors(cbm_ctx* c, int32_t* counts, int32_t* list, int64_t cap) {
+  if (!c) return CBM_ERR_ARG;
+  if (!c->has_list) return fail(c, CBM_ERR_STATE, "this neighbor algorithm has no Verlet list");
+  cudaSetDevice(c->device);
+  Counters hc;
+  int rc = read_counters(c, &hc);
+  if (rc) return rc;
+  const long long N = hc.N[c->parity];
+  const long long M = c->cfg.n_max_neighbors, nmax = c->cfg.n_max;
+  if (list && cap < N * M) return fail(c, CBM_ERR_ARG, "list capacity %lld < N*n_max_neighbors", (long long)cap);
+  std::vector<int> n((size_t)N), col((size_t)(nmax * M));
+  if (N) CUDA_TRY(c, cudaMemcpy(n.data(), c->nbr_n, (size_t)N * 4, cudaMemcpyDeviceToHost));
+  if (list && N) CUDA_TRY(c, cudaMemcpy(col.data(), c->nbr_list, col.size() * 4, cudaMemcpyDeviceToHost));
+  for (long long i = 0; i < N; ++i) {
+    if (counts) counts[i] = n[(size_t)i];
+    if (list)
+      for (long long k = 0; k < M; ++k)
+        list[i * M + k] = k < n[(size_t)i] ? col[(size_t)(k * nmax + i)] : -1;
+  }
+  return CBM_OK;
+}
+
+int cbm_count_neighbors(cbm_ctx* c, double radius, int32_t* out) {
+  if (!c || !out) return CBM_ERR_ARG;
+  if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
+  cudaSetDevice(c->device);
+  Counters hc;
+  int rc = read_counters(c, &hc);
+  if (rc) return rc;
+  const long long N = hc.N[c->parity];
+  dispatch<CountNeighbors>(c, radius, c->scratch_int);
+  rc = check_launch(c);
+  if (rc) return rc;
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (N) CUDA_TRY(c, cudaMemcpy(out, c->scratch_int, (size_t)N * 4, cudaMemcpyDeviceToHost));
+  return CBM_OK;
+}
+
+int cbm_rng_fill(cbm_ctx* c, int32_t kind, double a, double b, int64_t n, int64_t stepc, void* out) {
+  if (!c || !out || n < 0) return CBM_ERR_ARG;
+  if (kind < 0 || kind > 2) return fail(c, CBM_ERR_ARG, "kind must be 0, 1 or 2");
+  cudaSetDevice(c->device);
+  void* buf = nullptr;
+  const size_t bytes = (size_t)(n > 0 ? n : 1) * c->tsize;
+  CUDA_TRY(c, cudaMallocAsync(&buf, bytes, c->stream));
+  const int blocks = (int)((n + kTile - 1) / kTile);
+  if (n > 0) {
+    if (c->cfg.precision == CBM_F64)
+      k_rng_fill<double><<<blocks, kTile, 0, c->stream>>>(c->cfg.seed, c->cfg.community, stepc, kind, a,
+                                                         b, n, (double*)buf);
+    else
+      k_rng_fill<float><<<blocks, kTile, 0, c->stream>>>(c->cfg.seed, c->cfg.community, stepc, kind,
+                                                        (float)a, (float)b, n, (float*)buf);
+  }
+  int rc = check_launch(c);
+  if (!rc && n > 0) {
+    cudaError_t e = cudaMemcpyAsync(out, buf, (size_t)n * c->tsize, cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) rc = fail(c, CBM_ERR_CUDA, "copy failed: %s", cudaGetErrorString(e));
+  }
+  cudaFreeAsync(buf, c->stream);
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (!rc && e != cudaSuccess) rc = fail(c, CBM_ERR_CUDA, "rng fill failed: %s", cudaGetErrorString(e));
+  return rc;
+}
+
+void* cbm_stream(cbm_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int cbm_profile_step(cbm_ctx* c, int32_t max_kernels, float* ms, const char** names,
+                     int32_t* n_kernels) {
+  if (!c || !n_kernels) return CBM_ERR_ARG;
+  if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
+  if (c->rule_done || c->de_done || c->mrule_done || c->mde_done)
+    return fail(c, CBM_ERR_STATE, "a step is half done through the stage calls; call cbm_update first");
+  cudaSetDevice(c->device);
+  c->prof = true;
+  c->mark_used = 0;
+  dispatch<FullStep>(c, c->parity);
+  c->prof = false;
+  int rc = check_launch(c);
+  if (rc) return rc;
+  c->parity ^= 1;
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  *n_kernels = (int32_t)c->mark_used;
+  for (size_t q = 0; q < c->mark_used && (int)q < max_kernels; ++q) {
+    float t = 0.f;
+    CUDA_TRY(c, cudaEventElapsedTime(&t, c->marks[q].ev[0], c->marks[q].ev[1]));
+    if (ms) ms[q] = t;
+    if (names) names[q] = c->marks[q].name;
+  }
+  return cbm_sync(c);
+}
+
+int cbm_kernels_per_step(cbm_ctx* c) { return c ? kernels_per_step(c) : 0; }
+
+}  // extern "C"

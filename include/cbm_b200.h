@@ -1,0 +1,238 @@
+/*
+ * cbm_b200.h — C ABI of the B200 per-step path of CellBasedModels.jl.
+ *
+ * The reference runs one simulation step as (src/CommunityStructure/step.jl:96-107)
+ *     agentStepRule! -> agentStepDE! -> mediumStepRule! -> mediumStepDE!
+ *     -> modelStepRule! -> modelStepDE! -> update! -> computeNeighbors!
+ * over a Community whose state lives on a Platform (src/platforms.jl:1-121).
+ * This library is that Platform for one fixed model family (soft spheres with
+ * repulsion/adhesion, Euler or Euler–Maruyama, volume growth with division and
+ * death, an FTCS-diffused medium with secretion and chemotaxis), evaluated by
+ * hand-written sm_100a kernels.  A Julia `B200 <: Platform` binds these entry
+ * points with `ccall`; every entry point names the reference function it
+ * replaces.
+ *
+ * Conventions
+ *  - All functions return CBM_OK (0) or a CBM_ERR_* code; cbm_last_error()
+ *    gives the message.  The device never traps: device-side faults of the
+ *    model (capacity or neighbor-list overflow) are recorded in a flag word and
+ *    reported at the next synchronising call.
+ *  - Indices are 0-based inside the library; agent ids are kept as given.
+ *  - Host pointers are borrowed for the duration of the call only.
+ *  - One context = one CUDA stream; a context is not re-entrant.  Different
+ *    contexts may be driven from different host threads.
+ *  - Arrays of reals are `float` when cfg.precision == CBM_F32 and `double`
+ *    when CBM_F64 (void* in the signatures).
+ */
+#ifndef CBM_B200_H
+#define CBM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define CBM_OK 0
+#define CBM_ERR_ARG 1              /* invalid argument or configuration */
+#define CBM_ERR_CUDA 2             /* a CUDA runtime call failed */
+#define CBM_ERR_AGENT_OVERFLOW 3   /* births dropped: N would exceed n_max */
+#define CBM_ERR_NEIGHBOR_OVERFLOW 4 /* a Verlet row needed more than n_max_neighbors */
+#define CBM_ERR_TIMEOUT 5          /* a bounded device-side wait gave up */
+#define CBM_ERR_STATE 6            /* call out of order (e.g. step before upload) */
+#define CBM_ERR_NOMEM 7            /* device allocation failed */
+
+/* ---- enumerations ------------------------------------------------------- */
+enum { CBM_F32 = 0, CBM_F64 = 1 };
+
+/* src/neighbors.jl: Full :26, VerletDisplacement :310, CellLinked :587, CLVD :997 */
+enum {
+  CBM_NEIGH_NONE = 0,       /* no pair interactions */
+  CBM_NEIGH_FULL = 1,       /* all pairs, ascending j            (neighbors.jl:36-38) */
+  CBM_NEIGH_CELL_LINKED = 2, /* cell grid rebuilt every step     (neighbors.jl:587-979) */
+  CBM_NEIGH_VERLET_DISPLACEMENT = 3, /* list, ascending j, rebuilt on displacement (:310-570) */
+  CBM_NEIGH_CLVD = 4        /* list built over the cell grid, cell order (:997-1275) */
+};
+
+/* src/integrators.jl: Euler :465-505, EM :683-734 */
+enum { CBM_INT_EULER = 0, CBM_INT_EM = 1 };
+
+/* How the pair force enters dt(x).
+ *  DIRECT: dt(x) += F(d)/d * (x - x[j]) inside @loopOverNeighbors.
+ *  LAGGED: fx__ accumulates the pair force; dt(x) = fx reads the value committed
+ *          at the previous update! (docs/src/Aggregation.md:81-114). */
+enum { CBM_FORCE_DIRECT = 0, CBM_FORCE_LAGGED = 1 };
+
+/* Adhesion branch for r_rep <= d < r_att:
+ *  FROM_REP: F = -k_att (d - r_rep)   (linear growth past contact)
+ *  TO_ATT:   F = -k_att (r_att - d)   (docs/src/Aggregation.md:96-99) */
+enum { CBM_ATT_FROM_REP = 0, CBM_ATT_TO_ATT = 1 };
+
+/* Walls.  REFLECT: agentRule sets x = 2 lo - x / 2 hi - x.  PUSH: the ODE adds
+ * +wall_force within wall_range of lo and -wall_force within wall_range of hi
+ * (docs/src/Aggregation.md:101-111). */
+enum { CBM_WALLS_NONE = 0, CBM_WALLS_REFLECT = 1, CBM_WALLS_PUSH = 2 };
+
+/* Agent fate rule evaluated in agentStepRule!.
+ *  VOLUME: if v >= v_div divide into two daughters at +-div_sep along a random
+ *          unit vector with v/2 each (@addAgent x2 + @removeAgent, docs/src/
+ *          Development.md:153-190), elseif uniform(0,1) < p_death die.
+ *  ID_PARITY: odd ids die, even ids add one child that copies the parent
+ *          (test/testCommunity.jl:239-316). */
+enum { CBM_FATE_NONE = 0, CBM_FATE_VOLUME = 1, CBM_FATE_ID_PARITY = 2 };
+
+/* Where agents read and write the medium.  NEAREST is the reference's
+ * cellInMesh (src/metrics.jl:18-20); BILINEAR spreads over the four (eight)
+ * surrounding medium nodes. */
+enum { CBM_MEDIUM_NEAREST = 0, CBM_MEDIUM_BILINEAR = 1 };
+
+/* cbm_step flags */
+#define CBM_SYNC 1          /* synchronise and report device flags before returning */
+#define CBM_NO_GRAPH 2      /* launch kernels one by one instead of replaying a graph */
+
+/* cbm_download / cbm_upload `which` */
+#define CBM_VIEW_COMMITTED 0 /* x  : values committed by the last update! */
+#define CBM_VIEW_NEW 1       /* x__: values written by this step's rule / DE */
+
+/* ---- configuration (ABM(...) + Community(...) keyword arguments) --------- */
+typedef struct cbm_config {
+  int32_t dims;          /* 1, 2 or 3 (ABM(dims, ...)) */
+  int32_t precision;     /* CBM_F32 | CBM_F64 (src/constants.jl:1-4) */
+  int64_t n_max;         /* agent capacity = N + preallocateAgents (nMax_) */
+  double box_lo[3];      /* simBox[:,1] */
+  double box_hi[3];      /* simBox[:,2] */
+  double dt;
+  uint64_t seed;         /* key of the counter-based stream (cbm_rng.h) */
+  uint32_t community;    /* community index inside the random stream */
+  int32_t neighbors;     /* CBM_NEIGH_* */
+  int32_t n_max_neighbors; /* Verlet row capacity (nMaxNeighbors) */
+  int32_t integrator;    /* CBM_INT_* */
+  double cell_edge;      /* CellLinked / CLVD cellEdge */
+  double skin;           /* Verlet list radius (the reference's `skin`) */
+  double rebuild_threshold; /* rebuild when a displacement >= this; <= 0 means skin/2 */
+  double sigma;          /* EM noise amplitude: dt(x) = sigma in agentSDE */
+  int32_t force_mode;    /* CBM_FORCE_* */
+  int32_t att_form;      /* CBM_ATT_* */
+  double k_rep;          /* repulsion stiffness (k) */
+  double r_rep;          /* repulsion range (2r) */
+  double k_att;          /* adhesion stiffness (a) */
+  double r_att;          /* interaction cutoff (3r); no pair term for d >= r_att */
+  int32_t walls;         /* CBM_WALLS_* */
+  int32_t fate;          /* CBM_FATE_* */
+  double wall_force;
+  double wall_range;
+  double drift_linear;   /* dt(x) += -drift_linear * x  (test/testCommunity.jl:418-464) */
+  int32_t growth;        /* 1: volume v is a DE variable with dt(v) = g */
+  int32_t medium;        /* 1: coupled medium field c on an n_medium grid */
+  double v_div;          /* division volume */
+  double div_sep;        /* daughters at +-div_sep along the division axis */
+  double p_death;        /* per-step death probability */
+  int32_t n_medium[3];   /* NMedium; node spacing dx = (hi - lo) / n_medium */
+  int32_t medium_sampling; /* CBM_MEDIUM_* */
+  double diff_D;         /* medium diffusion coefficient */
+  double decay;          /* medium decay rate lambda */
+  double secretion;      /* amount per unit time each agent adds to c */
+  double chemotaxis;     /* dt(x) += chemotaxis * dc/dx / (1 + |grad c|) */
+} cbm_config;
+
+/* ---- state exchanged with the host (Community fields) ------------------- */
+typedef struct cbm_state_view {
+  int64_t N;             /* number of agents */
+  int64_t capacity;      /* length of the host agent arrays (download) */
+  double t;              /* time */
+  int64_t step;          /* step counter: the random stream's step key */
+  int64_t id_max;        /* idMax_ */
+  void* pos[3];          /* x, y, z */
+  void* v;               /* volume (growth) or NULL */
+  void* g;               /* growth rate (growth) or NULL */
+  void* f[3];            /* lagged force fx, fy, fz (CBM_FORCE_LAGGED) or NULL */
+  int64_t* id;           /* ids or NULL (upload: NULL means 1..N) */
+  int64_t* parent;       /* id of the parent at birth (0 = initial agent) or NULL */
+  void* medium_c;        /* medium field, x fastest, prod(n_medium) nodes, or NULL */
+  void* medium_grad[3];  /* committed gradient fields (chemotaxis) or NULL */
+} cbm_state_view;
+
+typedef struct cbm_ctx cbm_ctx;
+
+/* ---- library ------------------------------------------------------------- */
+const char* cbm_version(void);
+/* Message of the last failed call on ctx (or of the last failed cbm_create
+ * when ctx is NULL). */
+const char* cbm_last_error(const cbm_ctx* ctx);
+
+/* ---- lifetime ------------------------------------------------------------ */
+/* Replaces ABM(...) + Community(...) + CBMNeighbors.initialize!
+ * (src/AgentStructure/agentStructure.jl:131-304, src/CommunityStructure/
+ * communityStructure.jl:108-186, src/neighbors.jl:601-619,1021-1047):
+ * validates cfg and allocates every device buffer for n_max agents. */
+int cbm_create(cbm_ctx** out, const cbm_config* cfg);
+/* Frees the device buffers and the stream. */
+void cbm_destroy(cbm_ctx* ctx);
+
+/* loadToPlatform! (src/CommunityStructure/communityStructure.jl:606-654):
+ * copies N agents (and the medium) to the device, zero-pads to n_max, resets
+ * NAdd_/NRemove_/flagSurvive_, computes neighbors.  Synchronous. */
+int cbm_upload(cbm_ctx* ctx, const cbm_state_view* host);
+/* bringFromPlatform! (communityStructure.jl:663-712): copies the first N
+ * agents back (which = CBM_VIEW_COMMITTED or CBM_VIEW_NEW).  Synchronous;
+ * fails with CBM_ERR_ARG if host->capacity < N. */
+int cbm_download(cbm_ctx* ctx, cbm_state_view* host, int32_t which);
+
+/* ---- stepping (src/CommunityStructure/step.jl) ---------------------------- */
+/* step! x nsteps (step.jl:96-107).  Enqueues the steps (as CUDA graph replays
+ * unless CBM_NO_GRAPH) and returns; CBM_SYNC waits and reports device flags. */
+int cbm_step(cbm_ctx* ctx, int32_t nsteps, int32_t flags);
+/* The stages of step!, for custom loops (docs/src/Usage_Community.md:236-345) */
+int cbm_agent_step_rule(cbm_ctx* ctx);   /* agentStepRule!  step.jl:6-14 */
+int cbm_agent_step_de(cbm_ctx* ctx);     /* agentStepDE!    step.jl:51-59 */
+int cbm_medium_step_rule(cbm_ctx* ctx);  /* mediumStepRule! step.jl:28-36 */
+int cbm_medium_step_de(cbm_ctx* ctx);    /* mediumStepDE!   step.jl:81-89 */
+int cbm_update(cbm_ctx* ctx);            /* update!         update.jl:310-320 */
+int cbm_compute_neighbors(cbm_ctx* ctx); /* computeNeighbors! neighbors.jl:18 */
+/* Waits for the stream and returns the first device flag as a status. */
+int cbm_sync(cbm_ctx* ctx);
+
+/* ---- inspection ----------------------------------------------------------- */
+/* N, NAdd_, NRemove_, idMax_, flagRecomputeNeighbors_ and the step counter.
+ * Synchronous. */
+int cbm_get_counters(cbm_ctx* ctx, int64_t* N, int64_t* n_add, int64_t* n_remove,
+                     int64_t* id_max, int32_t* flag_recompute, int64_t* step);
+/* Number of cells per axis of the cell grid (nCells_, neighbors.jl:605). */
+int cbm_grid_shape(cbm_ctx* ctx, int32_t* n_cells3);
+/* CellLinked arrays (neighbors.jl:601-619), 0-based: cell of each agent
+ * (N), first slot of each cell (prod(nCells)), agents per cell
+ * (prod(nCells)), agent indices in cell order (N) (cellAssignedToAgent_). */
+int cbm_get_grid(cbm_ctx* ctx, int32_t* agent_cell, int32_t* cell_start,
+                 int32_t* cell_count, int32_t* cell_agents);
+/* Verlet arrays (neighbors.jl:314-331): counts (N) and the row-major list
+ * list[i * n_max_neighbors + k] (N x n_max_neighbors); cap = list length. */
+int cbm_get_neighbors(cbm_ctx* ctx, int32_t* counts, int32_t* list, int64_t cap);
+/* The reference's neighbor-counting rule (test/testCommunity.jl:359-415):
+ * out[i] = number of neighbors j of i (per the configured algorithm) with
+ * euclidean distance < radius. */
+int cbm_count_neighbors(cbm_ctx* ctx, double radius, int32_t* out);
+
+/* Fills out[n] with draws of the shared stream (cbm_rng.h) on the device:
+ * kind 0 normal(mu=a, sigma=b), 1 uniform(a, b), 2 exponential(theta=a)
+ * (src/random.jl:8-22).  out is a host array of the context's precision. */
+int cbm_rng_fill(cbm_ctx* ctx, int32_t kind, double a, double b, int64_t n, int64_t step,
+                 void* out);
+
+/* The context's CUDA stream (cudaStream_t), for event timing by the caller. */
+void* cbm_stream(cbm_ctx* ctx);
+/* Number of kernels one step launches with this configuration. */
+int cbm_kernels_per_step(cbm_ctx* ctx);
+/* Runs one step! with kernels launched one by one, each bracketed by CUDA
+ * events on the context's stream (the reference has no stage timers; its
+ * evolve! only offers a progressMessage callback, step.jl:129,146).  Writes
+ * up to max_kernels durations (ms) and static kernel names; *n_kernels gets
+ * the number of kernels the step launched.  Synchronous. */
+int cbm_profile_step(cbm_ctx* ctx, int32_t max_kernels, float* ms, const char** names,
+                     int32_t* n_kernels);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CBM_B200_H */

@@ -1,0 +1,903 @@
+/*
+ * cbm_oracle.cpp — TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement of the reference's per-step path (CellBasedModels.jl
+ * v0.1.1, CPU platform), used by the tests and by bench.py's CPU baseline as
+ * the checker.  Nothing in the product links, loads or calls this file.
+ *
+ * It follows the reference's data layout and loop order, 0-based:
+ *   - committed agent arrays (x, v, fx ...) and their "__" copies, the
+ *     DE state u, exactly as loadToPlatform!/linkVariables set them up
+ *     (src/CommunityStructure/communityStructure.jl:606-654,724-743);
+ *   - agentStepRule! as a serial loop over agents with @addAgent/@removeAgent
+ *     (src/AgentStructure/functionRule.jl:9-111);
+ *   - agentStepDE!: cleanArray, the generated f(du,u,p,t) with
+ *     @loopOverNeighbors, then the Euler / EM update
+ *     (src/integrators.jl:442-505,683-734, src/AgentStructure/functionDE.jl:13-117);
+ *   - mediumStepRule!/mediumStepDE!: central difference and @∂2 FTCS with an
+ *     Euler step u <- u + dt f(u) (src/AgentStructure/macros.jl:148-311);
+ *   - update!: kernelListSurvived, kernelFillHolesParameters, commit
+ *     (src/CommunityStructure/update.jl:15-298);
+ *   - computeNeighbors!: CellLinked serial assign / cumsum / sort, Verlet
+ *     displacement check + rebuild, CLVD list over the cell grid
+ *     (src/neighbors.jl:92-133,367-570,636-979,1071-1131).
+ * Random draws come from the shared counter-based stream (include/cbm_rng.h)
+ * so that the device path and this checker see the same numbers.
+ *
+ * Build: oracle/build.sh (g++ -O2 -ffp-contract=off -fopenmp).  Single-thread
+ * and OpenMP runs give identical bits: every parallel loop writes per-agent
+ * results whose summation order is fixed.
+ */
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/cbm_b200.h"
+#include "../include/cbm_rng.h"
+
+namespace {
+
+int g_threads = 1;
+
+template <typename T>
+struct Com {
+  cbm_config cfg;
+  int dims = 3;
+  int64_t N = 0, nMax = 0, NAdd = 0, NRemove = 0, idMax = 0, step = 0;
+  double t = 0;
+  bool loaded = false;
+  int err = 0;  // first model fault seen (CBM_ERR_*), sticky until read
+
+  // agent arrays: committed and "__" (u rows for DE variables)
+  std::vector<T> x[3], x_[3];
+  std::vector<T> v, v_;
+  std::vector<T> g;
+  std::vector<T> f[3], f_[3];
+  std::vector<int64_t> id, parent;
+  std::vector<int64_t> flagSurvive, holeFromRemoveAt, repositionAgentInPos;
+  int flagRecompute = 1;
+
+  // neighbors
+  int64_t nCells[3] = {1, 1, 1};
+  T edge = 0;
+  std::vector<int64_t> cellAssignedToAgent, cellNumAgents, cellCumSum;
+  std::vector<int64_t> neighborN, neighborList;  // list column-major (nMax x nMaxNeighbors)
+  std::vector<T> posOld[3], accumulatedDistance;
+
+  // medium: committed c, u (c__), gradient committed / new
+  int64_t nm[3] = {1, 1, 1};
+  int64_t nNodes = 0;
+  T dxm[3] = {1, 1, 1};
+  std::vector<T> c, c_, gr[3], gr_[3];
+
+  std::vector<T> du[4];  // scratch of the integrator
+};
+
+template <typename T>
+inline T rint_t(T a) { return std::rint(a); }
+template <typename T>
+inline T fmod_t(T a, T b) { return std::fmod(a, b); }
+
+/* Julia's float `÷` (round((a - rem(a,b))/b)), a >= 0 here. */
+template <typename T>
+inline int64_t floordiv(T a, T b) {
+  return (int64_t)rint_t((a - fmod_t(a, b)) / b);
+}
+
+/* cellPos, src/neighbors.jl:636-638 (0-based).  A NaN coordinate falls in
+ * the first cell. */
+template <typename T>
+inline int64_t cellPos1(T edge, T x, T lo, T hi, int64_t n) {
+  if (x > hi) return n - 1;
+  if (!(x >= lo)) return 0;
+  int64_t p = floordiv<T>(x - lo, edge) + 1;
+  return p > n - 1 ? n - 1 : p;
+}
+
+/* cellInMesh, src/metrics.jl:18-20 (0-based, clamped at the top). */
+template <typename T>
+inline int64_t cellInMesh(T dx, T x, T lo, T hi, int64_t n) {
+  if (x > hi) return n - 1;
+  if (!(x >= lo)) return 0;
+  int64_t p = floordiv<T>(x - lo, dx);
+  return p > n - 1 ? n - 1 : p;
+}
+
+template <typename T>
+inline T euclid(const Com<T>& C, const std::vector<T>* a, int64_t i, const std::vector<T>* b,
+                int64_t j) {
+  T s = 0;
+  for (int d = 0; d < C.dims; ++d) {
+    T e = a[d][i] - b[d][j];
+    s = (d == 0) ? e * e : s + e * e;
+  }
+  return std::sqrt(s);
+}
+
+template <typename T>
+int64_t cellOf(const Com<T>& C, const std::vector<T>* P, int64_t i) {
+  int64_t lin = 0, mul = 1;
+  for (int d = 0; d < C.dims; ++d) {
+    int64_t p = cellPos1<T>(C.edge, P[d][i], (T)C.cfg.box_lo[d], (T)C.cfg.box_hi[d], C.nCells[d]);
+    lin += p * mul;
+    mul *= C.nCells[d];
+  }
+  return lin;
+}
+
+/* cellPosNeigh, src/neighbors.jl:658-708: k-th of 3^d neighbor cells, x
+ * fastest, -1 outside the grid.  (2D uses nX for the row stride.) */
+template <typename T>
+int64_t cellNeigh(const Com<T>& C, int64_t pos, int k) {
+  int64_t q[3] = {0, 0, 0};
+  int64_t r = pos;
+  for (int d = 0; d < C.dims; ++d) { q[d] = r % C.nCells[d]; r /= C.nCells[d]; }
+  int off[3] = {k % 3 - 1, (k / 3) % 3 - 1, k / 9 - 1};
+  int64_t lin = 0, mul = 1;
+  for (int d = 0; d < C.dims; ++d) {
+    int64_t p = q[d] + off[d];
+    if (p < 0 || p >= C.nCells[d]) return -1;
+    lin += p * mul;
+    mul *= C.nCells[d];
+  }
+  return lin;
+}
+
+/* Walk the neighbors of agent i as @loopOverNeighbors does, with positions P
+ * (u inside the DE, committed x inside a rule). */
+template <typename T, typename F>
+void forNeighbors(const Com<T>& C, const std::vector<T>* P, int64_t i, int64_t N, F&& body) {
+  switch (C.cfg.neighbors) {
+    case CBM_NEIGH_FULL:
+      for (int64_t j = 0; j < N; ++j)
+        if (j != i) body(j);
+      break;
+    case CBM_NEIGH_CELL_LINKED: {
+      int64_t pos = cellOf(C, P, i);
+      int nk = C.dims == 1 ? 3 : (C.dims == 2 ? 9 : 27);
+      for (int k = 0; k < nk; ++k) {
+        int64_t pn = cellNeigh(C, pos, k);
+        if (pn < 0) continue;
+        for (int64_t s = C.cellCumSum[pn] - C.cellNumAgents[pn]; s < C.cellCumSum[pn]; ++s) {
+          int64_t j = C.cellAssignedToAgent[s];
+          if (j != i) body(j);
+        }
+      }
+      break;
+    }
+    case CBM_NEIGH_VERLET_DISPLACEMENT:
+    case CBM_NEIGH_CLVD:
+      for (int64_t k = 0; k < C.neighborN[i]; ++k) body(C.neighborList[i + k * C.nMax]);
+      break;
+    default:
+      break;
+  }
+}
+
+template <typename T>
+void alloc(Com<T>& C) {
+  const cbm_config& k = C.cfg;
+  C.dims = k.dims;
+  C.nMax = k.n_max;
+  size_t n = (size_t)C.nMax;
+  for (int d = 0; d < 3; ++d) {
+    C.x[d].assign(n, 0); C.x_[d].assign(n, 0);
+    C.f[d].assign(n, 0); C.f_[d].assign(n, 0);
+    C.posOld[d].assign(n, 0);
+  }
+  C.v.assign(n, 0); C.v_.assign(n, 0); C.g.assign(n, 0);
+  C.id.assign(n, 0); C.parent.assign(n, 0);
+  C.flagSurvive.assign(n, 1); C.holeFromRemoveAt.assign(n, 0); C.repositionAgentInPos.assign(n, 0);
+  for (int d = 0; d < 4; ++d) C.du[d].assign(n, 0);
+  C.accumulatedDistance.assign(n, 0);
+  C.edge = (T)(k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT ? k.skin : k.cell_edge);
+  int64_t nc = 1;
+  for (int d = 0; d < C.dims; ++d) {
+    if (k.neighbors == CBM_NEIGH_CELL_LINKED || k.neighbors == CBM_NEIGH_CLVD) {
+      // nCells_ = ceil((hi - lo)/edge + 2), src/neighbors.jl:605
+      // evaluated in Float64 on the host in both reference platforms
+      double e = k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT ? k.skin : k.cell_edge;
+      C.nCells[d] = (int64_t)std::ceil((k.box_hi[d] - k.box_lo[d]) / e + 2.0);
+    } else {
+      C.nCells[d] = 1;
+    }
+    nc *= C.nCells[d];
+  }
+  C.cellAssignedToAgent.assign(n, 0);
+  C.cellNumAgents.assign((size_t)nc, 0);
+  C.cellCumSum.assign((size_t)nc, 0);
+  C.neighborN.assign(n, 0);
+  if (k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT || k.neighbors == CBM_NEIGH_CLVD)
+    C.neighborList.assign(n * (size_t)k.n_max_neighbors, 0);
+  C.nNodes = 0;
+  if (k.medium) {
+    C.nNodes = 1;
+    for (int d = 0; d < C.dims; ++d) {
+      C.nm[d] = k.n_medium[d];
+      C.dxm[d] = (T)((k.box_hi[d] - k.box_lo[d]) / (double)k.n_medium[d]);  // communityStructure.jl:274
+      C.nNodes *= C.nm[d];
+    }
+    C.c.assign((size_t)C.nNodes, 0); C.c_.assign((size_t)C.nNodes, 0);
+    for (int d = 0; d < 3; ++d) { C.gr[d].assign((size_t)C.nNodes, 0); C.gr_[d].assign((size_t)C.nNodes, 0); }
+  }
+}
+
+/* ---------------------------------------------------------------------------
+ * computeNeighbors!
+ * ------------------------------------------------------------------------- */
+template <typename T>
+void buildCells(Com<T>& C) {
+  // neighborsCellLinked{d}CPU!, src/neighbors.jl:918-979
+  std::fill(C.cellNumAgents.begin(), C.cellNumAgents.end(), 0);
+  for (int64_t i = 0; i < C.N; ++i) C.cellNumAgents[cellOf(C, C.x, i)] += 1;  // assignCells :776-786
+  int64_t acc = 0;
+  for (size_t c = 0; c < C.cellNumAgents.size(); ++c) {  // cumsum! .- counts :934-937
+    C.cellCumSum[c] = acc;
+    acc += C.cellNumAgents[c];
+  }
+  for (int64_t i = 0; i < C.N; ++i) {  // sortAgentsInCells :851-862
+    int64_t p = cellOf(C, C.x, i);
+    C.cellCumSum[p] += 1;
+    C.cellAssignedToAgent[C.cellCumSum[p] - 1] = i;
+  }
+}
+
+template <typename T>
+void verletDisplacement(Com<T>& C) {
+  // verletDisplacementCPU!, src/neighbors.jl:367-391
+  T thr = C.cfg.rebuild_threshold > 0 ? (T)C.cfg.rebuild_threshold : (T)C.cfg.skin / (T)2;
+  for (int64_t i = 0; i < C.N; ++i) {
+    C.accumulatedDistance[i] = euclid(C, C.x, i, C.posOld, i);
+    if (C.accumulatedDistance[i] >= thr) C.flagRecompute = 1;
+  }
+}
+
+template <typename T>
+void appendNeighbor(Com<T>& C, int64_t i, int64_t j) {
+  int64_t k = C.neighborN[i];
+  if (k >= C.cfg.n_max_neighbors) {
+#pragma omp atomic write
+    C.err = CBM_ERR_NEIGHBOR_OVERFLOW;
+    return;
+  }
+  C.neighborList[i + k * C.nMax] = j;
+  C.neighborN[i] = k + 1;
+}
+
+template <typename T>
+void computeNeighbors(Com<T>& C) {
+  const int alg = C.cfg.neighbors;
+  if (alg == CBM_NEIGH_CELL_LINKED) {
+    buildCells(C);
+    return;
+  }
+  if (alg != CBM_NEIGH_VERLET_DISPLACEMENT && alg != CBM_NEIGH_CLVD) return;
+  verletDisplacement(C);
+  if (C.flagRecompute != 1) return;
+  const T skin = (T)C.cfg.skin;
+  if (alg == CBM_NEIGH_CLVD) buildCells(C);  // neighborsCLVD, :1206-1228
+  std::fill(C.neighborN.begin(), C.neighborN.end(), 0);
+  std::fill(C.accumulatedDistance.begin(), C.accumulatedDistance.end(), 0);
+  C.flagRecompute = 0;
+  for (int64_t i = 0; i < C.N; ++i)  // verletResetDisplacement :438-487
+    for (int d = 0; d < C.dims; ++d) C.posOld[d][i] = C.x[d][i];
+  if (alg == CBM_NEIGH_VERLET_DISPLACEMENT) {
+    // verletNeighborsCPU!, :92-133: ascending j
+#pragma omp parallel for schedule(static) num_threads(g_threads)
+    for (int64_t i = 0; i < C.N; ++i)
+      for (int64_t j = 0; j < C.N; ++j)
+        if (i != j && euclid(C, C.x, i, C.x, j) < skin) appendNeighbor(C, i, j);
+  } else {
+    // verletNeighborsCLVD{d}CPU!, :1071-1131: cell order, ascending within a cell
+    const int nk = C.dims == 1 ? 3 : (C.dims == 2 ? 9 : 27);
+#pragma omp parallel for schedule(static) num_threads(g_threads)
+    for (int64_t i = 0; i < C.N; ++i) {
+      int64_t pos = cellOf(C, C.x, i);
+      for (int k = 0; k < nk; ++k) {
+        int64_t pn = cellNeigh(C, pos, k);
+        if (pn < 0) continue;
+        for (int64_t s = C.cellCumSum[pn] - C.cellNumAgents[pn]; s < C.cellCumSum[pn]; ++s) {
+          int64_t j = C.cellAssignedToAgent[s];
+          if (j != i && euclid(C, C.x, i, C.x, j) < skin) appendNeighbor(C, i, j);
+        }
+      }
+    }
+  }
+}
+
+/* ---------------------------------------------------------------------------
+ * agentStepRule!
+ * ------------------------------------------------------------------------- */
+template <typename T>
+void bilinear(const Com<T>& C, const T* p, int64_t* node, T* w) {
+  // corners of the medium cell whose nodes (cell centres lo + (i+1/2) dx)
+  // surround p; node indices clamped to the grid.
+  int64_t i0[3], i1[3];
+  T tt[3];
+  for (int d = 0; d < C.dims; ++d) {
+    T s = (p[d] - (T)C.cfg.box_lo[d]) / C.dxm[d] - (T)0.5;
+    T fl = std::floor(s);
+    tt[d] = s - fl;
+    int64_t a = (int64_t)fl;
+    int64_t b = a + 1;
+    a = a < 0 ? 0 : (a > C.nm[d] - 1 ? C.nm[d] - 1 : a);
+    b = b < 0 ? 0 : (b > C.nm[d] - 1 ? C.nm[d] - 1 : b);
+    i0[d] = a; i1[d] = b;
+  }
+  int nc = 1 << C.dims;
+  for (int q = 0; q < nc; ++q) {
+    int64_t lin = 0, mul = 1;
+    T wq = 1;
+    for (int d = 0; d < C.dims; ++d) {
+      bool hi = (q >> d) & 1;
+      lin += (hi ? i1[d] : i0[d]) * mul;
+      mul *= C.nm[d];
+      wq = wq * (hi ? tt[d] : (T)1 - tt[d]);
+    }
+    node[q] = lin;
+    w[q] = wq;
+  }
+}
+
+template <typename T>
+int64_t nearestNode(const Com<T>& C, const T* p) {
+  int64_t lin = 0, mul = 1;
+  for (int d = 0; d < C.dims; ++d) {
+    lin += cellInMesh<T>(C.dxm[d], p[d], (T)C.cfg.box_lo[d], (T)C.cfg.box_hi[d], C.nm[d]) * mul;
+    mul *= C.nm[d];
+  }
+  return lin;
+}
+
+/* @addAgent, src/AgentStructure/functionRule.jl:9-79.  Returns the new slot
+ * or -1 when nMax is reached (the birth is dropped; the id is consumed). */
+template <typename T>
+int64_t addAgent(Com<T>& C, int64_t i) {
+  int64_t slot = C.N + C.NAdd;
+  C.NAdd += 1;
+  int64_t idNew = ++C.idMax;
+  if (slot < C.nMax) {
+    C.id[slot] = idNew;
+    C.flagRecompute = 1;
+    C.flagSurvive[slot] = 1;
+    // parameters not given to @addAgent are copied from the parent
+    for (int d = 0; d < C.dims; ++d) {
+      C.x_[d][slot] = C.x[d][i];
+      C.f_[d][slot] = C.f[d][i];
+    }
+    C.v_[slot] = C.v[i];
+    C.g[slot] = C.g[i];
+    C.parent[slot] = C.id[i];
+    return slot;
+  }
+  C.NAdd -= 1;
+  if (!C.err) C.err = CBM_ERR_AGENT_OVERFLOW;
+  return -1;
+}
+
+/* @removeAgent, functionRule.jl:89-111 */
+template <typename T>
+void removeAgent(Com<T>& C, int64_t i) {
+  C.holeFromRemoveAt[C.NRemove] = i;
+  C.NRemove += 1;
+  C.flagSurvive[i] = 0;
+  C.flagRecompute = 1;
+}
+
+template <typename T>
+void agentStepRule(Com<T>& C) {
+  const cbm_config& k = C.cfg;
+  const int D = C.dims;
+  const T amt = (T)k.secretion * (T)k.dt;
+  for (int64_t i = 0; i < C.N; ++i) {
+    T p[3];
+    for (int d = 0; d < D; ++d) p[d] = C.x[d][i];
+    if (k.walls == CBM_WALLS_REFLECT) {
+      for (int d = 0; d < D; ++d) {
+        T lo = (T)k.box_lo[d], hi = (T)k.box_hi[d];
+        if (p[d] < lo) C.x_[d][i] = (T)2 * lo - p[d];
+        else if (p[d] > hi) C.x_[d][i] = (T)2 * hi - p[d];
+      }
+    }
+    if (k.medium && k.secretion != 0) {
+      // c += secretion*dt at the agent (auxiliar.jl:353-365)
+      if (k.medium_sampling == CBM_MEDIUM_NEAREST) {
+        int64_t n = nearestNode(C, p);
+        C.c_[n] = C.c_[n] + amt;
+      } else {
+        int64_t nodes[8];
+        T w[8];
+        bilinear(C, p, nodes, w);
+        for (int q = 0; q < (1 << D); ++q) C.c_[nodes[q]] = C.c_[nodes[q]] + w[q] * amt;
+      }
+    }
+    if (k.fate == CBM_FATE_VOLUME) {
+      if (k.growth && C.v[i] >= (T)k.v_div) {
+        T a[3] = {0, 0, 0};
+        cbm_normals(k.seed, C.step, (uint32_t)i, CBM_STREAM_DIVISION, k.community, D, a);
+        T s = 0;
+        for (int d = 0; d < D; ++d) s = (d == 0) ? a[d] * a[d] : s + a[d] * a[d];
+        T Ta = std::sqrt(s);
+        for (int d = 0; d < D; ++d) a[d] = a[d] / Ta;
+        T rsep = (T)k.div_sep;
+        T vh = C.v[i] / (T)2;
+        int64_t s1 = addAgent(C, i);
+        if (s1 >= 0) {
+          for (int d = 0; d < D; ++d) C.x_[d][s1] = p[d] + rsep * a[d];
+          C.v_[s1] = vh;
+        }
+        int64_t s2 = addAgent(C, i);
+        if (s2 >= 0) {
+          for (int d = 0; d < D; ++d) C.x_[d][s2] = p[d] - rsep * a[d];
+          C.v_[s2] = vh;
+        }
+        removeAgent(C, i);
+      } else if (k.p_death > 0 &&
+                 cbm_uniform<T>(k.seed, C.step, (uint32_t)i, CBM_STREAM_DEATH, k.community) <
+                     (T)k.p_death) {
+        removeAgent(C, i);
+      }
+    } else if (k.fate == CBM_FATE_ID_PARITY) {
+      if (C.id[i] % 2 == 1) removeAgent(C, i);
+      else addAgent(C, i);
+    }
+  }
+}
+
+/* ---------------------------------------------------------------------------
+ * agentStepDE!
+ * ------------------------------------------------------------------------- */
+template <typename T>
+void sampleGrad(const Com<T>& C, const T* p, T* gv) {
+  const int D = C.dims;
+  if (C.cfg.medium_sampling == CBM_MEDIUM_NEAREST) {
+    int64_t n = nearestNode(C, p);
+    for (int d = 0; d < D; ++d) gv[d] = C.gr[d][n];
+  } else {
+    int64_t nodes[8];
+    T w[8];
+    bilinear(C, p, nodes, w);
+    for (int d = 0; d < D; ++d) {
+      T s = 0;
+      for (int q = 0; q < (1 << D); ++q) s = s + w[q] * C.gr[d][nodes[q]];
+      gv[d] = s;
+    }
+  }
+}
+
+template <typename T>
+void agentStepDE(Com<T>& C) {
+  const cbm_config& k = C.cfg;
+  const int D = C.dims;
+  const int64_t N = C.N;
+  const T dt = (T)k.dt, krep = (T)k.k_rep, rrep = (T)k.r_rep, katt = (T)k.k_att,
+          ratt = (T)k.r_att;
+  const bool lagged = k.force_mode == CBM_FORCE_LAGGED;
+#pragma omp parallel for schedule(static) num_threads(g_threads)
+  for (int64_t i = 0; i < N; ++i) {
+    T acc[3] = {0, 0, 0};  // cleanArray: du = 0 (integrators.jl:442-450)
+    T pi[3];
+    for (int d = 0; d < D; ++d) pi[d] = C.x_[d][i];
+    if (k.neighbors != CBM_NEIGH_NONE) {
+      forNeighbors(C, C.x_, i, N, [&](int64_t j) {
+        T e[3];
+        T s2 = 0;
+        for (int d = 0; d < D; ++d) {
+          e[d] = pi[d] - C.x_[d][j];
+          s2 = (d == 0) ? e[d] * e[d] : s2 + e[d] * e[d];
+        }
+        T dist = std::sqrt(s2);
+        T F;
+        if (dist < rrep) F = krep * (rrep - dist);
+        else if (dist < ratt) F = k.att_form == CBM_ATT_FROM_REP ? -(katt * (dist - rrep))
+                                                                : -(katt * (ratt - dist));
+        else return;
+        T s = F / dist;
+        for (int d = 0; d < D; ++d) acc[d] = acc[d] + s * e[d];
+      });
+    }
+    if (k.walls == CBM_WALLS_PUSH) {
+      for (int d = 0; d < D; ++d) {
+        if (pi[d] < (T)k.box_lo[d] + (T)k.wall_range) acc[d] = acc[d] + (T)k.wall_force;
+        else if (pi[d] > (T)k.box_hi[d] - (T)k.wall_range) acc[d] = acc[d] - (T)k.wall_force;
+      }
+    }
+    T dv[3];
+    if (lagged) {
+      for (int d = 0; d < D; ++d) { C.f_[d][i] = acc[d]; dv[d] = C.f[d][i]; }
+    } else {
+      for (int d = 0; d < D; ++d) dv[d] = acc[d];
+    }
+    if (k.drift_linear != 0)
+      for (int d = 0; d < D; ++d) dv[d] = dv[d] + (-(T)k.drift_linear) * pi[d];
+    if (k.medium && k.chemotaxis != 0) {
+      T gv[3] = {0, 0, 0};
+      sampleGrad(C, pi, gv);
+      T s = 0;
+      for (int d = 0; d < D; ++d) s = (d == 0) ? gv[d] * gv[d] : s + gv[d] * gv[d];
+      T den = (T)1 + std::sqrt(s);
+      for (int d = 0; d < D; ++d) dv[d] = dv[d] + ((T)k.chemotaxis * gv[d]) / den;
+    }
+    for (int d = 0; d < D; ++d) C.du[d][i] = dv[d];
+  }
+  // integrator update over 1:N (integrators.jl:495-496 / :720-721)
+  const T sq = std::sqrt(dt);
+  const T sig = (T)k.sigma;
+  for (int64_t i = 0; i < N; ++i) {
+    if (k.integrator == CBM_INT_EM) {
+      T xi[3] = {0, 0, 0};
+      cbm_normals(k.seed, C.step, (uint32_t)i, CBM_STREAM_NOISE, k.community, D, xi);
+      for (int d = 0; d < D; ++d) C.x_[d][i] = (C.x_[d][i] + C.du[d][i] * dt) + (sig * xi[d]) * sq;
+    } else {
+      for (int d = 0; d < D; ++d) C.x_[d][i] = C.x_[d][i] + C.du[d][i] * dt;
+    }
+    if (k.growth) C.v_[i] = C.v_[i] + C.g[i] * dt;
+  }
+}
+
+/* ---------------------------------------------------------------------------
+ * mediumStepRule! / mediumStepDE!
+ * ------------------------------------------------------------------------- */
+template <typename T>
+bool interiorNode(const Com<T>& C, int64_t n, int64_t* q) {
+  int64_t r = n;
+  bool in = true;
+  for (int d = 0; d < C.dims; ++d) {
+    q[d] = r % C.nm[d];
+    r /= C.nm[d];
+    if (q[d] == 0 || q[d] == C.nm[d] - 1) in = false;  // @mediumInside, macros.jl:240-255
+  }
+  return in;
+}
+
+template <typename T>
+void mediumStepRule(Com<T>& C) {
+  if (!C.cfg.medium || C.cfg.chemotaxis == 0) return;
+  // gx = @∂(1,c) inside, 0 on the border (macros.jl:148-190)
+  int64_t stride[3] = {1, C.nm[0], C.nm[0] * C.nm[1]};
+  for (int64_t n = 0; n < C.nNodes; ++n) {
+    int64_t q[3];
+    bool in = interiorNode(C, n, q);
+    for (int d = 0; d < C.dims; ++d)
+      C.gr_[d][n] = in ? (C.c[n + stride[d]] - C.c[n - stride[d]]) / ((T)2 * C.dxm[d]) : (T)0;
+  }
+}
+
+template <typename T>
+void mediumStepDE(Com<T>& C) {
+  if (!C.cfg.medium) return;
+  const T D = (T)C.cfg.diff_D, lam = (T)C.cfg.decay, dt = (T)C.cfg.dt;
+  int64_t stride[3] = {1, C.nm[0], C.nm[0] * C.nm[1]};
+  std::vector<T> k(C.nNodes, (T)0);
+  for (int64_t n = 0; n < C.nNodes; ++n) {
+    int64_t q[3];
+    if (!interiorNode(C, n, q)) continue;  // du stays 0 on the border
+    T u = C.c_[n];
+    T lap = 0;
+    for (int d = 0; d < C.dims; ++d) {
+      // @∂2: (m[i+1] - 2 m[i] + m[i-1]) / dx^2, macros.jl:203-258
+      T l = ((C.c_[n + stride[d]] - (T)2 * u) + C.c_[n - stride[d]]) / (C.dxm[d] * C.dxm[d]);
+      lap = (d == 0) ? l : lap + l;
+    }
+    k[n] = D * lap - lam * u;
+  }
+  for (int64_t n = 0; n < C.nNodes; ++n) C.c_[n] = C.c_[n] + dt * k[n];  // u = uprev + dt*k
+}
+
+/* ---------------------------------------------------------------------------
+ * update!
+ * ------------------------------------------------------------------------- */
+template <typename T, typename V>
+void fillHoles(Com<T>& C, std::vector<V>& par, int64_t count) {
+  // kernelFillHolesParametersCPU!, update.jl:67-84
+  for (int64_t k = 0; k < count; ++k) {
+    int64_t posNew = C.holeFromRemoveAt[k], posOld = C.repositionAgentInPos[k];
+    if (posNew < posOld) par[posNew] = par[posOld];
+  }
+}
+
+template <typename T>
+void update(Com<T>& C) {
+  const int D = C.dims;
+  if (C.cfg.fate != CBM_FATE_NONE) {
+    // kernelListSurvived, update.jl:15-33
+    int64_t count = 0;
+    int64_t lastPos = C.N + C.NAdd - 1;
+    while (C.NRemove > count && lastPos >= 0) {
+      if (C.flagSurvive[lastPos] == 1) C.repositionAgentInPos[count++] = lastPos;
+      lastPos -= 1;
+    }
+    // entries beyond `count` would only touch rows >= the new N
+    fillHoles(C, C.id, count);
+    fillHoles(C, C.parent, count);
+    for (int d = 0; d < D; ++d) { fillHoles(C, C.x_[d], count); fillHoles(C, C.f_[d], count); }
+    fillHoles(C, C.v_, count);
+    fillHoles(C, C.g, count);
+  }
+  C.N = C.N + C.NAdd - C.NRemove;
+  C.NAdd = 0;
+  C.NRemove = 0;
+  for (int64_t i = 0; i < C.N; ++i) C.flagSurvive[i] = 1;
+  // commit par <- par__ (kernelUpdateParameters, update.jl:126-158)
+  for (int64_t i = 0; i < C.N; ++i) {
+    for (int d = 0; d < D; ++d) { C.x[d][i] = C.x_[d][i]; C.f[d][i] = C.f_[d][i]; }
+    C.v[i] = C.v_[i];
+  }
+  if (C.cfg.medium) {
+    C.c = C.c_;
+    for (int d = 0; d < D; ++d) C.gr[d] = C.gr_[d];
+  }
+  C.t = C.t + C.cfg.dt;
+  C.step += 1;
+}
+
+template <typename T>
+void step(Com<T>& C) {
+  // step!, step.jl:96-107 (model stages are empty in this family)
+  agentStepRule(C);
+  agentStepDE(C);
+  mediumStepRule(C);
+  mediumStepDE(C);
+  update(C);
+  computeNeighbors(C);
+}
+
+/* ---------------------------------------------------------------------------
+ * host exchange
+ * ------------------------------------------------------------------------- */
+template <typename T>
+int upload(Com<T>& C, const cbm_state_view* h) {
+  const int D = C.dims;
+  if (h->N < 0 || h->N > C.nMax) return CBM_ERR_ARG;
+  alloc(C);
+  C.N = h->N;
+  C.t = h->t;
+  C.step = h->step;
+  C.idMax = h->id_max > 0 ? h->id_max : h->N;
+  C.NAdd = C.NRemove = 0;
+  C.err = 0;
+  for (int64_t i = 0; i < C.N; ++i) {
+    for (int d = 0; d < D; ++d) {
+      C.x[d][i] = ((const T*)h->pos[d])[i];
+      C.f[d][i] = h->f[d] ? ((const T*)h->f[d])[i] : (T)0;
+    }
+    C.v[i] = h->v ? ((const T*)h->v)[i] : (T)0;
+    C.g[i] = h->g ? ((const T*)h->g)[i] : (T)0;
+    C.id[i] = h->id ? h->id[i] : i + 1;
+    C.parent[i] = h->parent ? h->parent[i] : 0;
+  }
+  for (int d = 0; d < 3; ++d) { C.x_[d] = C.x[d]; C.f_[d] = C.f[d]; }
+  C.v_ = C.v;
+  if (C.cfg.medium) {
+    for (int64_t n = 0; n < C.nNodes; ++n) {
+      C.c[n] = h->medium_c ? ((const T*)h->medium_c)[n] : (T)0;
+      for (int d = 0; d < D; ++d)
+        C.gr[d][n] = h->medium_grad[d] ? ((const T*)h->medium_grad[d])[n] : (T)0;
+    }
+    C.c_ = C.c;
+    for (int d = 0; d < 3; ++d) C.gr_[d] = C.gr[d];
+  }
+  C.flagRecompute = 1;  // loadBaseParameters!, communityStructure.jl:480
+  C.loaded = true;
+  computeNeighbors(C);  // communityStructure.jl:648
+  return CBM_OK;
+}
+
+template <typename T>
+int download(Com<T>& C, cbm_state_view* h, int which) {
+  const int D = C.dims;
+  if (h->capacity < C.N) return CBM_ERR_ARG;
+  h->N = C.N;
+  h->t = C.t;
+  h->step = C.step;
+  h->id_max = C.idMax;
+  const bool nw = which == CBM_VIEW_NEW;
+  for (int64_t i = 0; i < C.N; ++i) {
+    for (int d = 0; d < D; ++d) {
+      if (h->pos[d]) ((T*)h->pos[d])[i] = nw ? C.x_[d][i] : C.x[d][i];
+      if (h->f[d]) ((T*)h->f[d])[i] = nw ? C.f_[d][i] : C.f[d][i];
+    }
+    if (h->v) ((T*)h->v)[i] = nw ? C.v_[i] : C.v[i];
+    if (h->g) ((T*)h->g)[i] = C.g[i];
+    if (h->id) h->id[i] = C.id[i];
+    if (h->parent) h->parent[i] = C.parent[i];
+  }
+  if (C.cfg.medium) {
+    for (int64_t n = 0; n < C.nNodes; ++n) {
+      if (h->medium_c) ((T*)h->medium_c)[n] = nw ? C.c_[n] : C.c[n];
+      for (int d = 0; d < D; ++d)
+        if (h->medium_grad[d]) ((T*)h->medium_grad[d])[n] = nw ? C.gr_[d][n] : C.gr[d][n];
+    }
+  }
+  return CBM_OK;
+}
+
+struct Handle {
+  int prec;
+  void* p;
+};
+
+template <typename T>
+Com<T>* as(Handle* h) { return (Com<T>*)h->p; }
+
+}  // namespace
+
+#define DISPATCH(h, expr)                          \
+  do {                                             \
+    if ((h)->prec == CBM_F64) { auto* C = as<double>(h); expr; } \
+    else { auto* C = as<float>(h); expr; }         \
+  } while (0)
+
+extern "C" {
+
+void oracle_set_threads(int n) { g_threads = n > 0 ? n : 1; }
+
+int oracle_max_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+void* oracle_create(const cbm_config* cfg) {
+  if (!cfg || cfg->dims < 1 || cfg->dims > 3 || cfg->n_max < 0) return nullptr;
+  Handle* h = new Handle;
+  h->prec = cfg->precision;
+  if (h->prec == CBM_F64) {
+    auto* C = new Com<double>;
+    C->cfg = *cfg;
+    alloc(*C);
+    h->p = C;
+  } else {
+    auto* C = new Com<float>;
+    C->cfg = *cfg;
+    alloc(*C);
+    h->p = C;
+  }
+  return h;
+}
+
+void oracle_destroy(void* vh) {
+  Handle* h = (Handle*)vh;
+  if (!h) return;
+  if (h->prec == CBM_F64) delete as<double>(h);
+  else delete as<float>(h);
+  delete h;
+}
+
+int oracle_upload(void* vh, const cbm_state_view* s) {
+  int rc = 0;
+  DISPATCH((Handle*)vh, rc = upload(*C, s));
+  return rc;
+}
+
+int oracle_download(void* vh, cbm_state_view* s, int which) {
+  int rc = 0;
+  DISPATCH((Handle*)vh, rc = download(*C, s, which));
+  return rc;
+}
+
+/* stage: 0 agentRule, 1 agentDE, 2 mediumRule, 3 mediumDE, 4 update, 5 neighbors */
+int oracle_stage(void* vh, int stage) {
+  DISPATCH((Handle*)vh, {
+    switch (stage) {
+      case 0: agentStepRule(*C); break;
+      case 1: agentStepDE(*C); break;
+      case 2: mediumStepRule(*C); break;
+      case 3: mediumStepDE(*C); break;
+      case 4: update(*C); break;
+      case 5: computeNeighbors(*C); break;
+      default: return CBM_ERR_ARG;
+    }
+  });
+  return CBM_OK;
+}
+
+int oracle_step(void* vh, int nsteps) {
+  DISPATCH((Handle*)vh, for (int s = 0; s < nsteps; ++s) step(*C));
+  return CBM_OK;
+}
+
+/* returns and clears the first model fault */
+int oracle_take_error(void* vh) {
+  int e = 0;
+  DISPATCH((Handle*)vh, { e = C->err; C->err = 0; });
+  return e;
+}
+
+int oracle_get_counters(void* vh, int64_t* N, int64_t* nadd, int64_t* nrem, int64_t* idmax,
+                        int32_t* flag, int64_t* stepc) {
+  DISPATCH((Handle*)vh, {
+    *N = C->N; *nadd = C->NAdd; *nrem = C->NRemove; *idmax = C->idMax;
+    *flag = C->flagRecompute; *stepc = C->step;
+  });
+  return CBM_OK;
+}
+
+int oracle_grid_shape(void* vh, int32_t* n3) {
+  DISPATCH((Handle*)vh, for (int d = 0; d < 3; ++d) n3[d] = (int32_t)C->nCells[d]);
+  return CBM_OK;
+}
+
+int oracle_get_grid(void* vh, int32_t* agent_cell, int32_t* cell_start, int32_t* cell_count,
+                    int32_t* cell_agents) {
+  DISPATCH((Handle*)vh, {
+    for (int64_t i = 0; i < C->N; ++i) {
+      agent_cell[i] = (int32_t)cellOf(*C, C->x, i);
+      cell_agents[i] = (int32_t)C->cellAssignedToAgent[i];
+    }
+    for (size_t c = 0; c < C->cellNumAgents.size(); ++c) {
+      cell_count[c] = (int32_t)C->cellNumAgents[c];
+      cell_start[c] = (int32_t)(C->cellCumSum[c] - C->cellNumAgents[c]);
+    }
+  });
+  return CBM_OK;
+}
+
+int oracle_get_neighbors(void* vh, int32_t* counts, int32_t* list, int64_t cap) {
+  DISPATCH((Handle*)vh, {
+    int64_t m = C->cfg.n_max_neighbors;
+    if (cap < C->N * m) return CBM_ERR_ARG;
+    for (int64_t i = 0; i < C->N; ++i) {
+      counts[i] = (int32_t)C->neighborN[i];
+      for (int64_t k = 0; k < m; ++k)
+        list[i * m + k] = k < C->neighborN[i] ? (int32_t)C->neighborList[i + k * C->nMax] : -1;
+    }
+  });
+  return CBM_OK;
+}
+
+int oracle_count_neighbors(void* vh, double radius, int32_t* out) {
+  DISPATCH((Handle*)vh, {
+    auto r = (decltype(C->edge))radius;
+    for (int64_t i = 0; i < C->N; ++i) {
+      int32_t n = 0;
+      forNeighbors(*C, C->x, i, C->N, [&](int64_t j) {
+        if (euclid(*C, C->x, i, C->x, j) < r) n += 1;
+      });
+      out[i] = n;
+    }
+  });
+  return CBM_OK;
+}
+
+/* kind 0 normal(a,b), 1 uniform(a,b), 2 exponential(a): src/random.jl:8-22 */
+int oracle_rng_fill(int precision, uint64_t seed, uint32_t community, int kind, double a,
+                    double b, int64_t n, int64_t stepc, void* out) {
+  for (int64_t i = 0; i < n; ++i) {
+    if (precision == CBM_F64) {
+      double z;
+      if (kind == 0) { cbm_normals(seed, stepc, (uint32_t)i, CBM_STREAM_USER, community, 1, &z); z = b * z + a; }
+      else if (kind == 1) z = (b - a) * cbm_uniform_f64(seed, stepc, (uint32_t)i, CBM_STREAM_USER, community) + a;
+      else z = -cbm_log_f64(1.0 - cbm_uniform_f64(seed, stepc, (uint32_t)i, CBM_STREAM_USER, community)) * a;
+      ((double*)out)[i] = z;
+    } else {
+      float z;
+      if (kind == 0) { cbm_normals(seed, stepc, (uint32_t)i, CBM_STREAM_USER, community, 1, &z); z = (float)b * z + (float)a; }
+      else if (kind == 1) z = ((float)b - (float)a) * cbm_uniform_f32(seed, stepc, (uint32_t)i, CBM_STREAM_USER, community) + (float)a;
+      else z = -cbm_log_f32(1.0f - cbm_uniform_f32(seed, stepc, (uint32_t)i, CBM_STREAM_USER, community)) * (float)a;
+      ((float*)out)[i] = z;
+    }
+  }
+  return CBM_OK;
+}
+
+/* own log / cos-sin, exposed for accuracy tests */
+double oracle_log_f64(double x) { return cbm_log_f64(x); }
+float oracle_log_f32(float x) { return cbm_log_f32(x); }
+void oracle_cossin_f64(double w, double* c, double* s) { cbm_cossin_turns_f64(w, c, s); }
+void oracle_cossin_f32(float w, float* c, float* s) { cbm_cossin_turns_f32(w, c, s); }
+void oracle_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1,
+                   uint32_t* out) {
+  cbm_u32x4 r = cbm_philox4x32_10(c0, c1, c2, c3, k0, k1);
+  for (int i = 0; i < 4; ++i) out[i] = r.v[i];
+}
+
+}  // extern "C"

@@ -1,0 +1,71 @@
+"""Seeded synthetic scenarios shared by the parity tests and bench.py.
+
+Each builder returns (config keyword arguments, initial state dict).  Shapes
+and value distributions follow the workloads the reference's hot path is
+measured on (soft-sphere aggregation, a growing 3D colony, chemotaxis on a
+medium, many small communities, a differentiable ODE trajectory); sizes are
+parameters so that tests run small cases and the bench the full ones.
+"""
+import numpy as np
+
+
+def aggregation_2d(abi, N=4096, L=100.0, seed=1, precision=None, steps_hint=1000):
+    """2D soft spheres in [0,L]^2, r=1, k=10, a=1, reflecting walls, Euler,
+    dt=0.01, cell grid edge 3 (CellLinked)."""
+    rng = np.random.default_rng(seed)
+    kw = dict(dims=2, precision=abi.F64 if precision is None else precision, n_max=N,
+              box_lo=(0.0, 0.0), box_hi=(L, L), dt=0.01, seed=seed,
+              neighbors=abi.NEIGH_CELL_LINKED, cell_edge=3.0, integrator=abi.INT_EULER,
+              k_rep=10.0, r_rep=2.0, k_att=1.0, r_att=3.0, att_form=abi.ATT_FROM_REP,
+              walls=abi.WALLS_REFLECT)
+    state = dict(x=rng.uniform(0, L, N), y=rng.uniform(0, L, N))
+    return kw, state
+
+
+def colony_3d(abi, N=10000, R=20.0, L=400.0, n_max=None, seed=2, precision=None,
+              neighbors=None, p_death=1e-4, sigma=0.05):
+    """3D colony: N agents uniform in a radius-R ball centred in [0,L]^3,
+    v ~ U(1,2), g ~ U(0.8,1.2), EM sigma, divide at v >= 2 into daughters at
+    +-0.5 r, death probability p_death, CLVD with R_list 3.3 and rebuild at 0.15,
+    dt = 0.005."""
+    rng = np.random.default_rng(seed)
+    u = rng.normal(size=(N, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    rad = R * rng.uniform(size=N) ** (1 / 3)
+    p = L / 2 + u * rad[:, None]
+    alg = abi.NEIGH_CLVD if neighbors is None else neighbors
+    kw = dict(dims=3, precision=abi.F32 if precision is None else precision,
+              n_max=n_max or int(1.2 * N), box_lo=(0.0,) * 3, box_hi=(L,) * 3, dt=0.005,
+              seed=seed, neighbors=alg, cell_edge=3.3, skin=3.3, rebuild_threshold=0.15,
+              n_max_neighbors=64, integrator=abi.INT_EM, sigma=sigma, k_rep=10.0, r_rep=2.0,
+              k_att=1.0, r_att=3.0, att_form=abi.ATT_FROM_REP, growth=1, fate=abi.FATE_VOLUME,
+              v_div=2.0, div_sep=0.5, p_death=p_death)
+    state = dict(x=p[:, 0], y=p[:, 1], z=p[:, 2], v=rng.uniform(1, 2, N), g=rng.uniform(0.8, 1.2, N))
+    return kw, state
+
+
+def packed_colony_3d(abi, N=1_000_000, density=0.15, L=400.0, seed=2, n_max=None, precision=None,
+                     p_death=1e-4):
+    """A grown colony snapshot: N agents at the packed density (agents per unit
+    volume) in a ball centred in [0,L]^3, ages spread so that divisions occur
+    every step (v ~ U(1,2))."""
+    R = (3 * N / (4 * np.pi * density)) ** (1 / 3)
+    kw, state = colony_3d(abi, N=N, R=R, L=L, n_max=n_max or int(1.2 * N), seed=seed,
+                          precision=precision, p_death=p_death)
+    return kw, state
+
+
+def chemotaxis_2d(abi, N=200000, L=1024.0, n_medium=1024, seed=3, bilinear=True, precision=None):
+    """2D chemotaxis: agents in [0,L]^2 on an n_medium^2 FTCS grid (D=1, dt=0.2,
+    decay 0.01, secretion 0.1), drift 0.5 grad c / (1 + |grad c|), sigma 0.1,
+    repulsion k=10, r=1 (cutoff 2r), CellLinked edge 2."""
+    rng = np.random.default_rng(seed)
+    kw = dict(dims=2, precision=abi.F32 if precision is None else precision, n_max=N,
+              box_lo=(0.0, 0.0), box_hi=(L, L), dt=0.2, seed=seed,
+              neighbors=abi.NEIGH_CELL_LINKED, cell_edge=2.0, integrator=abi.INT_EM, sigma=0.1,
+              k_rep=10.0, r_rep=2.0, k_att=0.0, r_att=2.0, medium=1,
+              n_medium=(n_medium, n_medium), diff_D=1.0, decay=0.01, secretion=0.1,
+              chemotaxis=0.5,
+              medium_sampling=abi.MEDIUM_BILINEAR if bilinear else abi.MEDIUM_NEAREST)
+    state = dict(x=rng.uniform(0, L, N), y=rng.uniform(0, L, N))
+    return kw, state
