@@ -222,7 +222,13 @@ void enqueue_medium_rule(cbm_ctx* c, const Params<T>& P) {
 template <typename T, int D>
 void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P) {
   const cbm_config& k = c->cfg;
-  bool needed = k.walls == CBM_WALLS_REFLECT || (k.medium && k.secretion != 0) ||
+  const bool gather = k.medium && k.secretion != 0 && k.medium_sampling == CBM_MEDIUM_BILINEAR &&
+                      k.neighbors == CBM_NEIGH_CELL_LINKED;
+  if (gather) {
+    PROF("k_secrete_gather");
+    k_secrete_gather<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
+  }
+  bool needed = k.walls == CBM_WALLS_REFLECT || (k.medium && k.secretion != 0 && !gather) ||
                 k.fate != CBM_FATE_NONE;
   if (!needed) return;
   {
@@ -289,7 +295,12 @@ int kernels_per_step(const cbm_ctx* c) {
   const cbm_config& k = c->cfg;
   int n = 0;
   if (k.medium && k.chemotaxis != 0) n += 1;
-  if (k.walls == CBM_WALLS_REFLECT || (k.medium && k.secretion != 0) || k.fate != CBM_FATE_NONE) n += 1;
+  const bool gather = k.medium && k.secretion != 0 && k.medium_sampling == CBM_MEDIUM_BILINEAR &&
+                      k.neighbors == CBM_NEIGH_CELL_LINKED;
+  if (gather) n += 1;
+  if (k.walls == CBM_WALLS_REFLECT || (k.medium && k.secretion != 0 && !gather) ||
+      k.fate != CBM_FATE_NONE)
+    n += 1;
   if (k.fate != CBM_FATE_NONE) n += 2;  // fate scan, compaction
   n += 1;                               // agent DE
   if (k.medium) n += 1;

@@ -317,6 +317,94 @@ __global__ void __launch_bounds__(kTile) k_medium_grad(Params<T> P) {
 }
 
 // ---------------------------------------------------------------------------
+// Bilinear secretion as a gather over medium nodes.  Atomic adds of unequal
+// amounts would sum in an arbitrary order; here every node adds the
+// contributions of the agents whose stencil covers it in ascending agent
+// index, the order of the reference's serial agent loop.  The agents are
+// found through the cell grid, which holds exactly the committed positions
+// the rule reads when the grid is rebuilt every step (CellLinked).
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ bool secretion_by_gather(const Params<T>& P) {
+  return P.medium_sampling == CBM_MEDIUM_BILINEAR && P.neighbors == CBM_NEIGH_CELL_LINKED;
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
+  constexpr int kMaxCells = D == 1 ? 4 : (D == 2 ? 16 : 64);
+  const int n = blockIdx.x * kTile + threadIdx.x;
+  if (n >= P.n_nodes) return;
+  int q[3] = {0, 0, 0};
+  q[0] = n % P.n_medium[0];
+  if (D > 1) q[1] = (n / P.n_medium[0]) % P.n_medium[1];
+  if (D > 2) q[2] = n / (P.n_medium[0] * P.n_medium[1]);
+  // agents touching node q along an axis lie in x in [lo+(q-1/2)dx, lo+(q+3/2)dx)
+  // (unbounded below for q = 0, above for the last node); widen by one cell
+  int c0[3] = {0, 0, 0}, c1[3] = {0, 0, 0};
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const int nc = P.n_cells_d[d];
+    int a = q[d] == 0 ? 0
+                      : cell_pos1<T>(P.edge, P.box_lo[d] + ((T)q[d] - (T)0.5) * P.dx_m[d],
+                                     P.box_lo[d], P.box_hi[d], nc) - 1;
+    int b = q[d] == P.n_medium[d] - 1
+                ? nc - 1
+                : cell_pos1<T>(P.edge, P.box_lo[d] + ((T)q[d] + (T)1.5) * P.dx_m[d],
+                               P.box_lo[d], P.box_hi[d], nc) + 1;
+    c0[d] = a < 0 ? 0 : a;
+    c1[d] = b > nc - 1 ? nc - 1 : b;
+  }
+  int cur[kMaxCells], end[kMaxCells];
+  int ncand = 0;
+  bool all = true;
+  for (int cz = c0[2]; cz <= c1[2]; ++cz)
+    for (int cy = c0[1]; cy <= c1[1]; ++cy)
+      for (int cx = c0[0]; cx <= c1[0]; ++cx) {
+        if (ncand == kMaxCells) { all = false; continue; }
+        int c = cx + P.n_cells_d[0] * (cy + P.n_cells_d[1] * cz);
+        int s0 = P.cell_start[c], s1 = P.cell_start[c + 1];
+        if (s0 < s1) { cur[ncand] = s0; end[ncand] = s1; ++ncand; }
+      }
+  const T amt = P.secretion_amt;
+  T acc = P.c_cur[n];
+  if (all) {
+    while (true) {  // k-way merge: next smallest agent index among the cells
+      int best = -1, bj = 0x7fffffff;
+      for (int k = 0; k < ncand; ++k)
+        if (cur[k] < end[k]) {
+          int j = P.cell_agents[cur[k]];
+          if (j < bj) { bj = j; best = k; }
+        }
+      if (best < 0) break;
+      ++cur[best];
+      T x[3];
+      load_pos<T, D>(P.pos_cur, bj, x);
+      int nodes[8];
+      T w[8];
+      bilinear<T, D>(P, x, nodes, w);
+#pragma unroll
+      for (int k = 0; k < (1 << D); ++k)
+        if (nodes[k] == n) acc = acc + w[k] * amt;
+    }
+  } else {
+    // the cell box is too large (cells much smaller than the medium spacing):
+    // visit every agent in index order
+    const int N = (int)P.ctr->N[P.parity];
+    for (int j = 0; j < N; ++j) {
+      T x[3];
+      load_pos<T, D>(P.pos_cur, j, x);
+      int nodes[8];
+      T w[8];
+      bilinear<T, D>(P, x, nodes, w);
+#pragma unroll
+      for (int k = 0; k < (1 << D); ++k)
+        if (nodes[k] == n) acc = acc + w[k] * amt;
+    }
+  }
+  P.c_cur[n] = acc;
+}
+
+// ---------------------------------------------------------------------------
 // agentStepRule!: walls, secretion, fate decision + per-tile event counts
 // (src/AgentStructure/functionRule.jl:9-111)
 // ---------------------------------------------------------------------------
@@ -339,7 +427,7 @@ __global__ void __launch_bounds__(kTile) k_agent_rule(Params<T> P) {
         P.pos_u[d][i] = y;
       }
     }
-    if (P.medium && P.secretion_amt != (T)0) {
+    if (P.medium && P.secretion_amt != (T)0 && !secretion_by_gather(P)) {
       if (P.medium_sampling == CBM_MEDIUM_NEAREST) {
         atomicAdd(P.c_cur + nearest_node<T, D>(P, x), P.secretion_amt);
       } else {

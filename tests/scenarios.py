@@ -22,13 +22,21 @@ def aggregation_2d(abi, N=4096, L=100.0, seed=1, precision=None, steps_hint=1000
     return kw, state
 
 
-def colony_3d(abi, N=10000, R=20.0, L=400.0, n_max=None, seed=2, precision=None,
+def ball_radius(N, density=0.15):
+    """Radius of a ball holding N agents at `density` agents per unit volume
+    (0.15 is the packing density of spheres of radius 1)."""
+    return (3 * N / (4 * np.pi * density)) ** (1 / 3)
+
+
+def colony_3d(abi, N=10000, R=None, L=400.0, n_max=None, seed=2, precision=None,
               neighbors=None, p_death=1e-4, sigma=0.05):
-    """3D colony: N agents uniform in a radius-R ball centred in [0,L]^3,
+    """3D colony: N agents uniform in a radius-R ball centred in [0,L]^3 (R from
+    the packing density 0.15 when not given),
     v ~ U(1,2), g ~ U(0.8,1.2), EM sigma, divide at v >= 2 into daughters at
     +-0.5 r, death probability p_death, CLVD with R_list 3.3 and rebuild at 0.15,
     dt = 0.005."""
     rng = np.random.default_rng(seed)
+    R = ball_radius(N) if R is None else R
     u = rng.normal(size=(N, 3))
     u /= np.linalg.norm(u, axis=1, keepdims=True)
     rad = R * rng.uniform(size=N) ** (1 / 3)
@@ -49,7 +57,7 @@ def packed_colony_3d(abi, N=1_000_000, density=0.15, L=400.0, seed=2, n_max=None
     """A grown colony snapshot: N agents at the packed density (agents per unit
     volume) in a ball centred in [0,L]^3, ages spread so that divisions occur
     every step (v ~ U(1,2))."""
-    R = (3 * N / (4 * np.pi * density)) ** (1 / 3)
+    R = ball_radius(N, density)
     kw, state = colony_3d(abi, N=N, R=R, L=L, n_max=n_max or int(1.2 * N), seed=seed,
                           precision=precision, p_death=p_death)
     return kw, state

@@ -1,0 +1,47 @@
+"""The C ABI library loads without a GPU and exports every declared function."""
+import ctypes as C
+import os
+import re
+
+import conftest
+
+ROOT = conftest.ROOT
+
+
+def declared_functions():
+    names = []
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if not h.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", h)).read()
+        if 'extern "C"' not in text:
+            continue  # C++-only headers (cbm_rng.h) declare inline functions, not exports
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(cbm_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_the_boundary():
+    names = declared_functions()
+    for core in ("cbm_create", "cbm_upload", "cbm_step", "cbm_download", "cbm_destroy",
+                 "cbm_get_neighbors", "cbm_get_grid", "cbm_last_error"):
+        assert core in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.CDLL(conftest.cbm._abi.LIB_PATH)  # no CUDA call is made
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    lib.cbm_version.restype = C.c_char_p
+    assert lib.cbm_version().startswith(b"cbm_b200")
+
+
+def test_create_without_device_fails_loudly():
+    """On a machine without a CUDA device cbm_create returns an error (no CPU fallback)."""
+    import pytest
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    abi = conftest.cbm._abi
+    with pytest.raises(abi.CbmError):
+        conftest.cbm.Context(abi.make_config(dims=2, n_max=4, box_hi=(1, 1), dt=0.1))
