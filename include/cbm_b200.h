@@ -231,6 +231,42 @@ int cbm_kernels_per_step(cbm_ctx* ctx);
 int cbm_profile_step(cbm_ctx* ctx, int32_t max_kernels, float* ms, const char** names,
                      int32_t* n_kernels);
 
+/* ---- allocation-free cell grid -------------------------------------------
+ * This entry point has no counterpart in the reference.  It is for callers
+ * that cannot allocate device memory when they need a grid: code running
+ * while a framework captures the stream into a CUDA graph (cudaMalloc is
+ * refused in a capturing thread), hosts whose device memory belongs to a pool
+ * allocator that must account for every byte (such as a Julia process whose
+ * CUDA.jl pool owns the GPU), and real-time loops that cannot wait for
+ * cudaMalloc/cudaFree.
+ *
+ * It builds the same CellLinked grid as cbm_upload/cbm_compute_neighbors
+ * (cellPos + counting sort, ascending agent index within a cell,
+ * src/neighbors.jl:636-638,918-979) for n_agents positions x, y, z (device
+ * arrays of the given precision; y/z may be NULL below 2/3 dims) and writes,
+ * 0-based, agent_cell[n_agents], cell_start[prod(nCells) + 1] (the last entry
+ * is n_agents) and cell_agents[n_agents], all caller-allocated device arrays.
+ * Work is enqueued on `stream` (a cudaStream_t, NULL for the legacy default
+ * stream); the call returns before it finishes.
+ *
+ * Scratch memory is a static device array inside the library (about 8.4 MB,
+ * held by every GPU that loads the library until the process exits), so
+ * n_agents <= CBM_NOALLOC_MAX_AGENTS and prod(nCells) <= CBM_NOALLOC_MAX_CELLS;
+ * larger requests return CBM_ERR_ARG.  All calls share that array and it keeps
+ * the last call's contents: calls that overlap on the GPU (on different
+ * streams, or from different host threads without ordering) race and corrupt
+ * each other's results.  The first call on a device looks up the array's
+ * device address (once per device, with that device current); make that first
+ * call before any stream capture begins.  Errors are described by
+ * cbm_noalloc_last_error(). */
+#define CBM_NOALLOC_MAX_AGENTS 524288
+#define CBM_NOALLOC_MAX_CELLS 1048576
+int cbm_cell_grid_noalloc(const void* x, const void* y, const void* z, int32_t n_agents,
+                          int32_t dims, int32_t precision, const double* box_lo,
+                          const double* box_hi, double cell_edge, int32_t* agent_cell,
+                          int32_t* cell_start, int32_t* cell_agents, void* stream);
+const char* cbm_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
