@@ -1,12 +1,13 @@
 // cbm_api.cu — host side of the C ABI declared in include/cbm_b200.h.
 //
 // A context owns every device buffer of one Community (capacity n_max) and
-// one CUDA stream.  Agent state that a step both reads and writes is held in
-// two copies selected by step parity (committed "x" and written "x__" of the
-// reference, swapped by update! instead of copied, update.jl:126-158); a full
-// step of each parity is captured once as a CUDA graph and replayed.
+// one CUDA stream.  Its committed agent state lives in cell-sorted slots (set
+// A) and each step writes set B (see cbm_kernels.cuh); a full step of each
+// counter parity is captured once as a CUDA graph and replayed.
 #include <cuda_runtime.h>
 
+#include <cmath>
+#include <cstddef>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -26,27 +27,41 @@ struct cbm_ctx {
   std::string err;
   std::vector<void*> allocs;
 
-  // device buffers (typed views are built in params<T>())
-  void* pos[2][3] = {};
-  void* pos_u[3] = {};
-  void* v[2] = {};
-  void* f[2][3] = {};
-  void* g = nullptr;
-  long long* id = nullptr;
-  long long* parent = nullptr;
+  // slot-ordered state
+  void* PA = nullptr;
+  void* PB = nullptr;
+  void* VA = nullptr;
+  void* VB = nullptr;
+  void* FA = nullptr;
+  void* FB = nullptr;
+  int* IA = nullptr;
+  int* IB = nullptr;
+  void* U = nullptr;
+  void* POLD = nullptr;
+  int* inv = nullptr;
+  int* cell_of_slot = nullptr;
+  // index-ordered constants and staging
+  void* G = nullptr;
+  long long* ID = nullptr;
+  long long* PAR = nullptr;
+  void* hx[3] = {};
+  void* hv = nullptr;
+  void* hf[3] = {};
+  // fate
   unsigned char* fate = nullptr;
   int* holes = nullptr;
   int* blk[4] = {};
-  int* agent_cell = nullptr;
-  int* agent_rank = nullptr;
+  // sort and grid
+  int* s_cell = nullptr;
+  int* s_rank = nullptr;
+  int* s_key = nullptr;
   int* cell_count = nullptr;
   int* cell_start = nullptr;
-  int* cell_tmp = nullptr;
-  int* cell_agents = nullptr;
   unsigned long long* scan_state = nullptr;
+  // Verlet
   int* nbr_n = nullptr;
   int* nbr_list = nullptr;
-  void* pos_old[3] = {};
+  // medium
   void* c[2] = {};
   void* grad[2][3] = {};
   Counters* ctr = nullptr;
@@ -55,9 +70,10 @@ struct cbm_ctx {
   int n_blocks = 0;
   int n_cells = 1;
   int n_cells_d[3] = {1, 1, 1};
-  int n_scan_tiles = 0;
+  int n_scan_tiles = 1;
   int n_nodes = 0;
-  bool has_grid = false, has_list = false;
+  bool grid_exposed = false;  // CellLinked / CLVD: the reference has a cell grid
+  bool has_list = false;      // CLVD / VerletDisplacement
 
   // host-side bookkeeping
   bool loaded = false;
@@ -74,6 +90,8 @@ struct cbm_ctx {
   std::vector<Mark> marks;
   size_t mark_used = 0;
 };
+
+extern "C" int cbm_sync(cbm_ctx* c);
 
 namespace {
 
@@ -97,7 +115,12 @@ int fail(cbm_ctx* ctx, int code, const char* fmt, ...) {
       return fail(ctx, CBM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));      \
   } while (0)
 
-int grid_blocks(long long n) { return (int)((n + kTile - 1) / kTile); }
+int grid_blocks(long long n) { return n > 0 ? (int)((n + kTile - 1) / kTile) : 1; }
+
+// device address of the counter block's re-sort flag
+const int* resort_flag(const cbm_ctx* c) {
+  return (const int*)((const char*)c->ctr + offsetof(Counters, resort));
+}
 
 // Brackets one kernel launch with events when profiling an eager step.
 struct Prof {
@@ -121,39 +144,66 @@ struct Prof {
 };
 #define PROF(name) Prof prof_scope_(c, name)
 
+// r^2 (1 + 1e-5) rounded up to T: a squared distance at or above it has a
+// correctly rounded sqrt >= (T)r, so the exact `d < r` test can be skipped
+template <typename T>
+T bound2(double r) {
+  if (!(r > 0)) return (T)0;
+  double v = r * r * (1.0 + 1e-5);
+  T t = (T)v;
+  return (double)t < v ? std::nextafter(t, (T)INFINITY) : t;
+}
+
+// r^2 (1 - 1e-5) rounded down to T: a squared distance below it has a
+// correctly rounded sqrt < (T)r
+template <typename T>
+T bound2_lo(double r) {
+  if (!(r > 0)) return (T)0;
+  double v = r * r * (1.0 - 1e-5);
+  T t = (T)v;
+  return (double)t > v ? std::nextafter(t, (T)0) : t;
+}
+
 template <typename T>
 Params<T> params(const cbm_ctx* c, int parity) {
+  using V4 = typename V4T<T>::type;
   Params<T> P;
   memset(&P, 0, sizeof P);
   const cbm_config& k = c->cfg;
   const int p = parity, q = parity ^ 1;
+  P.PA = (V4*)c->PA;
+  P.PB = (V4*)c->PB;
+  P.VA = (T*)c->VA;
+  P.VB = (T*)c->VB;
+  P.FA = (V4*)c->FA;
+  P.FB = (V4*)c->FB;
+  P.IA = c->IA;
+  P.IB = c->IB;
+  P.U = (V4*)c->U;
+  P.POLD = (V4*)c->POLD;
+  P.inv = c->inv;
+  P.cell_of_slot = c->cell_of_slot;
+  P.G = (T*)c->G;
+  P.ID = c->ID;
+  P.PAR = c->PAR;
   for (int d = 0; d < 3; ++d) {
-    P.pos_cur[d] = (T*)c->pos[p][d];
-    P.pos_nxt[d] = (T*)c->pos[q][d];
-    P.pos_u[d] = c->pos_u[d] ? (T*)c->pos_u[d] : (T*)c->pos[p][d];
-    P.f_cur[d] = (T*)c->f[p][d];
-    P.f_nxt[d] = (T*)c->f[q][d];
-    P.pos_old[d] = (T*)c->pos_old[d];
+    P.hx[d] = (T*)c->hx[d];
+    P.hf[d] = (T*)c->hf[d];
     P.grad_cur[d] = (T*)c->grad[p][d];
     P.grad_nxt[d] = (T*)c->grad[q][d];
   }
-  P.v_cur = (T*)c->v[p];
-  P.v_nxt = (T*)c->v[q];
-  P.g = (T*)c->g;
-  P.id = c->id;
-  P.parent = c->parent;
+  P.hv = (T*)c->hv;
   P.fate = c->fate;
   P.holes = c->holes;
   P.blk_children = c->blk[0];
   P.blk_deaths = c->blk[1];
   P.blk_child_off = c->blk[2];
   P.blk_death_off = c->blk[3];
-  P.agent_cell = c->agent_cell;
-  P.agent_rank = c->agent_rank;
+  P.s_cell = c->s_cell;
+  P.s_rank = c->s_rank;
+  P.s_key = c->s_key;
   P.cell_count = c->cell_count;
   P.cell_start = c->cell_start;
-  P.cell_tmp = c->cell_tmp;
-  P.cell_agents = c->cell_agents;
   P.scan_state = c->scan_state;
   P.nbr_n = c->nbr_n;
   P.nbr_list = c->nbr_list;
@@ -186,7 +236,7 @@ Params<T> params(const cbm_ctx* c, int parity) {
   P.medium = k.medium;
   P.medium_sampling = k.medium_sampling;
   P.dt = (T)k.dt;
-  P.sqrt_dt = sqrt((T)k.dt);
+  P.sqrt_dt = std::sqrt((T)k.dt);
   P.sigma = (T)k.sigma;
   P.edge = (T)(k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT ? k.skin : k.cell_edge);
   P.skin = (T)k.skin;
@@ -195,6 +245,12 @@ Params<T> params(const cbm_ctx* c, int parity) {
   P.r_rep = (T)k.r_rep;
   P.k_att = (T)k.k_att;
   P.r_att = (T)k.r_att;
+  P.cut2 = bound2<T>(k.r_rep > k.r_att ? k.r_rep : k.r_att);
+  P.skin2 = bound2<T>(k.skin);
+  P.skin2_lo = bound2_lo<T>(k.skin);
+  P.force_in_list = (T)(k.r_rep > k.r_att ? k.r_rep : k.r_att) <= (T)k.skin ? 1 : 0;
+  P.cut_reach = (T)((k.r_rep > k.r_att ? k.r_rep : k.r_att) * (1.0 + 1e-4));
+  P.skin_reach = (T)(k.skin * (1.0 + 1e-4));
   P.wall_force = (T)k.wall_force;
   P.wall_range = (T)k.wall_range;
   P.drift_linear = (T)k.drift_linear;
@@ -210,6 +266,15 @@ Params<T> params(const cbm_ctx* c, int parity) {
   return P;
 }
 
+bool uses_gather(const cbm_config& k) {
+  return k.medium && k.secretion != 0 && k.medium_sampling == CBM_MEDIUM_BILINEAR &&
+         k.neighbors == CBM_NEIGH_CELL_LINKED;
+}
+bool rule_needed(const cbm_config& k) {
+  return k.walls == CBM_WALLS_REFLECT || (k.medium && k.secretion != 0 && !uses_gather(k)) ||
+         k.fate != CBM_FATE_NONE;
+}
+
 // ---- stage launches (enqueue only) -----------------------------------------
 template <typename T, int D>
 void enqueue_medium_rule(cbm_ctx* c, const Params<T>& P) {
@@ -222,22 +287,22 @@ void enqueue_medium_rule(cbm_ctx* c, const Params<T>& P) {
 template <typename T, int D>
 void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P) {
   const cbm_config& k = c->cfg;
-  const bool gather = k.medium && k.secretion != 0 && k.medium_sampling == CBM_MEDIUM_BILINEAR &&
-                      k.neighbors == CBM_NEIGH_CELL_LINKED;
-  if (gather) {
+  if (uses_gather(k)) {
     PROF("k_secrete_gather");
     k_secrete_gather<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
   }
-  bool needed = k.walls == CBM_WALLS_REFLECT || (k.medium && k.secretion != 0 && !gather) ||
-                k.fate != CBM_FATE_NONE;
-  if (!needed) return;
+  if (!rule_needed(k)) return;
   {
     PROF("k_agent_rule");
     k_agent_rule<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
   }
   if (k.fate != CBM_FATE_NONE) {
-    PROF("k_fate_scan");
-    k_fate_scan<T><<<1, 1024, 0, c->stream>>>(P);
+    {
+      PROF("k_fate_scan");
+      k_fate_scan<T><<<1, 1024, 0, c->stream>>>(P);
+    }
+    PROF("k_births");
+    k_births<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
   }
 }
 
@@ -255,39 +320,44 @@ void enqueue_medium_de(cbm_ctx* c, const Params<T>& P) {
   }
 }
 
+// update!: compaction, commit, then B -> A (copy, or re-sort = grid rebuild)
 template <typename T, int D>
 void enqueue_update(cbm_ctx* c, const Params<T>& P) {
   if (c->cfg.fate != CBM_FATE_NONE) {
     PROF("k_compact");
-    k_compact<T, D><<<2 * 148, kTile, 0, c->stream>>>(P);
+    k_compact<T, D><<<1, kCompactThreads, 0, c->stream>>>(P);
   }
-  PROF("k_commit");
-  k_commit<T><<<1, 1, 0, c->stream>>>(P);
+  {
+    PROF("k_commit");
+    k_commit<T><<<1, 1, 0, c->stream>>>(P);
+  }
+  {
+    PROF("k_sort_hist");
+    k_sort_hist<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+  }
+  {
+    PROF("k_scan_cells");
+    ScanArgs A{c->cell_count, c->cell_start, c->scan_state, c->n_cells, c->n_scan_tiles, c->ctr,
+               resort_flag(c)};
+    k_scan_cells<<<c->n_scan_tiles, kTile, 0, c->stream>>>(A);
+  }
+  {
+    PROF("k_sort_scatter");
+    k_sort_scatter<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+  }
+  PROF("k_sort_place");
+  k_sort_place<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
 }
 
-// computeNeighbors! of the step whose parity is P.parity (reads parity ^ 1)
+// computeNeighbors! after update!: the grid was rebuilt by the re-sort; a
+// VerletDisplacement list is rebuilt eagerly (ascending agent order), a CLVD
+// list is walked from the grid by the next DE stage.  Q has the parity of the
+// step that starts.
 template <typename T, int D>
-void enqueue_neighbors(cbm_ctx* c, const Params<T>& P) {
-  if (!c->has_grid) return;
-  {
-    PROF("k_cells_hist");
-    k_cells_hist<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
-  }
-  {
-    PROF("k_cells_scan");
-    k_cells_scan<T><<<c->n_scan_tiles, kTile, 0, c->stream>>>(P);
-  }
-  {
-    PROF("k_cells_scatter");
-    k_cells_scatter<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
-  }
-  {
-    PROF("k_cells_stable");
-    k_cells_stable<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
-  }
-  if (c->has_list) {
+void enqueue_neighbors(cbm_ctx* c, const Params<T>& Q) {
+  if (c->cfg.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT) {
     PROF("k_verlet_list");
-    k_verlet_list<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+    k_verlet_list<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(Q, 1);
   }
 }
 
@@ -295,17 +365,13 @@ int kernels_per_step(const cbm_ctx* c) {
   const cbm_config& k = c->cfg;
   int n = 0;
   if (k.medium && k.chemotaxis != 0) n += 1;
-  const bool gather = k.medium && k.secretion != 0 && k.medium_sampling == CBM_MEDIUM_BILINEAR &&
-                      k.neighbors == CBM_NEIGH_CELL_LINKED;
-  if (gather) n += 1;
-  if (k.walls == CBM_WALLS_REFLECT || (k.medium && k.secretion != 0 && !gather) ||
-      k.fate != CBM_FATE_NONE)
-    n += 1;
-  if (k.fate != CBM_FATE_NONE) n += 2;  // fate scan, compaction
+  if (uses_gather(k)) n += 1;
+  if (rule_needed(k)) n += 1;
+  if (k.fate != CBM_FATE_NONE) n += 3;  // fate scan, births, compaction
   n += 1;                               // agent DE
   if (k.medium) n += 1;
-  n += 1;                               // commit
-  if (c->has_grid) n += 4 + (c->has_list ? 1 : 0);
+  n += 5;                               // commit, sort hist, scan, scatter, place
+  if (k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT) n += 1;
   return n;
 }
 
@@ -317,7 +383,7 @@ void enqueue_full_step(cbm_ctx* c, int parity) {
   enqueue_agent_de<T, D>(c, P);
   enqueue_medium_de<T, D>(c, P);
   enqueue_update<T, D>(c, P);
-  enqueue_neighbors<T, D>(c, P);
+  enqueue_neighbors<T, D>(c, params<T>(c, parity ^ 1));
 }
 
 // dispatch on (precision, dims)
@@ -364,15 +430,9 @@ struct StageMediumDE {
 };
 template <typename T, int D>
 struct StageUpdate {
-  static void run(cbm_ctx* c, int copy_agents, int copy_c, int copy_grad, int births) {
+  static void run(cbm_ctx* c, int copy_agents, int use_u, int copy_c, int copy_grad) {
     Params<T> P = params<T>(c, c->parity);
-    if (births) {
-      // the rule's births are written by the DE kernel's placement phase
-      Params<T> B = P;
-      B.births_only = 1;
-      k_agent_de<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(B);
-    }
-    if (copy_agents) k_copy_agents<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+    if (copy_agents) k_copy_ab<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P, use_u);
     if (c->cfg.medium && (copy_c || copy_grad))
       k_copy_medium<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P, copy_c ? 0 : 1);
     enqueue_update<T, D>(c, P);
@@ -380,13 +440,46 @@ struct StageUpdate {
 };
 template <typename T, int D>
 struct StageNeighbors {
-  static void run(cbm_ctx* c) { enqueue_neighbors<T, D>(c, params<T>(c, c->parity ^ 1)); }
+  static void run(cbm_ctx* c) { enqueue_neighbors<T, D>(c, params<T>(c, c->parity)); }
+};
+template <typename T, int D>
+struct BuildList {  // the list of the current slots, on request
+  static void run(cbm_ctx* c) {
+    k_verlet_list<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(params<T>(c, c->parity), 0);
+  }
 };
 template <typename T, int D>
 struct CountNeighbors {
   static void run(cbm_ctx* c, double radius, int* out) {
     k_count_neighbors<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(params<T>(c, c->parity),
                                                                   (T)radius, out);
+  }
+};
+template <typename T, int D>
+struct Pack {
+  static void run(cbm_ctx* c, int N) {
+    k_pack_upload<T, D><<<grid_blocks(N), kTile, 0, c->stream>>>(params<T>(c, c->parity), N);
+  }
+};
+template <typename T, int D>
+struct Gather {
+  static void run(cbm_ctx* c, int N, int which) {
+    k_gather_download<T, D><<<grid_blocks(N), kTile, 0, c->stream>>>(params<T>(c, c->parity), N,
+                                                                      which);
+  }
+};
+template <typename T, int D>
+struct FirstSort {  // the re-sort half of update!, for loadToPlatform!
+  static void run(cbm_ctx* c) {
+    Params<T> P = params<T>(c, c->parity);
+    k_sort_hist<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+    ScanArgs A{c->cell_count, c->cell_start, c->scan_state, c->n_cells, c->n_scan_tiles, c->ctr,
+               resort_flag(c)};
+    k_scan_cells<<<c->n_scan_tiles, kTile, 0, c->stream>>>(A);
+    k_sort_scatter<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+    k_sort_place<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+    if (c->cfg.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT)
+      k_verlet_list<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P, 0);
   }
 };
 
@@ -439,6 +532,20 @@ void reset_stage_flags(cbm_ctx* c) {
   c->rule_done = c->de_done = c->mrule_done = c->mde_done = false;
 }
 
+// CLVD builds its list lazily; inspection calls build it when missing
+int ensure_list(cbm_ctx* c) {
+  Counters hc;
+  int rc = read_counters(c, &hc);
+  if (rc) return rc;
+  if (!hc.list_valid) {
+    dispatch<BuildList>(c);
+    rc = check_launch(c);
+    if (rc) return rc;
+    return cbm_sync(c);  // reports a row that exceeded n_max_neighbors
+  }
+  return CBM_OK;
+}
+
 }  // namespace
 
 // ============================================================================
@@ -446,7 +553,7 @@ void reset_stage_flags(cbm_ctx* c) {
 // ============================================================================
 extern "C" {
 
-const char* cbm_version(void) { return "cbm_b200 0.1.0 (sm_100a)"; }
+const char* cbm_version(void) { return "cbm_b200 0.2.0 (sm_100a)"; }
 
 const char* cbm_last_error(const cbm_ctx* ctx) {
   return ctx ? ctx->err.c_str() : g_create_error.c_str();
@@ -468,18 +575,16 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     return fail(nullptr, CBM_ERR_ARG, "unknown integrator %d", k.integrator);
   for (int d = 0; d < k.dims; ++d)
     if (!(k.box_hi[d] > k.box_lo[d])) return fail(nullptr, CBM_ERR_ARG, "empty simBox on axis %d", d);
-  const bool grid = k.neighbors == CBM_NEIGH_CELL_LINKED || k.neighbors == CBM_NEIGH_CLVD ||
-                    k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT;
+  const bool cells = k.neighbors == CBM_NEIGH_CELL_LINKED || k.neighbors == CBM_NEIGH_CLVD;
   const bool list = k.neighbors == CBM_NEIGH_CLVD || k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT;
-  if ((k.neighbors == CBM_NEIGH_CELL_LINKED || k.neighbors == CBM_NEIGH_CLVD) && !(k.cell_edge > 0))
-    return fail(nullptr, CBM_ERR_ARG, "cell_edge must be positive");
+  if (cells && !(k.cell_edge > 0)) return fail(nullptr, CBM_ERR_ARG, "cell_edge must be positive");
   if (list && !(k.skin > 0)) return fail(nullptr, CBM_ERR_ARG, "skin must be positive");
+  if (k.neighbors == CBM_NEIGH_CLVD && k.cell_edge < k.skin)
+    return fail(nullptr, CBM_ERR_ARG, "CLVD needs cell_edge >= skin");
   if (list && (k.n_max_neighbors < 1 ||
                (k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT && k.n_max_neighbors > kVdSortMax)))
     return fail(nullptr, CBM_ERR_ARG, "n_max_neighbors must be in [1, %d]",
                 k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT ? kVdSortMax : (1 << 20));
-  if (k.fate == CBM_FATE_VOLUME && !k.growth && !(k.p_death > 0) )
-    ;  // a volume rule without growth only kills
   if (k.medium) {
     for (int d = 0; d < k.dims; ++d)
       if (k.n_medium[d] < 1) return fail(nullptr, CBM_ERR_ARG, "n_medium[%d] must be >= 1", d);
@@ -495,16 +600,17 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     return rc;
   }
   const size_t n = (size_t)(k.n_max > 0 ? k.n_max : 1);
-  const size_t S = c->tsize;
+  const size_t S = c->tsize, S4 = 4 * c->tsize;
   c->n_blocks = grid_blocks((long long)n);
-  c->has_grid = grid;
+  c->grid_exposed = cells;
   c->has_list = list;
-  if (grid) {
+  // slots are sorted by cell for every algorithm; without a grid there is one cell
+  if (cells || k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT) {
     double e = k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT ? k.skin : k.cell_edge;
     long long nc = 1;
     for (int d = 0; d < k.dims; ++d) {
       // nCells_ = ceil((hi - lo) / edge + 2), neighbors.jl:605 (Float64 on the host)
-      double v = ceil((k.box_hi[d] - k.box_lo[d]) / e + 2.0);
+      double v = std::ceil((k.box_hi[d] - k.box_lo[d]) / e + 2.0);
       if (!(v >= 1 && v < 2.0e9)) {
         int rc = fail(nullptr, CBM_ERR_ARG, "cell grid too large on axis %d", d);
         free_all(c);
@@ -521,8 +627,8 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
       return rc;
     }
     c->n_cells = (int)nc;
-    c->n_scan_tiles = (c->n_cells + kScanTile - 1) / kScanTile;
   }
+  c->n_scan_tiles = (c->n_cells + kScanTile - 1) / kScanTile;
   if (k.medium) {
     long long nn = 1;
     for (int d = 0; d < k.dims; ++d) nn *= k.n_medium[d];
@@ -536,35 +642,39 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
   }
 
   bool ok = true;
-  for (int q = 0; q < 2; ++q) {
-    for (int d = 0; d < 3; ++d) {
-      c->pos[q][d] = dalloc(c, n * S, &ok);
-      c->f[q][d] = dalloc(c, n * S, &ok);
-    }
-    c->v[q] = dalloc(c, n * S, &ok);
+  c->PA = dalloc(c, n * S4, &ok);
+  c->PB = dalloc(c, n * S4, &ok);
+  c->VA = dalloc(c, n * S, &ok);
+  c->VB = dalloc(c, n * S, &ok);
+  c->FA = dalloc(c, n * S4, &ok);
+  c->FB = dalloc(c, n * S4, &ok);
+  c->IA = (int*)dalloc(c, n * 4, &ok);
+  c->IB = (int*)dalloc(c, n * 4, &ok);
+  if (k.walls == CBM_WALLS_REFLECT) c->U = dalloc(c, n * S4, &ok);
+  if (list) c->POLD = dalloc(c, n * S4, &ok);
+  c->inv = (int*)dalloc(c, n * 4, &ok);
+  c->cell_of_slot = (int*)dalloc(c, n * 4, &ok);
+  c->G = dalloc(c, n * S, &ok);
+  c->ID = (long long*)dalloc(c, n * 8, &ok);
+  c->PAR = (long long*)dalloc(c, n * 8, &ok);
+  for (int d = 0; d < 3; ++d) {
+    c->hx[d] = dalloc(c, n * S, &ok);
+    c->hf[d] = dalloc(c, n * S, &ok);
   }
-  if (k.walls == CBM_WALLS_REFLECT)
-    for (int d = 0; d < 3; ++d) c->pos_u[d] = dalloc(c, n * S, &ok);
-  c->g = dalloc(c, n * S, &ok);
-  c->id = (long long*)dalloc(c, n * 8, &ok);
-  c->parent = (long long*)dalloc(c, n * 8, &ok);
+  c->hv = dalloc(c, n * S, &ok);
   c->fate = (unsigned char*)dalloc(c, n, &ok);
   c->holes = (int*)dalloc(c, n * 4, &ok);
   for (int q = 0; q < 4; ++q) c->blk[q] = (int*)dalloc(c, (size_t)c->n_blocks * 4, &ok);
+  c->s_cell = (int*)dalloc(c, n * 4, &ok);
+  c->s_rank = (int*)dalloc(c, n * 4, &ok);
+  c->s_key = (int*)dalloc(c, n * 4, &ok);
+  c->cell_count = (int*)dalloc(c, (size_t)c->n_cells * 4, &ok);
+  c->cell_start = (int*)dalloc(c, ((size_t)c->n_cells + 1) * 4, &ok);
+  c->scan_state = (unsigned long long*)dalloc(c, (size_t)c->n_scan_tiles * 8, &ok);
   c->scratch_int = (int*)dalloc(c, n * 4, &ok);
-  if (grid) {
-    c->agent_cell = (int*)dalloc(c, n * 4, &ok);
-    c->agent_rank = (int*)dalloc(c, n * 4, &ok);
-    c->cell_count = (int*)dalloc(c, (size_t)c->n_cells * 4, &ok);
-    c->cell_start = (int*)dalloc(c, ((size_t)c->n_cells + 1) * 4, &ok);
-    c->cell_tmp = (int*)dalloc(c, n * 4, &ok);
-    c->cell_agents = (int*)dalloc(c, n * 4, &ok);
-    c->scan_state = (unsigned long long*)dalloc(c, (size_t)c->n_scan_tiles * 8, &ok);
-  }
   if (list) {
     c->nbr_n = (int*)dalloc(c, n * 4, &ok);
     c->nbr_list = (int*)dalloc(c, n * (size_t)k.n_max_neighbors * 4, &ok);
-    for (int d = 0; d < 3; ++d) c->pos_old[d] = dalloc(c, n * S, &ok);
   }
   if (k.medium) {
     for (int q = 0; q < 2; ++q) {
@@ -579,11 +689,8 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     delete c;
     return rc;
   }
-  for (void* p : c->allocs) cudaMemsetAsync(p, 0, 0, c->stream);
-  if (grid) {
-    cudaMemsetAsync(c->cell_count, 0, (size_t)c->n_cells * 4, c->stream);
-    cudaMemsetAsync(c->scan_state, 0, (size_t)c->n_scan_tiles * 8, c->stream);
-  }
+  cudaMemsetAsync(c->cell_count, 0, (size_t)c->n_cells * 4, c->stream);
+  cudaMemsetAsync(c->scan_state, 0, (size_t)c->n_scan_tiles * 8, c->stream);
   cudaMemsetAsync(c->ctr, 0, sizeof(Counters), c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
     int rc = fail(nullptr, CBM_ERR_CUDA, "device initialisation failed");
@@ -609,70 +716,61 @@ int cbm_upload(cbm_ctx* c, const cbm_state_view* h) {
   const cbm_config& k = c->cfg;
   if (h->N < 0 || h->N > k.n_max)
     return fail(c, CBM_ERR_ARG, "N=%lld exceeds n_max=%lld", (long long)h->N, (long long)k.n_max);
-  const size_t N = (size_t)h->N, S = c->tsize;
+  const size_t N = (size_t)h->N, S = c->tsize, nm = (size_t)k.n_max;
   for (int d = 0; d < k.dims; ++d)
     if (N && !h->pos[d]) return fail(c, CBM_ERR_ARG, "pos[%d] is NULL", d);
   if (k.growth && N && (!h->v || !h->g)) return fail(c, CBM_ERR_ARG, "growth needs v and g");
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  // every buffer starts as zeros past N (loadToPlatform! pads with zeros)
-  for (int q = 0; q < 2; ++q) {
-    for (int d = 0; d < 3; ++d) {
-      CUDA_TRY(c, cudaMemset(c->pos[q][d], 0, (size_t)k.n_max * S));
-      CUDA_TRY(c, cudaMemset(c->f[q][d], 0, (size_t)k.n_max * S));
-    }
-    CUDA_TRY(c, cudaMemset(c->v[q], 0, (size_t)k.n_max * S));
+  cudaStream_t st = c->stream;
+  // staging: index order; absent fields are zeros (loadToPlatform! pads with zeros)
+  for (int d = 0; d < 3; ++d) {
+    CUDA_TRY(c, cudaMemsetAsync(c->hx[d], 0, nm * S, st));
+    CUDA_TRY(c, cudaMemsetAsync(c->hf[d], 0, nm * S, st));
+    if (d < k.dims && N) CUDA_TRY(c, cudaMemcpyAsync(c->hx[d], h->pos[d], N * S, cudaMemcpyHostToDevice, st));
+    if (d < k.dims && N && h->f[d])
+      CUDA_TRY(c, cudaMemcpyAsync(c->hf[d], h->f[d], N * S, cudaMemcpyHostToDevice, st));
   }
-  CUDA_TRY(c, cudaMemset(c->g, 0, (size_t)k.n_max * S));
-  CUDA_TRY(c, cudaMemset(c->parent, 0, (size_t)k.n_max * 8));
-  for (int q = 0; q < 2; ++q) {
-    for (int d = 0; d < k.dims; ++d) {
-      if (N) CUDA_TRY(c, cudaMemcpy(c->pos[q][d], h->pos[d], N * S, cudaMemcpyHostToDevice));
-      if (N && h->f[d]) CUDA_TRY(c, cudaMemcpy(c->f[q][d], h->f[d], N * S, cudaMemcpyHostToDevice));
-    }
-    if (N && h->v) CUDA_TRY(c, cudaMemcpy(c->v[q], h->v, N * S, cudaMemcpyHostToDevice));
-  }
-  if (N && h->g) CUDA_TRY(c, cudaMemcpy(c->g, h->g, N * S, cudaMemcpyHostToDevice));
-  {
-    std::vector<long long> ids((size_t)k.n_max > 0 ? (size_t)k.n_max : 1, 0);
-    for (size_t i = 0; i < N; ++i) ids[i] = h->id ? h->id[i] : (long long)i + 1;
-    CUDA_TRY(c, cudaMemcpy(c->id, ids.data(), (size_t)k.n_max * 8, cudaMemcpyHostToDevice));
-    if (N && h->parent) CUDA_TRY(c, cudaMemcpy(c->parent, h->parent, N * 8, cudaMemcpyHostToDevice));
-  }
+  CUDA_TRY(c, cudaMemsetAsync(c->hv, 0, nm * S, st));
+  if (N && h->v) CUDA_TRY(c, cudaMemcpyAsync(c->hv, h->v, N * S, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(c, cudaMemsetAsync(c->G, 0, nm * S, st));
+  if (N && h->g) CUDA_TRY(c, cudaMemcpyAsync(c->G, h->g, N * S, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(c, cudaMemsetAsync(c->PAR, 0, nm * 8, st));
+  if (N && h->parent)
+    CUDA_TRY(c, cudaMemcpyAsync(c->PAR, h->parent, N * 8, cudaMemcpyHostToDevice, st));
+  std::vector<long long> ids(nm > 0 ? nm : 1, 0);
+  for (size_t i = 0; i < N; ++i) ids[i] = h->id ? h->id[i] : (long long)i + 1;
+  CUDA_TRY(c, cudaMemcpyAsync(c->ID, ids.data(), nm * 8, cudaMemcpyHostToDevice, st));
   if (k.medium) {
     const size_t nb = (size_t)c->n_nodes * S;
     for (int q = 0; q < 2; ++q) {
-      if (h->medium_c) CUDA_TRY(c, cudaMemcpy(c->c[q], h->medium_c, nb, cudaMemcpyHostToDevice));
-      else CUDA_TRY(c, cudaMemset(c->c[q], 0, nb));
+      if (h->medium_c) CUDA_TRY(c, cudaMemcpyAsync(c->c[q], h->medium_c, nb, cudaMemcpyHostToDevice, st));
+      else CUDA_TRY(c, cudaMemsetAsync(c->c[q], 0, nb, st));
       for (int d = 0; d < 3; ++d) {
         if (d < k.dims && h->medium_grad[d])
-          CUDA_TRY(c, cudaMemcpy(c->grad[q][d], h->medium_grad[d], nb, cudaMemcpyHostToDevice));
-        else CUDA_TRY(c, cudaMemset(c->grad[q][d], 0, nb));
+          CUDA_TRY(c, cudaMemcpyAsync(c->grad[q][d], h->medium_grad[d], nb, cudaMemcpyHostToDevice, st));
+        else CUDA_TRY(c, cudaMemsetAsync(c->grad[q][d], 0, nb, st));
       }
     }
   }
-  if (c->has_grid) CUDA_TRY(c, cudaMemset(c->cell_count, 0, (size_t)c->n_cells * 4));
+  CUDA_TRY(c, cudaMemsetAsync(c->cell_count, 0, (size_t)c->n_cells * 4, st));
+  Counters old;
+  CUDA_TRY(c, cudaMemcpyAsync(&old, c->ctr, sizeof old, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(c, cudaStreamSynchronize(st));
   Counters hc;
   memset(&hc, 0, sizeof hc);
   hc.N[0] = hc.N[1] = h->N;
   hc.step[0] = hc.step[1] = h->step;
   hc.t[0] = hc.t[1] = h->t;
   hc.id_max = h->id_max > 0 ? h->id_max : h->N;
-  hc.flag[0] = 0;
-  hc.flag[1] = 1;  // flagRecomputeNeighbors_ = [1] (communityStructure.jl:480)
-  hc.scan_epoch = 1;
-  // keep the epoch monotonic across uploads so stale scan states never match
-  {
-    Counters old;
-    if (cudaMemcpy(&old, c->ctr, sizeof old, cudaMemcpyDeviceToHost) == cudaSuccess)
-      hc.scan_epoch = old.scan_epoch + 1;
-  }
-  CUDA_TRY(c, cudaMemcpy(c->ctr, &hc, sizeof hc, cudaMemcpyHostToDevice));
+  hc.slots = h->N;
+  hc.resort = 1;  // flagRecomputeNeighbors_ = [1] and computeNeighbors! at load (communityStructure.jl:480,648)
+  hc.scan_epoch = old.scan_epoch + 1;  // keep the epoch monotonic so stale tile states never match
+  CUDA_TRY(c, cudaMemcpyAsync(c->ctr, &hc, sizeof hc, cudaMemcpyHostToDevice, st));
   c->parity = 0;
   reset_stage_flags(c);
   c->loaded = true;
-  // computeNeighbors! at load (communityStructure.jl:648): end-of-step
-  // convention with parity 1 reads buffers/N of parity 0 and flag[1]
-  dispatch<StageNeighbors>(c);  // uses c->parity ^ 1 = 1
+  dispatch<Pack>(c, (int)N);
+  dispatch<FirstSort>(c);
   int rc = check_launch(c);
   if (rc) return rc;
   return cbm_sync(c);
@@ -696,17 +794,21 @@ int cbm_download(cbm_ctx* c, cbm_state_view* h, int32_t which) {
   h->id_max = hc.id_max;
   const size_t S = c->tsize, nb = (size_t)N * S;
   const bool nw = which == CBM_VIEW_NEW;
-  const int qa = nw && c->de_done ? p ^ 1 : p;
-  for (int d = 0; d < k.dims; ++d) {
-    const void* src = c->pos[qa][d];
-    if (nw && !c->de_done && c->rule_done && c->pos_u[d]) src = c->pos_u[d];
-    if (h->pos[d] && N) CUDA_TRY(c, cudaMemcpy(h->pos[d], src, nb, cudaMemcpyDeviceToHost));
-    if (h->f[d] && N) CUDA_TRY(c, cudaMemcpy(h->f[d], c->f[qa][d], nb, cudaMemcpyDeviceToHost));
+  const int src = nw && c->de_done ? 1 : (nw && c->rule_done && c->U ? 2 : 0);
+  if (N) {
+    dispatch<Gather>(c, (int)N, src);
+    rc = check_launch(c);
+    if (rc) return rc;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   }
-  if (h->v && N) CUDA_TRY(c, cudaMemcpy(h->v, c->v[qa], nb, cudaMemcpyDeviceToHost));
-  if (h->g && N) CUDA_TRY(c, cudaMemcpy(h->g, c->g, nb, cudaMemcpyDeviceToHost));
-  if (h->id && N) CUDA_TRY(c, cudaMemcpy(h->id, c->id, (size_t)N * 8, cudaMemcpyDeviceToHost));
-  if (h->parent && N) CUDA_TRY(c, cudaMemcpy(h->parent, c->parent, (size_t)N * 8, cudaMemcpyDeviceToHost));
+  for (int d = 0; d < k.dims; ++d) {
+    if (h->pos[d] && N) CUDA_TRY(c, cudaMemcpy(h->pos[d], c->hx[d], nb, cudaMemcpyDeviceToHost));
+    if (h->f[d] && N) CUDA_TRY(c, cudaMemcpy(h->f[d], c->hf[d], nb, cudaMemcpyDeviceToHost));
+  }
+  if (h->v && N) CUDA_TRY(c, cudaMemcpy(h->v, c->hv, nb, cudaMemcpyDeviceToHost));
+  if (h->g && N) CUDA_TRY(c, cudaMemcpy(h->g, c->G, nb, cudaMemcpyDeviceToHost));
+  if (h->id && N) CUDA_TRY(c, cudaMemcpy(h->id, c->ID, (size_t)N * 8, cudaMemcpyDeviceToHost));
+  if (h->parent && N) CUDA_TRY(c, cudaMemcpy(h->parent, c->PAR, (size_t)N * 8, cudaMemcpyDeviceToHost));
   if (k.medium) {
     const size_t mb = (size_t)c->n_nodes * S;
     const int qc = nw && c->mde_done ? p ^ 1 : p;
@@ -734,16 +836,9 @@ int cbm_agent_step_de(cbm_ctx* c) {
   if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
   cudaSetDevice(c->device);
   const cbm_config& k = c->cfg;
-  if (!c->rule_done) {
-    if (k.fate != CBM_FATE_NONE) {
-      CUDA_TRY(c, cudaMemsetAsync(c->blk[0], 0, (size_t)c->n_blocks * 4, c->stream));
-      CUDA_TRY(c, cudaMemsetAsync(c->blk[1], 0, (size_t)c->n_blocks * 4, c->stream));
-    }
-    if (k.walls == CBM_WALLS_REFLECT)
-      for (int d = 0; d < k.dims; ++d)
-        CUDA_TRY(c, cudaMemcpyAsync(c->pos_u[d], c->pos[c->parity][d], (size_t)k.n_max * c->tsize,
-                                    cudaMemcpyDeviceToDevice, c->stream));
-  }
+  if (!c->rule_done && k.walls == CBM_WALLS_REFLECT)
+    CUDA_TRY(c, cudaMemcpyAsync(c->U, c->PA, (size_t)k.n_max * 4 * c->tsize,
+                                cudaMemcpyDeviceToDevice, c->stream));
   dispatch<StageDE>(c);
   c->de_done = true;
   return check_launch(c);
@@ -772,16 +867,11 @@ int cbm_update(cbm_ctx* c) {
   if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
   cudaSetDevice(c->device);
   const cbm_config& k = c->cfg;
-  int births = (!c->de_done && c->rule_done && k.fate != CBM_FATE_NONE) ? 1 : 0;
   int copy_agents = c->de_done ? 0 : 1;
+  int use_u = (c->rule_done && k.walls == CBM_WALLS_REFLECT) ? 1 : 0;
   int copy_c = (k.medium && !c->mde_done) ? 1 : 0;
   int copy_grad = (k.medium && !c->mrule_done) ? 1 : 0;
-  if (!c->rule_done && k.fate != CBM_FATE_NONE) {
-    // no rule this step: no events for the compaction
-    CUDA_TRY(c, cudaMemsetAsync(c->blk[0], 0, (size_t)c->n_blocks * 4, c->stream));
-    CUDA_TRY(c, cudaMemsetAsync(c->blk[1], 0, (size_t)c->n_blocks * 4, c->stream));
-  }
-  dispatch<StageUpdate>(c, copy_agents, copy_c, copy_grad, births);
+  dispatch<StageUpdate>(c, copy_agents, use_u, copy_c, copy_grad);
   c->parity ^= 1;
   reset_stage_flags(c);
   return check_launch(c);
@@ -868,27 +958,34 @@ int cbm_get_counters(cbm_ctx* c, int64_t* N, int64_t* n_add, int64_t* n_remove, 
 
 int cbm_grid_shape(cbm_ctx* c, int32_t* n3) {
   if (!c || !n3) return CBM_ERR_ARG;
-  for (int d = 0; d < 3; ++d) n3[d] = c->n_cells_d[d];
+  for (int d = 0; d < 3; ++d) n3[d] = c->grid_exposed ? c->n_cells_d[d] : 1;
   return CBM_OK;
 }
 
 int cbm_get_grid(cbm_ctx* c, int32_t* agent_cell, int32_t* cell_start, int32_t* cell_count,
                  int32_t* cell_agents) {
   if (!c) return CBM_ERR_ARG;
-  if (!c->has_grid) return fail(c, CBM_ERR_STATE, "this neighbor algorithm has no cell grid");
+  if (!c->grid_exposed) return fail(c, CBM_ERR_STATE, "this neighbor algorithm has no cell grid");
   cudaSetDevice(c->device);
   Counters hc;
   int rc = read_counters(c, &hc);
   if (rc) return rc;
   const long long N = hc.N[c->parity];
-  std::vector<int> start((size_t)c->n_cells + 1);
+  std::vector<int> start((size_t)c->n_cells + 1), ia((size_t)N), inv((size_t)N), cos((size_t)N);
   CUDA_TRY(c, cudaMemcpy(start.data(), c->cell_start, start.size() * 4, cudaMemcpyDeviceToHost));
+  if (N) {
+    CUDA_TRY(c, cudaMemcpy(ia.data(), c->IA, (size_t)N * 4, cudaMemcpyDeviceToHost));
+    CUDA_TRY(c, cudaMemcpy(inv.data(), c->inv, (size_t)N * 4, cudaMemcpyDeviceToHost));
+    CUDA_TRY(c, cudaMemcpy(cos.data(), c->cell_of_slot, (size_t)N * 4, cudaMemcpyDeviceToHost));
+  }
   for (int q = 0; q < c->n_cells; ++q) {
     if (cell_start) cell_start[q] = start[q];
     if (cell_count) cell_count[q] = start[q + 1] - start[q];
   }
-  if (agent_cell && N) CUDA_TRY(c, cudaMemcpy(agent_cell, c->agent_cell, (size_t)N * 4, cudaMemcpyDeviceToHost));
-  if (cell_agents && N) CUDA_TRY(c, cudaMemcpy(cell_agents, c->cell_agents, (size_t)N * 4, cudaMemcpyDeviceToHost));
+  for (long long i = 0; i < N; ++i) {
+    if (cell_agents) cell_agents[i] = ia[(size_t)i];  // slots are in cell order
+    if (agent_cell) agent_cell[i] = cos[(size_t)inv[(size_t)i]];
+  }
   return CBM_OK;
 }
 
@@ -896,20 +993,30 @@ int cbm_get_neighbors(cbm_ctx* c, int32_t* counts, int32_t* list, int64_t cap) {
   if (!c) return CBM_ERR_ARG;
   if (!c->has_list) return fail(c, CBM_ERR_STATE, "this neighbor algorithm has no Verlet list");
   cudaSetDevice(c->device);
+  int rc = ensure_list(c);
+  if (rc) return rc;
   Counters hc;
-  int rc = read_counters(c, &hc);
+  rc = read_counters(c, &hc);
   if (rc) return rc;
   const long long N = hc.N[c->parity];
   const long long M = c->cfg.n_max_neighbors, nmax = c->cfg.n_max;
   if (list && cap < N * M) return fail(c, CBM_ERR_ARG, "list capacity %lld < N*n_max_neighbors", (long long)cap);
-  std::vector<int> n((size_t)N), col((size_t)(nmax * M));
-  if (N) CUDA_TRY(c, cudaMemcpy(n.data(), c->nbr_n, (size_t)N * 4, cudaMemcpyDeviceToHost));
-  if (list && N) CUDA_TRY(c, cudaMemcpy(col.data(), c->nbr_list, col.size() * 4, cudaMemcpyDeviceToHost));
+  std::vector<int> n((size_t)N), ia((size_t)N), inv((size_t)N), col;
+  if (N) {
+    CUDA_TRY(c, cudaMemcpy(n.data(), c->nbr_n, (size_t)N * 4, cudaMemcpyDeviceToHost));
+    CUDA_TRY(c, cudaMemcpy(ia.data(), c->IA, (size_t)N * 4, cudaMemcpyDeviceToHost));
+    CUDA_TRY(c, cudaMemcpy(inv.data(), c->inv, (size_t)N * 4, cudaMemcpyDeviceToHost));
+  }
+  if (list && N) {
+    col.resize((size_t)(nmax * M));
+    CUDA_TRY(c, cudaMemcpy(col.data(), c->nbr_list, col.size() * 4, cudaMemcpyDeviceToHost));
+  }
   for (long long i = 0; i < N; ++i) {
-    if (counts) counts[i] = n[(size_t)i];
+    const long long s = inv[(size_t)i];
+    if (counts) counts[i] = n[(size_t)s];
     if (list)
-      for (long long k = 0; k < M; ++k)
-        list[i * M + k] = k < n[(size_t)i] ? col[(size_t)(k * nmax + i)] : -1;
+      for (long long q = 0; q < M; ++q)
+        list[i * M + q] = q < n[(size_t)s] ? ia[(size_t)col[(size_t)(q * nmax + s)]] : -1;
   }
   return CBM_OK;
 }
@@ -937,7 +1044,7 @@ int cbm_rng_fill(cbm_ctx* c, int32_t kind, double a, double b, int64_t n, int64_
   void* buf = nullptr;
   const size_t bytes = (size_t)(n > 0 ? n : 1) * c->tsize;
   CUDA_TRY(c, cudaMallocAsync(&buf, bytes, c->stream));
-  const int blocks = (int)((n + kTile - 1) / kTile);
+  const int blocks = grid_blocks(n);
   if (n > 0) {
     if (c->cfg.precision == CBM_F64)
       k_rng_fill<double><<<blocks, kTile, 0, c->stream>>>(c->cfg.seed, c->cfg.community, stepc, kind, a,

@@ -1,86 +1,84 @@
-// cbm_kernels.cuh — device kernels of the per-step path.
+// cbm_kernels.cuh — the stepping engine's kernels.
 //
-// Every kernel here reads the live agent count, step number and flags from
-// the device counter block, so a whole step can be captured once in a CUDA
-// graph and replayed without host round trips (the reference syncs the host
-// after every stage and reads flagRecomputeNeighbors_ / NAdd_ on the host,
-// src/neighbors.jl:548, src/CommunityStructure/update.jl:214).
+// Layout.  The committed agent state (positions and the DE variables) is kept
+// in "slots" sorted by grid cell and, inside a cell, by agent index: the order
+// in which the reference visits neighbor candidates (src/neighbors.jl:715-747,
+// cells x fastest, agents ascending inside a cell).  Positions are packed as
+// float4 / double4, so a warp of consecutive slots reads its candidates'
+// positions as a few contiguous runs instead of scattered loads.  Per-agent
+// constants (growth rate, id, parent id) stay in agent-index order.  `IA`
+// maps slot -> agent index and `inv` maps agent index -> slot.
 //
-// Arithmetic follows the reference's expression order with no FMA
-// contraction (the library is built with -fmad=false), so float and double
-// results are bit-identical to a CPU evaluation of the same expressions.
+// Every reference semantic that depends on the agent index is evaluated on
+// the index: random keys, the ascending order inside a cell, birth slots
+// (N + rank of the parent), and the tail-fill compaction (update.jl:15-119),
+// which here relabels slots.  A step ends by re-sorting the working slots
+// (survivors with their new indices plus newborns) by (cell, index): that one
+// pass is the compaction gather and the grid rebuild of computeNeighbors!.
+//
+// Set A holds the committed state, set B the state being written by the
+// current step (the reference's x__).  Every kernel reads N, the step and the
+// flags from the device counter block, so a whole step is a static CUDA
+// graph without host round trips (the reference reads flagRecomputeNeighbors_
+// and NAdd_ on the host every step, src/neighbors.jl:548, update.jl:214).
 #pragma once
 
-#include <cuda_runtime.h>
-#include <stdint.h>
-
-#include "../../include/cbm_b200.h"
-#include "../../include/cbm_rng.h"
+#include "cbm_common.cuh"
 
 namespace cbm {
 
-constexpr int kTile = 256;          // agents per block in every agent kernel
-constexpr unsigned kFull = 0xffffffffu;
-constexpr int kScanItems = 8;       // cells per thread in the cell scan
-constexpr int kScanTile = kTile * kScanItems;
-constexpr long long kSpinLimit = 1ll << 20;  // bounded look-back wait
-
-// device error bits (reported through cbm_sync as the lowest set code)
-enum : int {
-  kErrAgentOverflow = 1 << 0,
-  kErrNeighborOverflow = 1 << 1,
-  kErrTimeout = 1 << 2,
+template <typename T>
+struct V4T;
+template <>
+struct V4T<float> {
+  using type = float4;
 };
-
-// Device counters.  Values that a step both reads and produces are indexed
-// by step parity p: a step of parity p reads [p] and writes [p ^ 1].
-struct Counters {
-  long long N[2];
-  long long step[2];
-  double t[2];
-  long long n_add;      // NAdd_ of the step in flight
-  long long n_remove;   // NRemove_
-  long long id_max;     // idMax_
-  long long id_base;    // idMax_ before this step's births
-  long long children;   // births requested (including dropped ones)
-  int flag[2];          // flagRecomputeNeighbors_ of the step of that parity
-  int err;              // kErr* bits
-  unsigned scan_ticket; // tile tickets of the cell scan
-  unsigned scan_epoch;  // generation of the cell-scan tile states
-  int pad;
+template <>
+struct V4T<double> {
+  using type = double4;
 };
 
 template <typename T>
 struct Params {
-  // agent arrays: committed ("cur", parity p) and written ("nxt", p ^ 1)
-  T* pos_cur[3];
-  T* pos_nxt[3];
-  T* pos_u[3];          // positions after the rule's wall reflection (u); = pos_cur without walls
-  T* v_cur;
-  T* v_nxt;
-  T* f_cur[3];
-  T* f_nxt[3];
-  T* g;
-  long long* id;
-  long long* parent;
+  using V4 = typename V4T<T>::type;
+  // slot-ordered state: committed (A) and written (B)
+  V4* PA;
+  V4* PB;
+  T* VA;
+  T* VB;
+  V4* FA;               // lagged force
+  V4* FB;
+  int* IA;              // slot -> agent index
+  int* IB;              // working labels (relabelled by the compaction, -1 = dead)
+  V4* U;                // positions after the rule's wall reflection (walls only)
+  V4* POLD;             // positions at the last Verlet rebuild (slot order)
+  int* inv;             // agent index -> slot of A
+  int* cell_of_slot;    // cell of each A slot
+  // agent-index-ordered constants
+  T* G;
+  long long* ID;
+  long long* PAR;
+  // index-ordered host exchange staging
+  T* hx[3];
+  T* hv;
+  T* hf[3];
+  // fate
   unsigned char* fate;
   int* holes;
   int* blk_children;
   int* blk_deaths;
   int* blk_child_off;
   int* blk_death_off;
-  // grid
-  int* agent_cell;
-  int* agent_rank;
+  // re-sort
+  int* s_cell;          // cell of each working slot (-1 dead)
+  int* s_rank;          // atomic rank inside the cell
+  int* s_key;           // agent index at each sorted position
   int* cell_count;
   int* cell_start;      // n_cells + 1
-  int* cell_tmp;
-  int* cell_agents;
-  unsigned long long* scan_state;  // per scan tile: epoch | flag | value
-  // Verlet
+  unsigned long long* scan_state;
+  // Verlet list in slot space: entry k of the row of slot s at k * n_max + s
   int* nbr_n;
-  int* nbr_list;        // column-major: slot k of agent i at k * n_max + i
-  T* pos_old[3];
+  int* nbr_list;
   // medium: committed / written
   T* c_cur;
   T* c_nxt;
@@ -89,7 +87,7 @@ struct Params {
   Counters* ctr;
   // sizes
   int n_max;
-  int n_blocks;         // agent tiles = ceil(n_max / kTile)
+  int n_blocks;         // ceil(n_max / kTile)
   int n_cells;
   int n_cells_d[3];
   int n_scan_tiles;
@@ -97,7 +95,6 @@ struct Params {
   int n_medium[3];
   int max_nbrs;
   int parity;
-  int births_only;      // k_agent_de: place the rule's births, integrate nothing
   // model
   int neighbors, integrator, force_mode, att_form, walls, fate_rule, growth, medium,
       medium_sampling;
@@ -106,6 +103,13 @@ struct Params {
   T edge;               // grid cell edge
   T skin, rebuild_thr;
   T k_rep, r_rep, k_att, r_att;
+  // Squared-distance bounds above which sqrt(s2) is certain to fail the
+  // reference's `d < cutoff` (resp. `d < skin`) test; pairs below them take
+  // the exact test.  (cutoff^2 and skin^2 times 1 + 1e-5, rounded up.)
+  T cut2, skin2;
+  T skin2_lo;               // skin^2 times 1 - 1e-5, rounded down: below it d < skin for certain
+  int force_in_list;        // (T)cutoff <= (T)skin: every pair with a force term is in the list
+  T cut_reach, skin_reach;  // cutoff and skin times 1 + 1e-4: cell-pruning radii
   T wall_force, wall_range, drift_linear;
   T v_div, div_sep, p_death;
   T dx_m[3];
@@ -114,52 +118,37 @@ struct Params {
   uint32_t community;
 };
 
-// ---------------------------------------------------------------------------
-// helpers
-// ---------------------------------------------------------------------------
 template <typename T>
-__device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
-
-// Julia's float `÷` on a >= 0: round((a - rem(a, b)) / b)
-__device__ __forceinline__ int floordiv(double a, double b) {
-  return (int)rint((a - fmod(a, b)) / b);
+__device__ __forceinline__ void to3(const typename V4T<T>::type& v, T* x) {
+  x[0] = v.x;
+  x[1] = v.y;
+  x[2] = v.z;
 }
-__device__ __forceinline__ int floordiv(float a, float b) {
-  return (int)rintf((a - fmodf(a, b)) / b);
-}
-
-// cellPos, src/neighbors.jl:636-638, 0-based; NaN goes to the first cell
 template <typename T>
-__device__ __forceinline__ int cell_pos1(T edge, T x, T lo, T hi, int n) {
-  if (x > hi) return n - 1;
-  if (!(x >= lo)) return 0;
-  int p = floordiv(x - lo, edge) + 1;
-  return p > n - 1 ? n - 1 : p;
+__device__ __forceinline__ typename V4T<T>::type from3(const T* x) {
+  typename V4T<T>::type v;
+  v.x = x[0];
+  v.y = x[1];
+  v.z = x[2];
+  v.w = (T)0;
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ bool is_verlet(const Params<T>& P) {
+  return P.neighbors == CBM_NEIGH_CLVD || P.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT;
 }
 
 template <typename T, int D>
-__device__ __forceinline__ int cell_of(const Params<T>& P, const T* x) {
-  int lin = cell_pos1<T>(P.edge, x[0], P.box_lo[0], P.box_hi[0], P.n_cells_d[0]);
-  if (D > 1) lin += P.n_cells_d[0] * cell_pos1<T>(P.edge, x[1], P.box_lo[1], P.box_hi[1], P.n_cells_d[1]);
-  if (D > 2)
-    lin += P.n_cells_d[0] * P.n_cells_d[1] *
-           cell_pos1<T>(P.edge, x[2], P.box_lo[2], P.box_hi[2], P.n_cells_d[2]);
-  return lin;
-}
-
-// cellInMesh, src/metrics.jl:18-20 (0-based, clamped at the top)
-template <typename T>
-__device__ __forceinline__ int cell_in_mesh(T dx, T x, T lo, T hi, int n) {
-  if (x > hi) return n - 1;
-  if (!(x >= lo)) return 0;
-  int p = floordiv(x - lo, dx);
-  return p > n - 1 ? n - 1 : p;
+__device__ __forceinline__ int cell_of_pos(const Params<T>& P, const T* x) {
+  return cell_of<T, D>(P.edge, P.box_lo, P.box_hi, P.n_cells_d, x);
 }
 
 template <typename T, int D>
 __device__ __forceinline__ int nearest_node(const Params<T>& P, const T* x) {
   int lin = cell_in_mesh<T>(P.dx_m[0], x[0], P.box_lo[0], P.box_hi[0], P.n_medium[0]);
-  if (D > 1) lin += P.n_medium[0] * cell_in_mesh<T>(P.dx_m[1], x[1], P.box_lo[1], P.box_hi[1], P.n_medium[1]);
+  if (D > 1)
+    lin += P.n_medium[0] * cell_in_mesh<T>(P.dx_m[1], x[1], P.box_lo[1], P.box_hi[1], P.n_medium[1]);
   if (D > 2)
     lin += P.n_medium[0] * P.n_medium[1] *
            cell_in_mesh<T>(P.dx_m[2], x[2], P.box_lo[2], P.box_hi[2], P.n_medium[2]);
@@ -198,99 +187,112 @@ __device__ __forceinline__ void bilinear(const Params<T>& P, const T* x, int* no
   }
 }
 
-// cellPosNeigh, src/neighbors.jl:658-708: k-th of 3^D cells, x fastest, -1 outside
-template <int D>
-__device__ __forceinline__ int cell_neigh(const int* nc, const int* q, int k) {
-  int px = q[0] + (k % 3) - 1;
-  if (px < 0 || px >= nc[0]) return -1;
-  int lin = px;
-  if (D > 1) {
-    int py = q[1] + ((k / 3) % 3) - 1;
-    if (py < 0 || py >= nc[1]) return -1;
-    lin += nc[0] * py;
-  }
-  if (D > 2) {
-    int pz = q[2] + (k / 9) - 1;
-    if (pz < 0 || pz >= nc[2]) return -1;
-    lin += nc[0] * nc[1] * pz;
-  }
-  return lin;
-}
-
-template <int D>
-__device__ __forceinline__ void cell_coords(const int* nc, int pos, int* q) {
-  q[0] = pos % nc[0];
-  if (D > 1) q[1] = (pos / nc[0]) % nc[1];
-  if (D > 2) q[2] = pos / (nc[0] * nc[1]);
-}
-
+// euclidean, src/metrics.jl:34-36: sqrt((a1-b1)^2 + (a2-b2)^2 + (a3-b3)^2)
 template <typename T, int D>
-__device__ __forceinline__ void load_pos(T* const* arr, int i, T* x) {
-#pragma unroll
-  for (int d = 0; d < D; ++d) x[d] = arr[d][i];
+__device__ __forceinline__ T dist(const T* a, const T* b) {
+  T e = a[0] - b[0];
+  T s = e * e;
+  if (D > 1) { e = a[1] - b[1]; s = s + e * e; }
+  if (D > 2) { e = a[2] - b[2]; s = s + e * e; }
+  return sqrt(s);
 }
 
-// Visit neighbor candidates of agent i in the reference's order.  `pos` are
-// the positions used to locate i's own cell (u in the DE, x in a rule).
+// Visit the candidate slots of the 3^D cells around the cell holding x, in
+// the reference's order (cells x fastest; a row of three x-neighbor cells is
+// one contiguous run of slots).
 template <typename T, int D, typename F>
-__device__ __forceinline__ void for_neighbors(const Params<T>& P, const T* xi, int i, int N,
-                                              F&& body) {
-  switch (P.neighbors) {
-    case CBM_NEIGH_FULL:
-      for (int j = 0; j < N; ++j)
-        if (j != i) body(j);
-      break;
-    case CBM_NEIGH_CELL_LINKED: {
-      int q[3];
-      cell_coords<D>(P.n_cells_d, cell_of<T, D>(P, xi), q);
-      constexpr int nk = D == 1 ? 3 : (D == 2 ? 9 : 27);
-      for (int k = 0; k < nk; ++k) {
-        int pn = cell_neigh<D>(P.n_cells_d, q, k);
-        if (pn < 0) continue;
-        int s0 = ld(P.cell_start + pn), s1 = ld(P.cell_start + pn + 1);
-        for (int s = s0; s < s1; ++s) {
-          int j = ld(P.cell_agents + s);
-          if (j != i) body(j);
-        }
-      }
-      break;
+__device__ __forceinline__ void for_cell_slots(const Params<T>& P, const T* x, F&& body) {
+  int q[3] = {0, 0, 0};
+  cell_coords<D>(P.n_cells_d, cell_of_pos<T, D>(P, x), q);
+  const int nx = P.n_cells_d[0];
+  const int x0 = q[0] > 0 ? q[0] - 1 : 0;
+  const int x1 = q[0] < nx - 1 ? q[0] + 1 : nx - 1;
+  constexpr int ny_rows = D > 1 ? 3 : 1;
+  constexpr int nz_rows = D > 2 ? 3 : 1;
+  for (int dz = 0; dz < nz_rows; ++dz) {
+    int pz = D > 2 ? q[2] + dz - 1 : 0;
+    if (D > 2 && (pz < 0 || pz >= P.n_cells_d[2])) continue;
+    for (int dy = 0; dy < ny_rows; ++dy) {
+      int py = D > 1 ? q[1] + dy - 1 : 0;
+      if (D > 1 && (py < 0 || py >= P.n_cells_d[1])) continue;
+      int row = nx * (py + P.n_cells_d[1] * pz);
+      int s0 = ld(P.cell_start + row + x0), s1 = ld(P.cell_start + row + x1 + 1);
+      for (int s = s0; s < s1; ++s) body(s);
     }
-    case CBM_NEIGH_VERLET_DISPLACEMENT:
-    case CBM_NEIGH_CLVD: {
-      int n = P.nbr_n[i];
-      for (int k = 0; k < n; ++k) body(ld(P.nbr_list + (size_t)k * P.n_max + i));
-      break;
-    }
-    default:
-      break;
   }
 }
 
-// exclusive block scan of one int per thread (kTile threads)
-__device__ __forceinline__ int block_exscan(int v, int* warp_sums, int* total) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int x = v;
+constexpr int kQueue = 32;  // per-thread force queue of k_agent_de (32 KB per block)
+
+template <typename T>
+struct Eps;
+template <>
+struct Eps<float> {
+  static constexpr float v = 1.1920929e-07f;
+};
+template <>
+struct Eps<double> {
+  static constexpr double v = 2.220446049250313e-16;
+};
+
+// Like for_cell_slots, but cells whose nearest face is farther than `reach`
+// from x are skipped (their agents cannot pass a `d < reach` test), and the
+// positions of a run are loaded four at a time.  body(slot, position).
+// Skipping cells keeps the order of the visited candidates, so the sums that
+// follow are unchanged.  The face gaps carry a margin for the rounding of the
+// cell assignment; cells next to the ghost layer are never skipped.
+template <typename T, int D, typename F>
+__device__ __forceinline__ void walk_runs(const Params<T>& P, const T* x, T reach, F&& run);
+
+template <typename T, int D, typename F>
+__device__ __forceinline__ void walk_cells(const Params<T>& P, const typename V4T<T>::type* X,
+                                           const T* x, T reach, F&& body) {
+  using V4 = typename V4T<T>::type;
+  walk_runs<T, D>(P, x, reach, [&](int s0, int s1) {
+    for (int s = s0; s < s1; ++s) body(s, X[s]);
+  });
+}
+
+// The pruned cell walk as a sequence of contiguous slot runs run(s0, s1).
+template <typename T, int D, typename F>
+__device__ __forceinline__ void walk_runs(const Params<T>& P, const T* x, T reach, F&& run) {
+  int q[3] = {0, 0, 0};
+  T gm[3] = {(T)0, (T)0, (T)0}, gp[3] = {(T)0, (T)0, (T)0};
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(kFull, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) warp_sums[w] = x;
-  __syncthreads();
-  if (w == 0) {
-    int s = lane < kTile / 32 ? warp_sums[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(kFull, s, o);
-      if (lane >= o) s += y;
+  for (int d = 0; d < D; ++d) {
+    const int n = P.n_cells_d[d];
+    const int c = cell_pos1<T>(P.edge, x[d], P.box_lo[d], P.box_hi[d], n);
+    q[d] = c;
+    if (c >= 2 && c <= n - 3) {
+      const T rel = x[d] - P.box_lo[d];
+      const T k = (T)(c - 1);
+      const T margin = (T)16 * Eps<T>::v * (fabs(rel) + (k + (T)1) * P.edge) + (T)1e-4 * reach;
+      T a = rel - k * P.edge - margin;
+      T b = (k + (T)1) * P.edge - rel - margin;
+      gm[d] = a > (T)0 ? a : (T)0;
+      gp[d] = b > (T)0 ? b : (T)0;
     }
-    if (lane < kTile / 32) warp_sums[lane] = s;
   }
-  __syncthreads();
-  int prefix = w > 0 ? warp_sums[w - 1] : 0;
-  *total = warp_sums[kTile / 32 - 1];
-  __syncthreads();
-  return prefix + x - v;
+  const T r2 = reach * reach;
+  const int nx = P.n_cells_d[0];
+  constexpr int ny_rows = D > 1 ? 3 : 1;
+  constexpr int nz_rows = D > 2 ? 3 : 1;
+  for (int dz = 0; dz < nz_rows; ++dz) {
+    const int pz = D > 2 ? q[2] + dz - 1 : 0;
+    if (D > 2 && (pz < 0 || pz >= P.n_cells_d[2])) continue;
+    const T gz = dz == 0 ? gm[2] : (dz == 2 ? gp[2] : (T)0);
+    for (int dy = 0; dy < ny_rows; ++dy) {
+      const int py = D > 1 ? q[1] + dy - 1 : 0;
+      if (D > 1 && (py < 0 || py >= P.n_cells_d[1])) continue;
+      const T gy = dy == 0 ? gm[1] : (dy == 2 ? gp[1] : (T)0);
+      const T gyz = (D > 1 ? gy * gy : (T)0) + (D > 2 ? gz * gz : (T)0);
+      if (!(gyz < r2)) continue;
+      const int xa = (q[0] > 0 && gm[0] * gm[0] + gyz < r2) ? q[0] - 1 : q[0];
+      const int xb = (q[0] < nx - 1 && gp[0] * gp[0] + gyz < r2) ? q[0] + 1 : q[0];
+      const int row = nx * (py + P.n_cells_d[1] * pz);
+      run(ld(P.cell_start + row + xa), ld(P.cell_start + row + xb + 1));
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -354,6 +356,7 @@ __global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
     c0[d] = a < 0 ? 0 : a;
     c1[d] = b > nc - 1 ? nc - 1 : b;
   }
+  // one cursor per cell: agents are ascending inside a cell
   int cur[kMaxCells], end[kMaxCells];
   int ncand = 0;
   bool all = true;
@@ -367,65 +370,59 @@ __global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
       }
   const T amt = P.secretion_amt;
   T acc = P.c_cur[n];
+  auto add = [&](int slot) {
+    T x[3];
+    to3<T>(P.PA[slot], x);
+    int nodes[8];
+    T w[8];
+    bilinear<T, D>(P, x, nodes, w);
+#pragma unroll
+    for (int k = 0; k < (1 << D); ++k)
+      if (nodes[k] == n) acc = acc + w[k] * amt;
+  };
   if (all) {
     while (true) {  // k-way merge: next smallest agent index among the cells
       int best = -1, bj = 0x7fffffff;
       for (int k = 0; k < ncand; ++k)
         if (cur[k] < end[k]) {
-          int j = P.cell_agents[cur[k]];
+          int j = P.IA[cur[k]];
           if (j < bj) { bj = j; best = k; }
         }
       if (best < 0) break;
-      ++cur[best];
-      T x[3];
-      load_pos<T, D>(P.pos_cur, bj, x);
-      int nodes[8];
-      T w[8];
-      bilinear<T, D>(P, x, nodes, w);
-#pragma unroll
-      for (int k = 0; k < (1 << D); ++k)
-        if (nodes[k] == n) acc = acc + w[k] * amt;
+      add(cur[best]++);
     }
   } else {
     // the cell box is too large (cells much smaller than the medium spacing):
     // visit every agent in index order
     const int N = (int)P.ctr->N[P.parity];
-    for (int j = 0; j < N; ++j) {
-      T x[3];
-      load_pos<T, D>(P.pos_cur, j, x);
-      int nodes[8];
-      T w[8];
-      bilinear<T, D>(P, x, nodes, w);
-#pragma unroll
-      for (int k = 0; k < (1 << D); ++k)
-        if (nodes[k] == n) acc = acc + w[k] * amt;
-    }
+    for (int j = 0; j < N; ++j) add(P.inv[j]);
   }
   P.c_cur[n] = acc;
 }
 
 // ---------------------------------------------------------------------------
 // agentStepRule!: walls, secretion, fate decision + per-tile event counts
-// (src/AgentStructure/functionRule.jl:9-111)
+// (src/AgentStructure/functionRule.jl:9-111).  One thread per agent index.
 // ---------------------------------------------------------------------------
 template <typename T, int D>
 __global__ void __launch_bounds__(kTile) k_agent_rule(Params<T> P) {
   const int p = P.parity;
   const int N = (int)P.ctr->N[p];
   const int i = blockIdx.x * kTile + threadIdx.x;
-  const bool live = i < N;
   int fate = 0;  // 0 none, 1 die, 2 divide (2 children + die), 3 one child
-  if (live) {
-    T x[3];
-    load_pos<T, D>(P.pos_cur, i, x);
+  if (i < N) {
+    const int s = P.inv[i];
+    T x[3] = {(T)0, (T)0, (T)0};
+    if (P.walls == CBM_WALLS_REFLECT || (P.medium && P.secretion_amt != (T)0))
+      to3<T>(P.PA[s], x);
     if (P.walls == CBM_WALLS_REFLECT) {
+      T y[3] = {x[0], x[1], x[2]};
 #pragma unroll
       for (int d = 0; d < D; ++d) {
-        T y = x[d];
-        if (x[d] < P.box_lo[d]) y = (T)2 * P.box_lo[d] - x[d];
-        else if (x[d] > P.box_hi[d]) y = (T)2 * P.box_hi[d] - x[d];
-        P.pos_u[d][i] = y;
+        if (x[d] < P.box_lo[d]) y[d] = (T)2 * P.box_lo[d] - x[d];
+        else if (x[d] > P.box_hi[d]) y[d] = (T)2 * P.box_hi[d] - x[d];
       }
+      P.U[s] = from3<T>(y);
     }
     if (P.medium && P.secretion_amt != (T)0 && !secretion_by_gather(P)) {
       if (P.medium_sampling == CBM_MEDIUM_NEAREST) {
@@ -439,15 +436,16 @@ __global__ void __launch_bounds__(kTile) k_agent_rule(Params<T> P) {
       }
     }
     if (P.fate_rule == CBM_FATE_VOLUME) {
-      if (P.growth && P.v_cur[i] >= P.v_div) fate = 2;
+      if (P.growth && P.VA[s] >= P.v_div) fate = 2;
       else if (P.p_death > (T)0 &&
                cbm_uniform<T>(P.seed, P.ctr->step[p], (uint32_t)i, CBM_STREAM_DEATH, P.community) <
                    P.p_death)
         fate = 1;
     } else if (P.fate_rule == CBM_FATE_ID_PARITY) {
-      fate = (P.id[i] % 2 == 1) ? 1 : 3;
+      fate = (P.ID[i] % 2 == 1) ? 1 : 3;
     }
   }
+  if (P.fate_rule == CBM_FATE_NONE) return;  // uniform over the grid
   if (i < P.n_max) P.fate[i] = (unsigned char)fate;
   int n_div = __syncthreads_count(fate == 2);
   int n_one = __syncthreads_count(fate == 3);
@@ -503,21 +501,24 @@ __global__ void __launch_bounds__(1024) k_fate_scan(Params<T> P) {
     C->children = tc;
     C->id_base = C->id_max;
     C->id_max += tc;  // ids are consumed even by dropped births
+    C->events = (tc > 0 || td > 0) ? 1 : 0;
     if (tc > 0 || td > 0) C->flag[p] = 1;
   }
 }
 
-// ---------------------------------------------------------------------------
-// agentStepDE!: fused neighbor force + Euler / EM update, births and holes
-// (src/integrators.jl:465-505,683-734, functionDE.jl:13-117,
-//  functionRule.jl:59-70,97-102)
-// ---------------------------------------------------------------------------
+// Births and holes of @addAgent/@removeAgent, ranked in agent-index order.
+// Newborn k of the step gets index and working slot N + k; its DE variables
+// go to set B, its constants to index N + k.  Parameters not given to
+// @addAgent are copied from the parent's committed values.
 template <typename T, int D>
-__device__ __forceinline__ void place_births(const Params<T>& P, int i, int fate, int N) {
+__global__ void __launch_bounds__(kTile) k_births(Params<T> P) {
   __shared__ int warp_sums[kTile / 32];
+  const int p = P.parity;
+  const int N = (int)P.ctr->N[p];
   const int b = blockIdx.x;
-  int has_events = P.blk_children[b] + P.blk_deaths[b];
-  if (has_events == 0) return;  // uniform over the block
+  const int i = b * kTile + threadIdx.x;
+  if (P.blk_children[b] + P.blk_deaths[b] == 0) return;  // uniform over the block
+  const int fate = i < N ? P.fate[i] : 0;
   const int nch = fate == 2 ? 2 : (fate == 3 ? 1 : 0);
   const int die = (fate == 1 || fate == 2) ? 1 : 0;
   int tot;
@@ -525,77 +526,218 @@ __device__ __forceinline__ void place_births(const Params<T>& P, int i, int fate
   int rd = block_exscan(die, warp_sums, &tot) + P.blk_death_off[b];
   if (die) P.holes[rd] = i;
   if (nch == 0) return;
+  const int s = P.inv[i];
   T x[3];
-  load_pos<T, D>(P.pos_cur, i, x);
-  T a[3] = {0, 0, 0};
+  to3<T>(P.PA[s], x);
+  T a[3] = {(T)0, (T)0, (T)0};
   if (fate == 2) {
-    cbm_normals(P.seed, P.ctr->step[P.parity], (uint32_t)i, CBM_STREAM_DIVISION, P.community, D, a);
-    T s = a[0] * a[0];
-    if (D > 1) s = s + a[1] * a[1];
-    if (D > 2) s = s + a[2] * a[2];
-    T Ta = sqrt(s);
+    cbm_normals(P.seed, P.ctr->step[p], (uint32_t)i, CBM_STREAM_DIVISION, P.community, D, a);
+    T ss = a[0] * a[0];
+    if (D > 1) ss = ss + a[1] * a[1];
+    if (D > 2) ss = ss + a[2] * a[2];
+    T Ta = sqrt(ss);
 #pragma unroll
     for (int d = 0; d < D; ++d) a[d] = a[d] / Ta;
   }
-  const long long idp = P.id[i];
-  const T vv = P.v_cur[i];
-  const T gg = P.g[i];
+  const long long idp = P.ID[i];
+  const T vv = P.VA[s];
+  const T gg = P.G[i];
   for (int k = 0; k < nch; ++k) {
     long long slot = (long long)N + rc + k;
     if (slot >= P.n_max) break;  // dropped birth (counted in k_fate_scan)
-    int s = (int)slot;
+    const int ns = (int)slot;
+    T y[3] = {x[0], x[1], x[2]};
     if (fate == 2) {
 #pragma unroll
-      for (int d = 0; d < D; ++d)
-        P.pos_nxt[d][s] = k == 0 ? x[d] + P.div_sep * a[d] : x[d] - P.div_sep * a[d];
-      P.v_nxt[s] = vv / (T)2;
+      for (int d = 0; d < D; ++d) y[d] = k == 0 ? x[d] + P.div_sep * a[d] : x[d] - P.div_sep * a[d];
+      P.VB[ns] = vv / (T)2;
     } else {
-#pragma unroll
-      for (int d = 0; d < D; ++d) P.pos_nxt[d][s] = x[d];
-      P.v_nxt[s] = vv;
+      P.VB[ns] = vv;
     }
-    if (P.force_mode == CBM_FORCE_LAGGED) {
-#pragma unroll
-      for (int d = 0; d < D; ++d) P.f_nxt[d][s] = P.f_cur[d][i];
-    }
-    P.g[s] = gg;
-    P.id[s] = P.ctr->id_base + rc + k + 1;
-    P.parent[s] = idp;
+    P.PB[ns] = from3<T>(y);
+    if (P.force_mode == CBM_FORCE_LAGGED) P.FB[ns] = P.FA[s];
+    P.IB[ns] = ns;
+    P.G[ns] = gg;
+    P.ID[ns] = P.ctr->id_base + rc + k + 1;
+    P.PAR[ns] = idp;
   }
 }
 
+// ---------------------------------------------------------------------------
+// agentStepDE!: fused neighbor force + Euler / EM update, one thread per slot
+// (src/integrators.jl:465-505,683-734, functionDE.jl:13-117)
+// ---------------------------------------------------------------------------
 template <typename T, int D>
 __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
+  using V4 = typename V4T<T>::type;
   const int p = P.parity;
   const int N = (int)P.ctr->N[p];
-  const int i = blockIdx.x * kTile + threadIdx.x;
-  if (P.fate_rule != CBM_FATE_NONE) {
-    int fate = i < N ? P.fate[i] : 0;
-    place_births<T, D>(P, i, fate, N);
-  }
-  if (i >= N || P.births_only) return;
-  T* const* U = P.walls == CBM_WALLS_REFLECT ? P.pos_u : P.pos_cur;
+  const int s = blockIdx.x * kTile + threadIdx.x;
+  if (s >= N) return;
+  const bool reflect = P.walls == CBM_WALLS_REFLECT;
+  const V4* U = reflect ? P.U : P.PA;
+  const int i = ld(P.IA + s);
   T xi[3];
-  load_pos<T, D>(U, i, xi);
+  to3<T>(U[s], xi);
   T acc[3] = {(T)0, (T)0, (T)0};
-  if (P.neighbors != CBM_NEIGH_NONE) {
-    const T krep = P.k_rep, rrep = P.r_rep, katt = P.k_att, ratt = P.r_att;
-    const bool from_rep = P.att_form == CBM_ATT_FROM_REP;
-    for_neighbors<T, D>(P, xi, i, N, [&](int j) {
-      T e[3];
-      e[0] = xi[0] - ld(U[0] + j);
-      T s2 = e[0] * e[0];
-      if (D > 1) { e[1] = xi[1] - ld(U[1] + j); s2 = s2 + e[1] * e[1]; }
-      if (D > 2) { e[2] = xi[2] - ld(U[2] + j); s2 = s2 + e[2] * e[2]; }
-      T dist = sqrt(s2);
-      T F;
-      if (dist < rrep) F = krep * (rrep - dist);
-      else if (dist < ratt) F = from_rep ? -(katt * (dist - rrep)) : -(katt * (ratt - dist));
-      else return;
-      T s = F / dist;
+  const T krep = P.k_rep, rrep = P.r_rep, katt = P.k_att, ratt = P.r_att;
+  const T cut2 = P.cut2;
+  const bool from_rep = P.att_form == CBM_ATT_FROM_REP;
+  // pair term with the difference e = xi - xj and its squared norm s2
+  auto pair_e = [&](const T* e, T s2) {
+    if (s2 >= cut2) return;  // d >= cutoff for certain (NaN takes the exact test)
+    T dd = sqrt(s2);
+    T F;
+    if (dd < rrep) F = krep * (rrep - dd);
+    else if (dd < ratt) F = from_rep ? -(katt * (dd - rrep)) : -(katt * (ratt - dd));
+    else return;
+    T sc = F / dd;
 #pragma unroll
-      for (int d = 0; d < D; ++d) acc[d] = acc[d] + s * e[d];
+    for (int d = 0; d < D; ++d) acc[d] = acc[d] + sc * e[d];
+  };
+  auto diff = [&](const T* xj, T* e) {
+    e[0] = xi[0] - xj[0];
+    T s2 = e[0] * e[0];
+    if (D > 1) { e[1] = xi[1] - xj[1]; s2 = s2 + e[1] * e[1]; }
+    if (D > 2) { e[2] = xi[2] - xj[2]; s2 = s2 + e[2] * e[2]; }
+    return s2;
+  };
+  auto pair = [&](const T* xj) {
+    T e[3];
+    T s2 = diff(xj, e);
+    pair_e(e, s2);
+  };
+  const int alg = P.neighbors;
+  if (alg == CBM_NEIGH_FULL) {
+    for (int j = 0; j < N; ++j) {
+      if (j == i) continue;
+      T xj[3];
+      to3<T>(U[ld(P.inv + j)], xj);
+      pair(xj);
+    }
+  } else if (alg == CBM_NEIGH_CELL_LINKED ||
+             (alg == CBM_NEIGH_CLVD && !P.ctr->list_valid && !reflect)) {
+    // Two phases.  The walk over the 3^D cells only filters: candidates that
+    // may be within the cutoff are queued, in visiting order, in this
+    // thread's column of a shared buffer.  The force terms are then
+    // evaluated from the queue, where nearly every lane has work; the queue
+    // is drained early when full, so the summation order is unchanged.
+    //
+    // For CLVD the grid is current, so the list the last rebuild defines
+    // (candidates within `skin` of the committed positions, in cell order)
+    // is this walk; the list is also written out when no birth or death this
+    // step forces another rebuild.
+    __shared__ int queue[kQueue * kTile];
+    int nq = 0;
+    auto drain = [&]() {
+      for (int k = 0; k < nq; ++k) {
+        T xj[3];
+        to3<T>(U[queue[k * kTile + threadIdx.x]], xj);
+        pair(xj);
+      }
+      nq = 0;
+    };
+    auto enqueue = [&](int q) {
+      queue[nq * kTile + threadIdx.x] = q;
+      if (++nq == kQueue) drain();
+    };
+    const bool clvd = alg == CBM_NEIGH_CLVD;
+    if (!(clvd && (P.ctr->events == 0 || !P.force_in_list))) {
+      // force-only walk (CellLinked, or a CLVD step that will rebuild anyway
+      // and whose cutoff lies inside the list radius): four independent
+      // candidates per iteration, then an in-order enqueue
+      walk_runs<T, D>(P, xi, P.cut_reach, [&](int s0, int s1) {
+        int q = s0;
+        for (; q + 4 <= s1; q += 4) {
+          T s2v[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            T xj[3], e[3];
+            to3<T>(U[q + u], xj);
+            s2v[u] = diff(xj, e);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (s2v[u] < cut2 && q + u != s) enqueue(q + u);
+        }
+        for (; q < s1; ++q) {
+          T xj[3], e[3];
+          to3<T>(U[q], xj);
+          if (diff(xj, e) < cut2 && q != s) enqueue(q);
+        }
+      });
+    } else {
+      const bool write = !P.ctr->events;
+      const T skin2 = P.skin2, skin2_lo = P.skin2_lo;
+      int n = 0;
+      bool over = false;
+      walk_cells<T, D>(P, U, xi, write ? P.skin_reach : P.cut_reach, [&](int q, const V4& v) {
+        if (q == s) return;
+        T xj[3], e[3];
+        to3<T>(v, xj);
+        const T s2 = diff(xj, e);
+        if (s2 >= skin2) return;                                   // d >= skin for certain
+        if (!write && s2 >= cut2) return;                          // in the list, no force
+        if (!(s2 < skin2_lo) && !(sqrt(s2) < P.skin)) return;      // exact test near skin
+        if (write) {
+          if (n < P.max_nbrs) P.nbr_list[(size_t)n * P.n_max + s] = q;
+          else over = true;
+          ++n;
+        }
+        if (s2 < cut2) enqueue(q);
+      });
+      if (write) {
+        if (over) atomicOr(&P.ctr->err, kErrNeighborOverflow);
+        P.nbr_n[s] = n < P.max_nbrs ? n : P.max_nbrs;
+        if (s == 0) P.ctr->list_written = 1;
+      }
+    }
+    drain();
+  } else if (alg == CBM_NEIGH_CLVD && !P.ctr->list_valid) {
+    // The grid is current, so the list the last rebuild defines (candidates
+    // within `skin` of the committed positions, in cell order) is walked
+    // directly.  It is also written out when no birth or death this step
+    // forces another rebuild.
+    const bool write = !P.ctr->events;
+    T xa[3];
+    to3<T>(P.PA[s], xa);
+    int n = 0;
+    bool over = false;
+    const T skin2 = P.skin2;
+    for_cell_slots<T, D>(P, xa, [&](int q) {
+      if (q == s) return;
+      T xj[3], e[3];
+      to3<T>(U[q], xj);
+      T s2 = diff(xj, e);
+      if (reflect) {
+        // list membership is decided on the committed positions
+        T xb[3];
+        to3<T>(P.PA[q], xb);
+        if (!(dist<T, D>(xa, xb) < P.skin)) return;
+      } else {
+        if (s2 >= skin2) return;                       // d >= skin for certain
+        if (!write && s2 >= cut2) return;              // in the list, no force
+        if (!(sqrt(s2) < P.skin)) return;
+      }
+      if (write) {
+        if (n < P.max_nbrs) P.nbr_list[(size_t)n * P.n_max + s] = q;
+        else over = true;
+      }
+      ++n;
+      pair_e(e, s2);
     });
+    if (write) {
+      if (over) atomicOr(&P.ctr->err, kErrNeighborOverflow);
+      P.nbr_n[s] = n < P.max_nbrs ? n : P.max_nbrs;
+      if (s == 0) P.ctr->list_written = 1;
+    }
+  } else if (is_verlet(P)) {
+    const int n = P.nbr_n[s];
+    for (int k = 0; k < n; ++k) {
+      T xj[3];
+      to3<T>(U[ld(P.nbr_list + (size_t)k * P.n_max + s)], xj);
+      pair(xj);
+    }
   }
   if (P.walls == CBM_WALLS_PUSH) {
 #pragma unroll
@@ -606,11 +748,11 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
   }
   T dv[3];
   if (P.force_mode == CBM_FORCE_LAGGED) {
+    T fc[3];
+    to3<T>(P.FA[s], fc);
+    P.FB[s] = from3<T>(acc);
 #pragma unroll
-    for (int d = 0; d < D; ++d) {
-      P.f_nxt[d][i] = acc[d];
-      dv[d] = P.f_cur[d][i];
-    }
+    for (int d = 0; d < D; ++d) dv[d] = fc[d];
   } else {
 #pragma unroll
     for (int d = 0; d < D; ++d) dv[d] = acc[d];
@@ -622,29 +764,29 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
   if (P.medium && P.chemotaxis != (T)0) {
     T gv[3] = {(T)0, (T)0, (T)0};
     if (P.medium_sampling == CBM_MEDIUM_NEAREST) {
-      int n = nearest_node<T, D>(P, xi);
+      int nn = nearest_node<T, D>(P, xi);
 #pragma unroll
-      for (int d = 0; d < D; ++d) gv[d] = ld(P.grad_cur[d] + n);
+      for (int d = 0; d < D; ++d) gv[d] = ld(P.grad_cur[d] + nn);
     } else {
       int nodes[8];
       T w[8];
       bilinear<T, D>(P, xi, nodes, w);
 #pragma unroll
       for (int d = 0; d < D; ++d) {
-        T s = (T)0;
+        T sm = (T)0;
 #pragma unroll
-        for (int q = 0; q < (1 << D); ++q) s = s + w[q] * ld(P.grad_cur[d] + nodes[q]);
-        gv[d] = s;
+        for (int q = 0; q < (1 << D); ++q) sm = sm + w[q] * ld(P.grad_cur[d] + nodes[q]);
+        gv[d] = sm;
       }
     }
-    T s = gv[0] * gv[0];
-    if (D > 1) s = s + gv[1] * gv[1];
-    if (D > 2) s = s + gv[2] * gv[2];
-    T den = (T)1 + sqrt(s);
+    T g2 = gv[0] * gv[0];
+    if (D > 1) g2 = g2 + gv[1] * gv[1];
+    if (D > 2) g2 = g2 + gv[2] * gv[2];
+    T den = (T)1 + sqrt(g2);
 #pragma unroll
     for (int d = 0; d < D; ++d) dv[d] = dv[d] + (P.chemotaxis * gv[d]) / den;
   }
-  T xn[3];
+  T xn[3] = {(T)0, (T)0, (T)0};
   if (P.integrator == CBM_INT_EM) {
     T xi_n[3] = {(T)0, (T)0, (T)0};
     cbm_normals(P.seed, P.ctr->step[p], (uint32_t)i, CBM_STREAM_NOISE, P.community, D, xi_n);
@@ -654,19 +796,16 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
 #pragma unroll
     for (int d = 0; d < D; ++d) xn[d] = xi[d] + dv[d] * P.dt;
   }
-#pragma unroll
-  for (int d = 0; d < D; ++d) P.pos_nxt[d][i] = xn[d];
-  if (P.growth) P.v_nxt[i] = P.v_cur[i] + P.g[i] * P.dt;
-  else P.v_nxt[i] = P.v_cur[i];
-  if (P.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT || P.neighbors == CBM_NEIGH_CLVD) {
+  P.PB[s] = from3<T>(xn);
+  P.VB[s] = P.growth ? P.VA[s] + ld(P.G + i) * P.dt : P.VA[s];
+  P.IB[s] = i;
+  if (is_verlet(P)) {
     // verletDisplacement (neighbors.jl:367-391) on the new positions; when
     // agents are added or removed the flag is already set, so checking the
     // pre-compaction positions decides the same rebuild.
-    T e = xn[0] - P.pos_old[0][i];
-    T s = e * e;
-    if (D > 1) { e = xn[1] - P.pos_old[1][i]; s = s + e * e; }
-    if (D > 2) { e = xn[2] - P.pos_old[2][i]; s = s + e * e; }
-    if (sqrt(s) >= P.rebuild_thr) P.ctr->flag[p] = 1;
+    T xo[3];
+    to3<T>(P.POLD[s], xo);
+    if (dist<T, D>(xn, xo) >= P.rebuild_thr) P.ctr->flag[p] = 1;
   }
 }
 
@@ -705,284 +844,257 @@ __global__ void __launch_bounds__(kTile) k_medium_de(Params<T> P) {
 // update!: tail-fill compaction (kernelListSurvived + kernelFillHolesParameters,
 // src/CommunityStructure/update.jl:15-119).  The k-th hole (ascending) takes
 // the k-th survivor counted from the tail when the hole lies before it, which
-// is the serial reference's permutation.
+// is the serial reference's permutation.  Agent constants move in index
+// order; slot-ordered variables keep their slot and get relabelled.
 // ---------------------------------------------------------------------------
+constexpr int kCompactThreads = 1024;
+
+// One block.  Survivors that fill holes all lie in the tail [N_new, N + NAdd)
+// and holes before N_new are exactly as many, so the tail is walked from its
+// end in chunks, survivors are ranked by a block scan, and the k-th survivor
+// from the tail moves into the k-th hole.
 template <typename T, int D>
-__global__ void __launch_bounds__(kTile) k_compact(Params<T> P) {
+__global__ void __launch_bounds__(kCompactThreads) k_compact(Params<T> P) {
+  __shared__ int warp_sums[kCompactThreads / 32];
+  __shared__ int s_total;
   const int p = P.parity;
   const Counters* C = P.ctr;
   const long long N = C->N[p];
   const long long R = C->n_remove;
   const long long total = N + C->n_add;
-  const long long surv = total - R;
-  const long long fills = R < surv ? R : surv;
-  for (long long k = blockIdx.x * (long long)kTile + threadIdx.x; k < fills;
-       k += (long long)gridDim.x * kTile) {
-    // survivor with tail rank k: the largest q with #survivors in [q, total) >= k + 1,
-    // #survivors in [q, total) = (total - q) - (R - #holes < q)
-    long long lo = 0, hi = total - 1;
-    while (lo < hi) {
-      long long mid = (lo + hi + 1) >> 1;
-      long long a = 0, b = R;  // lower_bound of mid in holes
-      while (a < b) {
-        long long m = (a + b) >> 1;
-        if (P.holes[m] < mid) a = m + 1; else b = m;
+  const long long n_new = total - R;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  for (long long k = tid; k < R; k += kCompactThreads)
+    P.IB[P.inv[P.holes[k]]] = -1;  // every dead agent's slot leaves the sort
+  long long offset = 0;            // survivors already ranked
+  for (long long base = 0; base < total - n_new; base += kCompactThreads) {
+    const long long q = total - 1 - base - tid;
+    bool live = false;
+    if (q >= n_new) {
+      live = true;
+      if (q < N) {
+        const int f = P.fate[q];
+        live = !(f == 1 || f == 2);
       }
-      long long s = (total - mid) - (R - a);
-      if (s >= k + 1) lo = mid; else hi = mid - 1;
     }
-    const int src = (int)lo, dst = P.holes[k];
-    if (dst < src) {
+    // exclusive block scan of `live`
+    unsigned bal = __ballot_sync(kFull, live);
+    int in_warp = __popc(bal & ((1u << lane) - 1u));
+    if (lane == 0) warp_sums[w] = __popc(bal);
+    __syncthreads();
+    if (w == 0) {
+      int v = warp_sums[lane];
+      int x = v;
 #pragma unroll
-      for (int d = 0; d < D; ++d) P.pos_nxt[d][dst] = P.pos_nxt[d][src];
-      P.v_nxt[dst] = P.v_nxt[src];
-      if (P.force_mode == CBM_FORCE_LAGGED) {
-#pragma unroll
-        for (int d = 0; d < D; ++d) P.f_nxt[d][dst] = P.f_nxt[d][src];
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
       }
-      P.g[dst] = P.g[src];
-      P.id[dst] = P.id[src];
-      P.parent[dst] = P.parent[src];
+      warp_sums[lane] = x - v;
+      if (lane == 31) s_total = x;
     }
+    __syncthreads();
+    if (live) {
+      const long long k = offset + warp_sums[w] + in_warp;  // tail rank of q
+      if (k < R) {
+        const int dst = P.holes[k];
+        const int src = (int)q;
+        if (dst < src) {
+          P.G[dst] = P.G[src];
+          P.ID[dst] = P.ID[src];
+          P.PAR[dst] = P.PAR[src];
+          // newborns sit in working slot == index; survivors in their A slot
+          P.IB[src < N ? P.inv[src] : src] = dst;
+        }
+      }
+    }
+    offset += s_total;
+    __syncthreads();
   }
 }
 
-// N <- N + NAdd - NRemove, t += dt, step += 1 (update.jl:201-298).  One thread.
+// N <- N + NAdd - NRemove, t += dt, step += 1 (update.jl:201-298), and the
+// re-sort decision of computeNeighbors!.  One thread.
 template <typename T>
 __global__ void k_commit(Params<T> P) {
   Counters* C = P.ctr;
   const int p = P.parity;
+  C->slots = C->N[p] + C->n_add;
   C->N[p ^ 1] = C->N[p] + C->n_add - C->n_remove;
   C->n_add = 0;
   C->n_remove = 0;
   C->t[p ^ 1] = C->t[p] + (double)P.dt;
   C->step[p ^ 1] = C->step[p] + 1;
   C->flag[p ^ 1] = 0;
+  C->resort = (P.neighbors == CBM_NEIGH_CELL_LINKED || C->flag[p]) ? 1 : 0;
+  C->events = 0;
+  if (C->list_written) C->list_valid = 1;
+  C->list_written = 0;
 }
 
 // ---------------------------------------------------------------------------
-// computeNeighbors!: cell grid (counting sort, stable within a cell) and the
-// Verlet list.  Kernels see the positions and N committed by update! (parity
-// p ^ 1 of the step that ends) and do nothing unless a rebuild is due.
+// End of step: B -> A.  Without a re-sort the working slots are copied; with
+// one, live working slots are counting-sorted by (cell, agent index) into A
+// (the grid rebuild of computeNeighbors!, neighbors.jl:918-979, and the
+// compaction gather in one pass).
 // ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ bool rebuild_due(const Params<T>& P) {
-  if (P.neighbors == CBM_NEIGH_CELL_LINKED) return true;
-  return P.ctr->flag[P.parity] != 0;
-}
-
-// assignCells (neighbors.jl:763-821) + verletResetDisplacement (:438-487)
 template <typename T, int D>
-__global__ void __launch_bounds__(kTile) k_cells_hist(Params<T> P) {
-  if (!rebuild_due(P)) return;
-  const int N = (int)P.ctr->N[P.parity ^ 1];
-  const int i = blockIdx.x * kTile + threadIdx.x;
-  if (i == 0) {
-    // fresh tickets and tile-state generation for this build's k_cells_scan
-    P.ctr->scan_ticket = 0u;
-    P.ctr->scan_epoch = P.ctr->scan_epoch + 1u;
-  }
-  if (i >= N) return;
-  T x[3];
-  load_pos<T, D>(P.pos_nxt, i, x);
-  int c = cell_of<T, D>(P, x);
-  P.agent_cell[i] = c;
-  P.agent_rank[i] = atomicAdd(P.cell_count + c, 1);
-  if (P.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT || P.neighbors == CBM_NEIGH_CLVD) {
-#pragma unroll
-    for (int d = 0; d < D; ++d) P.pos_old[d][i] = x[d];
-  }
-}
-
-// exclusive scan of the cell counts (cumsum .- counts, neighbors.jl:934-937)
-// in one pass with decoupled look-back; counts are zeroed for the next build.
-template <typename T>
-__global__ void __launch_bounds__(kTile) k_cells_scan(Params<T> P) {
-  __shared__ int warp_sums[kTile / 32];
-  __shared__ unsigned s_tile;
-  __shared__ int s_prefix;
-  if (!rebuild_due(P)) return;
-  Counters* C = P.ctr;
-  const unsigned epoch = C->scan_epoch;
-  if (threadIdx.x == 0) s_tile = atomicAdd(&C->scan_ticket, 1u);
-  __syncthreads();
-  const int tile = (int)s_tile;
-  if (tile >= P.n_scan_tiles) {  // tickets were not reset: never index past the tile states
-    if (threadIdx.x == 0) atomicOr(&C->err, kErrTimeout);
+__global__ void __launch_bounds__(kTile) k_sort_hist(Params<T> P) {
+  const Counters* C = P.ctr;
+  const int s = blockIdx.x * kTile + threadIdx.x;
+  const long long slots = C->slots;
+  if (!C->resort) {
+    if (s < slots) {
+      P.PA[s] = P.PB[s];
+      P.VA[s] = P.VB[s];
+      if (P.force_mode == CBM_FORCE_LAGGED) P.FA[s] = P.FB[s];
+    }
     return;
   }
-  const int base = tile * kScanTile + threadIdx.x * kScanItems;
-  int vals[kScanItems];
-  int sum = 0;
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    int c = base + k;
-    vals[k] = c < P.n_cells ? P.cell_count[c] : 0;
-    sum += vals[k];
+  if (s == 0) {
+    P.ctr->scan_ticket = 0u;  // fresh tickets and tile-state generation for the scan
+    P.ctr->scan_epoch = C->scan_epoch + 1u;
   }
-  int total;
-  int ex = block_exscan(sum, warp_sums, &total);
-  // publish aggregate, look back, publish inclusive prefix
-  const unsigned long long ep = (unsigned long long)epoch << 32;
-  if (threadIdx.x == 0) {
-    if (tile == 0) {
-      s_prefix = 0;
-      atomicExch(P.scan_state + tile, ep | (2ull << 30) | (unsigned)total);
-    } else {
-      atomicExch(P.scan_state + tile, ep | (1ull << 30) | (unsigned)total);
-      int prefix = 0;
-      int t = tile - 1;
-      long long spins = 0;
-      while (t >= 0) {
-        unsigned long long s = atomicAdd(P.scan_state + t, 0ull);
-        unsigned flag = (unsigned)(s >> 30) & 3u;
-        if ((s >> 32) != epoch || flag == 0) {
-          if (++spins > kSpinLimit) {
-            atomicOr(&C->err, kErrTimeout);
-            break;
-          }
-          continue;
-        }
-        prefix += (int)(s & 0x3fffffffu);
-        if (flag == 2) break;
-        --t;
-      }
-      s_prefix = prefix;
-      atomicExch(P.scan_state + tile, ep | (2ull << 30) | (unsigned)(prefix + total));
-    }
+  if (s >= slots) return;
+  if (P.IB[s] < 0) {
+    P.s_cell[s] = -1;
+    return;
   }
-  __syncthreads();
-  int run = s_prefix + ex;
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    int c = base + k;
-    if (c < P.n_cells) {
-      P.cell_start[c] = run;
-      P.cell_count[c] = 0;
-    }
-    run += vals[k];
-  }
-  // the thread holding the last cell writes the end sentinel
-  if (base <= P.n_cells - 1 && P.n_cells - 1 < base + kScanItems) P.cell_start[P.n_cells] = run;
+  T x[3];
+  to3<T>(P.PB[s], x);
+  int c = cell_of_pos<T, D>(P, x);
+  P.s_cell[s] = c;
+  P.s_rank[s] = atomicAdd(P.cell_count + c, 1);
 }
 
-// sortAgentsInCells (neighbors.jl:837-899), first pass: scatter by the
-// atomic rank taken in k_cells_hist
 template <typename T>
-__global__ void __launch_bounds__(kTile) k_cells_scatter(Params<T> P) {
-  if (!rebuild_due(P)) return;
-  const int N = (int)P.ctr->N[P.parity ^ 1];
-  const int i = blockIdx.x * kTile + threadIdx.x;
-  if (i >= N) return;
-  P.cell_tmp[P.cell_start[P.agent_cell[i]] + P.agent_rank[i]] = i;
+__global__ void __launch_bounds__(kTile) k_sort_scatter(Params<T> P) {
+  const Counters* C = P.ctr;
+  if (!C->resort) return;
+  const int s = blockIdx.x * kTile + threadIdx.x;
+  if (s >= C->slots) return;
+  const int c = P.s_cell[s];
+  if (c < 0) return;
+  P.s_key[P.cell_start[c] + P.s_rank[s]] = P.IB[s];
 }
 
-// second pass: place every agent by its rank among the cell's agents with a
-// smaller index, so agents are ascending within each cell as in the serial
-// CPU reference (neighbors.jl:851-862)
-template <typename T>
-__global__ void __launch_bounds__(kTile) k_cells_stable(Params<T> P) {
-  if (!rebuild_due(P)) return;
-  const int N = (int)P.ctr->N[P.parity ^ 1];
-  const int i = blockIdx.x * kTile + threadIdx.x;
-  if (i >= N) return;
-  const int c = P.agent_cell[i];
+template <typename T, int D>
+__global__ void __launch_bounds__(kTile) k_sort_place(Params<T> P) {
+  const Counters* C = P.ctr;
+  if (!C->resort) return;
+  const int s = blockIdx.x * kTile + threadIdx.x;
+  if (s == 0) P.ctr->list_valid = 0;
+  if (s >= C->slots) return;
+  const int c = P.s_cell[s];
+  if (c < 0) return;
+  const int key = P.IB[s];
   const int s0 = P.cell_start[c], s1 = P.cell_start[c + 1];
   int r = 0;
-  for (int s = s0; s < s1; ++s) r += ld(P.cell_tmp + s) < i;
-  P.cell_agents[s0 + r] = i;
+  for (int q = s0; q < s1; ++q) r += ld(P.s_key + q) < key;
+  const int ns = s0 + r;
+  const typename V4T<T>::type x = P.PB[s];
+  P.PA[ns] = x;
+  P.VA[ns] = P.VB[s];
+  if (P.force_mode == CBM_FORCE_LAGGED) P.FA[ns] = P.FB[s];
+  P.IA[ns] = key;
+  P.inv[key] = ns;
+  P.cell_of_slot[ns] = c;
+  if (is_verlet(P)) P.POLD[ns] = x;  // verletResetDisplacement (neighbors.jl:438-487)
 }
 
-// Verlet list over the cell grid: CLVD in cell order (verletNeighborsCLVD,
-// neighbors.jl:1071-1131); VerletDisplacement sorted ascending
-// (verletNeighbors, :92-133)
+// Verlet list of the committed slots over the grid: CLVD in cell order
+// (verletNeighborsCLVD, neighbors.jl:1071-1131); VerletDisplacement ascending
+// in agent index (verletNeighbors, :92-133).  Entries are slots.
 constexpr int kVdSortMax = 256;
 
 template <typename T, int D>
-__global__ void __launch_bounds__(kTile) k_verlet_list(Params<T> P) {
-  if (!rebuild_due(P)) return;
-  const int N = (int)P.ctr->N[P.parity ^ 1];
-  const int i = blockIdx.x * kTile + threadIdx.x;
-  if (i >= N) return;
+__global__ void __launch_bounds__(kTile) k_verlet_list(Params<T> P, int only_if_resorted) {
+  if (only_if_resorted && !P.ctr->resort) return;
+  const int N = (int)P.ctr->N[P.parity];
+  const int s = blockIdx.x * kTile + threadIdx.x;
+  if (s == 0) P.ctr->list_valid = 1;
+  if (s >= N) return;
   T xi[3];
-  load_pos<T, D>(P.pos_nxt, i, xi);
-  const T skin = P.skin;
+  to3<T>(P.PA[s], xi);
   const int M = P.max_nbrs;
   int n = 0;
   bool over = false;
-  int q[3];
-  cell_coords<D>(P.n_cells_d, cell_of<T, D>(P, xi), q);
-  constexpr int nk = D == 1 ? 3 : (D == 2 ? 9 : 27);
-  for (int k = 0; k < nk; ++k) {
-    int pn = cell_neigh<D>(P.n_cells_d, q, k);
-    if (pn < 0) continue;
-    int s0 = ld(P.cell_start + pn), s1 = ld(P.cell_start + pn + 1);
-    for (int s = s0; s < s1; ++s) {
-      int j = ld(P.cell_agents + s);
-      if (j == i) continue;
-      T e = xi[0] - ld(P.pos_nxt[0] + j);
-      T s2 = e * e;
-      if (D > 1) { e = xi[1] - ld(P.pos_nxt[1] + j); s2 = s2 + e * e; }
-      if (D > 2) { e = xi[2] - ld(P.pos_nxt[2] + j); s2 = s2 + e * e; }
-      if (sqrt(s2) < skin) {
-        if (n < M) P.nbr_list[(size_t)n * P.n_max + i] = j;
-        else over = true;
-        ++n;
-      }
+  walk_cells<T, D>(P, P.PA, xi, P.skin_reach, [&](int q, const typename V4T<T>::type& v) {
+    if (q == s) return;
+    T xj[3];
+    to3<T>(v, xj);
+    if (dist<T, D>(xi, xj) < P.skin) {
+      if (n < M) P.nbr_list[(size_t)n * P.n_max + s] = q;
+      else over = true;
+      ++n;
     }
-  }
+  });
   if (over) atomicOr(&P.ctr->err, kErrNeighborOverflow);
   n = n < M ? n : M;
   if (P.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT && n > 1) {
-    // insertion sort of the row (ascending j, the O(N^2) reference's order)
+    // insertion sort of the row by agent index (the O(N^2) reference's order)
     for (int a = 1; a < n; ++a) {
-      int key = P.nbr_list[(size_t)a * P.n_max + i];
+      int keyslot = P.nbr_list[(size_t)a * P.n_max + s];
+      int key = P.IA[keyslot];
       int b = a - 1;
-      while (b >= 0 && P.nbr_list[(size_t)b * P.n_max + i] > key) {
-        P.nbr_list[(size_t)(b + 1) * P.n_max + i] = P.nbr_list[(size_t)b * P.n_max + i];
+      while (b >= 0 && P.IA[P.nbr_list[(size_t)b * P.n_max + s]] > key) {
+        P.nbr_list[(size_t)(b + 1) * P.n_max + s] = P.nbr_list[(size_t)b * P.n_max + s];
         --b;
       }
-      P.nbr_list[(size_t)(b + 1) * P.n_max + i] = key;
+      P.nbr_list[(size_t)(b + 1) * P.n_max + s] = keyslot;
     }
   }
-  P.nbr_n[i] = n;
+  P.nbr_n[s] = n;
 }
 
 // ---------------------------------------------------------------------------
-// helpers for the host API
+// host exchange and inspection
 // ---------------------------------------------------------------------------
-// the neighbor-counting rule of test/testCommunity.jl:359-415 on committed x
+// index-ordered staging -> working slots (identity), before the first sort
 template <typename T, int D>
-__global__ void __launch_bounds__(kTile) k_count_neighbors(Params<T> P, T radius, int* out) {
-  const int N = (int)P.ctr->N[P.parity];
+__global__ void __launch_bounds__(kTile) k_pack_upload(Params<T> P, int N) {
   const int i = blockIdx.x * kTile + threadIdx.x;
   if (i >= N) return;
-  T xi[3];
-  load_pos<T, D>(P.pos_cur, i, xi);
-  int n = 0;
-  for_neighbors<T, D>(P, xi, i, N, [&](int j) {
-    T e = xi[0] - P.pos_cur[0][j];
-    T s2 = e * e;
-    if (D > 1) { e = xi[1] - P.pos_cur[1][j]; s2 = s2 + e * e; }
-    if (D > 2) { e = xi[2] - P.pos_cur[2][j]; s2 = s2 + e * e; }
-    if (sqrt(s2) < radius) ++n;
-  });
-  out[i] = n;
-}
-
-// committed -> written copies for a stage that was skipped within a step
-template <typename T, int D>
-__global__ void __launch_bounds__(kTile) k_copy_agents(Params<T> P) {
-  const int N = (int)P.ctr->N[P.parity];
-  const int i = blockIdx.x * kTile + threadIdx.x;
-  if (i >= N) return;
-  T* const* U = P.walls == CBM_WALLS_REFLECT ? P.pos_u : P.pos_cur;
+  T x[3] = {(T)0, (T)0, (T)0}, f[3] = {(T)0, (T)0, (T)0};
 #pragma unroll
   for (int d = 0; d < D; ++d) {
-    P.pos_nxt[d][i] = U[d][i];
-    P.f_nxt[d][i] = P.f_cur[d][i];
+    x[d] = P.hx[d][i];
+    f[d] = P.hf[d][i];
   }
-  P.v_nxt[i] = P.v_cur[i];
+  P.PB[i] = from3<T>(x);
+  P.FB[i] = from3<T>(f);
+  P.VB[i] = P.hv[i];
+  P.IB[i] = i;
+}
+
+// slot-ordered set (which: 0 committed A, 1 written B, 2 reflected U) ->
+// index-ordered staging
+template <typename T, int D>
+__global__ void __launch_bounds__(kTile) k_gather_download(Params<T> P, int N, int which) {
+  const int i = blockIdx.x * kTile + threadIdx.x;
+  if (i >= N) return;
+  const int s = P.inv[i];
+  T x[3], f[3];
+  to3<T>(which == 0 ? P.PA[s] : (which == 1 ? P.PB[s] : P.U[s]), x);
+  to3<T>(which == 1 ? P.FB[s] : P.FA[s], f);
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    P.hx[d][i] = x[d];
+    P.hf[d][i] = f[d];
+  }
+  P.hv[i] = which == 1 ? P.VB[s] : P.VA[s];
+}
+
+// committed -> working slots, for an update! without a DE stage
+template <typename T, int D>
+__global__ void __launch_bounds__(kTile) k_copy_ab(Params<T> P, int use_u) {
+  const int N = (int)P.ctr->N[P.parity];
+  const int s = blockIdx.x * kTile + threadIdx.x;
+  if (s >= N) return;
+  P.PB[s] = use_u ? P.U[s] : P.PA[s];
+  P.VB[s] = P.VA[s];
+  P.FB[s] = P.FA[s];
+  P.IB[s] = P.IA[s];
 }
 
 template <typename T, int D>
@@ -992,6 +1104,42 @@ __global__ void __launch_bounds__(kTile) k_copy_medium(Params<T> P, int grad_onl
   if (!grad_only) P.c_nxt[n] = P.c_cur[n];
 #pragma unroll
   for (int d = 0; d < D; ++d) P.grad_nxt[d][n] = P.grad_cur[d][n];
+}
+
+// the neighbor-counting rule of test/testCommunity.jl:359-415 on committed x
+template <typename T, int D>
+__global__ void __launch_bounds__(kTile) k_count_neighbors(Params<T> P, T radius, int* out) {
+  const int N = (int)P.ctr->N[P.parity];
+  const int i = blockIdx.x * kTile + threadIdx.x;
+  if (i >= N) return;
+  const int s = P.inv[i];
+  T xi[3];
+  to3<T>(P.PA[s], xi);
+  int n = 0;
+  auto visit = [&](int q) {
+    T xj[3];
+    to3<T>(P.PA[q], xj);
+    if (dist<T, D>(xi, xj) < radius) ++n;
+  };
+  if (P.neighbors == CBM_NEIGH_FULL) {
+    for (int j = 0; j < N; ++j)
+      if (j != i) visit(P.inv[j]);
+  } else if (P.neighbors == CBM_NEIGH_CELL_LINKED) {
+    for_cell_slots<T, D>(P, xi, [&](int q) {
+      if (q != s) visit(q);
+    });
+  } else if (is_verlet(P) && P.ctr->list_valid) {
+    const int m = P.nbr_n[s];
+    for (int k = 0; k < m; ++k) visit(P.nbr_list[(size_t)k * P.n_max + s]);
+  } else if (P.neighbors == CBM_NEIGH_CLVD) {
+    for_cell_slots<T, D>(P, xi, [&](int q) {
+      if (q == s) return;
+      T xj[3];
+      to3<T>(P.PA[q], xj);
+      if (dist<T, D>(xi, xj) < P.skin) visit(q);
+    });
+  }
+  out[i] = n;
 }
 
 template <typename T>

@@ -16,7 +16,7 @@
 #include <string>
 
 #include "../../include/cbm_b200.h"
-#include "cbm_kernels.cuh"
+#include "cbm_grid.cuh"
 
 using namespace cbm;
 
@@ -62,35 +62,33 @@ template <typename T, int D>
 void launch(const void* const* pos, int n, const double* lo, const double* hi, double edge,
             const int* ncd, int n_cells, int32_t* agent_cell, int32_t* cell_start,
             int32_t* cell_agents, unsigned char* base, cudaStream_t st) {
-  Params<T> P;
-  memset(&P, 0, sizeof P);
+  GridParams<T> G;
+  memset(&G, 0, sizeof G);
   for (int d = 0; d < 3; ++d) {
-    P.pos_nxt[d] = d < D ? (T*)pos[d] : nullptr;
-    P.box_lo[d] = (T)lo[d];
-    P.box_hi[d] = (T)hi[d];
-    P.n_cells_d[d] = ncd[d];
+    G.pos[d] = d < D ? (const T*)pos[d] : nullptr;
+    G.box_lo[d] = (T)lo[d];
+    G.box_hi[d] = (T)hi[d];
+    G.n_cells_d[d] = ncd[d];
   }
-  P.edge = (T)edge;
-  P.neighbors = CBM_NEIGH_CELL_LINKED;  // rebuild unconditionally
-  P.parity = 1;                         // kernels read N[0] and pos_nxt
-  P.n_max = n;
-  P.n_cells = n_cells;
-  P.n_scan_tiles = (n_cells + kScanTile - 1) / kScanTile;
-  P.ctr = (Counters*)base;
-  P.cell_count = (int*)(base + kCountOff);
-  P.agent_rank = (int*)(base + kRankOff);
-  P.cell_tmp = (int*)(base + kTmpOff);
-  P.scan_state = (unsigned long long*)(base + kScanOff);
-  P.agent_cell = agent_cell;
-  P.cell_start = cell_start;
-  P.cell_agents = cell_agents;
-  const int nb = (n + kTile - 1) / kTile > 0 ? (n + kTile - 1) / kTile : 1;
-  k_noalloc_setup<<<1, 1, 0, st>>>(P.ctr, n);
-  cudaMemsetAsync(P.cell_count, 0, (size_t)n_cells * 4, st);
-  k_cells_hist<T, D><<<nb, kTile, 0, st>>>(P);
-  k_cells_scan<T><<<P.n_scan_tiles, kTile, 0, st>>>(P);
-  k_cells_scatter<T><<<nb, kTile, 0, st>>>(P);
-  k_cells_stable<T><<<nb, kTile, 0, st>>>(P);
+  G.n = n;
+  G.edge = (T)edge;
+  G.n_cells = n_cells;
+  G.n_scan_tiles = (n_cells + kScanTile - 1) / kScanTile;
+  G.ctr = (Counters*)base;
+  G.cell_count = (int*)(base + kCountOff);
+  G.agent_rank = (int*)(base + kRankOff);
+  G.cell_tmp = (int*)(base + kTmpOff);
+  G.scan_state = (unsigned long long*)(base + kScanOff);
+  G.agent_cell = agent_cell;
+  G.cell_start = cell_start;
+  G.cell_agents = cell_agents;
+  const int nb = n > 0 ? (n + kTile - 1) / kTile : 1;
+  k_noalloc_setup<<<1, 1, 0, st>>>(G.ctr, n);
+  cudaMemsetAsync(G.cell_count, 0, (size_t)n_cells * 4, st);
+  k_grid_hist<T, D><<<nb, kTile, 0, st>>>(G);
+  k_scan_cells<<<G.n_scan_tiles, kTile, 0, st>>>(grid_scan_args(G));
+  k_grid_scatter<T><<<nb, kTile, 0, st>>>(G);
+  k_grid_stable<T><<<nb, kTile, 0, st>>>(G);
 }
 
 }  // namespace

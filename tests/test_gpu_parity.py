@@ -248,11 +248,20 @@ def test_agent_overflow_reported(gpu_lib, abi):
 
 
 def test_neighbor_overflow_reported(gpu_lib, abi):
-    kw, st = colony_3d(abi, N=400, R=3.0, L=20.0, p_death=0.0, precision=abi.F64)
+    kw, st = colony_3d(abi, N=400, R=3.0, L=20.0, p_death=0.0, precision=abi.F64,
+                       neighbors=abi.NEIGH_VERLET_DISPLACEMENT)
     kw["n_max_neighbors"] = 4
+    # VerletDisplacement builds its list at load
     with pytest.raises(cbm.CbmError) as e:
         g = cbm.Context(abi.make_config(**kw))
         g.upload(st)
+    assert e.value.code == abi.CBM_ERR_NEIGHBOR_OVERFLOW
+    # CLVD builds its list when it is first needed
+    kw["neighbors"] = abi.NEIGH_CLVD
+    g = cbm.Context(abi.make_config(**kw))
+    g.upload(st)
+    with pytest.raises(cbm.CbmError) as e:
+        g.neighbors()
     assert e.value.code == abi.CBM_ERR_NEIGHBOR_OVERFLOW
 
 
