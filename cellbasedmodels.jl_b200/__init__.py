@@ -25,12 +25,12 @@ from types import SimpleNamespace
 import numpy as np
 
 from . import _abi
-from ._abi import (CbmConfig, CbmError, Context, load_library, make_config)  # noqa: F401
+from ._abi import (Batch, CbmConfig, CbmError, Context, load_library, make_config)  # noqa: F401
 
 __all__ = ["ABM", "Community", "evolve", "step", "loadToPlatform", "bringFromPlatform",
            "agentStepRule", "agentStepDE", "mediumStepRule", "mediumStepDE", "update",
            "computeNeighbors", "CBMNeighbors", "CBMIntegrators", "SoftSpheres", "Growth",
-           "Medium", "B200", "Context", "CbmError", "make_config", "load_library"]
+           "Medium", "B200", "Context", "Batch", "CbmError", "make_config", "load_library"]
 
 
 # ---- algorithm descriptors (src/neighbors.jl, src/integrators.jl) -------------

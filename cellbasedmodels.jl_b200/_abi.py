@@ -322,3 +322,107 @@ class Context:
         n = C.c_int32()
         self._check(self.lib.cbm_profile_step(self.h, 64, ms, names, C.byref(n)))
         return [(names[i].decode(), ms[i]) for i in range(min(n.value, 64))]
+
+
+# ---- batched communities (cbm_batch_*) --------------------------------------
+class CbmCommunityDesc(C.Structure):
+    _fields_ = [("n", C.c_int64), ("box_lo", C.c_double * 3), ("box_hi", C.c_double * 3),
+                ("k_rep", C.c_double), ("r_rep", C.c_double), ("k_att", C.c_double),
+                ("r_att", C.c_double), ("sigma", C.c_double), ("community", C.c_uint32),
+                ("pad", C.c_int32)]
+
+
+class CbmBatchTuning(C.Structure):
+    _fields_ = [("threads", C.c_int32), ("ctas_per_sm", C.c_int32), ("skin", C.c_double),
+                ("rebuild_threshold", C.c_double)]
+
+    def as_dict(self):
+        return dict(threads=self.threads, ctas_per_sm=self.ctas_per_sm, skin=self.skin,
+                    rebuild_threshold=self.rebuild_threshold)
+
+
+def _bind_batch(lib):
+    if getattr(lib, "_batch_bound", False):
+        return
+    vp, i32 = C.c_void_p, C.c_int32
+    sig = {
+        "cbm_batch_create": (C.c_int, [C.POINTER(vp), C.POINTER(CbmConfig), i32,
+                                       C.POINTER(CbmCommunityDesc)]),
+        "cbm_batch_destroy": (None, [vp]),
+        "cbm_batch_last_error": (C.c_char_p, [vp]),
+        "cbm_batch_upload": (C.c_int, [vp, i32, C.POINTER(CbmStateView)]),
+        "cbm_batch_download": (C.c_int, [vp, i32, C.POINTER(CbmStateView)]),
+        "cbm_batch_step": (C.c_int, [vp, i32, i32]),
+        "cbm_batch_set_tuning": (C.c_int, [vp, C.POINTER(CbmBatchTuning)]),
+        "cbm_batch_get_tuning": (C.c_int, [vp, C.POINTER(CbmBatchTuning)]),
+        "cbm_batch_autotune": (C.c_int, [vp, i32, C.POINTER(CbmBatchTuning)]),
+        "cbm_batch_stream": (vp, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    lib._batch_bound = True
+
+
+class Batch:
+    """Many independent 3D communities advanced by one persistent launch."""
+
+    def __init__(self, base_cfg, descs):
+        self.lib = load_library()
+        _bind_batch(self.lib)
+        arr = (CbmCommunityDesc * len(descs))(*descs)
+        h = C.c_void_p()
+        rc = self.lib.cbm_batch_create(C.byref(h), C.byref(base_cfg), len(descs), arr)
+        if rc != CBM_OK:
+            raise CbmError(rc, self.lib.cbm_batch_last_error(None).decode())
+        self.h = h
+        self.cfg = base_cfg
+        self.sizes = [int(d.n) for d in descs]
+
+    def _check(self, rc):
+        if rc != CBM_OK:
+            raise CbmError(rc, self.lib.cbm_batch_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cbm_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def upload(self, c, x, y, z, step=0):
+        x, y, z = (np.ascontiguousarray(a, dtype=np.float32) for a in (x, y, z))
+        s = CbmStateView()
+        s.N, s.capacity, s.step = len(x), len(x), step
+        s.pos[0], s.pos[1], s.pos[2] = x.ctypes.data, y.ctypes.data, z.ctypes.data
+        self._check(self.lib.cbm_batch_upload(self.h, c, C.byref(s)))
+
+    def download(self, c):
+        n = self.sizes[c]
+        out = {k: np.zeros(max(n, 1), np.float32) for k in "xyz"}
+        s = CbmStateView()
+        s.capacity = n
+        s.pos[0], s.pos[1], s.pos[2] = (out[k].ctypes.data for k in "xyz")
+        self._check(self.lib.cbm_batch_download(self.h, c, C.byref(s)))
+        return {k: v[:n] for k, v in out.items()} | {"step": s.step, "N": n}
+
+    def step(self, n, flags=SYNC):
+        self._check(self.lib.cbm_batch_step(self.h, n, flags))
+
+    def tuning(self):
+        t = CbmBatchTuning()
+        self._check(self.lib.cbm_batch_get_tuning(self.h, C.byref(t)))
+        return t
+
+    def set_tuning(self, threads, ctas_per_sm, skin, rebuild_threshold=0.0):
+        t = CbmBatchTuning(threads, ctas_per_sm, skin, rebuild_threshold)
+        self._check(self.lib.cbm_batch_set_tuning(self.h, C.byref(t)))
+
+    def autotune(self, trial_steps=20):
+        t = CbmBatchTuning()
+        self._check(self.lib.cbm_batch_autotune(self.h, trial_steps, C.byref(t)))
+        return t
+
+    def stream(self):
+        return self.lib.cbm_batch_stream(self.h)

@@ -13,9 +13,11 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libcbm_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "cbm_api.cu"), os.path.join(HERE, "csrc", "cbm_noalloc.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("cbm_api.cu", "cbm_batch.cu", "cbm_noalloc.cu")]
 DEPS = SOURCES + [
     os.path.join(HERE, "csrc", "cbm_kernels.cuh"),
+    os.path.join(HERE, "csrc", "cbm_common.cuh"),
+    os.path.join(HERE, "csrc", "cbm_grid.cuh"),
     os.path.join(HERE, "..", "include", "cbm_b200.h"),
     os.path.join(HERE, "..", "include", "cbm_rng.h"),
 ]

@@ -231,6 +231,54 @@ int cbm_kernels_per_step(cbm_ctx* ctx);
 int cbm_profile_step(cbm_ctx* ctx, int32_t max_kernels, float* ms, const char** names,
                      int32_t* n_kernels);
 
+/* ---- batched communities ----------------------------------------------------
+ * Many independent communities (parameter sweeps, model fitting: the
+ * reference's fitting drivers run one whole simulation per parameter set,
+ * src/fitting/gridSearch.jl:19-65) advanced by one persistent kernel, each
+ * step count captured as one CUDA graph.  Every community is a 3D Float32
+ * soft-sphere community with Euler-Maruyama noise and CLVD neighbors whose
+ * trajectory is bit-identical to the plain path (cbm_create) with
+ * neighbors = CLVD, skin = cell_edge = cutoff + tuning.skin,
+ * rebuild_threshold = tuning.skin / 2 (unless set) and the same `community`.
+ * The base configuration gives dims = 3, precision = CBM_F32,
+ * integrator = CBM_INT_EM, neighbors = CBM_NEIGH_CLVD, dt, seed,
+ * n_max_neighbors, and an initial skin (list radius) and rebuild threshold. */
+typedef struct cbm_community_desc {
+  int64_t n;             /* agents (fixed: no division or death) */
+  double box_lo[3];
+  double box_hi[3];
+  double k_rep, r_rep, k_att, r_att; /* force parameters, as in cbm_config */
+  double sigma;          /* EM noise amplitude */
+  uint32_t community;    /* index in the random stream */
+  int32_t pad;
+} cbm_community_desc;
+
+typedef struct cbm_batch_tuning {
+  int32_t threads;       /* threads per CTA (one CTA runs one community): 128..1024 */
+  int32_t ctas_per_sm;   /* resident CTAs per SM of the persistent grid */
+  double skin;           /* Verlet skin: list radius = cutoff + skin */
+  double rebuild_threshold; /* displacement that triggers a rebuild; <= 0: skin / 2 */
+} cbm_batch_tuning;
+
+typedef struct cbm_batch cbm_batch;
+
+int cbm_batch_create(cbm_batch** out, const cbm_config* base, int32_t n_communities,
+                     const cbm_community_desc* communities);
+void cbm_batch_destroy(cbm_batch* b);
+const char* cbm_batch_last_error(const cbm_batch* b);
+/* loadToPlatform! / bringFromPlatform! of community c (positions only) */
+int cbm_batch_upload(cbm_batch* b, int32_t c, const cbm_state_view* host);
+int cbm_batch_download(cbm_batch* b, int32_t c, cbm_state_view* host);
+/* nsteps steps of every community in one persistent launch (graph replay
+ * unless CBM_NO_GRAPH); CBM_SYNC waits and reports device flags */
+int cbm_batch_step(cbm_batch* b, int32_t nsteps, int32_t flags);
+int cbm_batch_set_tuning(cbm_batch* b, const cbm_batch_tuning* tuning);
+int cbm_batch_get_tuning(cbm_batch* b, cbm_batch_tuning* tuning);
+/* Times trial_steps on a copy of the current state for every candidate
+ * (threads x CTAs per SM x skin), keeps the fastest and restores the state. */
+int cbm_batch_autotune(cbm_batch* b, int32_t trial_steps, cbm_batch_tuning* best);
+void* cbm_batch_stream(cbm_batch* b);
+
 /* ---- allocation-free cell grid -------------------------------------------
  * This entry point has no counterpart in the reference.  It is for callers
  * that cannot allocate device memory when they need a grid: code running

@@ -77,3 +77,49 @@ def chemotaxis_2d(abi, N=200000, L=1024.0, n_medium=1024, seed=3, bilinear=True,
               medium_sampling=abi.MEDIUM_BILINEAR if bilinear else abi.MEDIUM_NEAREST)
     state = dict(x=rng.uniform(0, L, N), y=rng.uniform(0, L, N))
     return kw, state
+
+
+def batched_sweep(abi, n_comm=512, n_lo=500, n_hi=20000, seed=4, dt=0.01, skin=0.3):
+    """Parameter sweep: n_comm 3D soft-sphere communities, N_i ~ U[n_lo, n_hi],
+    k, a, sigma each log-uniform in [0.3, 3] x (10, 1, 0.05), r = 1, cube side
+    2.5 N_i^(1/3), positions uniform in the cube, EM, Float32.
+    Returns (base config kwargs, community descriptor kwargs, initial states)."""
+    rng = np.random.default_rng(seed)
+    base = dict(dims=3, precision=abi.F32, n_max=1, dt=dt, seed=seed, neighbors=abi.NEIGH_CLVD,
+                integrator=abi.INT_EM, n_max_neighbors=48, skin=3.0 + skin, cell_edge=3.0 + skin,
+                rebuild_threshold=skin / 2, k_rep=10.0, r_rep=2.0, k_att=1.0, r_att=3.0)
+    descs, states = [], []
+    for c in range(n_comm):
+        n = int(rng.integers(n_lo, n_hi + 1))
+        L = 2.5 * n ** (1 / 3)
+        f = np.exp(rng.uniform(np.log(0.3), np.log(3.0), 3))
+        descs.append(dict(n=n, box_lo=(0.0, 0.0, 0.0), box_hi=(L, L, L), k_rep=10.0 * f[0],
+                          r_rep=2.0, k_att=1.0 * f[1], r_att=3.0, sigma=0.05 * f[2], community=c))
+        p = rng.uniform(0, L, size=(3, n))
+        states.append(dict(x=p[0], y=p[1], z=p[2]))
+    return base, descs, states
+
+
+def plain_config_for(abi, base, desc, tuning):
+    """The plain-path configuration whose trajectory a batched community reproduces."""
+    R = max(desc["r_rep"], desc["r_att"]) + tuning["skin"]
+    thr = tuning["rebuild_threshold"] if tuning["rebuild_threshold"] > 0 else tuning["skin"] / 2
+    return dict(dims=3, precision=abi.F32, n_max=desc["n"], box_lo=desc["box_lo"],
+                box_hi=desc["box_hi"], dt=base["dt"], seed=base["seed"],
+                community=desc["community"], neighbors=abi.NEIGH_CLVD, skin=R, cell_edge=R,
+                rebuild_threshold=thr, n_max_neighbors=base["n_max_neighbors"],
+                integrator=abi.INT_EM, sigma=desc["sigma"], k_rep=desc["k_rep"],
+                r_rep=desc["r_rep"], k_att=desc["k_att"], r_att=desc["r_att"])
+
+
+def make_descs(abi, descs):
+    out = []
+    for d in descs:
+        x = abi.CbmCommunityDesc()
+        x.n = d["n"]
+        x.box_lo = (C_double3 := type(x.box_lo))(*d["box_lo"])
+        x.box_hi = C_double3(*d["box_hi"])
+        for k in ("k_rep", "r_rep", "k_att", "r_att", "sigma", "community"):
+            setattr(x, k, d[k])
+        out.append(x)
+    return out
