@@ -25,7 +25,8 @@ from types import SimpleNamespace
 import numpy as np
 
 from . import _abi
-from ._abi import (Batch, CbmConfig, CbmError, Context, load_library, make_config)  # noqa: F401
+from ._abi import (Adjoint, Batch, CbmConfig, CbmError, Context, load_library,  # noqa: F401
+                   make_config)
 
 __all__ = ["ABM", "Community", "evolve", "step", "loadToPlatform", "bringFromPlatform",
            "agentStepRule", "agentStepDE", "mediumStepRule", "mediumStepDE", "update",

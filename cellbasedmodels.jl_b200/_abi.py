@@ -426,3 +426,74 @@ class Batch:
 
     def stream(self):
         return self.lib.cbm_batch_stream(self.h)
+
+
+# ---- adjoint (cbm_adjoint_*) --------------------------------------------------
+class Adjoint:
+    """Gradients of mean((x_T - target)^2) w.r.t. (k_rep, k_att, r_rep) and x0."""
+
+    def __init__(self, cfg):
+        self.lib = load_library()
+        lib = self.lib
+        if not getattr(lib, "_adj_bound", False):
+            vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
+            for name, res, args in (
+                    ("cbm_adjoint_create", C.c_int, [C.POINTER(vp), C.POINTER(CbmConfig)]),
+                    ("cbm_adjoint_destroy", None, [vp]),
+                    ("cbm_adjoint_last_error", C.c_char_p, [vp]),
+                    ("cbm_adjoint_run", C.c_int, [vp, i64, C.POINTER(vp), i32, i32, C.POINTER(vp),
+                                                  C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                                  C.POINTER(vp), C.POINTER(vp)]),
+                    ("cbm_adjoint_forward", C.c_int, [vp, i64, C.POINTER(vp), i32, C.POINTER(vp)]),
+                    ("cbm_adjoint_stream", vp, [vp])):
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            lib._adj_bound = True
+        h = C.c_void_p()
+        rc = lib.cbm_adjoint_create(C.byref(h), C.byref(cfg))
+        if rc != CBM_OK:
+            raise CbmError(rc, lib.cbm_adjoint_last_error(None).decode())
+        self.h = h
+        self.cfg = cfg
+        self.dtype = real_dtype(cfg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cbm_adjoint_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def _arrs(self, xyz):
+        arrs = [np.ascontiguousarray(a, dtype=self.dtype) for a in xyz]
+        return arrs, (C.c_void_p * 3)(*[a.ctypes.data for a in arrs])
+
+    def run(self, x0, target, nsteps, checkpoint_every=20, want_dx0=True):
+        n = len(x0[0])
+        xs, xp = self._arrs(x0)
+        ts, tp = self._arrs(target)
+        dx = [np.zeros(n, self.dtype) for _ in range(3)]
+        xT = [np.zeros(n, self.dtype) for _ in range(3)]
+        dxp = (C.c_void_p * 3)(*[a.ctypes.data for a in dx]) if want_dx0 else None
+        xTp = (C.c_void_p * 3)(*[a.ctypes.data for a in xT])
+        loss = C.c_double()
+        g = (C.c_double * 3)()
+        rc = self.lib.cbm_adjoint_run(self.h, n, xp, nsteps, checkpoint_every, tp, C.byref(loss), g,
+                                      dxp, xTp)
+        if rc != CBM_OK:
+            raise CbmError(rc, self.lib.cbm_adjoint_last_error(self.h).decode())
+        return dict(loss=loss.value, dtheta=np.array(list(g)), dx0=dx if want_dx0 else None, xT=xT)
+
+    def forward(self, x0, nsteps):
+        n = len(x0[0])
+        xs, xp = self._arrs(x0)
+        xT = [np.zeros(n, self.dtype) for _ in range(3)]
+        xTp = (C.c_void_p * 3)(*[a.ctypes.data for a in xT])
+        rc = self.lib.cbm_adjoint_forward(self.h, n, xp, nsteps, xTp)
+        if rc != CBM_OK:
+            raise CbmError(rc, self.lib.cbm_adjoint_last_error(self.h).decode())
+        return xT
+
+    def stream(self):
+        return self.lib.cbm_adjoint_stream(self.h)

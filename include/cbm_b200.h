@@ -279,6 +279,32 @@ int cbm_batch_get_tuning(cbm_batch* b, cbm_batch_tuning* tuning);
 int cbm_batch_autotune(cbm_batch* b, int32_t trial_steps, cbm_batch_tuning* best);
 void* cbm_batch_stream(cbm_batch* b);
 
+/* ---- adjoint (differentiable trajectories) ---------------------------------
+ * Exact gradients of L = mean((x_T - target)^2) over a trajectory of the 3D
+ * soft-sphere Euler ODE (agentODE + CBMIntegrators.Euler,
+ * src/integrators.jl:465-505) with respect to theta = (k_rep, k_att, r_rep)
+ * — (k, a, equilibrium distance 2r) — and to the initial positions, by a
+ * hand-written reverse sweep with step checkpointing: states are kept every
+ * checkpoint_every steps and each segment is recomputed before it is swept
+ * backwards.  The configuration must be dims = 3, Euler, CBM_FORCE_DIRECT,
+ * CBM_ATT_FROM_REP, CBM_NEIGH_CELL_LINKED, without walls, fate, growth,
+ * medium or drift; the cutoff r_att is held fixed in the derivative.  The
+ * forward map is the plain path's, bit for bit.  Arrays are host arrays of
+ * the configured precision (x, y, z each). */
+typedef struct cbm_adjoint cbm_adjoint;
+int cbm_adjoint_create(cbm_adjoint** out, const cbm_config* cfg);
+void cbm_adjoint_destroy(cbm_adjoint* a);
+const char* cbm_adjoint_last_error(const cbm_adjoint* a);
+/* loss, dtheta[3] = dL/d(k_rep, k_att, r_rep); dx0 (may be NULL) = dL/dx0;
+ * xT (may be NULL) = final positions */
+int cbm_adjoint_run(cbm_adjoint* a, int64_t n, const void* const* x0, int32_t nsteps,
+                    int32_t checkpoint_every, const void* const* target, double* loss,
+                    double* dtheta, void* const* dx0, void* const* xT);
+/* the same forward trajectory without the backward sweep (for timing) */
+int cbm_adjoint_forward(cbm_adjoint* a, int64_t n, const void* const* x0, int32_t nsteps,
+                        void* const* xT);
+void* cbm_adjoint_stream(cbm_adjoint* a);
+
 /* ---- allocation-free cell grid -------------------------------------------
  * This entry point has no counterpart in the reference.  It is for callers
  * that cannot allocate device memory when they need a grid: code running

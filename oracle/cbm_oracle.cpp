@@ -901,3 +901,132 @@ void oracle_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t 
 }
 
 }  // extern "C"
+
+/* ---------------------------------------------------------------------------
+ * Forward-mode dual numbers of the soft-sphere Euler trajectory: the
+ * gradient check for the adjoint.  It stands in for a ForwardDiff gradient of
+ * the reference's CPU path (ForwardDiff 0.10.36 is in the reference's
+ * Manifest.toml but Julia cannot run here).  Directions 0..2 carry
+ * d/d(k_rep, k_att, r_rep); further directions carry d/d of chosen initial
+ * coordinates.  The cutoff r_att is a plain number (held fixed), as in the
+ * adjoint.  All pairs are visited (small N).
+ * ------------------------------------------------------------------------- */
+namespace {
+
+constexpr int kDualMax = 12;
+
+struct Dual {
+  double v;
+  double d[kDualMax];
+};
+
+int g_dual_k = 3;
+
+inline Dual dconst(double v) {
+  Dual r;
+  r.v = v;
+  for (int q = 0; q < kDualMax; ++q) r.d[q] = 0.0;
+  return r;
+}
+inline Dual operator+(const Dual& a, const Dual& b) {
+  Dual r;
+  r.v = a.v + b.v;
+  for (int q = 0; q < g_dual_k; ++q) r.d[q] = a.d[q] + b.d[q];
+  return r;
+}
+inline Dual operator-(const Dual& a, const Dual& b) {
+  Dual r;
+  r.v = a.v - b.v;
+  for (int q = 0; q < g_dual_k; ++q) r.d[q] = a.d[q] - b.d[q];
+  return r;
+}
+inline Dual operator*(const Dual& a, const Dual& b) {
+  Dual r;
+  r.v = a.v * b.v;
+  for (int q = 0; q < g_dual_k; ++q) r.d[q] = a.d[q] * b.v + a.v * b.d[q];
+  return r;
+}
+inline Dual operator/(const Dual& a, const Dual& b) {
+  Dual r;
+  r.v = a.v / b.v;
+  for (int q = 0; q < g_dual_k; ++q) r.d[q] = (a.d[q] * b.v - a.v * b.d[q]) / (b.v * b.v);
+  return r;
+}
+inline Dual dsqrt(const Dual& a) {
+  Dual r;
+  r.v = std::sqrt(a.v);
+  for (int q = 0; q < g_dual_k; ++q) r.d[q] = a.d[q] / (2.0 * r.v);
+  return r;
+}
+
+}  // namespace
+
+extern "C" int oracle_adjoint_dual(const cbm_config* cfg, int64_t n, const double* const* x0,
+                                   int nsteps, const double* const* target, int n_seed,
+                                   const int64_t* seed_agent, const int32_t* seed_axis,
+                                   double* loss, double* dtheta, double* dx0_seeded) {
+  if (n_seed < 0 || 3 + n_seed > kDualMax) return CBM_ERR_ARG;
+  g_dual_k = 3 + n_seed;
+  std::vector<Dual> x[3], xn[3];
+  for (int d = 0; d < 3; ++d) {
+    x[d].resize((size_t)n);
+    xn[d].resize((size_t)n);
+    for (int64_t i = 0; i < n; ++i) x[d][(size_t)i] = dconst(x0[d][i]);
+  }
+  for (int s = 0; s < n_seed; ++s) x[seed_axis[s]][(size_t)seed_agent[s]].d[3 + s] = 1.0;
+  Dual k = dconst(cfg->k_rep), a = dconst(cfg->k_att), rho = dconst(cfg->r_rep);
+  k.d[0] = 1.0;
+  a.d[1] = 1.0;
+  rho.d[2] = 1.0;
+  const double ratt = cfg->r_att;
+  const Dual dt = dconst(cfg->dt);
+  // The pair set is the reference's CellLinked one: j interacts with i only
+  // if their cells (cellPos, neighbors.jl:636-638, on the values) are
+  // neighbors.  Agents beyond simBox fall in the ghost layer, so the set is
+  // not every pair within the cutoff.
+  int64_t ncell[3];
+  for (int d = 0; d < 3; ++d)
+    ncell[d] = (int64_t)std::ceil((cfg->box_hi[d] - cfg->box_lo[d]) / cfg->cell_edge + 2.0);
+  std::vector<int64_t> cpos((size_t)n * 3);
+  for (int st = 0; st < nsteps; ++st) {
+    for (int64_t i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d)
+        cpos[(size_t)i * 3 + d] = cellPos1<double>(cfg->cell_edge, x[d][(size_t)i].v, cfg->box_lo[d],
+                                                   cfg->box_hi[d], ncell[d]);
+    for (int64_t i = 0; i < n; ++i) {
+      Dual acc[3] = {dconst(0), dconst(0), dconst(0)};
+      for (int64_t j = 0; j < n; ++j) {
+        if (j == i) continue;
+        bool adjacent = true;
+        for (int d = 0; d < 3; ++d) {
+          int64_t dc = cpos[(size_t)i * 3 + d] - cpos[(size_t)j * 3 + d];
+          if (dc < -1 || dc > 1) adjacent = false;
+        }
+        if (!adjacent) continue;
+        Dual e[3];
+        for (int d = 0; d < 3; ++d) e[d] = x[d][(size_t)i] - x[d][(size_t)j];
+        Dual s2 = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
+        Dual dd = dsqrt(s2);
+        Dual F;
+        if (dd.v < rho.v) F = k * (rho - dd);
+        else if (dd.v < ratt) F = dconst(0) - a * (dd - rho);
+        else continue;
+        Dual sc = F / dd;
+        for (int d = 0; d < 3; ++d) acc[d] = acc[d] + sc * e[d];
+      }
+      for (int d = 0; d < 3; ++d) xn[d][(size_t)i] = x[d][(size_t)i] + acc[d] * dt;
+    }
+    for (int d = 0; d < 3; ++d) x[d].swap(xn[d]);
+  }
+  Dual L = dconst(0);
+  for (int64_t i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) {
+      Dual e = x[d][(size_t)i] - dconst(target[d][i]);
+      L = L + e * e;
+    }
+  L = L / dconst(3.0 * (double)n);
+  *loss = L.v;
+  for (int q = 0; q < 3; ++q) dtheta[q] = L.d[q];
+  for (int s = 0; s < n_seed; ++s) dx0_seeded[s] = L.d[3 + s];
+  return CBM_OK;
+}

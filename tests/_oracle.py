@@ -153,3 +153,26 @@ class OracleContext:
         self.lib.oracle_rng_fill(self.cfg.precision, self.cfg.seed, self.cfg.community, kind,
                                  float(a), float(b), n, step, out.ctypes.data)
         return out[:n]
+
+
+def oracle_adjoint_dual(abi, cfg, x0, target, nsteps, seeds=()):
+    """Forward-mode dual numbers of the Euler trajectory: (loss, dL/dtheta, dL/dx0[seeds])."""
+    lib = load_oracle(abi)
+    f = lib.oracle_adjoint_dual
+    f.restype = C.c_int
+    f.argtypes = [C.POINTER(abi.CbmConfig), C.c_int64, C.POINTER(C.c_void_p), C.c_int,
+                  C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                  C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    xs = [np.ascontiguousarray(a, dtype=np.float64) for a in x0]
+    ts = [np.ascontiguousarray(a, dtype=np.float64) for a in target]
+    xp = (C.c_void_p * 3)(*[a.ctypes.data for a in xs])
+    tp = (C.c_void_p * 3)(*[a.ctypes.data for a in ts])
+    ns = len(seeds)
+    sa = (C.c_int64 * max(ns, 1))(*[s[0] for s in seeds])
+    sx = (C.c_int32 * max(ns, 1))(*[s[1] for s in seeds])
+    loss = C.c_double()
+    g = (C.c_double * 3)()
+    dx = (C.c_double * max(ns, 1))()
+    rc = f(C.byref(cfg), len(xs[0]), xp, nsteps, tp, ns, sa, sx, C.byref(loss), g, dx)
+    assert rc == 0
+    return loss.value, np.array(list(g)), np.array(list(dx)[:ns])

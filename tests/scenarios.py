@@ -123,3 +123,19 @@ def make_descs(abi, descs):
             setattr(x, k, d[k])
         out.append(x)
     return out
+
+
+def adjoint_problem(abi, N=65536, L=80.0, seed=5, steps=200, precision=None, theta=(10.0, 1.0, 2.0)):
+    """Differentiable 3D ODE trajectory: N agents uniform in [0,L]^3, soft
+    spheres with theta = (k, a, 2r), forward Euler dt=0.01, CellLinked edge
+    3.3; the target comes from the same simulation at theta* = theta (1 +
+    0.1 N(0,1)).  Returns (config kwargs, x0, theta*)."""
+    rng = np.random.default_rng(seed)
+    k, a, rho = theta
+    kw = dict(dims=3, precision=abi.F64 if precision is None else precision, n_max=N,
+              box_lo=(0.0,) * 3, box_hi=(L,) * 3, dt=0.01, seed=seed,
+              neighbors=abi.NEIGH_CELL_LINKED, cell_edge=3.3, integrator=abi.INT_EULER,
+              k_rep=k, r_rep=rho, k_att=a, r_att=1.5 * rho, att_form=abi.ATT_FROM_REP)
+    x0 = [rng.uniform(0, L, N) for _ in range(3)]
+    star = tuple(t * (1 + 0.1 * z) for t, z in zip(theta, rng.normal(size=3)))
+    return kw, x0, star

@@ -240,3 +240,37 @@ def test_compaction_matches_serial_tail_fill(abi):
     expect_ids = np.concatenate([np.arange(1, N + 1), 60 + np.arange(1, n_add + 1)])
     np.testing.assert_array_equal(after["id"], expect_ids[order[: total - n_rem]])
     del before, ids_tail
+
+
+def test_dual_gradient_matches_central_differences(abi):
+    """The forward-mode checker of the adjoint against central differences
+    of its own loss (no pair near the cutoff in this small, dilute case)."""
+    from _oracle import oracle_adjoint_dual
+    rng = np.random.default_rng(21)
+    n, L, steps = 30, 9.0, 15
+    x0 = [rng.uniform(0, L, n) for _ in range(3)]
+    tgt = [x + rng.normal(scale=0.05, size=n) for x in x0]
+    theta = dict(k_rep=10.0, k_att=1.0, r_rep=2.0)
+
+    def cfg(**over):
+        t = dict(theta, **over)
+        return abi.make_config(dims=3, n_max=n, dt=0.01, box_hi=(L,) * 3, k_rep=t["k_rep"],
+                               k_att=t["k_att"], r_rep=t["r_rep"], r_att=3.0,
+                               neighbors=abi.NEIGH_CELL_LINKED, cell_edge=3.3)
+
+    loss, g, dx = oracle_adjoint_dual(abi, cfg(), x0, tgt, steps, seeds=[(3, 0), (7, 2)])
+    for q, name in enumerate(("k_rep", "k_att", "r_rep")):
+        h = 1e-6 * theta[name]
+        lp = oracle_adjoint_dual(abi, cfg(**{name: theta[name] + h}), x0, tgt, steps)[0]
+        lm = oracle_adjoint_dual(abi, cfg(**{name: theta[name] - h}), x0, tgt, steps)[0]
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[q]) <= 1e-5 * max(abs(g[q]), 1e-12), (name, fd, g[q])
+    for s, (i, ax) in enumerate([(3, 0), (7, 2)]):
+        h = 1e-6
+        xp = [a.copy() for a in x0]
+        xm = [a.copy() for a in x0]
+        xp[ax][i] += h
+        xm[ax][i] -= h
+        fd = (oracle_adjoint_dual(abi, cfg(), xp, tgt, steps)[0] -
+              oracle_adjoint_dual(abi, cfg(), xm, tgt, steps)[0]) / (2 * h)
+        assert abs(fd - dx[s]) <= 1e-5 * max(abs(dx[s]), 1e-9)
