@@ -60,7 +60,88 @@ def peaks():
         return 6650.0, "fallback"
 
 
-class Clocks:
+class NvmlClocks:
+    """SM clock and clock-event reasons polled through NVML every ~1 ms while
+    the timed region runs (a short region ends before nvidia-smi's first
+    sample).  Read-only: nothing is set."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown",
+                "nvmlClocksThrottleReasonHwSlowdown", 0x8),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown",
+                "nvmlClocksThrottleReasonHwThermalSlowdown", 0x40),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown",
+                "nvmlClocksThrottleReasonSwThermalSlowdown", 0x20),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap",
+                "nvmlClocksThrottleReasonSwPowerCap", 0x4))
+
+    def __init__(self, index):
+        import threading
+
+        import pynvml as N
+        self.N = N
+        N.nvmlInit()
+        self.h = None
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(index)
+            bus = "%08x:%02x:%02x.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+            self.h = N.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            self.h = None
+        if self.h is None:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            ids = [x for x in vis.split(",") if x.strip()]
+            phys = int(ids[index]) if index < len(ids) and ids[index].isdigit() else index
+            self.h = N.nvmlDeviceGetHandleByIndex(phys)
+        self.smax = float(N.nvmlDeviceGetMaxClockInfo(self.h, N.NVML_CLOCK_SM))
+        self.masks = [(n, getattr(N, a, getattr(N, b, m))) for n, a, b, m in self.REASONS]
+        get = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            getattr(N, "nvmlDeviceGetCurrentClocksThrottleReasons")
+        self.get_reasons = get
+        self.samples = []
+        self.stop_ev = threading.Event()
+        self.thread = threading.Thread(target=self._run, daemon=True)
+
+    def _sample(self):
+        sm = self.N.nvmlDeviceGetClockInfo(self.h, self.N.NVML_CLOCK_SM)
+        self.samples.append((float(sm), int(self.get_reasons(self.h))))
+
+    def _run(self):
+        while not self.stop_ev.is_set():
+            self._sample()
+            time.sleep(0.001)
+
+    def start(self):
+        self._sample()
+        self.thread.start()
+
+    def stop(self):
+        self._sample()
+        self.stop_ev.set()
+        self.thread.join(timeout=5)
+        reasons = set()
+        for _, r in self.samples:
+            for n, m in self.masks:
+                if r & m:
+                    reasons.add(n)
+        out = {"sm_mhz": float(np.median([s for s, _ in self.samples])),
+               "sm_max_mhz": self.smax, "reasons": sorted(reasons),
+               "samples": len(self.samples), "source": "nvml, 1 ms polling"}
+        try:
+            self.N.nvmlShutdown()
+        except Exception:
+            pass
+        return out
+
+
+def Clocks(index):
+    try:
+        return NvmlClocks(index)
+    except Exception:
+        return SmiClocks(index)
+
+
+class SmiClocks:
     """nvidia-smi sampling during the timed region."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -112,7 +193,19 @@ class Clocks:
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi -lms 200"}
+
+
+# DRAM bytes per agent of one launch, from one ncu capture (dram__bytes_read.sum
+# + dram__bytes_write.sum) of the default colony workload: k_agent_de in walk
+# mode, Float32, 52.6 MB for 1,029,015 agents.  Traffic grows in proportion to
+# the agents of the launch, so it is scaled to the bench's agent count.
+MEASURED_TRAFFIC_PER_AGENT = {("k_agent_de", 4, True): 51.1}
+
+
+def traffic_per_launch(name, s, walked, agents):
+    t = MEASURED_TRAFFIC_PER_AGENT.get((name, s, bool(walked)))
+    return None if t is None else round(t * agents)
 
 
 def alg_bytes_per_agent(name, s, d, nbar, verlet, fate):
@@ -215,7 +308,10 @@ def run_ours(args, rank, world, local_rank):
         for name, ms in ctx.profile_step():
             prof.setdefault(name, []).append(ms)
     n_now = ctx.counters()["N"]
-    verlet = cfg.neighbors in (abi.NEIGH_CLVD, abi.NEIGH_VERLET_DISPLACEMENT)
+    # A step that followed an add/remove walks the cells instead of reading the
+    # list (recompute-on-event), so its compulsory bytes are the cell-mode ones.
+    walked = ctx.counters()["flag"] == 1
+    verlet = cfg.neighbors in (abi.NEIGH_CLVD, abi.NEIGH_VERLET_DISPLACEMENT) and not walked
     nbar = float(np.mean(ctx.neighbors()[0])) if verlet else 0.0
     s = 8 if cfg.precision == abi.F64 else 4
     kern = {k: (float(np.mean(v)), float(np.sum(v))) for k, v in prof.items()}
@@ -227,7 +323,8 @@ def run_ours(args, rank, world, local_rank):
         achieved = bpa * n_now / (kern[top][0] / 1e3) / 1e9
         roof = {"kernel": top, "bound": "hbm", "achieved": round(achieved, 1),
                 "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-                "frac": round(achieved / hbm, 4), "traffic": None,
+                "frac": round(achieved / hbm, 4),
+                "traffic": traffic_per_launch(top, s, walked, n_now),
                 "alg_bytes_per_agent": round(bpa, 2), "agents": n_now, "nbar": round(nbar, 2),
                 "avg_ms": round(kern[top][0], 4)}
     step_share = {k: round(v[1] / sum(x[1] for x in kern.values()), 4) for k, v in kern.items()}
@@ -276,6 +373,95 @@ def run_ours(args, rank, world, local_rank):
                 launches=launches, cfg=cfg, state_n=len(state["x"]), kw=kw)
 
 
+def run_batched(args):
+    """512 communities (N_i ~ U[500, 20000]) x 500 EM steps in one persistent
+    launch, against the plain path run once per community (a sample)."""
+    import torch
+    from scenarios import batched_sweep, make_descs, plain_config_for
+    cbm = load_package()
+    abi = cbm._abi
+    base, descs, states = batched_sweep(abi, n_comm=args.batched_comms)
+    b = cbm.Batch(abi.make_config(**base), make_descs(abi, descs))
+    for c, st in enumerate(states):
+        b.upload(c, st["x"], st["y"], st["z"])
+    t0 = time.perf_counter()
+    tuning = b.autotune(trial_steps=args.batched_trial)
+    tune_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(b.stream())
+    b.step(args.batched_steps)  # first replay builds the graph
+    for c, st in enumerate(states):
+        b.upload(c, st["x"], st["y"], st["z"])
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    e0.record(stream)
+    b.step(args.batched_steps, 0)
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    b.step(0)  # report device flags
+    ms = e0.elapsed_time(e1)
+    total = sum(d["n"] for d in descs)
+    batched = total * args.batched_steps / (ms / 1e3)
+    # the plain path, one community at a time (contexts created beforehand)
+    rng = np.random.default_rng(7)
+    sample = sorted(rng.choice(len(descs), size=min(args.plain_sample, len(descs)), replace=False))
+    ctxs = [cbm.Context(abi.make_config(**plain_config_for(abi, base, descs[c], tuning.as_dict())))
+            for c in sample]
+    agents, secs = 0, 0.0
+    for c, g in zip(sample, ctxs):
+        st = states[c]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g.upload(st)
+        g.step(args.batched_steps)
+        g.download()
+        secs += time.perf_counter() - t0
+        agents += descs[c]["n"] * args.batched_steps
+        g.close()
+    plain = agents / secs
+    return {"communities": len(descs), "agents": int(total), "steps": args.batched_steps,
+            "value": round(batched, 1), "unit": UNIT, "ms": round(ms, 3),
+            "plain_value": round(plain, 1), "plain_sample": len(sample),
+            "speedup_vs_plain": round(batched / plain, 2), "tuning": tuning.as_dict(),
+            "autotune_s": round(tune_s, 3), "clocks": clk}
+
+
+def run_adjoint(args):
+    """Gradient of the trajectory MSE (65536 agents, 200 Euler steps, Float64,
+    checkpoint every 20) against the forward trajectory alone."""
+    import torch
+    from scenarios import adjoint_problem
+    cbm = load_package()
+    abi = cbm._abi
+    kw, x0, star = adjoint_problem(abi, N=args.adjoint_n, steps=args.adjoint_steps)
+    k, a, rho = star
+    tgt_fw = cbm.Adjoint(abi.make_config(**dict(kw, k_rep=k, k_att=a, r_rep=rho, r_att=1.5 * rho,
+                                                cell_edge=max(kw["cell_edge"], 1.5 * rho))))
+    tgt = tgt_fw.forward(x0, args.adjoint_steps)
+    adj = cbm.Adjoint(abi.make_config(**kw))
+    adj.forward(x0, args.adjoint_steps)  # warm-up
+    adj.run(x0, tgt, args.adjoint_steps, checkpoint_every=args.checkpoint_every)
+    reps = 3
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        adj.forward(x0, args.adjoint_steps)
+    fwd = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        res = adj.run(x0, tgt, args.adjoint_steps, checkpoint_every=args.checkpoint_every)
+    full = (time.perf_counter() - t0) / reps
+    return {"agents": args.adjoint_n, "steps": args.adjoint_steps, "dtype": "f64",
+            "checkpoint_every": args.checkpoint_every, "forward_ms": round(1e3 * fwd, 3),
+            "forward_plus_adjoint_ms": round(1e3 * full, 3),
+            "cost_ratio": round(full / fwd, 3), "loss": res["loss"],
+            "dL_dtheta": [float(v) for v in res["dtheta"]],
+            "timing": "host wall clock around synchronous calls, incl. host<->device copies"}
+
+
 def cpu_baseline(args, steps, threads=None):
     """The CPU checker on the same workload (CellLinked, rebuilt every step)."""
     cbm = load_package()
@@ -311,6 +497,15 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-comms", type=int, default=512)
+    ap.add_argument("--batched-steps", type=int, default=500)
+    ap.add_argument("--batched-trial", type=int, default=20)
+    ap.add_argument("--plain-sample", type=int, default=32)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-n", type=int, default=65536)
+    ap.add_argument("--adjoint-steps", type=int, default=200)
+    ap.add_argument("--checkpoint-every", type=int, default=20)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -348,9 +543,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     r = run_ours(args, rank, world, local_rank)
-    cb = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline(args, args.cpu_steps)
+    cb = batched = adjoint = None
+    if rank == 0 and world == 1:
+        if not args.no_batched:
+            batched = run_batched(args)
+        if not args.no_adjoint:
+            adjoint = run_adjoint(args)
+        if not args.no_cpu_baseline:
+            cb = cpu_baseline(args, args.cpu_steps)
     if rank == 0:
         line = {"metric": METRIC, "value": round(r["value"], 1), "unit": UNIT,
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -359,7 +559,8 @@ def main():
                 "data": "synthetic", "config": config, "roofline": r["roof"],
                 "cpu_baseline": cb, "e2e": r["e2e"], "gpu_launches": r["launches"],
                 "clocks": r["clocks"], "kernel_share": r["share"],
-                "kernel_avg_ms": {k: round(v[0], 4) for k, v in r["kern"].items()}}
+                "kernel_avg_ms": {k: round(v[0], 4) for k, v in r["kern"].items()},
+                "batched": batched, "adjoint": adjoint}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -86,7 +86,7 @@ def batched_sweep(abi, n_comm=512, n_lo=500, n_hi=20000, seed=4, dt=0.01, skin=0
     Returns (base config kwargs, community descriptor kwargs, initial states)."""
     rng = np.random.default_rng(seed)
     base = dict(dims=3, precision=abi.F32, n_max=1, dt=dt, seed=seed, neighbors=abi.NEIGH_CLVD,
-                integrator=abi.INT_EM, n_max_neighbors=48, skin=3.0 + skin, cell_edge=3.0 + skin,
+                integrator=abi.INT_EM, n_max_neighbors=256, skin=3.0 + skin, cell_edge=3.0 + skin,
                 rebuild_threshold=skin / 2, k_rep=10.0, r_rep=2.0, k_att=1.0, r_att=3.0)
     descs, states = [], []
     for c in range(n_comm):
