@@ -50,31 +50,26 @@ struct BatchParams {
   const int* order;     // communities by descending size
   int n_comm;
   int* head;            // work-queue head
-  float4* P[2];         // positions, ping-pong by per-community parity
-  float4* pold;
+  float4* P[2];         // positions in slot order, ping-pong by per-community parity;
+                        // w holds the agent index (int bits)
+  float4* pold;         // slot order: positions at the last rebuild
   int* parity;          // per community: which P holds the current positions
   int* rebuild;         // per community: the next step starts with a rebuild
   long long* step;      // per community step counter
-  int* cell_count;
-  int* cell_start;
-  int* agent_cell;
-  int* agent_rank;
-  int* tmp;
-  int* cell_agents;
+  int* cell_count;      // zero between rebuilds
+  int* cell_start;      // n_cells + 1 per community
+  int* key;             // rebuild scratch: cell of an old slot
+  int* rank;            // rebuild scratch: arrival rank of an old slot in its cell
+  int* sidx;            // rebuild scratch: agent index by (cell, arrival)
   int* nbr_n;
-  int* nbr_list;        // per community: entry k of agent i at off*M + k*n + i
+  int* nbr_list;        // per community: entry k of slot q at off*M + k*n + q
   int max_nbrs;
+  int tile;             // communities of at most this many agents gather from shared memory
   float dt, sqrt_dt;
   float edge, skin, skin2, skin2_lo, thr;
   uint64_t seed;
   int* err;
 };
-
-__device__ __forceinline__ void f4to3(const float4& v, float* x) {
-  x[0] = v.x;
-  x[1] = v.y;
-  x[2] = v.z;
-}
 
 // CTA-wide exclusive scan of one int per thread
 template <int NT>
@@ -104,67 +99,123 @@ __device__ __forceinline__ int cta_exscan(int v, int* warp_sums, int* total) {
   return prefix + x - v;
 }
 
-// Grid (counting sort, stable inside a cell) and CLVD list of one community
-// from positions X (neighbors.jl:918-979,1071-1131).
+__device__ __forceinline__ int agent_index(const float4& p) { return __float_as_int(p.w); }
+
+// Grid rebuild of one community (neighbors.jl:918-979): counting sort of the
+// agents by cell, ascending agent index inside a cell, from X (old slot
+// order) into Xs, which becomes the new slot order.  The slot order is then
+// the CLVD walk order: cells x fastest, ascending index inside a cell.
 template <int NT>
-__device__ void cta_rebuild(const BatchParams& B, const Comm& C, const float4* X, int* warp_sums) {
+__device__ void cta_sort(const BatchParams& B, const Comm& C, const float4* X, float4* Xs,
+                         int* warp_sums) {
   const int n = C.n, tid = threadIdx.x;
   int* count = B.cell_count + C.cell_off;
   int* start = B.cell_start + C.cell_off;
-  int* acell = B.agent_cell + C.off;
-  int* arank = B.agent_rank + C.off;
-  int* tmp = B.tmp + C.off;
-  int* cagents = B.cell_agents + C.off;
-  for (int i = tid; i < n; i += NT) {
-    float x[3];
-    f4to3(X[i], x);
-    int c = cell_of<float, 3>(B.edge, C.lo, C.hi, C.nc, x);
-    acell[i] = c;
-    arank[i] = atomicAdd(count + c, 1);
-    B.pold[C.off + i] = X[i];  // verletResetDisplacement
+  int* key = B.key + C.off;
+  int* rank = B.rank + C.off;
+  int* sidx = B.sidx + C.off;
+  for (int s = tid; s < n; s += NT) {
+    const float4 p = X[s];
+    const float x[3] = {p.x, p.y, p.z};
+    const int c = cell_of<float, 3>(B.edge, C.lo, C.hi, C.nc, x);
+    key[s] = c;
+    rank[s] = atomicAdd(count + c, 1);
   }
   __syncthreads();
-  int carry = 0;
-  for (int base = 0; base < C.n_cells; base += NT) {
-    const int c = base + tid;
-    const int v = c < C.n_cells ? count[c] : 0;
-    int tot;
-    const int ex = cta_exscan<NT>(v, warp_sums, &tot);
-    if (c < C.n_cells) {
-      start[c] = carry + ex;
-      count[c] = 0;
-    }
-    carry += tot;
+  // exclusive scan of the counts: a run of cells per thread
+  const int nc = C.n_cells;
+  const int per = (nc + NT - 1) / NT;
+  const int c0 = min(nc, tid * per), c1 = min(nc, c0 + per);
+  int local = 0;
+  for (int c = c0; c < c1; ++c) local += count[c];
+  int total;
+  int run = cta_exscan<NT>(local, warp_sums, &total);
+  for (int c = c0; c < c1; ++c) {
+    const int v = count[c];
+    start[c] = run;
+    run += v;
+    count[c] = 0;
   }
-  if (tid == 0) start[C.n_cells] = carry;
+  if (tid == 0) start[nc] = total;
   __syncthreads();
-  for (int i = tid; i < n; i += NT) tmp[start[acell[i]] + arank[i]] = i;
+  for (int s = tid; s < n; s += NT) sidx[start[key[s]] + rank[s]] = agent_index(X[s]);
   __syncthreads();
-  for (int i = tid; i < n; i += NT) {
-    const int c = acell[i];
+  for (int s = tid; s < n; s += NT) {
+    const float4 p = X[s];
+    const int c = key[s], me = agent_index(p);
     const int s0 = start[c], s1 = start[c + 1];
     int r = 0;
-    for (int s = s0; s < s1; ++s) r += tmp[s] < i;
-    cagents[s0 + r] = i;
+    for (int u = s0; u < s1; ++u) r += sidx[u] < me;
+    Xs[s0 + r] = p;
+    B.pold[C.off + s0 + r] = p;  // verletResetDisplacement
   }
   __syncthreads();
-  const int M = B.max_nbrs;
-  int* list = B.nbr_list + C.off * (long long)M;
-  for (int i = tid; i < n; i += NT) {
-    float xi[3];
-    f4to3(X[i], xi);
-    int q[3];
-    cell_coords<3>(C.nc, cell_of<float, 3>(B.edge, C.lo, C.hi, C.nc, xi), q);
-    int m = 0;
-    bool over = false;
-    for (int k = 0; k < 27; ++k) {
-      const int pn = cell_neigh<3>(C.nc, q, k);
-      if (pn < 0) continue;
-      for (int s = start[pn]; s < start[pn + 1]; ++s) {
-        const int j = cagents[s];
-        if (j == i) continue;
+}
+
+// position of slot j: from the shared-memory tile or from global memory
+template <bool SM>
+__device__ __forceinline__ void pos_of(const float4* X, const float* sx, const float* sy,
+                                       const float* sz, int j, float* xj) {
+  if (SM) {
+    xj[0] = sx[j];
+    xj[1] = sy[j];
+    xj[2] = sz[j];
+  } else {
+    const float4 p = X[j];
+    xj[0] = p.x;
+    xj[1] = p.y;
+    xj[2] = p.z;
+  }
+}
+
+// one pair of the soft-sphere force (the expression order of the plain path)
+__device__ __forceinline__ void pair_force(const Comm& C, const float* xi, const float* xj,
+                                           float* acc) {
+  float e[3];
+  e[0] = xi[0] - xj[0];
+  float s2 = e[0] * e[0];
+  e[1] = xi[1] - xj[1];
+  s2 = s2 + e[1] * e[1];
+  e[2] = xi[2] - xj[2];
+  s2 = s2 + e[2] * e[2];
+  if (s2 >= C.cut2) return;
+  const float dd = sqrtf(s2);
+  float F;
+  if (dd < C.r_rep) F = C.k_rep * (C.r_rep - dd);
+  else if (dd < C.r_att) F = -(C.k_att * (dd - C.r_rep));
+  else return;
+  const float sc = F / dd;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) acc[d] = acc[d] + sc * e[d];
+}
+
+// Rebuild step of slot q: the CLVD list row (verletNeighborsCLVD,
+// neighbors.jl:1071-1131 as intended: the 27 cells x fastest, d < list
+// radius) and, in the same pass and the same order, the force.  For fixed
+// (dz, dy) the cells x-1..x+1 are one contiguous run of slots.
+template <bool SM>
+__device__ __forceinline__ void build_row(const BatchParams& B, const Comm& C, const float4* X,
+                                          const float* sx, const float* sy, const float* sz,
+                                          int q, const float* xi, int* list, int* nbr_n,
+                                          float* acc) {
+  const int n = C.n, M = B.max_nbrs;
+  const int* start = B.cell_start + C.cell_off;
+  int q3[3];
+  cell_coords<3>(C.nc, cell_of<float, 3>(B.edge, C.lo, C.hi, C.nc, xi), q3);
+  const int xa = max(q3[0] - 1, 0), xb = min(q3[0] + 1, C.nc[0] - 1);
+  int m = 0;
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int z = q3[2] + dz;
+    if (z < 0 || z >= C.nc[2]) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int y = q3[1] + dy;
+      if (y < 0 || y >= C.nc[1]) continue;
+      const int row = (z * C.nc[1] + y) * C.nc[0];
+      const int s1 = start[row + xb + 1];
+      for (int s = start[row + xa]; s < s1; ++s) {
+        if (s == q) continue;
         float xj[3];
-        f4to3(X[j], xj);
+        pos_of<SM>(X, sx, sy, sz, s, xj);
         float e = xi[0] - xj[0];
         float s2 = e * e;
         e = xi[1] - xj[1];
@@ -173,22 +224,116 @@ __device__ void cta_rebuild(const BatchParams& B, const Comm& C, const float4* X
         s2 = s2 + e * e;
         if (s2 >= B.skin2) continue;
         if (!(s2 < B.skin2_lo) && !(sqrtf(s2) < B.skin)) continue;
-        if (m < M) list[(long long)m * n + i] = j;
-        else over = true;
+        if (m < M) list[(long long)m * n + q] = s;
         ++m;
+        pair_force(C, xi, xj, acc);
       }
     }
-    if (over) atomicOr(B.err, kErrNeighborOverflow);
-    B.nbr_n[C.off + i] = m < M ? m : M;
   }
-  __syncthreads();
+  if (m > M) atomicOr(B.err, kErrNeighborOverflow);
+  nbr_n[q] = m < M ? m : M;
+}
+
+// Non-rebuild step of slot q: the force over the list row, four entries in
+// flight, summed in list order.
+template <bool SM>
+__device__ __forceinline__ void list_row(const BatchParams& B, const Comm& C, const float4* X,
+                                         const float* sx, const float* sy, const float* sz,
+                                         int q, const float* xi, const int* list,
+                                         const int* nbr_n, float* acc) {
+  const int n = C.n;
+  const int m = nbr_n[q];
+  const int* row = list + q;
+  int k = 0;
+  for (; k + 4 <= m; k += 4) {
+    int j[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) j[u] = row[(long long)(k + u) * n];
+    float xj[4][3];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) pos_of<SM>(X, sx, sy, sz, j[u], xj[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) pair_force(C, xi, xj[u], acc);
+  }
+  for (; k < m; ++k) {
+    float xj[3];
+    pos_of<SM>(X, sx, sy, sz, row[(long long)k * n], xj);
+    pair_force(C, xi, xj, acc);
+  }
+}
+
+// all requested steps of one community
+template <int NT, bool SM>
+__device__ void run_comm(const BatchParams& B, const Comm& C, int ci, int nsteps, float* sx,
+                         float* sy, float* sz, int* warp_sums, int* s_flag) {
+  int par = B.parity[ci];
+  int rebuild = B.rebuild[ci];
+  long long step = B.step[ci];
+  const int n = C.n;
+  int* list = B.nbr_list + C.off * (long long)B.max_nbrs;
+  int* nbr_n = B.nbr_n + C.off;
+  const float4* pold = B.pold + C.off;
+  if (threadIdx.x == 0) s_flag[0] = s_flag[1] = 0;
+  for (int t = 0; t < nsteps; ++t) {
+    if (rebuild) {
+      cta_sort<NT>(B, C, B.P[par] + C.off, B.P[par ^ 1] + C.off, warp_sums);
+      par ^= 1;
+    }
+    const float4* Xc = B.P[par] + C.off;
+    float4* Xn = B.P[par ^ 1] + C.off;
+    if (SM) {
+      for (int s = threadIdx.x; s < n; s += NT) {
+        const float4 p = Xc[s];
+        sx[s] = p.x;
+        sy[s] = p.y;
+        sz[s] = p.z;
+      }
+    }
+    __syncthreads();
+    // the flag of the next step: every thread has read it last step
+    if (threadIdx.x == 0) s_flag[(t + 1) & 1] = 0;
+    for (int q = threadIdx.x; q < n; q += NT) {
+      const float4 me = Xc[q];
+      const float xi[3] = {me.x, me.y, me.z};
+      float acc[3] = {0.f, 0.f, 0.f};
+      if (rebuild) build_row<SM>(B, C, Xc, sx, sy, sz, q, xi, list, nbr_n, acc);
+      else list_row<SM>(B, C, Xc, sx, sy, sz, q, xi, list, nbr_n, acc);
+      float z[3];
+      cbm_normals(B.seed, step, (uint32_t)agent_index(me), CBM_STREAM_NOISE, C.community, 3, z);
+      float xn[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) xn[d] = (xi[d] + acc[d] * B.dt) + (C.sigma * z[d]) * B.sqrt_dt;
+      Xn[q] = make_float4(xn[0], xn[1], xn[2], me.w);
+      const float4 po = pold[q];
+      float e = xn[0] - po.x;
+      float s2 = e * e;
+      e = xn[1] - po.y;
+      s2 = s2 + e * e;
+      e = xn[2] - po.z;
+      s2 = s2 + e * e;
+      if (sqrtf(s2) >= B.thr) s_flag[t & 1] = 1;  // verletDisplacement (neighbors.jl:367-391)
+    }
+    __syncthreads();
+    rebuild = s_flag[t & 1];
+    par ^= 1;
+    ++step;
+  }
+  if (threadIdx.x == 0) {
+    B.parity[ci] = par;
+    B.rebuild[ci] = rebuild;
+    B.step[ci] = step;
+  }
 }
 
 template <int NT>
 __global__ void __launch_bounds__(NT) k_batch(BatchParams B, int nsteps) {
+  extern __shared__ float s_tile[];
   __shared__ int s_comm;
-  __shared__ int s_flag;
+  __shared__ int s_flag[2];
   __shared__ int warp_sums[NT / 32];
+  float* sx = s_tile;
+  float* sy = s_tile + B.tile;
+  float* sz = s_tile + 2 * B.tile;
   for (;;) {
     if (threadIdx.x == 0) {
       const int q = atomicAdd(B.head, 1);
@@ -198,69 +343,8 @@ __global__ void __launch_bounds__(NT) k_batch(BatchParams B, int nsteps) {
     const int ci = s_comm;
     if (ci < 0) return;
     const Comm C = B.comms[ci];
-    int par = B.parity[ci];
-    int rebuild = B.rebuild[ci];
-    long long step = B.step[ci];
-    const int M = B.max_nbrs;
-    const int* list = B.nbr_list + C.off * (long long)M;
-    for (int t = 0; t < nsteps; ++t) {
-      const float4* Xc = B.P[par] + C.off;
-      float4* Xn = B.P[par ^ 1] + C.off;
-      if (rebuild) cta_rebuild<NT>(B, C, Xc, warp_sums);
-      if (threadIdx.x == 0) s_flag = 0;
-      __syncthreads();
-      for (int i = threadIdx.x; i < C.n; i += NT) {
-        float xi[3];
-        f4to3(Xc[i], xi);
-        float acc[3] = {0.f, 0.f, 0.f};
-        const int m = B.nbr_n[C.off + i];
-        for (int k = 0; k < m; ++k) {
-          float xj[3];
-          f4to3(Xc[list[(long long)k * C.n + i]], xj);
-          float e[3];
-          e[0] = xi[0] - xj[0];
-          float s2 = e[0] * e[0];
-          e[1] = xi[1] - xj[1];
-          s2 = s2 + e[1] * e[1];
-          e[2] = xi[2] - xj[2];
-          s2 = s2 + e[2] * e[2];
-          if (s2 >= C.cut2) continue;
-          const float dd = sqrtf(s2);
-          float F;
-          if (dd < C.r_rep) F = C.k_rep * (C.r_rep - dd);
-          else if (dd < C.r_att) F = -(C.k_att * (dd - C.r_rep));
-          else continue;
-          const float sc = F / dd;
-#pragma unroll
-          for (int d = 0; d < 3; ++d) acc[d] = acc[d] + sc * e[d];
-        }
-        float z[3];
-        cbm_normals(B.seed, step, (uint32_t)i, CBM_STREAM_NOISE, C.community, 3, z);
-        float xn[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) xn[d] = (xi[d] + acc[d] * B.dt) + (C.sigma * z[d]) * B.sqrt_dt;
-        Xn[i] = make_float4(xn[0], xn[1], xn[2], 0.f);
-        float xo[3];
-        f4to3(B.pold[C.off + i], xo);
-        float e = xn[0] - xo[0];
-        float s2 = e * e;
-        e = xn[1] - xo[1];
-        s2 = s2 + e * e;
-        e = xn[2] - xo[2];
-        s2 = s2 + e * e;
-        if (sqrtf(s2) >= B.thr) s_flag = 1;  // verletDisplacement (neighbors.jl:367-391)
-      }
-      __syncthreads();
-      rebuild = s_flag;
-      par ^= 1;
-      ++step;
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-      B.parity[ci] = par;
-      B.rebuild[ci] = rebuild;
-      B.step[ci] = step;
-    }
+    if (C.n <= B.tile) run_comm<NT, true>(B, C, ci, nsteps, sx, sy, sz, warp_sums, s_flag);
+    else run_comm<NT, false>(B, C, ci, nsteps, sx, sy, sz, warp_sums, s_flag);
     __syncthreads();
   }
 }
@@ -298,14 +382,13 @@ struct cbm_batch {
   long long* step = nullptr;
   int* cell_count = nullptr;
   int* cell_start = nullptr;
-  int* agent_cell = nullptr;
-  int* agent_rank = nullptr;
-  int* tmp = nullptr;
-  int* cell_agents = nullptr;
+  int* key = nullptr;
+  int* rank = nullptr;
+  int* sidx = nullptr;
   int* nbr_n = nullptr;
   int* nbr_list = nullptr;
   int* d_err = nullptr;
-  cbm_batch_tuning tune{256, 2, 0.3, 0.0};
+  cbm_batch_tuning tune{256, 2, 0.3, 0.0, 0, 0};
   std::map<int, cudaGraphExec_t> graphs;  // per nsteps
   int n_sm = 148;
 };
@@ -360,6 +443,19 @@ void free_batch(cbm_batch* b) {
 
 double list_radius(const cbm_batch* b) { return b->cutoff + b->tune.skin; }
 
+// dynamic shared memory of a position tile (x, y, z arrays)
+constexpr int kMaxTileBytes = 220 * 1024;
+size_t tile_bytes(int tile_agents) { return (size_t)std::max(tile_agents, 0) * 3 * sizeof(float); }
+
+int set_smem_limit(cbm_batch* b) {
+  const int bytes = (int)tile_bytes(b->tune.tile_agents);
+  BCUDA(b, cudaFuncSetAttribute(k_batch<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  BCUDA(b, cudaFuncSetAttribute(k_batch<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  BCUDA(b, cudaFuncSetAttribute(k_batch<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  BCUDA(b, cudaFuncSetAttribute(k_batch<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  return CBM_OK;
+}
+
 BatchParams batch_params(const cbm_batch* b) {
   BatchParams B;
   memset(&B, 0, sizeof B);
@@ -375,10 +471,10 @@ BatchParams batch_params(const cbm_batch* b) {
   B.step = b->step;
   B.cell_count = b->cell_count;
   B.cell_start = b->cell_start;
-  B.agent_cell = b->agent_cell;
-  B.agent_rank = b->agent_rank;
-  B.tmp = b->tmp;
-  B.cell_agents = b->cell_agents;
+  B.key = b->key;
+  B.rank = b->rank;
+  B.sidx = b->sidx;
+  B.tile = b->tune.tile_agents;
   B.nbr_n = b->nbr_n;
   B.nbr_list = b->nbr_list;
   B.max_nbrs = b->base.n_max_neighbors;
@@ -400,11 +496,12 @@ int enqueue_batch(cbm_batch* b, int nsteps) {
   BatchParams B = batch_params(b);
   cudaMemsetAsync(b->d_head, 0, sizeof(int), b->stream);
   const int grid = b->n_sm * std::max(1, b->tune.ctas_per_sm);
+  const size_t smem = tile_bytes(b->tune.tile_agents);
   switch (b->tune.threads) {
-    case 128: k_batch<128><<<grid, 128, 0, b->stream>>>(B, nsteps); break;
-    case 512: k_batch<512><<<grid, 512, 0, b->stream>>>(B, nsteps); break;
-    case 1024: k_batch<1024><<<grid, 1024, 0, b->stream>>>(B, nsteps); break;
-    default: k_batch<256><<<grid, 256, 0, b->stream>>>(B, nsteps); break;
+    case 128: k_batch<128><<<grid, 128, smem, b->stream>>>(B, nsteps); break;
+    case 512: k_batch<512><<<grid, 512, smem, b->stream>>>(B, nsteps); break;
+    case 1024: k_batch<1024><<<grid, 1024, smem, b->stream>>>(B, nsteps); break;
+    default: k_batch<256><<<grid, 256, smem, b->stream>>>(B, nsteps); break;
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return bfail(b, CBM_ERR_CUDA, "batch launch failed: %s", cudaGetErrorString(e));
@@ -428,6 +525,7 @@ int batch_sync(cbm_batch* b) {
 // rebuilds its list at its next step
 int apply_tuning(cbm_batch* b) {
   drop_graphs(b);
+  if (int rc = set_smem_limit(b)) return rc;
   for (void* p : b->cell_allocs) cudaFree(p);
   b->cell_allocs.clear();
   const double R = list_radius(b);
@@ -529,10 +627,9 @@ int cbm_batch_create(cbm_batch** out, const cbm_config* base, int32_t n_comm,
   b->P[0] = (float4*)balloc(b->allocs, n * 16, &ok);
   b->P[1] = (float4*)balloc(b->allocs, n * 16, &ok);
   b->pold = (float4*)balloc(b->allocs, n * 16, &ok);
-  b->agent_cell = (int*)balloc(b->allocs, n * 4, &ok);
-  b->agent_rank = (int*)balloc(b->allocs, n * 4, &ok);
-  b->tmp = (int*)balloc(b->allocs, n * 4, &ok);
-  b->cell_agents = (int*)balloc(b->allocs, n * 4, &ok);
+  b->key = (int*)balloc(b->allocs, n * 4, &ok);
+  b->rank = (int*)balloc(b->allocs, n * 4, &ok);
+  b->sidx = (int*)balloc(b->allocs, n * 4, &ok);
   b->nbr_n = (int*)balloc(b->allocs, n * 4, &ok);
   b->nbr_list = (int*)balloc(b->allocs, n * (size_t)base->n_max_neighbors * 4, &ok);
   b->parity = (int*)balloc(b->allocs, nc * 4, &ok);
@@ -580,6 +677,8 @@ int cbm_batch_set_tuning(cbm_batch* b, const cbm_batch_tuning* t) {
     return bfail(b, CBM_ERR_ARG, "threads must be 128, 256, 512 or 1024");
   if (t->ctas_per_sm < 1 || t->ctas_per_sm > 8 || !(t->skin > 0))
     return bfail(b, CBM_ERR_ARG, "ctas_per_sm must be in [1, 8] and skin positive");
+  if (t->tile_agents < 0 || tile_bytes(t->tile_agents) > (size_t)kMaxTileBytes)
+    return bfail(b, CBM_ERR_ARG, "tile_agents must be in [0, %d]", kMaxTileBytes / 12);
   cudaSetDevice(b->device);
   BCUDA(b, cudaStreamSynchronize(b->stream));
   b->tune = *t;
@@ -602,7 +701,11 @@ int cbm_batch_upload(cbm_batch* b, int32_t c, const cbm_state_view* h) {
   const float* x = (const float*)h->pos[0];
   const float* y = (const float*)h->pos[1];
   const float* z = (const float*)h->pos[2];
-  for (int i = 0; i < C.n; ++i) packed[(size_t)i] = make_float4(x[i], y[i], z[i], 0.f);
+  for (int i = 0; i < C.n; ++i) {
+    float w;
+    memcpy(&w, &i, sizeof w);  // the agent index rides in w
+    packed[(size_t)i] = make_float4(x[i], y[i], z[i], w);
+  }
   BCUDA(b, cudaStreamSynchronize(b->stream));
   if (C.n) BCUDA(b, cudaMemcpy(b->P[0] + C.off, packed.data(), (size_t)C.n * 16, cudaMemcpyHostToDevice));
   int zero = 0, one = 1;
@@ -628,10 +731,15 @@ int cbm_batch_download(cbm_batch* b, int32_t c, cbm_state_view* h) {
   float* x = (float*)h->pos[0];
   float* y = (float*)h->pos[1];
   float* z = (float*)h->pos[2];
-  for (int i = 0; i < C.n; ++i) {
-    if (x) x[i] = packed[(size_t)i].x;
-    if (y) y[i] = packed[(size_t)i].y;
-    if (z) z[i] = packed[(size_t)i].z;
+  // slot order -> index order
+  for (int s = 0; s < C.n; ++s) {
+    const float4& p = packed[(size_t)s];
+    int i;
+    memcpy(&i, &p.w, sizeof i);
+    if (i < 0 || i >= C.n) return bfail(b, CBM_ERR_CUDA, "community %d: corrupt agent index", c);
+    if (x) x[i] = p.x;
+    if (y) y[i] = p.y;
+    if (z) z[i] = p.z;
   }
   h->N = C.n;
   h->step = st;
@@ -682,9 +790,11 @@ int cbm_batch_autotune(cbm_batch* b, int32_t trial_steps, cbm_batch_tuning* best
   BCUDA(b, cudaMemcpy(par.data(), b->parity, nc * 4, cudaMemcpyDeviceToHost));
   BCUDA(b, cudaMemcpy(st.data(), b->step, nc * 8, cudaMemcpyDeviceToHost));
   const cbm_batch_tuning start = b->tune;
-  const int threads[] = {128, 256, 512, 1024};
-  const int ctas[] = {1, 2, 4};
-  const double skins[] = {0.15, 0.3, 0.6};
+  const int threads[] = {256, 512, 1024};
+  const int ctas[] = {1, 2};
+  const double skins[] = {0.3, 0.6, 1.0, 1.5};
+  int largest = 0;
+  for (const Comm& C : b->comms) largest = std::max(largest, C.n);
   cbm_batch_tuning best = start;
   float best_ms = 1e30f;
   cudaEvent_t e0, e1;
@@ -692,9 +802,14 @@ int cbm_batch_autotune(cbm_batch* b, int32_t trial_steps, cbm_batch_tuning* best
   cudaEventCreate(&e1);
   for (double sk : skins)
     for (int th : threads)
-      for (int cp : ctas) {
+      for (int cp : ctas)
+        for (int staged = 0; staged < 2; ++staged) {
         if (th * cp > 2048) continue;
-        cbm_batch_tuning t{th, cp, sk, 0.0};
+        // tile: the shared memory a CTA can hold when cp CTAs share an SM
+        const int fit = (int)std::min<long long>(kMaxTileBytes, 227 * 1024 / cp - 1024) / 12;
+        const int tile = staged ? std::min(fit, largest) : 0;
+        if (staged && tile < 1) continue;
+        cbm_batch_tuning t{th, cp, sk, 0.0, tile, 0};
         if (cbm_batch_set_tuning(b, &t)) continue;
         BCUDA(b, cudaMemcpy(b->P[0], p0.data(), n * 16, cudaMemcpyHostToDevice));
         BCUDA(b, cudaMemcpy(b->P[1], p1.data(), n * 16, cudaMemcpyHostToDevice));

@@ -258,6 +258,10 @@ typedef struct cbm_batch_tuning {
   int32_t ctas_per_sm;   /* resident CTAs per SM of the persistent grid */
   double skin;           /* Verlet skin: list radius = cutoff + skin */
   double rebuild_threshold; /* displacement that triggers a rebuild; <= 0: skin / 2 */
+  int32_t tile_agents;   /* communities of at most this many agents gather neighbor
+                            positions from a shared-memory tile (12 B per agent,
+                            at most 220 KiB); 0: every gather goes through L1/L2 */
+  int32_t pad;
 } cbm_batch_tuning;
 
 typedef struct cbm_batch cbm_batch;
@@ -275,7 +279,8 @@ int cbm_batch_step(cbm_batch* b, int32_t nsteps, int32_t flags);
 int cbm_batch_set_tuning(cbm_batch* b, const cbm_batch_tuning* tuning);
 int cbm_batch_get_tuning(cbm_batch* b, cbm_batch_tuning* tuning);
 /* Times trial_steps on a copy of the current state for every candidate
- * (threads x CTAs per SM x skin), keeps the fastest and restores the state. */
+ * (threads x CTAs per SM x shared-memory tile x skin), keeps the fastest and
+ * restores the state.  A candidate whose lists overflow is skipped. */
 int cbm_batch_autotune(cbm_batch* b, int32_t trial_steps, cbm_batch_tuning* best);
 void* cbm_batch_stream(cbm_batch* b);
 

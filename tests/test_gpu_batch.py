@@ -22,9 +22,13 @@ def run_plain(abi, base, desc, state, tuning, steps):
     return g.download()
 
 
-@pytest.mark.parametrize("tuning", [dict(threads=256, ctas_per_sm=2, skin=0.3, rebuild_threshold=0.0),
-                                    dict(threads=128, ctas_per_sm=4, skin=0.15, rebuild_threshold=0.0),
-                                    dict(threads=1024, ctas_per_sm=1, skin=0.6, rebuild_threshold=0.0)])
+# tile_agents: 0 gathers through L1/L2; 1000 mixes staged and unstaged
+# communities in one launch; 18000 stages every community
+@pytest.mark.parametrize("tuning", [
+    dict(threads=256, ctas_per_sm=2, skin=0.3, rebuild_threshold=0.0, tile_agents=0),
+    dict(threads=128, ctas_per_sm=4, skin=0.15, rebuild_threshold=0.0, tile_agents=1000),
+    dict(threads=1024, ctas_per_sm=1, skin=0.6, rebuild_threshold=0.0, tile_agents=18000),
+    dict(threads=512, ctas_per_sm=2, skin=1.5, rebuild_threshold=0.2, tile_agents=9000)])
 def test_batch_matches_plain_path(gpu_lib, abi, tuning):
     base, descs, states = small_sweep(abi)
     b = cbm.Batch(abi.make_config(**base), make_descs(abi, descs))
