@@ -373,60 +373,94 @@ def run_ours(args, rank, world, local_rank):
                 launches=launches, cfg=cfg, state_n=len(state["x"]), kw=kw)
 
 
-def run_batched(args):
+def run_batched(args, rank=0, world=1, dist=None):
     """512 communities (N_i ~ U[500, 20000]) x 500 EM steps in one persistent
-    launch, against the plain path run once per community (a sample)."""
+    launch per GPU, against the plain path run once per community (a sample).
+    Under torchrun the communities are partitioned across ranks by agent count
+    (no data-path collective; strong scaling of the fixed sweep) and the time
+    is the max over ranks."""
     import torch
     from scenarios import batched_sweep, make_descs, plain_config_for
     cbm = load_package()
     abi = cbm._abi
     base, descs, states = batched_sweep(abi, n_comm=args.batched_comms)
-    b = cbm.Batch(abi.make_config(**base), make_descs(abi, descs))
-    for c, st in enumerate(states):
-        b.upload(c, st["x"], st["y"], st["z"])
-    t0 = time.perf_counter()
-    tuning = b.autotune(trial_steps=args.batched_trial)
-    tune_s = time.perf_counter() - t0
-    stream = torch.cuda.ExternalStream(b.stream())
-    b.step(args.batched_steps)  # first replay builds the graph
-    for c, st in enumerate(states):
-        b.upload(c, st["x"], st["y"], st["z"])
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    clocks = Clocks(torch.cuda.current_device())
-    clocks.start()
-    e0.record(stream)
-    b.step(args.batched_steps, 0)
-    e1.record(stream)
-    e1.synchronize()
-    clk = clocks.stop()
-    b.step(0)  # report device flags
-    ms = e0.elapsed_time(e1)
+    sb = cbm.ShardedBatch(abi.make_config(**base), make_descs(abi, descs), rank=rank, world=world)
+    b = sb.batch
+
+    def load_all():
+        for c, st in enumerate(states):
+            sb.upload(c, st["x"], st["y"], st["z"])
+
+    load_all()
+    tuning, tune_s = None, 0.0
+    if b is not None:
+        t0 = time.perf_counter()
+        tuning = b.autotune(trial_steps=args.batched_trial)
+        tune_s = time.perf_counter() - t0
+        b.step(args.batched_steps)  # first replay builds the graph
+    load_all()
+    ms, clk = 0.0, None
+    if dist:
+        dist.barrier()
+    if b is not None:
+        stream = torch.cuda.ExternalStream(b.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        clocks = Clocks(torch.cuda.current_device())
+        clocks.start()
+        e0.record(stream)
+        b.step(args.batched_steps, 0)
+        e1.record(stream)
+        e1.synchronize()
+        clk = clocks.stop()
+        b.step(0)  # report device flags
+        ms = e0.elapsed_time(e1)
+    ms_job = cbm.sweep.max_over_ranks(dist, ms)
     total = sum(d["n"] for d in descs)
-    batched = total * args.batched_steps / (ms / 1e3)
-    # the plain path, one community at a time (contexts created beforehand)
+    batched = total * args.batched_steps / (ms_job / 1e3)
+    out = {"communities": len(descs), "agents": int(total), "steps": args.batched_steps,
+           "value": round(batched, 1), "unit": UNIT, "ms": round(ms_job, 3),
+           "ranks": world, "scaling": "strong" if world > 1 else None,
+           "rank0_communities": len(sb.mine), "rank0_agents": int(sb.n_agents),
+           "tuning": tuning.as_dict() if tuning is not None else None,
+           "autotune_s": round(tune_s, 3), "clocks": clk}
+    if rank != 0 or tuning is None:
+        return out
+    # The plain path, one community at a time, on a sample of the communities:
+    # device time of the 500 steps (graphs built beforehand by a 2-step run of
+    # the same context) and end to end (upload + 500 steps + download).
     rng = np.random.default_rng(7)
     sample = sorted(rng.choice(len(descs), size=min(args.plain_sample, len(descs)), replace=False))
-    ctxs = [cbm.Context(abi.make_config(**plain_config_for(abi, base, descs[c], tuning.as_dict())))
-            for c in sample]
-    agents, secs = 0, 0.0
-    for c, g in zip(sample, ctxs):
+    agents, dev_ms, e2e_s = 0, 0.0, 0.0
+    for c in sample:
         st = states[c]
+        g = cbm.Context(abi.make_config(**plain_config_for(abi, base, descs[c], tuning.as_dict())))
+        g.upload(st)
+        g.step(2)  # builds the step graph of both parities
+        stream = torch.cuda.ExternalStream(g.stream())
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g.upload(st)
-        g.step(args.batched_steps)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.step(args.batched_steps, 0)
+        e1.record(stream)
         g.download()
-        secs += time.perf_counter() - t0
+        e2e_s += time.perf_counter() - t0
+        dev_ms += e0.elapsed_time(e1)
         agents += descs[c]["n"] * args.batched_steps
         g.close()
-    plain = agents / secs
-    return {"communities": len(descs), "agents": int(total), "steps": args.batched_steps,
-            "value": round(batched, 1), "unit": UNIT, "ms": round(ms, 3),
-            "plain_value": round(plain, 1), "plain_sample": len(sample),
-            "speedup_vs_plain": round(batched / plain, 2), "tuning": tuning.as_dict(),
-            "autotune_s": round(tune_s, 3), "clocks": clk}
+    plain_dev = agents / (dev_ms / 1e3)
+    out.update({"plain_value": round(plain_dev, 1), "plain_e2e_value": round(agents / e2e_s, 1),
+                "plain_sample": len(sample),
+                "plain_timing": "device events around the 500 graph-replayed steps of each "
+                                "sampled community (graphs built beforehand); e2e adds "
+                                "upload and download"})
+    if world == 1:
+        out["speedup_vs_plain"] = round(batched / plain_dev, 2)
+    return out
 
 
 def run_adjoint(args):
@@ -442,24 +476,34 @@ def run_adjoint(args):
                                                 cell_edge=max(kw["cell_edge"], 1.5 * rho))))
     tgt = tgt_fw.forward(x0, args.adjoint_steps)
     adj = cbm.Adjoint(abi.make_config(**kw))
-    adj.forward(x0, args.adjoint_steps)  # warm-up
+    adj.forward(x0, args.adjoint_steps)  # warm-up: builds the forward plan (buffers + graph)
     adj.run(x0, tgt, args.adjoint_steps, checkpoint_every=args.checkpoint_every)
-    reps = 3
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        adj.forward(x0, args.adjoint_steps)
-    fwd = (time.perf_counter() - t0) / reps
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        res = adj.run(x0, tgt, args.adjoint_steps, checkpoint_every=args.checkpoint_every)
-    full = (time.perf_counter() - t0) / reps
+    stream = torch.cuda.ExternalStream(adj.stream())
+
+    def timed(fn, reps=5):
+        out, ms = None, []
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            out = fn()  # synchronous: copies in, graph replay, copies out
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return out, float(np.median(ms))
+
+    _, fwd = timed(lambda: adj.forward(x0, args.adjoint_steps))
+    res, full = timed(lambda: adj.run(x0, tgt, args.adjoint_steps,
+                                      checkpoint_every=args.checkpoint_every))
     return {"agents": args.adjoint_n, "steps": args.adjoint_steps, "dtype": "f64",
-            "checkpoint_every": args.checkpoint_every, "forward_ms": round(1e3 * fwd, 3),
-            "forward_plus_adjoint_ms": round(1e3 * full, 3),
+            "checkpoint_every": args.checkpoint_every, "forward_ms": round(fwd, 3),
+            "forward_plus_adjoint_ms": round(full, 3), "backward_ms": round(full - fwd, 3),
             "cost_ratio": round(full / fwd, 3), "loss": res["loss"],
             "dL_dtheta": [float(v) for v in res["dtheta"]],
-            "timing": "host wall clock around synchronous calls, incl. host<->device copies"}
+            "timing": "CUDA events on the adjoint stream around each synchronous call "
+                      "(host<->device copies included), median of 5; cost_ratio = "
+                      "(forward + checkpointed backward) / forward"}
 
 
 def cpu_baseline(args, steps, threads=None):
@@ -544,9 +588,9 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
     r = run_ours(args, rank, world, local_rank)
     cb = batched = adjoint = None
+    if not args.no_batched:
+        batched = run_batched(args, rank, world, dist if world > 1 else None)
     if rank == 0 and world == 1:
-        if not args.no_batched:
-            batched = run_batched(args)
         if not args.no_adjoint:
             adjoint = run_adjoint(args)
         if not args.no_cpu_baseline:

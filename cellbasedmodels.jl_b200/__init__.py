@@ -24,14 +24,16 @@ from types import SimpleNamespace
 
 import numpy as np
 
-from . import _abi
+from . import _abi, sweep  # noqa: F401
 from ._abi import (Adjoint, Batch, CbmConfig, CbmError, Context, load_library,  # noqa: F401
                    make_config)
+from .sweep import ShardedBatch, partition_communities  # noqa: F401
 
 __all__ = ["ABM", "Community", "evolve", "step", "loadToPlatform", "bringFromPlatform",
            "agentStepRule", "agentStepDE", "mediumStepRule", "mediumStepDE", "update",
            "computeNeighbors", "CBMNeighbors", "CBMIntegrators", "SoftSpheres", "Growth",
-           "Medium", "B200", "Context", "Batch", "CbmError", "make_config", "load_library"]
+           "Medium", "B200", "Context", "Batch", "Adjoint", "ShardedBatch",
+           "partition_communities", "CbmError", "make_config", "load_library"]
 
 
 # ---- algorithm descriptors (src/neighbors.jl, src/integrators.jl) -------------
