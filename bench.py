@@ -506,6 +506,156 @@ def run_adjoint(args):
                       "(forward + checkpointed backward) / forward"}
 
 
+def _device_steps(cbm, ctx, steps, flush=None):
+    """Device time (ms) of `steps` graph-replayed steps, one event pair per step."""
+    import torch
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    total = 0.0
+    for _ in range(steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.step(1, 0)
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+        if flush is not None:
+            flush.zero_()
+            torch.cuda.synchronize()
+    ctx.sync()
+    return total
+
+
+def _rel_err(a, b):
+    """max |a - b| over max |b| (positions: relative to the box scale)."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)) if b.size else 0.0
+
+
+def run_configs(args):
+    """The other configurations of the path: the 2D aggregation (Float64,
+    L2-resident, launch-bound: us/step) and 2D chemotaxis on a 1024^2 medium
+    (agent-steps/s and medium cell-updates/s), each with the CPU checker
+    beside it; the 3D colony in Float64; and the error of every Float32 result
+    against a Float64 run of the same seeded inputs after 100 steps."""
+    import torch
+    from _oracle import OracleContext
+    from scenarios import aggregation_2d, chemotaxis_2d, colony_3d, packed_colony_3d
+    cbm = load_package()
+    abi = cbm._abi
+    out = {}
+    threads = os.cpu_count()
+
+    # c1: 2D aggregation, N=4096, Float64, 1000 steps
+    kw, st = aggregation_2d(abi)
+    g = cbm.Context(abi.make_config(**kw))
+    g.upload(st)
+    g.step(3)
+    ms = _device_steps(cbm, g, args.config_steps)
+    o = OracleContext(abi, abi.make_config(**kw), threads=threads)
+    o.upload(st)
+    t0 = time.perf_counter()
+    o.step(args.config_cpu_steps)
+    cpu_s = (time.perf_counter() - t0) / args.config_cpu_steps
+    o.close()
+    g.close()
+    out["aggregation_2d"] = {
+        "agents": 4096, "dtype": "f64", "steps_timed": args.config_steps,
+        "us_per_step": round(1e3 * ms / args.config_steps, 2),
+        "value": round(4096 * args.config_steps / (ms / 1e3), 1), "unit": UNIT,
+        "cpu_us_per_step": round(1e6 * cpu_s, 2), "cpu_cores": threads,
+        "note": "L2-resident and launch-bound: one graph replay per step (rule, DE, update, grid)"}
+
+    # c3: 2D chemotaxis, 2e5 agents, 1024^2 Float32 medium
+    kw, st = chemotaxis_2d(abi)
+    g = cbm.Context(abi.make_config(**kw))
+    g.upload(st)
+    g.step(3)
+    ms = _device_steps(cbm, g, args.config_steps)
+    prof = {}
+    for _ in range(3):
+        for name, kms in g.profile_step():
+            prof.setdefault(name, []).append(kms)
+    nodes = 1024 * 1024
+    o = OracleContext(abi, abi.make_config(**kw), threads=threads)
+    o.upload(st)
+    t0 = time.perf_counter()
+    o.step(args.config_cpu_steps)
+    cpu_s = (time.perf_counter() - t0) / args.config_cpu_steps
+    o.close()
+    g.close()
+    out["chemotaxis_2d"] = {
+        "agents": 200000, "medium": "1024x1024", "dtype": "f32", "steps_timed": args.config_steps,
+        "us_per_step": round(1e3 * ms / args.config_steps, 2),
+        "value": round(200000 * args.config_steps / (ms / 1e3), 1), "unit": UNIT,
+        "cell_updates_per_s": round(nodes * args.config_steps / (ms / 1e3), 1),
+        "cpu_value": round(200000 / cpu_s, 1), "cpu_cores": threads,
+        "kernel_avg_ms": {k: round(float(np.mean(v)), 4) for k, v in prof.items()},
+        "note": "bilinear secretion as an ordered gather, FTCS, chemotactic drift"}
+
+    # c2 in Float64: the same 1M colony snapshot
+    kw, st = packed_colony_3d(abi, N=args.n, precision=abi.F64)
+    g = cbm.Context(abi.make_config(**kw))
+    g.upload(st)
+    g.step(3)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    n0 = g.counters()["N"]
+    ms = _device_steps(cbm, g, args.config_f64_steps, flush=flush)
+    g.close()
+    del flush
+    out["colony_3d_f64"] = {"agents": int(n0), "steps_timed": args.config_f64_steps,
+                            "ms_per_step": round(ms / args.config_f64_steps, 4),
+                            "value": round(n0 * args.config_f64_steps / (ms / 1e3), 1),
+                            "unit": UNIT}
+
+    # Error of the Float32 results against Float64 runs, 100 steps.  The noise
+    # of an SDE run is drawn in the run's precision (Box-Muller in float or
+    # double), so the two precisions follow different sample paths; the
+    # comparison therefore runs each configuration with sigma = 0, which
+    # isolates the arithmetic precision.
+    def colony_nodiv(abi, precision):
+        # division thresholds (v >= 2) are crossed at different steps in the two
+        # precisions, which changes the agent set; growth and death are off here
+        kw, st = colony_3d(abi, N=20000, precision=precision, p_death=0.0, sigma=0.0)
+        return dict(kw, growth=0, fate=abi.FATE_NONE), st
+
+    def chemo_ode(abi, precision):
+        kw, st = chemotaxis_2d(abi, N=20000, L=256.0, n_medium=256, precision=precision)
+        return dict(kw, sigma=0.0, integrator=abi.INT_EULER), st
+
+    def pair(builder, keys, steps=100):
+        res = []
+        for prec in (abi.F32, abi.F64):
+            kw, st = builder(abi, precision=prec)
+            g = cbm.Context(abi.make_config(**kw))
+            g.upload(st)
+            g.step(steps)
+            res.append(g.download())
+            g.close()
+        f32, f64 = res
+        if f32["N"] != f64["N"]:
+            return {"N_f32": int(f32["N"]), "N_f64": int(f64["N"])}
+        out = {}
+        for k in keys:
+            a = np.asarray(f32[k], np.float64)
+            b = np.asarray(f64[k], np.float64)
+            scale = max(float(np.max(np.abs(b))), 1e-300)
+            d = np.abs(a - b) / scale
+            out[k] = {"max": float(np.max(d)), "median": float(np.median(d))}
+        return out
+
+    out["error_vs_f64_100_steps"] = {
+        "aggregation_2d": pair(aggregation_2d, ("x", "y")),
+        "chemotaxis_2d_sigma0": pair(chemo_ode, ("x", "y", "c")),
+        "colony_3d_sigma0_no_division": pair(colony_nodiv, ("x", "y", "z")),
+        "definition": "|v_f32 - v_f64| / max |v_f64| per field after 100 steps from the same "
+                      "seeded inputs, max and median over agents (medium nodes for c); "
+                      "Float32 and Float64 runs on the GPU, each bit-identical to the CPU "
+                      "checker in its own precision"}
+    return out
+
+
 def cpu_baseline(args, steps, threads=None):
     """The CPU checker on the same workload (CellLinked, rebuilt every step)."""
     cbm = load_package()
@@ -547,6 +697,10 @@ def main():
     ap.add_argument("--batched-trial", type=int, default=20)
     ap.add_argument("--plain-sample", type=int, default=32)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-configs", action="store_true")
+    ap.add_argument("--config-steps", type=int, default=200)
+    ap.add_argument("--config-cpu-steps", type=int, default=5)
+    ap.add_argument("--config-f64-steps", type=int, default=10)
     ap.add_argument("--adjoint-n", type=int, default=65536)
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--checkpoint-every", type=int, default=20)
@@ -590,7 +744,10 @@ def main():
     cb = batched = adjoint = None
     if not args.no_batched:
         batched = run_batched(args, rank, world, dist if world > 1 else None)
+    configs = None
     if rank == 0 and world == 1:
+        if not args.no_configs:
+            configs = run_configs(args)
         if not args.no_adjoint:
             adjoint = run_adjoint(args)
         if not args.no_cpu_baseline:
@@ -604,7 +761,7 @@ def main():
                 "cpu_baseline": cb, "e2e": r["e2e"], "gpu_launches": r["launches"],
                 "clocks": r["clocks"], "kernel_share": r["share"],
                 "kernel_avg_ms": {k: round(v[0], 4) for k, v in r["kern"].items()},
-                "batched": batched, "adjoint": adjoint}
+                "batched": batched, "adjoint": adjoint, "configs": configs}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -334,40 +334,13 @@ __device__ __forceinline__ bool secretion_by_gather(const Params<T>& P) {
 template <typename T, int D>
 __global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
   constexpr int kMaxCells = D == 1 ? 4 : (D == 2 ? 16 : 64);
+  constexpr int kTouch = 32;  // agents collected per node before the merge fallback
   const int n = blockIdx.x * kTile + threadIdx.x;
   if (n >= P.n_nodes) return;
   int q[3] = {0, 0, 0};
   q[0] = n % P.n_medium[0];
   if (D > 1) q[1] = (n / P.n_medium[0]) % P.n_medium[1];
   if (D > 2) q[2] = n / (P.n_medium[0] * P.n_medium[1]);
-  // agents touching node q along an axis lie in x in [lo+(q-1/2)dx, lo+(q+3/2)dx)
-  // (unbounded below for q = 0, above for the last node); widen by one cell
-  int c0[3] = {0, 0, 0}, c1[3] = {0, 0, 0};
-#pragma unroll
-  for (int d = 0; d < D; ++d) {
-    const int nc = P.n_cells_d[d];
-    int a = q[d] == 0 ? 0
-                      : cell_pos1<T>(P.edge, P.box_lo[d] + ((T)q[d] - (T)0.5) * P.dx_m[d],
-                                     P.box_lo[d], P.box_hi[d], nc) - 1;
-    int b = q[d] == P.n_medium[d] - 1
-                ? nc - 1
-                : cell_pos1<T>(P.edge, P.box_lo[d] + ((T)q[d] + (T)1.5) * P.dx_m[d],
-                               P.box_lo[d], P.box_hi[d], nc) + 1;
-    c0[d] = a < 0 ? 0 : a;
-    c1[d] = b > nc - 1 ? nc - 1 : b;
-  }
-  // one cursor per cell: agents are ascending inside a cell
-  int cur[kMaxCells], end[kMaxCells];
-  int ncand = 0;
-  bool all = true;
-  for (int cz = c0[2]; cz <= c1[2]; ++cz)
-    for (int cy = c0[1]; cy <= c1[1]; ++cy)
-      for (int cx = c0[0]; cx <= c1[0]; ++cx) {
-        if (ncand == kMaxCells) { all = false; continue; }
-        int c = cx + P.n_cells_d[0] * (cy + P.n_cells_d[1] * cz);
-        int s0 = P.cell_start[c], s1 = P.cell_start[c + 1];
-        if (s0 < s1) { cur[ncand] = s0; end[ncand] = s1; ++ncand; }
-      }
   const T amt = P.secretion_amt;
   T acc = P.c_cur[n];
   auto add = [&](int slot) {
@@ -380,6 +353,85 @@ __global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
     for (int k = 0; k < (1 << D); ++k)
       if (nodes[k] == n) acc = acc + w[k] * amt;
   };
+  auto touches = [&](int slot) {
+    T x[3];
+    to3<T>(P.PA[slot], x);
+    int nodes[8];
+    T w[8];
+    bilinear<T, D>(P, x, nodes, w);
+    bool t = false;
+#pragma unroll
+    for (int k = 0; k < (1 << D); ++k) t = t || nodes[k] == n;
+    return t;
+  };
+  // Agents whose stencil covers node q along an axis lie in x in
+  // [lo+(q-1/2)dx, lo+(q+3/2)dx) (unbounded below for q = 0, above for the
+  // last node).  The cells of that box, widened by a rounding margin, are
+  // scanned; the agents that touch the node are kept sorted by index and
+  // added in that order, the order of the reference's serial agent loop.
+  int c0[3] = {0, 0, 0}, c1[3] = {0, 0, 0};
+  int ncell = 1;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const int nc = P.n_cells_d[d];
+    const T dx = P.dx_m[d];
+    const T margin = (T)1e-3 * dx + (T)64 * Eps<T>::v * (fabs(P.box_lo[d]) + fabs(P.box_hi[d]));
+    c0[d] = q[d] == 0 ? 0
+                      : cell_pos1<T>(P.edge, P.box_lo[d] + ((T)q[d] - (T)0.5) * dx - margin,
+                                     P.box_lo[d], P.box_hi[d], nc);
+    c1[d] = q[d] == P.n_medium[d] - 1
+                ? nc - 1
+                : cell_pos1<T>(P.edge, P.box_lo[d] + ((T)q[d] + (T)1.5) * dx + margin,
+                               P.box_lo[d], P.box_hi[d], nc);
+    ncell *= c1[d] - c0[d] + 1;
+  }
+  int tj[kTouch], ts[kTouch];
+  int nt = 0;
+  bool ok = ncell <= kMaxCells;
+  for (int cz = c0[2]; ok && cz <= c1[2]; ++cz)
+    for (int cy = c0[1]; ok && cy <= c1[1]; ++cy) {
+      const int row = P.n_cells_d[0] * (cy + P.n_cells_d[1] * cz);
+      const int s1 = P.cell_start[row + c1[0] + 1];
+      for (int sl = P.cell_start[row + c0[0]]; sl < s1; ++sl) {
+        if (!touches(sl)) continue;
+        if (nt == kTouch) {
+          ok = false;
+          break;
+        }
+        const int j = P.IA[sl];
+        int k = nt++;
+        for (; k > 0 && tj[k - 1] > j; --k) {
+          tj[k] = tj[k - 1];
+          ts[k] = ts[k - 1];
+        }
+        tj[k] = j;
+        ts[k] = sl;
+      }
+    }
+  if (ok) {
+    for (int k = 0; k < nt; ++k) add(ts[k]);
+    P.c_cur[n] = acc;
+    return;
+  }
+  // Fallback (a crowded node, or cells much smaller than the medium spacing):
+  // k-way merge over the cells of the box widened by one cell, or every agent
+  // in index order when even that box is too large.
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    c0[d] = c0[d] > 0 ? c0[d] - 1 : 0;
+    c1[d] = c1[d] < P.n_cells_d[d] - 1 ? c1[d] + 1 : P.n_cells_d[d] - 1;
+  }
+  int cur[kMaxCells], end[kMaxCells];
+  int ncand = 0;
+  bool all = true;
+  for (int cz = c0[2]; cz <= c1[2]; ++cz)
+    for (int cy = c0[1]; cy <= c1[1]; ++cy)
+      for (int cx = c0[0]; cx <= c1[0]; ++cx) {
+        if (ncand == kMaxCells) { all = false; continue; }
+        int c = cx + P.n_cells_d[0] * (cy + P.n_cells_d[1] * cz);
+        int s0 = P.cell_start[c], s1 = P.cell_start[c + 1];
+        if (s0 < s1) { cur[ncand] = s0; end[ncand] = s1; ++ncand; }
+      }
   if (all) {
     while (true) {  // k-way merge: next smallest agent index among the cells
       int best = -1, bj = 0x7fffffff;
@@ -392,8 +444,6 @@ __global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
       add(cur[best]++);
     }
   } else {
-    // the cell box is too large (cells much smaller than the medium spacing):
-    // visit every agent in index order
     const int N = (int)P.ctr->N[P.parity];
     for (int j = 0; j < N; ++j) add(P.inv[j]);
   }
