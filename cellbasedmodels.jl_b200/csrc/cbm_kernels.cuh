@@ -222,7 +222,15 @@ __device__ __forceinline__ void for_cell_slots(const Params<T>& P, const T* x, F
   }
 }
 
-constexpr int kQueue = 32;  // per-thread force queue of k_agent_de (32 KB per block)
+// Per-thread force queue of k_agent_de, in shared memory (kQueue * 1 KB per
+// block, 48 KB: the static limit).  A drain is cheapest when it runs once,
+// converged, at the end of an agent's walk: 48 entries hold every candidate
+// inside the cutoff of nearly every agent (about 17 on average in a packed
+// colony), which measured faster than 8 to 40 entries.
+#ifndef CBM_FORCE_QUEUE
+#define CBM_FORCE_QUEUE 48
+#endif
+constexpr int kQueue = CBM_FORCE_QUEUE;
 
 template <typename T>
 struct Eps;
@@ -696,9 +704,19 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
       // force-only walk (CellLinked, or a CLVD step that will rebuild anyway
       // and whose cutoff lies inside the list radius): four independent
       // candidates per iteration, then an in-order enqueue
+      // The queue is drained by every active lane together when one of them
+      // may run out of room, so drains run converged.
+      auto push = [&](int q) {
+        queue[nq * kTile + threadIdx.x] = q;
+        ++nq;
+      };
+      auto room = [&](int k) {
+        if (__any_sync(__activemask(), nq > kQueue - k)) drain();
+      };
       walk_runs<T, D>(P, xi, P.cut_reach, [&](int s0, int s1) {
         int q = s0;
         for (; q + 4 <= s1; q += 4) {
+          room(4);
           T s2v[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
@@ -708,12 +726,13 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
           }
 #pragma unroll
           for (int u = 0; u < 4; ++u)
-            if (s2v[u] < cut2 && q + u != s) enqueue(q + u);
+            if (s2v[u] < cut2 && q + u != s) push(q + u);
         }
         for (; q < s1; ++q) {
+          room(1);
           T xj[3], e[3];
           to3<T>(U[q], xj);
-          if (diff(xj, e) < cut2 && q != s) enqueue(q);
+          if (diff(xj, e) < cut2 && q != s) push(q);
         }
       });
     } else {
