@@ -68,6 +68,7 @@ struct cbm_ctx {
   int* scratch_int = nullptr;  // n_max ints for inspection calls
 
   int n_blocks = 0;
+  int n_sm = 148;             // multiprocessors of the device (grid of the compaction)
   int n_cells = 1;
   int n_cells_d[3] = {1, 1, 1};
   int n_scan_tiles = 1;
@@ -325,7 +326,7 @@ template <typename T, int D>
 void enqueue_update(cbm_ctx* c, const Params<T>& P) {
   if (c->cfg.fate != CBM_FATE_NONE) {
     PROF("k_compact");
-    k_compact<T, D><<<1, kCompactThreads, 0, c->stream>>>(P);
+    k_compact<T, D><<<c->n_sm, kCompactThreads, 0, c->stream>>>(P);
   }
   {
     PROF("k_commit");
@@ -594,6 +595,7 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
   c->cfg = k;
   c->tsize = k.precision == CBM_F64 ? 8 : 4;
   cudaGetDevice(&c->device);
+  cudaDeviceGetAttribute(&c->n_sm, cudaDevAttrMultiProcessorCount, c->device);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
     int rc = fail(nullptr, CBM_ERR_CUDA, "cudaStreamCreate failed (is a CUDA device present?)");
     delete c;

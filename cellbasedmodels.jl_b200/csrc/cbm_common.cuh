@@ -16,7 +16,8 @@ namespace cbm {
 
 constexpr int kTile = 256;          // threads per block of the per-agent kernels
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kScanItems = 8;       // cells per thread in the cell scan
+constexpr int kScanItems = 32;      // cells per thread in the cell scan (8192 per tile, so
+                                    // the look-back spans few tiles)
 constexpr int kScanTile = kTile * kScanItems;
 constexpr long long kSpinLimit = 1ll << 20;  // bounded look-back wait
 
@@ -161,10 +162,15 @@ struct ScanArgs {
   const int* due;                  // skip the scan when *due == 0 (nullptr: always)
 };
 
+// Shared-memory index of cell k of a tile: one padding word per 32 cells, so
+// that a thread reading its 32 consecutive cells hits 32 different banks.
+__device__ __forceinline__ int scan_pad(int k) { return k + (k >> 5); }
+
 static __global__ void __launch_bounds__(kTile) k_scan_cells(ScanArgs A) {
   __shared__ int warp_sums[kTile / 32];
   __shared__ unsigned s_tile;
   __shared__ int s_prefix;
+  __shared__ int s_cells[kScanTile + kScanTile / 32];
   if (A.due && *A.due == 0) return;
   Counters* C = A.ctr;
   const unsigned epoch = C->scan_epoch;
@@ -175,21 +181,33 @@ static __global__ void __launch_bounds__(kTile) k_scan_cells(ScanArgs A) {
     if (threadIdx.x == 0) atomicOr(&C->err, kErrTimeout);
     return;
   }
-  const int base = tile * kScanTile + threadIdx.x * kScanItems;
-  static_assert(kScanItems == 8, "two int4 loads per thread");
-  int vals[kScanItems];
-  if (base + kScanItems <= A.n) {
-    const int4 a = reinterpret_cast<const int4*>(A.count + base)[0];
-    const int4 b = reinterpret_cast<const int4*>(A.count + base)[1];
-    vals[0] = a.x; vals[1] = a.y; vals[2] = a.z; vals[3] = a.w;
-    vals[4] = b.x; vals[5] = b.y; vals[6] = b.z; vals[7] = b.w;
-  } else {
+  static_assert(kScanItems % 4 == 0 && kScanItems == 32, "int4 staging, 32 cells per thread");
+  const int tile_base = tile * kScanTile;
+  const bool full = tile_base + kScanTile <= A.n;
+  // coalesced load of the tile's counts into shared memory
+  if (full) {
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) vals[k] = base + k < A.n ? A.count[base + k] : 0;
+    for (int v = 0; v < kScanItems / 4; ++v) {
+      const int q = v * kTile + threadIdx.x;  // int4 index inside the tile
+      const int4 a = reinterpret_cast<const int4*>(A.count + tile_base)[q];
+      s_cells[scan_pad(4 * q)] = a.x;
+      s_cells[scan_pad(4 * q + 1)] = a.y;
+      s_cells[scan_pad(4 * q + 2)] = a.z;
+      s_cells[scan_pad(4 * q + 3)] = a.w;
+    }
+  } else {
+    for (int k = threadIdx.x; k < kScanTile; k += kTile)
+      s_cells[scan_pad(k)] = tile_base + k < A.n ? A.count[tile_base + k] : 0;
   }
+  __syncthreads();
+  const int first = threadIdx.x * kScanItems;  // this thread's cells inside the tile
+  int vals[kScanItems];
   int sum = 0;
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k) sum += vals[k];
+  for (int k = 0; k < kScanItems; ++k) {
+    vals[k] = s_cells[scan_pad(first + k)];
+    sum += vals[k];
+  }
   int total;
   int ex = block_exscan(sum, warp_sums, &total);
   const unsigned long long ep = (unsigned long long)epoch << 32;
@@ -240,33 +258,31 @@ static __global__ void __launch_bounds__(kTile) k_scan_cells(ScanArgs A) {
     }
   }
   __syncthreads();
+  // exclusive offsets back into shared memory, then coalesced stores
   int run = s_prefix + ex;
-  if (base + kScanItems <= A.n) {
-    int o[kScanItems];
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-      o[k] = run;
-      run += vals[k];
-    }
-    // start is only 4-byte aligned at this offset for odd tiles of a shifted
-    // array, so it is written as plain ints; counts are cleared as int4
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) A.start[base + k] = o[k];
-    reinterpret_cast<int4*>(A.count + base)[0] = make_int4(0, 0, 0, 0);
-    reinterpret_cast<int4*>(A.count + base)[1] = make_int4(0, 0, 0, 0);
-  } else {
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-      int c = base + k;
-      if (c < A.n) {
-        A.start[c] = run;
-        A.count[c] = 0;
-      }
-      run += vals[k];
-    }
+  for (int k = 0; k < kScanItems; ++k) {
+    s_cells[scan_pad(first + k)] = run;
+    run += vals[k];
   }
   // the thread holding the last cell writes the end sentinel
-  if (base <= A.n - 1 && A.n - 1 < base + kScanItems) A.start[A.n] = run;
+  if (A.n - 1 >= tile_base + first && A.n - 1 < tile_base + first + kScanItems) A.start[A.n] = run;
+  __syncthreads();
+  if (full) {
+    // start is only 4-byte aligned for a shifted array, so it is written as
+    // plain ints; counts are cleared as int4
+#pragma unroll 8
+    for (int k = threadIdx.x; k < kScanTile; k += kTile) A.start[tile_base + k] = s_cells[scan_pad(k)];
+#pragma unroll
+    for (int v = 0; v < kScanItems / 4; ++v)
+      reinterpret_cast<int4*>(A.count + tile_base)[v * kTile + threadIdx.x] = make_int4(0, 0, 0, 0);
+  } else {
+    for (int k = threadIdx.x; k < kScanTile; k += kTile)
+      if (tile_base + k < A.n) {
+        A.start[tile_base + k] = s_cells[scan_pad(k)];
+        A.count[tile_base + k] = 0;
+      }
+  }
 }
 
 }  // namespace cbm

@@ -918,10 +918,14 @@ __global__ void __launch_bounds__(kTile) k_medium_de(Params<T> P) {
 // ---------------------------------------------------------------------------
 constexpr int kCompactThreads = 1024;
 
-// One block.  Survivors that fill holes all lie in the tail [N_new, N + NAdd)
+// Survivors that fill holes all lie in the tail [N_new, N + NAdd)
 // and holes before N_new are exactly as many, so the tail is walked from its
 // end in chunks, survivors are ranked by a block scan, and the k-th survivor
 // from the tail moves into the k-th hole.
+//
+// When the step's births are at least its removals (a growing colony), the
+// tail holds newborns only, which all survive: the k-th survivor from the
+// tail is then slot total-1-k, and every block relabels its share directly.
 template <typename T, int D>
 __global__ void __launch_bounds__(kCompactThreads) k_compact(Params<T> P) {
   __shared__ int warp_sums[kCompactThreads / 32];
@@ -933,6 +937,20 @@ __global__ void __launch_bounds__(kCompactThreads) k_compact(Params<T> P) {
   const long long total = N + C->n_add;
   const long long n_new = total - R;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (n_new >= N) {
+    for (long long k = (long long)blockIdx.x * kCompactThreads + tid; k < R;
+         k += (long long)gridDim.x * kCompactThreads) {
+      const int dst = P.holes[k];
+      const int src = (int)(total - 1 - k);  // a newborn: working slot == index
+      P.IB[P.inv[dst]] = -1;                 // the dead agent's slot leaves the sort
+      P.G[dst] = P.G[src];
+      P.ID[dst] = P.ID[src];
+      P.PAR[dst] = P.PAR[src];
+      P.IB[src] = dst;
+    }
+    return;
+  }
+  if (blockIdx.x != 0) return;
   for (long long k = tid; k < R; k += kCompactThreads)
     P.IB[P.inv[P.holes[k]]] = -1;  // every dead agent's slot leaves the sort
   long long offset = 0;            // survivors already ranked
