@@ -50,7 +50,7 @@ struct cbm_ctx {
   // fate
   unsigned char* fate = nullptr;
   int* holes = nullptr;
-  int* blk[4] = {};
+  unsigned long long* fate_state = nullptr;  // per tile of the fused rule / births kernel
   // sort and grid
   int* s_cell = nullptr;
   int* s_rank = nullptr;
@@ -196,10 +196,7 @@ Params<T> params(const cbm_ctx* c, int parity) {
   P.hv = (T*)c->hv;
   P.fate = c->fate;
   P.holes = c->holes;
-  P.blk_children = c->blk[0];
-  P.blk_deaths = c->blk[1];
-  P.blk_child_off = c->blk[2];
-  P.blk_death_off = c->blk[3];
+  P.fate_state = c->fate_state;
   P.s_cell = c->s_cell;
   P.s_rank = c->s_rank;
   P.s_key = c->s_key;
@@ -293,17 +290,12 @@ void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P) {
     k_secrete_gather<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
   }
   if (!rule_needed(k)) return;
-  {
+  if (k.fate != CBM_FATE_NONE) {
+    PROF("k_agent_fate");
+    k_agent_fate<T, D><<<fate_tiles(c->cfg.n_max), kTile, 0, c->stream>>>(P);
+  } else {
     PROF("k_agent_rule");
     k_agent_rule<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
-  }
-  if (k.fate != CBM_FATE_NONE) {
-    {
-      PROF("k_fate_scan");
-      k_fate_scan<T><<<1, 1024, 0, c->stream>>>(P);
-    }
-    PROF("k_births");
-    k_births<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
   }
 }
 
@@ -367,8 +359,8 @@ int kernels_per_step(const cbm_ctx* c) {
   int n = 0;
   if (k.medium && k.chemotaxis != 0) n += 1;
   if (uses_gather(k)) n += 1;
-  if (rule_needed(k)) n += 1;
-  if (k.fate != CBM_FATE_NONE) n += 3;  // fate scan, births, compaction
+  if (rule_needed(k)) n += 1;           // rule (with births and deaths when fate is on)
+  if (k.fate != CBM_FATE_NONE) n += 1;  // compaction
   n += 1;                               // agent DE
   if (k.medium) n += 1;
   n += 5;                               // commit, sort hist, scan, scatter, place
@@ -569,6 +561,9 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     return fail(nullptr, CBM_ERR_ARG, "precision must be CBM_F32 or CBM_F64");
   if (k.n_max < 0 || k.n_max >= (1ll << 30))
     return fail(nullptr, CBM_ERR_ARG, "n_max must be in [0, 2^30)");
+  // the births/deaths scan packs two prefix counts of up to 2 n_max into 29 bits each
+  if (k.fate != CBM_FATE_NONE && k.n_max >= (1ll << 28))
+    return fail(nullptr, CBM_ERR_ARG, "with births and deaths n_max must be below 2^28");
   if (!(k.dt > 0)) return fail(nullptr, CBM_ERR_ARG, "dt must be positive");
   if (k.neighbors < CBM_NEIGH_NONE || k.neighbors > CBM_NEIGH_CLVD)
     return fail(nullptr, CBM_ERR_ARG, "unknown neighbor algorithm %d", k.neighbors);
@@ -666,7 +661,7 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
   c->hv = dalloc(c, n * S, &ok);
   c->fate = (unsigned char*)dalloc(c, n, &ok);
   c->holes = (int*)dalloc(c, n * 4, &ok);
-  for (int q = 0; q < 4; ++q) c->blk[q] = (int*)dalloc(c, (size_t)c->n_blocks * 4, &ok);
+  c->fate_state = (unsigned long long*)dalloc(c, (size_t)c->n_blocks * 8, &ok);
   c->s_cell = (int*)dalloc(c, n * 4, &ok);
   c->s_rank = (int*)dalloc(c, n * 4, &ok);
   c->s_key = (int*)dalloc(c, n * 4, &ok);
@@ -693,6 +688,7 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
   }
   cudaMemsetAsync(c->cell_count, 0, (size_t)c->n_cells * 4, c->stream);
   cudaMemsetAsync(c->scan_state, 0, (size_t)c->n_scan_tiles * 8, c->stream);
+  cudaMemsetAsync(c->fate_state, 0, (size_t)c->n_blocks * 8, c->stream);
   cudaMemsetAsync(c->ctr, 0, sizeof(Counters), c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
     int rc = fail(nullptr, CBM_ERR_CUDA, "device initialisation failed");
@@ -767,6 +763,7 @@ int cbm_upload(cbm_ctx* c, const cbm_state_view* h) {
   hc.slots = h->N;
   hc.resort = 1;  // flagRecomputeNeighbors_ = [1] and computeNeighbors! at load (communityStructure.jl:480,648)
   hc.scan_epoch = old.scan_epoch + 1;  // keep the epoch monotonic so stale tile states never match
+  hc.fate_epoch = old.fate_epoch + 1;
   CUDA_TRY(c, cudaMemcpyAsync(c->ctr, &hc, sizeof hc, cudaMemcpyHostToDevice, st));
   c->parity = 0;
   reset_stage_flags(c);

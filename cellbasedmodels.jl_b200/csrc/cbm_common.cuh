@@ -48,7 +48,8 @@ struct Counters {
   int events;           // births or deaths in the step in flight
   int list_valid;       // the Verlet list matches the current slots
   int list_written;     // this step wrote the Verlet list lazily
-  int pad;
+  unsigned fate_ticket; // tile tickets of the fused rule / births kernel
+  unsigned fate_epoch;  // generation of its tile states
 };
 
 template <typename T>

@@ -65,10 +65,7 @@ struct Params {
   // fate
   unsigned char* fate;
   int* holes;
-  int* blk_children;
-  int* blk_deaths;
-  int* blk_child_off;
-  int* blk_death_off;
+  unsigned long long* fate_state;  // per tile: epoch | flag | children | deaths
   // re-sort
   int* s_cell;          // cell of each working slot (-1 dead)
   int* s_rank;          // atomic rank inside the cell
@@ -459,137 +456,100 @@ __global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
 }
 
 // ---------------------------------------------------------------------------
-// agentStepRule!: walls, secretion, fate decision + per-tile event counts
-// (src/AgentStructure/functionRule.jl:9-111).  One thread per agent index.
+// agentStepRule! of one agent index i < N: walls, secretion, and the fate
+// decision (src/AgentStructure/functionRule.jl:9-111).  Returns 0 none,
+// 1 die, 2 divide (two children, the parent is removed), 3 one child.
 // ---------------------------------------------------------------------------
+template <typename T, int D>
+__device__ __forceinline__ int rule_agent(const Params<T>& P, int i, long long step) {
+  const int s = P.inv[i];
+  T x[3] = {(T)0, (T)0, (T)0};
+  if (P.walls == CBM_WALLS_REFLECT || (P.medium && P.secretion_amt != (T)0))
+    to3<T>(P.PA[s], x);
+  if (P.walls == CBM_WALLS_REFLECT) {
+    T y[3] = {x[0], x[1], x[2]};
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      if (x[d] < P.box_lo[d]) y[d] = (T)2 * P.box_lo[d] - x[d];
+      else if (x[d] > P.box_hi[d]) y[d] = (T)2 * P.box_hi[d] - x[d];
+    }
+    P.U[s] = from3<T>(y);
+  }
+  if (P.medium && P.secretion_amt != (T)0 && !secretion_by_gather(P)) {
+    if (P.medium_sampling == CBM_MEDIUM_NEAREST) {
+      atomicAdd(P.c_cur + nearest_node<T, D>(P, x), P.secretion_amt);
+    } else {
+      int nodes[8];
+      T w[8];
+      bilinear<T, D>(P, x, nodes, w);
+#pragma unroll
+      for (int q = 0; q < (1 << D); ++q) atomicAdd(P.c_cur + nodes[q], w[q] * P.secretion_amt);
+    }
+  }
+  int fate = 0;
+  if (P.fate_rule == CBM_FATE_VOLUME) {
+    if (P.growth && P.VA[s] >= P.v_div) fate = 2;
+    else if (P.p_death > (T)0 &&
+             cbm_uniform<T>(P.seed, step, (uint32_t)i, CBM_STREAM_DEATH, P.community) < P.p_death)
+      fate = 1;
+  } else if (P.fate_rule == CBM_FATE_ID_PARITY) {
+    fate = (P.ID[i] % 2 == 1) ? 1 : 3;
+  }
+  return fate;
+}
+
+// agentStepRule! without births or deaths: one thread per agent index
 template <typename T, int D>
 __global__ void __launch_bounds__(kTile) k_agent_rule(Params<T> P) {
   const int p = P.parity;
   const int N = (int)P.ctr->N[p];
   const int i = blockIdx.x * kTile + threadIdx.x;
-  int fate = 0;  // 0 none, 1 die, 2 divide (2 children + die), 3 one child
-  if (i < N) {
-    const int s = P.inv[i];
-    T x[3] = {(T)0, (T)0, (T)0};
-    if (P.walls == CBM_WALLS_REFLECT || (P.medium && P.secretion_amt != (T)0))
-      to3<T>(P.PA[s], x);
-    if (P.walls == CBM_WALLS_REFLECT) {
-      T y[3] = {x[0], x[1], x[2]};
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        if (x[d] < P.box_lo[d]) y[d] = (T)2 * P.box_lo[d] - x[d];
-        else if (x[d] > P.box_hi[d]) y[d] = (T)2 * P.box_hi[d] - x[d];
-      }
-      P.U[s] = from3<T>(y);
-    }
-    if (P.medium && P.secretion_amt != (T)0 && !secretion_by_gather(P)) {
-      if (P.medium_sampling == CBM_MEDIUM_NEAREST) {
-        atomicAdd(P.c_cur + nearest_node<T, D>(P, x), P.secretion_amt);
-      } else {
-        int nodes[8];
-        T w[8];
-        bilinear<T, D>(P, x, nodes, w);
-#pragma unroll
-        for (int q = 0; q < (1 << D); ++q) atomicAdd(P.c_cur + nodes[q], w[q] * P.secretion_amt);
-      }
-    }
-    if (P.fate_rule == CBM_FATE_VOLUME) {
-      if (P.growth && P.VA[s] >= P.v_div) fate = 2;
-      else if (P.p_death > (T)0 &&
-               cbm_uniform<T>(P.seed, P.ctr->step[p], (uint32_t)i, CBM_STREAM_DEATH, P.community) <
-                   P.p_death)
-        fate = 1;
-    } else if (P.fate_rule == CBM_FATE_ID_PARITY) {
-      fate = (P.ID[i] % 2 == 1) ? 1 : 3;
-    }
-  }
-  if (P.fate_rule == CBM_FATE_NONE) return;  // uniform over the grid
-  if (i < P.n_max) P.fate[i] = (unsigned char)fate;
-  int n_div = __syncthreads_count(fate == 2);
-  int n_one = __syncthreads_count(fate == 3);
-  int n_die = __syncthreads_count(fate == 1 || fate == 2);
-  if (threadIdx.x == 0) {
-    P.blk_children[blockIdx.x] = 2 * n_div + n_one;
-    P.blk_deaths[blockIdx.x] = n_die;
-  }
+  if (i < N) rule_agent<T, D>(P, i, P.ctr->step[p]);
 }
 
-// Offsets of every tile's births and deaths; NAdd_ / NRemove_ / idMax_
-// bookkeeping of @addAgent/@removeAgent (functionRule.jl:59-70,97-102).
-// One block.
-template <typename T>
-__global__ void __launch_bounds__(1024) k_fate_scan(Params<T> P) {
-  __shared__ long long s_c[1024], s_d[1024];
-  const int p = P.parity;
-  const int nb = P.n_blocks;
-  const int per = (nb + 1023) / 1024;
-  const int b0 = threadIdx.x * per;
-  long long c = 0, d = 0;
-  for (int b = b0; b < b0 + per && b < nb; ++b) {
-    c += P.blk_children[b];
-    d += P.blk_deaths[b];
-  }
-  s_c[threadIdx.x] = c;
-  s_d[threadIdx.x] = d;
-  __syncthreads();
-  for (int o = 1; o < 1024; o <<= 1) {
-    long long yc = threadIdx.x >= o ? s_c[threadIdx.x - o] : 0;
-    long long yd = threadIdx.x >= o ? s_d[threadIdx.x - o] : 0;
-    __syncthreads();
-    s_c[threadIdx.x] += yc;
-    s_d[threadIdx.x] += yd;
-    __syncthreads();
-  }
-  long long oc = s_c[threadIdx.x] - c, od = s_d[threadIdx.x] - d;
-  for (int b = b0; b < b0 + per && b < nb; ++b) {
-    P.blk_child_off[b] = (int)oc;
-    P.blk_death_off[b] = (int)od;
-    oc += P.blk_children[b];
-    od += P.blk_deaths[b];
-  }
-  if (threadIdx.x == 1023) {
-    Counters* C = P.ctr;
-    long long N = C->N[p];
-    long long tc = s_c[1023], td = s_d[1023];
-    long long room = (long long)P.n_max - N;
-    long long added = tc < room ? tc : room;
-    if (added < tc) atomicOr(&C->err, kErrAgentOverflow);
-    C->n_add = added;
-    C->n_remove = td;
-    C->children = tc;
-    C->id_base = C->id_max;
-    C->id_max += tc;  // ids are consumed even by dropped births
-    C->events = (tc > 0 || td > 0) ? 1 : 0;
-    if (tc > 0 || td > 0) C->flag[p] = 1;
-  }
+// Tile state of the fate scan: epoch (4 bits) | flag (2) | children (29) |
+// deaths (29).  Every launch rewrites every tile's state, so a state from the
+// previous launch differs from the current one in the epoch.
+__device__ __forceinline__ unsigned long long fate_word(unsigned epoch, unsigned flag,
+                                                        unsigned long long children,
+                                                        unsigned long long deaths) {
+  return ((unsigned long long)(epoch & 15u) << 60) | ((unsigned long long)flag << 58) |
+         (children << 29) | deaths;
 }
 
-// Births and holes of @addAgent/@removeAgent, ranked in agent-index order.
-// Newborn k of the step gets index and working slot N + k; its DE variables
-// go to set B, its constants to index N + k.  Parameters not given to
-// @addAgent are copied from the parent's committed values.
+// ---------------------------------------------------------------------------
+// agentStepRule! with @addAgent / @removeAgent (functionRule.jl:9-111), one
+// kernel: each tile of kFateTile agent indices (kFateItems consecutive ones
+// per thread) decides the fates, ranks its births and deaths, takes their
+// offsets from the preceding tiles with a decoupled look-back (tiles numbered
+// in launch order, bounded wait), and then places its newborns and holes in
+// agent-index order.  Newborn k of the step gets index and working slot
+// N + k (dropped beyond n_max, but its id is still consumed,
+// functionRule.jl:59-70); its DE variables go to set B, its constants to
+// index N + k; parameters not given to @addAgent are copied from the parent's
+// committed values.  The last tile writes NAdd_, NRemove_ and idMax_
+// (functionRule.jl:59-70,97-102) and resets the tile tickets.
+// ---------------------------------------------------------------------------
+#ifndef CBM_FATE_ITEMS
+#define CBM_FATE_ITEMS 8
+#endif
+constexpr int kFateItems = CBM_FATE_ITEMS;  // agents per thread of k_agent_fate
+constexpr int kFateTile = kTile * kFateItems;
+__host__ __device__ inline int fate_tiles(long long n_max) {
+  return n_max > 0 ? (int)((n_max + kFateTile - 1) / kFateTile) : 1;
+}
+
 template <typename T, int D>
-__global__ void __launch_bounds__(kTile) k_births(Params<T> P) {
-  __shared__ int warp_sums[kTile / 32];
-  const int p = P.parity;
-  const int N = (int)P.ctr->N[p];
-  const int b = blockIdx.x;
-  const int i = b * kTile + threadIdx.x;
-  if (P.blk_children[b] + P.blk_deaths[b] == 0) return;  // uniform over the block
-  const int fate = i < N ? P.fate[i] : 0;
+__device__ __forceinline__ void place_births(const Params<T>& P, int i, int fate, int N,
+                                             long long step, long long first_child,
+                                             long long id_base) {
   const int nch = fate == 2 ? 2 : (fate == 3 ? 1 : 0);
-  const int die = (fate == 1 || fate == 2) ? 1 : 0;
-  int tot;
-  int rc = block_exscan(nch, warp_sums, &tot) + P.blk_child_off[b];
-  int rd = block_exscan(die, warp_sums, &tot) + P.blk_death_off[b];
-  if (die) P.holes[rd] = i;
-  if (nch == 0) return;
   const int s = P.inv[i];
   T x[3];
   to3<T>(P.PA[s], x);
   T a[3] = {(T)0, (T)0, (T)0};
   if (fate == 2) {
-    cbm_normals(P.seed, P.ctr->step[p], (uint32_t)i, CBM_STREAM_DIVISION, P.community, D, a);
+    cbm_normals(P.seed, step, (uint32_t)i, CBM_STREAM_DIVISION, P.community, D, a);
     T ss = a[0] * a[0];
     if (D > 1) ss = ss + a[1] * a[1];
     if (D > 2) ss = ss + a[2] * a[2];
@@ -601,8 +561,8 @@ __global__ void __launch_bounds__(kTile) k_births(Params<T> P) {
   const T vv = P.VA[s];
   const T gg = P.G[i];
   for (int k = 0; k < nch; ++k) {
-    long long slot = (long long)N + rc + k;
-    if (slot >= P.n_max) break;  // dropped birth (counted in k_fate_scan)
+    const long long slot = (long long)N + first_child + k;
+    if (slot >= P.n_max) break;  // dropped birth (its id is still consumed)
     const int ns = (int)slot;
     T y[3] = {x[0], x[1], x[2]};
     if (fate == 2) {
@@ -616,8 +576,139 @@ __global__ void __launch_bounds__(kTile) k_births(Params<T> P) {
     if (P.force_mode == CBM_FORCE_LAGGED) P.FB[ns] = P.FA[s];
     P.IB[ns] = ns;
     P.G[ns] = gg;
-    P.ID[ns] = P.ctr->id_base + rc + k + 1;
+    P.ID[ns] = id_base + first_child + k + 1;
     P.PAR[ns] = idp;
+  }
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(kTile) k_agent_fate(Params<T> P) {
+  __shared__ int warp_sums[kTile / 32];
+  __shared__ unsigned s_tile;
+  __shared__ long long s_off[2];
+  Counters* C = P.ctr;
+  const int p = P.parity;
+  const int n_tiles = fate_tiles(P.n_max);
+  if (threadIdx.x == 0) s_tile = atomicAdd(&C->fate_ticket, 1u);
+  __syncthreads();
+  const int tile = (int)s_tile;
+  if (tile >= n_tiles) {  // tickets were not reset: never index past the tile states
+    if (threadIdx.x == 0) atomicOr(&C->err, kErrTimeout);
+    return;
+  }
+  // read before this tile publishes anything: the last tile updates id_max
+  // and the epoch only after every tile's publication
+  const unsigned epoch = C->fate_epoch;
+  const int N = (int)C->N[p];
+  const long long step = C->step[p];
+  const long long id_base = C->id_max;  // idMax_ before this step's births
+  const int i0 = tile * kFateTile + threadIdx.x * kFateItems;
+  unsigned char fates[kFateItems];
+  int mc = 0, md = 0;  // this thread's children and deaths
+#pragma unroll
+  for (int k = 0; k < kFateItems; ++k) {
+    const int i = i0 + k;
+    const int f = i < N ? rule_agent<T, D>(P, i, step) : 0;
+    fates[k] = (unsigned char)f;
+    if (i < P.n_max) P.fate[i] = (unsigned char)f;
+    mc += f == 2 ? 2 : (f == 3 ? 1 : 0);
+    md += (f == 1 || f == 2) ? 1 : 0;
+  }
+  // children in the high half, deaths in the low half (at most 4096 / 2048 a tile)
+  int tot;
+  const int ex = block_exscan((mc << 16) | md, warp_sums, &tot);
+  const int tc = tot >> 16, td = tot & 0xffff;
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    if (tile == 0) {
+      if (lane == 0) {
+        s_off[0] = 0;
+        s_off[1] = 0;
+        __threadfence();
+        atomicExch(P.fate_state, fate_word(epoch, 2u, (unsigned)tc, (unsigned)td));
+      }
+    } else {
+      if (lane == 0) {
+        __threadfence();
+        atomicExch(P.fate_state + tile, fate_word(epoch, 1u, (unsigned)tc, (unsigned)td));
+      }
+      long long pc = 0, pd = 0;
+      int t = tile - 1;
+      long long spins = 0;
+      const unsigned long long mask29 = (1ull << 29) - 1ull;
+      while (true) {
+        const int idx = t - lane;
+        unsigned flag = 2u;  // before tile 0: an inclusive prefix of 0
+        unsigned long long vc = 0, vd = 0;
+        if (idx >= 0) {
+          const unsigned long long w = atomicAdd(P.fate_state + idx, 0ull);
+          flag = ((unsigned)(w >> 60) == (epoch & 15u)) ? (unsigned)(w >> 58) & 3u : 0u;
+          vc = (w >> 29) & mask29;
+          vd = w & mask29;
+        }
+        const unsigned incl = __ballot_sync(kFull, flag == 2u);
+        const unsigned pend = __ballot_sync(kFull, flag == 0u);
+        const unsigned upto = incl ? ((incl & (0u - incl)) << 1) - 1u : kFull;
+        if (pend & upto) {
+          if (++spins > kSpinLimit) {
+            if (lane == 0) atomicOr(&C->err, kErrTimeout);
+            break;
+          }
+          continue;
+        }
+        unsigned long long sc = ((1u << lane) & upto) ? vc : 0ull;
+        unsigned long long sd = ((1u << lane) & upto) ? vd : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          sc += __shfl_xor_sync(kFull, sc, o);
+          sd += __shfl_xor_sync(kFull, sd, o);
+        }
+        pc += (long long)sc;
+        pd += (long long)sd;
+        if (incl) break;
+        t -= 32;
+      }
+      if (lane == 0) {
+        s_off[0] = pc;
+        s_off[1] = pd;
+        __threadfence();
+        atomicExch(P.fate_state + tile, fate_word(epoch, 2u, (unsigned long long)(pc + tc),
+                                                  (unsigned long long)(pd + td)));
+      }
+    }
+  }
+  __syncthreads();
+  long long rc = s_off[0] + (ex >> 16), rd = s_off[1] + (ex & 0xffff);
+  if (mc + md > 0) {
+#pragma unroll 1
+    for (int k = 0; k < kFateItems; ++k) {
+      const int f = fates[k];
+      if (f == 0) continue;
+      const int i = i0 + k;
+      if (f == 1 || f == 2) {
+        if (rd < P.n_max) P.holes[rd] = i;
+        ++rd;
+      }
+      if (f == 2 || f == 3) {
+        place_births<T, D>(P, i, f, N, step, rc, id_base);
+        rc += f == 2 ? 2 : 1;
+      }
+    }
+  }
+  if (tile == n_tiles - 1 && threadIdx.x == 0) {
+    const long long tcs = s_off[0] + tc, tds = s_off[1] + td;
+    const long long room = (long long)P.n_max - N;
+    const long long added = tcs < room ? tcs : room;
+    if (added < tcs) atomicOr(&C->err, kErrAgentOverflow);
+    C->n_add = added;
+    C->n_remove = tds;
+    C->children = tcs;
+    C->id_base = id_base;
+    C->id_max = id_base + tcs;  // ids are consumed even by dropped births
+    C->events = (tcs > 0 || tds > 0) ? 1 : 0;
+    if (tcs > 0 || tds > 0) C->flag[p] = 1;
+    C->fate_ticket = 0u;
+    C->fate_epoch = epoch + 1u;
   }
 }
 
