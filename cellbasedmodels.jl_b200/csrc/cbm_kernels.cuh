@@ -247,7 +247,8 @@ struct Eps<double> {
 // follow are unchanged.  The face gaps carry a margin for the rounding of the
 // cell assignment; cells next to the ghost layer are never skipped.
 template <typename T, int D, typename F>
-__device__ __forceinline__ void walk_runs(const Params<T>& P, const T* x, T reach, F&& run);
+__device__ __forceinline__ void walk_runs(const Params<T>& P, const T* x, T reach, F&& run,
+                                          int cell = -1);
 
 template <typename T, int D, typename F>
 __device__ __forceinline__ void walk_cells(const Params<T>& P, const typename V4T<T>::type* X,
@@ -259,14 +260,21 @@ __device__ __forceinline__ void walk_cells(const Params<T>& P, const typename V4
 }
 
 // The pruned cell walk as a sequence of contiguous slot runs run(s0, s1).
+// `cell`, when given, is the linear cell of x (the grid's own assignment).
 template <typename T, int D, typename F>
-__device__ __forceinline__ void walk_runs(const Params<T>& P, const T* x, T reach, F&& run) {
+__device__ __forceinline__ void walk_runs(const Params<T>& P, const T* x, T reach, F&& run,
+                                          int cell) {
   int q[3] = {0, 0, 0};
+  if (cell >= 0) {
+    q[0] = cell % P.n_cells_d[0];
+    if (D > 1) q[1] = (cell / P.n_cells_d[0]) % P.n_cells_d[1];
+    if (D > 2) q[2] = cell / (P.n_cells_d[0] * P.n_cells_d[1]);
+  }
   T gm[3] = {(T)0, (T)0, (T)0}, gp[3] = {(T)0, (T)0, (T)0};
 #pragma unroll
   for (int d = 0; d < D; ++d) {
     const int n = P.n_cells_d[d];
-    const int c = cell_pos1<T>(P.edge, x[d], P.box_lo[d], P.box_hi[d], n);
+    const int c = cell >= 0 ? q[d] : cell_pos1<T>(P.edge, x[d], P.box_lo[d], P.box_hi[d], n);
     q[d] = c;
     if (c >= 2 && c <= n - 3) {
       const T rel = x[d] - P.box_lo[d];
@@ -804,6 +812,9 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
       auto room = [&](int k) {
         if (__any_sync(__activemask(), nq > kQueue - k)) drain();
       };
+      // the slot's cell is the grid's assignment of the committed position,
+      // which the walk starts from unless the rule reflected it off a wall
+      const int own_cell = reflect ? -1 : ld(P.cell_of_slot + s);
       walk_runs<T, D>(P, xi, P.cut_reach, [&](int s0, int s1) {
         int q = s0;
         for (; q + 4 <= s1; q += 4) {
@@ -825,7 +836,7 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
           to3<T>(U[q], xj);
           if (diff(xj, e) < cut2 && q != s) push(q);
         }
-      });
+      }, own_cell);
     } else {
       const bool write = !P.ctr->events;
       const T skin2 = P.skin2, skin2_lo = P.skin2_lo;
@@ -959,10 +970,10 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
   P.PB[s] = from3<T>(xn);
   P.VB[s] = P.growth ? P.VA[s] + ld(P.G + i) * P.dt : P.VA[s];
   P.IB[s] = i;
-  if (is_verlet(P)) {
+  if (is_verlet(P) && !P.ctr->events) {
     // verletDisplacement (neighbors.jl:367-391) on the new positions; when
-    // agents are added or removed the flag is already set, so checking the
-    // pre-compaction positions decides the same rebuild.
+    // agents are added or removed this step the flag is already set and the
+    // check is skipped.
     T xo[3];
     to3<T>(P.POLD[s], xo);
     if (dist<T, D>(xn, xo) >= P.rebuild_thr) P.ctr->flag[p] = 1;
