@@ -395,7 +395,7 @@ def run_batched(args, rank=0, world=1, dist=None):
     tuning, tune_s = None, 0.0
     if b is not None:
         t0 = time.perf_counter()
-        tuning = b.autotune(trial_steps=args.batched_trial)
+        tuning = b.tuning() if args.batched_no_autotune else b.autotune(trial_steps=args.batched_trial)
         tune_s = time.perf_counter() - t0
         b.step(args.batched_steps)  # first replay builds the graph
     load_all()
@@ -696,6 +696,8 @@ def main():
     ap.add_argument("--batched-steps", type=int, default=500)
     ap.add_argument("--batched-trial", type=int, default=20)
     ap.add_argument("--plain-sample", type=int, default=32)
+    ap.add_argument("--batched-no-autotune", action="store_true",
+                    help="keep the default tuning (for profiling one known launch)")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--config-steps", type=int, default=200)

@@ -788,8 +788,10 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
     int nq = 0;
     auto drain = [&]() {
       for (int k = 0; k < nq; ++k) {
+        const int q = queue[k * kTile + threadIdx.x];
+        if (q == s) continue;  // the agent itself (queued by the force-only filter)
         T xj[3];
-        to3<T>(U[queue[k * kTile + threadIdx.x]], xj);
+        to3<T>(U[q], xj);
         pair(xj);
       }
       nq = 0;
@@ -828,13 +830,13 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
           }
 #pragma unroll
           for (int u = 0; u < 4; ++u)
-            if (s2v[u] < cut2 && q + u != s) push(q + u);
+            if (s2v[u] < cut2) push(q + u);  // the agent itself is skipped in the drain
         }
         for (; q < s1; ++q) {
           room(1);
           T xj[3], e[3];
           to3<T>(U[q], xj);
-          if (diff(xj, e) < cut2 && q != s) push(q);
+          if (diff(xj, e) < cut2) push(q);
         }
       }, own_cell);
     } else {
