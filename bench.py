@@ -198,9 +198,9 @@ class SmiClocks:
 
 # DRAM bytes per agent of one launch, from one ncu capture (dram__bytes_read.sum
 # + dram__bytes_write.sum) of the default colony workload: k_agent_de in walk
-# mode, Float32, 52.6 MB for 1,029,015 agents.  Traffic grows in proportion to
-# the agents of the launch, so it is scaled to the bench's agent count.
-MEASURED_TRAFFIC_PER_AGENT = {("k_agent_de", 4, True): 51.1}
+# mode, Float32, 35.0 MB for about 1.03M agents.  Traffic grows in proportion
+# to the agents of the launch, so it is scaled to the bench's agent count.
+MEASURED_TRAFFIC_PER_AGENT = {("k_agent_de", 4, True): 34.0}
 
 
 def traffic_per_launch(name, s, walked, agents):
