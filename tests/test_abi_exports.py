@@ -45,3 +45,18 @@ def test_create_without_device_fails_loudly():
     abi = conftest.cbm._abi
     with pytest.raises(abi.CbmError):
         conftest.cbm.Context(abi.make_config(dims=2, n_max=4, box_hi=(1, 1), dt=0.1))
+
+
+def test_create_rejects_capacities_beyond_the_fate_scan():
+    """Births and deaths pack two prefix counts of up to 2 n_max into 29 bits
+    each, so cbm_create refuses n_max >= 2^28 with a fate rule.  The argument
+    check comes before any CUDA call, so it runs without a GPU."""
+    import ctypes as C2
+    abi = conftest.cbm._abi
+    lib = abi.load_library()
+    cfg = abi.make_config(dims=3, n_max=1 << 28, box_hi=(1, 1, 1), dt=0.1, fate=abi.FATE_VOLUME,
+                          growth=1, v_div=2.0)
+    h = C2.c_void_p()
+    rc = lib.cbm_create(C2.byref(h), C2.byref(cfg))
+    assert rc == 1  # CBM_ERR_ARG
+    assert b"2^28" in lib.cbm_last_error(None)

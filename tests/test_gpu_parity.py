@@ -154,6 +154,55 @@ def test_colony_3d_bitexact(gpu_lib, abi, prec, alg):
         assert_same_lists(g, o)
 
 
+def test_packed_colony_1m_bitexact(gpu_lib, abi):
+    """The bench workload at its full size (10^6 agents, Float32, CLVD,
+    divisions every step): three steps, bit-exact against the checker."""
+    from scenarios import packed_colony_3d
+    kw, st = packed_colony_3d(abi, N=1_000_000)
+    cfg = abi.make_config(**kw)
+    g = cbm.Context(cfg)
+    o = OracleContext(abi, cfg, threads=16)
+    g.upload(st)
+    o.upload(st)
+    g.step(3)
+    o.step(3)
+    a, b = g.download(), o.download()
+    assert a["N"] > 1_000_000
+    assert_same_state(a, b, ["x", "y", "z", "v", "g", "id", "parent"])
+    assert a["id_max"] == b["id_max"]
+    # size-independent invariants of the state
+    assert len(np.unique(a["id"])) == a["N"]
+    born = a["id"] > 1_000_000
+    assert born.sum() > 0
+    assert np.all(a["parent"][born] >= 1) and np.all(a["parent"][born] < a["id"][born])
+    assert a["id"].max() <= a["id_max"]
+
+
+@pytest.mark.parametrize("alg", ["CellLinked", "CLVD"])
+def test_agents_beyond_the_box_gpu(gpu_lib, abi, alg):
+    """Agents outside simBox fall in the ghost cells (cellPos clamps,
+    neighbors.jl:636-638); the grid, the lists and the trajectories follow the
+    reference, including the pairs its ghost layer does not see."""
+    rng = np.random.default_rng(21)
+    n = 1200
+    L = 24.0
+    p = rng.uniform(-4.0, L + 4.0, size=(3, n))  # a shell of agents beyond every face
+    neigh = abi.NEIGH_CELL_LINKED if alg == "CellLinked" else abi.NEIGH_CLVD
+    kw = dict(dims=3, precision=abi.F64, n_max=n, box_lo=(0.0,) * 3, box_hi=(L,) * 3, dt=0.01,
+              seed=21, neighbors=neigh, cell_edge=3.3, skin=3.3, rebuild_threshold=0.15,
+              n_max_neighbors=64, integrator=abi.INT_EM, sigma=0.05, k_rep=10.0, r_rep=2.0,
+              k_att=1.0, r_att=3.0)
+    g, o = both(abi, kw, dict(x=p[0], y=p[1], z=p[2]))
+    for _ in range(3):
+        g.step(10)
+        o.step(10)
+        assert_same_state(g.download(), o.download(), ["x", "y", "z", "id"])
+    if alg == "CellLinked":
+        assert_same_grid(g, o)
+    else:
+        assert_same_lists(g, o)
+
+
 @pytest.mark.parametrize("bilinear", [False, True])
 def test_chemotaxis_2d(gpu_lib, abi, bilinear):
     kw, st = chemotaxis_2d(abi, N=3000, L=128.0, n_medium=128, bilinear=bilinear)
