@@ -55,11 +55,25 @@ struct Counters {
 template <typename T>
 __device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
 
-// Julia's float `÷` on a >= 0: round((a - rem(a, b)) / b)
+// Julia's float `÷` on a >= 0: round((a - rem(a, b)) / b), which is the exact
+// floor of a / b (quotients below 4e6).  Fast path: when the correctly
+// rounded quotient f has a fractional part farther than m from 0 and 1, the
+// exact quotient lies within half an ulp of f (< m) and so in the same unit
+// interval, and floor(f) is that floor; otherwise the remainder formula runs.
 __device__ __forceinline__ int floordiv(double a, double b) {
+  const double f = a / b;
+  const double n = floor(f);
+  const double fr = f - n;  // exact below 2^52
+  const double m = f * 1e-12 + 1e-14;
+  if (fr > m && fr < 1.0 - m) return (int)n;
   return (int)rint((a - fmod(a, b)) / b);
 }
 __device__ __forceinline__ int floordiv(float a, float b) {
+  const float f = a / b;
+  const float n = floorf(f);
+  const float fr = f - n;  // exact below 2^23
+  const float m = f * 1e-5f + 1e-6f;
+  if (fr > m && fr < 1.0f - m) return (int)n;
   return (int)rintf((a - fmodf(a, b)) / b);
 }
 
