@@ -325,8 +325,10 @@ __device__ void run_comm(const BatchParams& B, const Comm& C, int ci, int nsteps
   }
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NT) k_batch(BatchParams B, int nsteps) {
+// MINB: resident CTAs per SM the register allocation must allow (the
+// tuning's ctas_per_sm when it is 1 or 2)
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams B, int nsteps) {
   extern __shared__ float s_tile[];
   __shared__ int s_comm;
   __shared__ int s_flag[2];
@@ -443,16 +445,24 @@ void free_batch(cbm_batch* b) {
 
 double list_radius(const cbm_batch* b) { return b->cutoff + b->tune.skin; }
 
+using BatchKernel = void (*)(BatchParams, int);
+
+// registers limited for two resident CTAs when the tuning asks for two or more
+template <int NT>
+void launch_batch(cbm_batch* b, const BatchParams& B, int nsteps, int grid, size_t smem) {
+  if (b->tune.ctas_per_sm >= 2) k_batch<NT, 2><<<grid, NT, smem, b->stream>>>(B, nsteps);
+  else k_batch<NT, 1><<<grid, NT, smem, b->stream>>>(B, nsteps);
+}
+
 // dynamic shared memory of a position tile (x, y, z arrays)
 constexpr int kMaxTileBytes = 220 * 1024;
 size_t tile_bytes(int tile_agents) { return (size_t)std::max(tile_agents, 0) * 3 * sizeof(float); }
 
 int set_smem_limit(cbm_batch* b) {
   const int bytes = (int)tile_bytes(b->tune.tile_agents);
-  BCUDA(b, cudaFuncSetAttribute(k_batch<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  BCUDA(b, cudaFuncSetAttribute(k_batch<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  BCUDA(b, cudaFuncSetAttribute(k_batch<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  BCUDA(b, cudaFuncSetAttribute(k_batch<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  for (const BatchKernel k : {k_batch<128, 1>, k_batch<128, 2>, k_batch<256, 1>, k_batch<256, 2>,
+                              k_batch<512, 1>, k_batch<512, 2>, k_batch<1024, 1>, k_batch<1024, 2>})
+    BCUDA(b, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   return CBM_OK;
 }
 
@@ -498,10 +508,10 @@ int enqueue_batch(cbm_batch* b, int nsteps) {
   const int grid = b->n_sm * std::max(1, b->tune.ctas_per_sm);
   const size_t smem = tile_bytes(b->tune.tile_agents);
   switch (b->tune.threads) {
-    case 128: k_batch<128><<<grid, 128, smem, b->stream>>>(B, nsteps); break;
-    case 512: k_batch<512><<<grid, 512, smem, b->stream>>>(B, nsteps); break;
-    case 1024: k_batch<1024><<<grid, 1024, smem, b->stream>>>(B, nsteps); break;
-    default: k_batch<256><<<grid, 256, smem, b->stream>>>(B, nsteps); break;
+    case 128: launch_batch<128>(b, B, nsteps, grid, smem); break;
+    case 512: launch_batch<512>(b, B, nsteps, grid, smem); break;
+    case 1024: launch_batch<1024>(b, B, nsteps, grid, smem); break;
+    default: launch_batch<256>(b, B, nsteps, grid, smem); break;
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return bfail(b, CBM_ERR_CUDA, "batch launch failed: %s", cudaGetErrorString(e));
