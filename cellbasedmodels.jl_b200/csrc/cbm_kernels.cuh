@@ -366,15 +366,21 @@ __global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
     for (int k = 0; k < (1 << D); ++k)
       if (nodes[k] == n) acc = acc + w[k] * amt;
   };
+  // The stencil of bilinear() covers node q exactly when, on every axis, one
+  // of its two clamped indices is q (the same expressions, without weights).
   auto touches = [&](int slot) {
     T x[3];
     to3<T>(P.PA[slot], x);
-    int nodes[8];
-    T w[8];
-    bilinear<T, D>(P, x, nodes, w);
-    bool t = false;
+    bool t = true;
 #pragma unroll
-    for (int k = 0; k < (1 << D); ++k) t = t || nodes[k] == n;
+    for (int d = 0; d < D; ++d) {
+      const T sd = (x[d] - P.box_lo[d]) / P.dx_m[d] - (T)0.5;
+      const int a = (int)floor(sd), b = a + 1;
+      const int hi = P.n_medium[d] - 1;
+      const int i0 = a < 0 ? 0 : (a > hi ? hi : a);
+      const int i1 = b < 0 ? 0 : (b > hi ? hi : b);
+      t = t && (i0 == q[d] || i1 == q[d]);
+    }
     return t;
   };
   // Agents whose stencil covers node q along an axis lie in x in
