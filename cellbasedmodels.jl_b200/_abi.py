@@ -124,6 +124,7 @@ def load_library(path=LIB_PATH):
         "cbm_upload": (C.c_int, [vp, C.POINTER(CbmStateView)]),
         "cbm_download": (C.c_int, [vp, C.POINTER(CbmStateView), i32]),
         "cbm_step": (C.c_int, [vp, i32, i32]),
+        "cbm_step_noise": (C.c_int, [vp, vp, i32]),
         "cbm_agent_step_rule": (C.c_int, [vp]),
         "cbm_agent_step_de": (C.c_int, [vp]),
         "cbm_medium_step_rule": (C.c_int, [vp]),
@@ -260,6 +261,12 @@ class Context:
 
     def step(self, n=1, flags=SYNC):
         return self._check(self.lib.cbm_step(self.h, n, flags))
+
+    def step_noise(self, noise, flags=SYNC):
+        """One step whose EM increments are `noise` (N x dims, index order)."""
+        dt = np.float64 if self.cfg.precision == F64 else np.float32
+        buf = np.ascontiguousarray(noise, dtype=dt)
+        return self._check(self.lib.cbm_step_noise(self.h, buf.ctypes.data, flags))
 
     def stage(self, name):
         fn = {"agent_rule": self.lib.cbm_agent_step_rule, "agent_de": self.lib.cbm_agent_step_de,

@@ -66,6 +66,8 @@ struct cbm_ctx {
   void* grad[2][3] = {};
   Counters* ctr = nullptr;
   int* scratch_int = nullptr;  // n_max ints for inspection calls
+  void* ext_noise = nullptr;   // EM increments of cbm_step_noise (n_max * dims reals, lazy)
+  bool ext_noise_on = false;   // the step being enqueued reads ext_noise
 
   int n_blocks = 0;
   int n_sm = 148;             // multiprocessors of the device (grid of the compaction)
@@ -197,6 +199,7 @@ Params<T> params(const cbm_ctx* c, int parity) {
   P.fate = c->fate;
   P.holes = c->holes;
   P.fate_state = c->fate_state;
+  P.noise = c->ext_noise_on ? (const T*)c->ext_noise : nullptr;
   P.s_cell = c->s_cell;
   P.s_rank = c->s_rank;
   P.s_key = c->s_key;
@@ -933,6 +936,38 @@ int cbm_step(cbm_ctx* c, int32_t nsteps, int32_t flags) {
     }
     c->parity ^= 1;
   }
+  if (flags & CBM_SYNC) return cbm_sync(c);
+  return CBM_OK;
+}
+
+int cbm_step_noise(cbm_ctx* c, const void* noise, int32_t flags) {
+  if (!c) return CBM_ERR_ARG;
+  if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
+  if (c->cfg.integrator != CBM_INT_EM)
+    return fail(c, CBM_ERR_ARG, "external noise needs the Euler-Maruyama integrator");
+  if (c->rule_done || c->de_done || c->mrule_done || c->mde_done)
+    return fail(c, CBM_ERR_STATE, "a step is half done through the stage calls; call cbm_update first");
+  cudaSetDevice(c->device);
+  Counters hc;
+  int rc = read_counters(c, &hc);
+  if (rc) return rc;
+  const long long N = hc.N[c->parity];
+  const size_t bytes = (size_t)N * (size_t)c->cfg.dims * c->tsize;
+  if (N > 0 && !noise) return fail(c, CBM_ERR_ARG, "noise is NULL");
+  if (!c->ext_noise) {
+    CUDA_TRY(c, cudaMalloc(&c->ext_noise,
+                           (size_t)(c->cfg.n_max > 0 ? c->cfg.n_max : 1) * c->cfg.dims * c->tsize));
+    c->allocs.push_back(c->ext_noise);
+  }
+  if (bytes) CUDA_TRY(c, cudaMemcpyAsync(c->ext_noise, noise, bytes, cudaMemcpyHostToDevice, c->stream));
+  c->ext_noise_on = true;  // read by params() for this step only; the step graphs keep the stream
+  dispatch<FullStep>(c, c->parity);
+  c->ext_noise_on = false;
+  rc = check_launch(c);
+  if (rc) return rc;
+  c->parity ^= 1;
+  // the host buffer is borrowed for the call only
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   if (flags & CBM_SYNC) return cbm_sync(c);
   return CBM_OK;
 }

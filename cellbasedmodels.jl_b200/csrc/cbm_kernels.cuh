@@ -82,6 +82,7 @@ struct Params {
   T* grad_cur[3];
   T* grad_nxt[3];
   Counters* ctr;
+  const T* noise;       // EM increments given by the caller for this step (i * D + d), or null
   // sizes
   int n_max;
   int n_blocks;         // ceil(n_max / kTile)
@@ -968,7 +969,12 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
   T xn[3] = {(T)0, (T)0, (T)0};
   if (P.integrator == CBM_INT_EM) {
     T xi_n[3] = {(T)0, (T)0, (T)0};
-    cbm_normals(P.seed, P.ctr->step[p], (uint32_t)i, CBM_STREAM_NOISE, P.community, D, xi_n);
+    if (P.noise) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) xi_n[d] = P.noise[(size_t)i * D + d];
+    } else {
+      cbm_normals(P.seed, P.ctr->step[p], (uint32_t)i, CBM_STREAM_NOISE, P.community, D, xi_n);
+    }
 #pragma unroll
     for (int d = 0; d < D; ++d) xn[d] = (xi[d] + dv[d] * P.dt) + (P.sigma * xi_n[d]) * P.sqrt_dt;
   } else {

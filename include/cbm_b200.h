@@ -183,6 +183,13 @@ int cbm_download(cbm_ctx* ctx, cbm_state_view* host, int32_t which);
 /* step! x nsteps (step.jl:96-107).  Enqueues the steps (as CUDA graph replays
  * unless CBM_NO_GRAPH) and returns; CBM_SYNC waits and reports device flags. */
 int cbm_step(cbm_ctx* ctx, int32_t nsteps, int32_t flags);
+/* One step! whose Euler–Maruyama increments are given instead of drawn:
+ * noise[i * dims + d] ~ N(0,1) for the N agents in index order, in the
+ * context's precision (the agentSDE draws of integrators.jl:718-724, fed to
+ * both this library and a CPU run).  Divisions and deaths keep their
+ * counter-based draws.  Runs without the step graph; noise is borrowed for
+ * the call only.  Needs integrator == CBM_INT_EM. */
+int cbm_step_noise(cbm_ctx* ctx, const void* noise, int32_t flags);
 /* The stages of step!, for custom loops (docs/src/Usage_Community.md:236-345) */
 int cbm_agent_step_rule(cbm_ctx* ctx);   /* agentStepRule!  step.jl:6-14 */
 int cbm_agent_step_de(cbm_ctx* ctx);     /* agentStepDE!    step.jl:51-59 */

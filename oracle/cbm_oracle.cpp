@@ -32,6 +32,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 #include <algorithm>
 #ifdef _OPENMP
@@ -69,6 +70,7 @@ struct Com {
   std::vector<int64_t> cellAssignedToAgent, cellNumAgents, cellCumSum;
   std::vector<int64_t> neighborN, neighborList;  // list column-major (nMax x nMaxNeighbors)
   std::vector<T> posOld[3], accumulatedDistance;
+  const T* ext_noise = nullptr;  // EM increments given by the caller for one step (i * D + d)
 
   // medium: committed c, u (c__), gradient committed / new
   int64_t nm[3] = {1, 1, 1};
@@ -532,7 +534,11 @@ void agentStepDE(Com<T>& C) {
   for (int64_t i = 0; i < N; ++i) {
     if (k.integrator == CBM_INT_EM) {
       T xi[3] = {0, 0, 0};
-      cbm_normals(k.seed, C.step, (uint32_t)i, CBM_STREAM_NOISE, k.community, D, xi);
+      if (C.ext_noise) {
+        for (int d = 0; d < D; ++d) xi[d] = C.ext_noise[i * D + d];
+      } else {
+        cbm_normals(k.seed, C.step, (uint32_t)i, CBM_STREAM_NOISE, k.community, D, xi);
+      }
       for (int d = 0; d < D; ++d) C.x_[d][i] = (C.x_[d][i] + C.du[d][i] * dt) + (sig * xi[d]) * sq;
     } else {
       for (int d = 0; d < D; ++d) C.x_[d][i] = C.x_[d][i] + C.du[d][i] * dt;
@@ -802,6 +808,18 @@ int oracle_stage(void* vh, int stage) {
 
 int oracle_step(void* vh, int nsteps) {
   DISPATCH((Handle*)vh, for (int s = 0; s < nsteps; ++s) step(*C));
+  return CBM_OK;
+}
+
+/* one step whose EM increments are given: noise[i * dims + d] for the N
+ * agents in index order, in the context's precision */
+int oracle_step_noise(void* vh, const void* noise) {
+  DISPATCH((Handle*)vh, {
+    using TT = typename std::remove_reference<decltype(C->g)>::type::value_type;
+    C->ext_noise = (const TT*)noise;
+    step(*C);
+    C->ext_noise = nullptr;
+  });
   return CBM_OK;
 }
 

@@ -35,6 +35,7 @@ def load_oracle(abi):
         "oracle_download": (C.c_int, [vp, C.POINTER(abi.CbmStateView), C.c_int]),
         "oracle_stage": (C.c_int, [vp, C.c_int]),
         "oracle_step": (C.c_int, [vp, C.c_int]),
+        "oracle_step_noise": (C.c_int, [vp, vp]),
         "oracle_take_error": (C.c_int, [vp]),
         "oracle_get_counters": (C.c_int, [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64),
                                           C.POINTER(i64), C.POINTER(i32), C.POINTER(i64)]),
@@ -103,6 +104,13 @@ class OracleContext:
 
     def step(self, n=1, flags=0):
         self.lib.oracle_step(self.h, n)
+        return self.take_error()
+
+    def step_noise(self, noise):
+        """One step whose EM increments are `noise` (N x dims, index order)."""
+        dt = np.float64 if self.cfg.precision == self.abi.F64 else np.float32
+        buf = np.ascontiguousarray(noise, dtype=dt)
+        self.lib.oracle_step_noise(self.h, buf.ctypes.data)
         return self.take_error()
 
     def take_error(self):

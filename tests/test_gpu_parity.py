@@ -203,6 +203,29 @@ def test_agents_beyond_the_box_gpu(gpu_lib, abi, alg):
         assert_same_lists(g, o)
 
 
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_external_noise_bitexact(gpu_lib, abi, prec):
+    """Noise generated once on the host and fed to both sides (cbm_step_noise):
+    a growing colony stays bit-identical while N changes every step."""
+    kw, st = colony_3d(abi, N=2000, L=50.0, n_max=8000, p_death=2e-3,
+                       precision=abi.F32 if prec == "f32" else abi.F64)
+    g, o = both(abi, kw, st)
+    rng = np.random.default_rng(77)
+    for _ in range(30):
+        n = g.counters()["N"]
+        assert n == o.counters()["N"]
+        xi = rng.standard_normal((n, 3))
+        g.step_noise(xi)
+        o.step_noise(xi)
+    a, b = g.download(), o.download()
+    assert a["N"] > 2000
+    assert_same_state(a, b, ["x", "y", "z", "v", "id", "parent"])
+    # and the given noise is what moved the agents: the drawn stream differs
+    g2, _ = both(abi, kw, st)
+    g2.step(30)
+    assert not np.array_equal(g2.download()["x"][:100], a["x"][:100])
+
+
 @pytest.mark.parametrize("bilinear", [False, True])
 def test_chemotaxis_2d(gpu_lib, abi, bilinear):
     kw, st = chemotaxis_2d(abi, N=3000, L=128.0, n_medium=128, bilinear=bilinear)

@@ -274,3 +274,21 @@ def test_dual_gradient_matches_central_differences(abi):
         fd = (oracle_adjoint_dual(abi, cfg(), xp, tgt, steps)[0] -
               oracle_adjoint_dual(abi, cfg(), xm, tgt, steps)[0]) / (2 * h)
         assert abs(fd - dx[s]) <= 1e-5 * max(abs(dx[s]), 1e-9)
+
+
+def test_external_noise_zero_equals_sigma_zero(abi):
+    """A step fed zero EM increments equals a step with sigma = 0: the given
+    noise replaces the drawn one and nothing else."""
+    from scenarios import colony_3d
+    kw, st = colony_3d(abi, N=300, L=40.0, precision=abi.F64, p_death=0.0)
+    kw = dict(kw, growth=0, fate=abi.FATE_NONE)
+    a = OracleContext(abi, abi.make_config(**kw))
+    b = OracleContext(abi, abi.make_config(**dict(kw, sigma=0.0)))
+    a.upload(st)
+    b.upload(st)
+    for _ in range(5):
+        a.step_noise(np.zeros((300, 3)))
+        b.step(1)
+    da, db = a.download(), b.download()
+    for k in "xyz":
+        np.testing.assert_array_equal(da[k], db[k])
