@@ -276,12 +276,22 @@ bool rule_needed(const cbm_config& k) {
          k.fate != CBM_FATE_NONE;
 }
 
+// blocks of the 2D shared-memory stencils (one tile per block)
+dim3 stencil_grid(const cbm_ctx* c) {
+  const int nx = c->cfg.n_medium[0] > 0 ? c->cfg.n_medium[0] : 1;
+  const int ny = c->cfg.n_medium[1] > 0 ? c->cfg.n_medium[1] : 1;
+  return dim3((unsigned)((nx + kStX - 1) / kStX), (unsigned)((ny + kStTileY - 1) / kStTileY));
+}
+
 // ---- stage launches (enqueue only) -----------------------------------------
 template <typename T, int D>
 void enqueue_medium_rule(cbm_ctx* c, const Params<T>& P) {
   if (c->cfg.medium && c->cfg.chemotaxis != 0) {
     PROF("k_medium_grad");
-    k_medium_grad<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
+    if (D == 2)
+      k_medium_grad_2d<T><<<stencil_grid(c), dim3(kStX, kStY), 0, c->stream>>>(P);
+    else
+      k_medium_grad<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
   }
 }
 
@@ -312,7 +322,10 @@ template <typename T, int D>
 void enqueue_medium_de(cbm_ctx* c, const Params<T>& P) {
   if (c->cfg.medium) {
     PROF("k_medium_de");
-    k_medium_de<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
+    if (D == 2)
+      k_medium_de_2d<T><<<stencil_grid(c), dim3(kStX, kStY), 0, c->stream>>>(P);
+    else
+      k_medium_de<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
   }
 }
 

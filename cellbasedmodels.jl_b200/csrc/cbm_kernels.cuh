@@ -1026,6 +1026,73 @@ __global__ void __launch_bounds__(kTile) k_medium_de(Params<T> P) {
 }
 
 // ---------------------------------------------------------------------------
+// 2D medium stencils on shared-memory tiles: a block of kStX x kStY threads
+// covers a kStX x (kStY * kStRows) tile of nodes and stages it with a
+// one-node halo, so every node is read from HBM/L2 once per block.  Same
+// expressions as k_medium_grad / k_medium_de.
+// ---------------------------------------------------------------------------
+constexpr int kStX = 32, kStY = 8, kStRows = 4;
+constexpr int kStTileY = kStY * kStRows;
+
+template <typename T>
+__device__ __forceinline__ void stage_tile2(const Params<T>& P, T (*tile)[kStX + 2], int x0, int y0) {
+  const int nx = P.n_medium[0], ny = P.n_medium[1];
+  for (int k = threadIdx.y * kStX + threadIdx.x; k < (kStTileY + 2) * (kStX + 2); k += kStX * kStY) {
+    const int ty = k / (kStX + 2), tx = k % (kStX + 2);
+    const int gx = x0 + tx - 1, gy = y0 + ty - 1;
+    tile[ty][tx] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny) ? P.c_cur[(size_t)gy * nx + gx] : (T)0;
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kStX * kStY) k_medium_grad_2d(Params<T> P) {
+  __shared__ T tile[kStTileY + 2][kStX + 2];
+  const int nx = P.n_medium[0], ny = P.n_medium[1];
+  const int x0 = blockIdx.x * kStX, y0 = blockIdx.y * kStTileY;
+  stage_tile2<T>(P, tile, x0, y0);
+  const int x = x0 + threadIdx.x;
+  if (x >= nx) return;
+#pragma unroll
+  for (int r = 0; r < kStRows; ++r) {
+    const int ty = threadIdx.y + r * kStY, y = y0 + ty;
+    if (y >= ny) break;
+    const size_t n = (size_t)y * nx + x;
+    const bool in = x > 0 && x < nx - 1 && y > 0 && y < ny - 1;
+    const int tx = threadIdx.x + 1, tyy = ty + 1;
+    P.grad_nxt[0][n] = in ? (tile[tyy][tx + 1] - tile[tyy][tx - 1]) / ((T)2 * P.dx_m[0]) : (T)0;
+    P.grad_nxt[1][n] = in ? (tile[tyy + 1][tx] - tile[tyy - 1][tx]) / ((T)2 * P.dx_m[1]) : (T)0;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kStX * kStY) k_medium_de_2d(Params<T> P) {
+  __shared__ T tile[kStTileY + 2][kStX + 2];
+  const int nx = P.n_medium[0], ny = P.n_medium[1];
+  const int x0 = blockIdx.x * kStX, y0 = blockIdx.y * kStTileY;
+  stage_tile2<T>(P, tile, x0, y0);
+  const int x = x0 + threadIdx.x;
+  if (x >= nx) return;
+#pragma unroll
+  for (int r = 0; r < kStRows; ++r) {
+    const int ty = threadIdx.y + r * kStY, y = y0 + ty;
+    if (y >= ny) break;
+    const size_t n = (size_t)y * nx + x;
+    const int tx = threadIdx.x + 1, tyy = ty + 1;
+    const T u = tile[tyy][tx];
+    if (!(x > 0 && x < nx - 1 && y > 0 && y < ny - 1)) {
+      P.c_nxt[n] = u;
+      continue;
+    }
+    const T l0 = ((tile[tyy][tx + 1] - (T)2 * u) + tile[tyy][tx - 1]) / (P.dx_m[0] * P.dx_m[0]);
+    const T l1 = ((tile[tyy + 1][tx] - (T)2 * u) + tile[tyy - 1][tx]) / (P.dx_m[1] * P.dx_m[1]);
+    const T lap = l0 + l1;
+    const T k = P.diff_D * lap - P.decay * u;
+    P.c_nxt[n] = u + P.dt * k;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // update!: tail-fill compaction (kernelListSurvived + kernelFillHolesParameters,
 // src/CommunityStructure/update.jl:15-119).  The k-th hole (ascending) takes
 // the k-th survivor counted from the tail when the hole lies before it, which
