@@ -724,6 +724,12 @@ void cbm_destroy(cbm_ctx* ctx) {
   delete ctx;
 }
 
+// ids 1..N for an upload that gives none (Community numbers its agents from 1)
+static __global__ void k_default_ids(long long* id, int n) {
+  const int i = blockIdx.x * kTile + threadIdx.x;
+  if (i < n) id[i] = (long long)i + 1;
+}
+
 int cbm_upload(cbm_ctx* c, const cbm_state_view* h) {
   if (!c || !h) return fail(c, CBM_ERR_ARG, "null argument");
   cudaSetDevice(c->device);
@@ -751,9 +757,10 @@ int cbm_upload(cbm_ctx* c, const cbm_state_view* h) {
   CUDA_TRY(c, cudaMemsetAsync(c->PAR, 0, nm * 8, st));
   if (N && h->parent)
     CUDA_TRY(c, cudaMemcpyAsync(c->PAR, h->parent, N * 8, cudaMemcpyHostToDevice, st));
-  std::vector<long long> ids(nm > 0 ? nm : 1, 0);
-  for (size_t i = 0; i < N; ++i) ids[i] = h->id ? h->id[i] : (long long)i + 1;
-  CUDA_TRY(c, cudaMemcpyAsync(c->ID, ids.data(), nm * 8, cudaMemcpyHostToDevice, st));
+  // ids: the caller's (copied straight from its array), else 1..N; zero beyond N
+  CUDA_TRY(c, cudaMemsetAsync(c->ID, 0, (nm > 0 ? nm : 1) * 8, st));
+  if (N && h->id) CUDA_TRY(c, cudaMemcpyAsync(c->ID, h->id, N * 8, cudaMemcpyHostToDevice, st));
+  else if (N) k_default_ids<<<grid_blocks((long long)N), kTile, 0, st>>>(c->ID, (int)N);
   if (k.medium) {
     const size_t nb = (size_t)c->n_nodes * S;
     for (int q = 0; q < 2; ++q) {
