@@ -235,7 +235,8 @@ def make_workload(abi, args, rank):
     packing density 0.15 in a ball, v ~ U(1,2)."""
     from scenarios import packed_colony_3d
     prec = abi.F64 if args.precision == "f64" else abi.F32
-    kw, state = packed_colony_3d(abi, N=args.n, seed=2 + rank, precision=prec)
+    kw, state = packed_colony_3d(abi, N=args.n, seed=2 + rank, precision=prec,
+                                 density=args.density)
     return kw, state
 
 
@@ -753,6 +754,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--density", type=float, default=0.15,
+                    help="agents per unit volume of the --workload packed snapshot (the grown "
+                         "colony reaches about 4 in its core)")
     ap.add_argument("--workload", default="grown", choices=["grown", "packed"],
                     help="grown: the colony grown from 10^4 to n (the configured run); "
                          "packed: a synthetic snapshot at packing density")
@@ -786,7 +790,7 @@ def main():
                     f"timed; {args.precision}, EM sigma 0.05, division at v=2 + death 1e-4, "
                     f"CLVD R_list 3.3 rebuild 0.15, dt 0.005")
     else:
-        workload = (f"3D colony snapshot, {args.n} agents at packing density 0.15 in a ball in "
+        workload = (f"3D colony snapshot, {args.n} agents at density {args.density} in a ball in "
                     f"[0,400]^3, {args.precision}, EM sigma 0.05, division at v=2 + death 1e-4 "
                     f"every step, CLVD R_list 3.3 rebuild 0.15, dt 0.005")
     config = {"workload": workload, "n_agents": args.n, "n_max": int(1.2 * args.n),

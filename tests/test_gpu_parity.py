@@ -178,6 +178,27 @@ def test_packed_colony_1m_bitexact(gpu_lib, abi):
     assert a["id"].max() <= a["id_max"]
 
 
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("alg", ["CellLinked", "CLVD"])
+def test_dense_colony_bitexact(gpu_lib, abi, prec, alg):
+    """A compressed colony (4 agents per unit volume, the core density a colony
+    grown from 10^4 reaches): warps of the force kernel sit inside one cell and
+    take the sub-cell walk; still bit-exact, through divisions, with the grid."""
+    from scenarios import packed_colony_3d
+    neigh = abi.NEIGH_CELL_LINKED if alg == "CellLinked" else abi.NEIGH_CLVD
+    kw, st = packed_colony_3d(abi, N=6000, density=4.0, L=60.0, n_max=12000,
+                              precision=abi.F32 if prec == "f32" else abi.F64)
+    kw = dict(kw, neighbors=neigh, n_max_neighbors=1024)
+    g, o = both(abi, kw, st)
+    for _ in range(3):
+        g.step(8)
+        o.step(8)
+        assert_same_state(g.download(), o.download(), ["x", "y", "z", "v", "id", "parent"])
+    assert g.counters()["N"] > 6000
+    if alg == "CellLinked":
+        assert_same_grid(g, o)
+
+
 @pytest.mark.parametrize("alg", ["CellLinked", "CLVD"])
 def test_agents_beyond_the_box_gpu(gpu_lib, abi, alg):
     """Agents outside simBox fall in the ghost cells (cellPos clamps,
