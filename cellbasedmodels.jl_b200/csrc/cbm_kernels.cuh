@@ -793,10 +793,27 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
     // step forces another rebuild.
     __shared__ int queue[kQueue * kTile];
     int nq = 0;
+    // Queued pairs four at a time: loads and differences of four entries are
+    // independent, their terms are then added in queue order.  The agent
+    // itself (queued by the force-only filter) is skipped here.
     auto drain = [&]() {
-      for (int k = 0; k < nq; ++k) {
+      int k = 0;
+      for (; k + 4 <= nq; k += 4) {
+        int qq[4];
+        T xx[4][3], ee[4][3], ss[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) qq[u] = queue[(k + u) * kTile + threadIdx.x];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) to3<T>(U[qq[u]], xx[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) ss[u] = diff(xx[u], ee[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (qq[u] != s) pair_e(ee[u], ss[u]);
+      }
+      for (; k < nq; ++k) {
         const int q = queue[k * kTile + threadIdx.x];
-        if (q == s) continue;  // the agent itself (queued by the force-only filter)
+        if (q == s) continue;
         T xj[3];
         to3<T>(U[q], xj);
         pair(xj);
@@ -835,9 +852,14 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
             to3<T>(U[q + u], xj);
             s2v[u] = diff(xj, e);
           }
+          // every candidate is written at the queue's end and kept only when it
+          // may be inside the cutoff (room() left space for four); the agent
+          // itself is skipped in the drain
 #pragma unroll
-          for (int u = 0; u < 4; ++u)
-            if (s2v[u] < cut2) push(q + u);  // the agent itself is skipped in the drain
+          for (int u = 0; u < 4; ++u) {
+            queue[nq * kTile + threadIdx.x] = q + u;
+            nq += s2v[u] < cut2 ? 1 : 0;
+          }
         }
         for (; q < s1; ++q) {
           room(1);
