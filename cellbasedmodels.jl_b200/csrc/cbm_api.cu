@@ -71,6 +71,8 @@ struct cbm_ctx {
 
   int n_blocks = 0;
   int n_sm = 148;             // multiprocessors of the device (grid of the compaction)
+  int de_blocks = 1;          // persistent grid of the force kernel
+  void* pair_list = nullptr;  // its partner lists (cell walks only)
   int n_cells = 1;
   int n_cells_d[3] = {1, 1, 1};
   int n_scan_tiles = 1;
@@ -208,6 +210,8 @@ Params<T> params(const cbm_ctx* c, int parity) {
   P.scan_state = c->scan_state;
   P.nbr_n = c->nbr_n;
   P.nbr_list = c->nbr_list;
+  P.pair_list = (int4*)c->pair_list;
+  P.pair_cap4 = kPairCap4;
   P.c_cur = (T*)c->c[p];
   P.c_nxt = (T*)c->c[q];
   P.ctr = c->ctr;
@@ -315,7 +319,7 @@ void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P) {
 template <typename T, int D>
 void enqueue_agent_de(cbm_ctx* c, const Params<T>& P) {
   PROF("k_agent_de");
-  k_agent_de<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+  k_agent_de<T, D><<<c->de_blocks, kTile, 0, c->stream>>>(P);
 }
 
 template <typename T, int D>
@@ -412,6 +416,17 @@ void dispatch(cbm_ctx* c, A... a) {
     }
   }
 }
+
+// resident blocks of the force kernel per multiprocessor
+template <typename T, int D>
+struct DEOccupancy {
+  static void run(cbm_ctx*, int* bps) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_agent_de<T, D>, kTile, 0) !=
+            cudaSuccess ||
+        *bps < 1)
+      *bps = 1;
+  }
+};
 
 template <typename T, int D>
 struct FullStep {
@@ -685,6 +700,15 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
   c->cell_start = (int*)dalloc(c, ((size_t)c->n_cells + 1) * 4, &ok);
   c->scan_state = (unsigned long long*)dalloc(c, (size_t)c->n_scan_tiles * 8, &ok);
   c->scratch_int = (int*)dalloc(c, n * 4, &ok);
+  {
+    // one partner-list region per resident block of the force kernel
+    int bps = 1;
+    dispatch<DEOccupancy>(c, &bps);
+    const long long resident = (long long)c->n_sm * bps;
+    c->de_blocks = (int)(resident < c->n_blocks ? resident : c->n_blocks);
+    if (cells)
+      c->pair_list = dalloc(c, (size_t)c->de_blocks * kTile * kPairCap4 * sizeof(int4), &ok);
+  }
   if (list) {
     c->nbr_n = (int*)dalloc(c, n * 4, &ok);
     c->nbr_list = (int*)dalloc(c, n * (size_t)k.n_max_neighbors * 4, &ok);

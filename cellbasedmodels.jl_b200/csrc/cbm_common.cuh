@@ -50,6 +50,8 @@ struct Counters {
   int list_written;     // this step wrote the Verlet list lazily
   unsigned fate_ticket; // tile tickets of the fused rule / births kernel
   unsigned fate_epoch;  // generation of its tile states
+  unsigned de_ticket;   // tile tickets of the force kernel (reset by its last block)
+  unsigned de_done;     // blocks of the force kernel that have finished
 };
 
 template <typename T>

@@ -76,6 +76,10 @@ struct Params {
   // Verlet list in slot space: entry k of the row of slot s at k * n_max + s
   int* nbr_n;
   int* nbr_list;
+  // partner lists of the force walk: per block of k_agent_de, pair_cap4
+  // blocks of four slots per thread (block j of thread t at j * kTile + t)
+  int4* pair_list;
+  int pair_cap4;
   // medium: committed / written
   T* c_cur;
   T* c_nxt;
@@ -221,14 +225,41 @@ __device__ __forceinline__ void for_cell_slots(const Params<T>& P, const T* x, F
 }
 
 // Per-thread force queue of k_agent_de, in shared memory (kQueue * 1 KB per
-// block, 48 KB: the static limit).  A drain is cheapest when it runs once,
-// converged, at the end of an agent's walk: 48 entries hold every candidate
-// inside the cutoff of nearly every agent (about 17 on average in a packed
-// colony), which measured faster than 8 to 40 entries.
+// block, 48 KB: the static limit).  48 entries hold every partner of nearly
+// every agent of a colony at the packing density (about 17 on average), whose
+// terms then follow the walk in one converged drain; in denser colonies a
+// full queue moves to the thread's partner list in global memory.
 #ifndef CBM_FORCE_QUEUE
 #define CBM_FORCE_QUEUE 48
 #endif
 constexpr int kQueue = CBM_FORCE_QUEUE;
+
+// Partner-list capacity of the force walk, in blocks of four slots per
+// thread: 1024 slots (4 KB), more than the partners of an agent in a colony
+// compressed to 4 agents per unit volume (about 600 at most).  A list that
+// fills is evaluated where it stands, so the capacity bounds memory, not
+// correctness.
+constexpr int kPairCap4 = 256;
+static_assert(kPairCap4 >= kQueue / 4, "a flush must fit an empty list");
+
+// Asynchronous 16-byte copy global -> shared that bypasses L1 (each thread
+// waits for its own copies; no block barrier is involved).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+// list blocks fetched ahead of the one being evaluated, and the ring they
+// land in (the force queue, empty by then: kQueue / 4 blocks per thread)
+constexpr int kListAhead = 8;
+constexpr int kListRing = kQueue / 4;
+static_assert(kListRing > kListAhead, "the staging ring must exceed the prefetch depth");
 
 template <typename T>
 struct Eps;
@@ -731,12 +762,75 @@ __global__ void __launch_bounds__(kTile) k_agent_fate(Params<T> P) {
 // agentStepDE!: fused neighbor force + Euler / EM update, one thread per slot
 // (src/integrators.jl:465-505,683-734, functionDE.jl:13-117)
 // ---------------------------------------------------------------------------
+// e = xi - xj and its squared norm, in the reference's order
 template <typename T, int D>
-__global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
+__device__ __forceinline__ T pair_diff(const T* xi, const T* xj, T* e) {
+  e[0] = xi[0] - xj[0];
+  T s2 = e[0] * e[0];
+  if (D > 1) {
+    e[1] = xi[1] - xj[1];
+    s2 = s2 + e[1] * e[1];
+  }
+  if (D > 2) {
+    e[2] = xi[2] - xj[2];
+    s2 = s2 + e[2] * e[2];
+  }
+  return s2;
+}
+
+// Coefficients of the soft-sphere pair term.
+template <typename T>
+struct PairCoef {
+  T cut2, rrep, ratt, krep, katt;
+  bool from_rep;
+};
+template <typename T>
+__device__ __forceinline__ PairCoef<T> pair_coef(const Params<T>& P) {
+  return PairCoef<T>{P.cut2, P.r_rep, P.r_att, P.k_rep, P.k_att, P.att_form == CBM_ATT_FROM_REP};
+}
+
+// Soft-sphere pair term (repulsion inside r_rep, attraction up to r_att) of
+// the difference e with squared norm s2, added to acc.
+template <typename T, int D>
+__device__ __forceinline__ void pair_term(const PairCoef<T>& c, const T* e, T s2, T* acc) {
+  if (s2 >= c.cut2) return;  // d >= cutoff for certain (NaN takes the exact test)
+  const T dd = sqrt(s2);
+  T F;
+  if (dd < c.rrep) F = c.krep * (c.rrep - dd);
+  else if (dd < c.ratt) F = c.from_rep ? -(c.katt * (dd - c.rrep)) : -(c.katt * (c.ratt - dd));
+  else return;
+  const T sc = F / dd;
+#pragma unroll
+  for (int d = 0; d < D; ++d) acc[d] = acc[d] + sc * e[d];
+}
+
+// Terms of the first nblk stored partner blocks of slot s, oldest first.
+// Out of line: it runs only when a partner list fills in the middle of a
+// walk, and keeping it out of the walk keeps the walk's code small.
+template <typename T, int D>
+__device__ __noinline__ void list_terms(const PairCoef<T> c, const typename V4T<T>::type* U,
+                                        const int4* list, int nblk, int s, const T* xi, T* acc) {
+  for (int j = 0; j < nblk; ++j) {
+    const int4 b = __ldcg(list + (size_t)j * kTile);
+    const int qq[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (qq[u] == s) continue;
+      T xj[3], e[3];
+      to3<T>(U[qq[u]], xj);
+      const T s2 = pair_diff<T, D>(xi, xj, e);
+      pair_term<T, D>(c, e, s2, acc);
+    }
+  }
+}
+
+// Slot s of N; `list` is this thread's partner list (null: none); `live`
+// holds the lanes of this warp whose slot is below N.
+template <typename T, int D>
+__device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const int s,
+                                         int4* const list, const unsigned live) {
   using V4 = typename V4T<T>::type;
   const int p = P.parity;
-  const int N = (int)P.ctr->N[p];
-  const int s = blockIdx.x * kTile + threadIdx.x;
   if (s >= N) return;
   const bool reflect = P.walls == CBM_WALLS_REFLECT;
   const V4* U = reflect ? P.U : P.PA;
@@ -748,24 +842,9 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
   const T cut2 = P.cut2;
   const bool from_rep = P.att_form == CBM_ATT_FROM_REP;
   // pair term with the difference e = xi - xj and its squared norm s2
-  auto pair_e = [&](const T* e, T s2) {
-    if (s2 >= cut2) return;  // d >= cutoff for certain (NaN takes the exact test)
-    T dd = sqrt(s2);
-    T F;
-    if (dd < rrep) F = krep * (rrep - dd);
-    else if (dd < ratt) F = from_rep ? -(katt * (dd - rrep)) : -(katt * (ratt - dd));
-    else return;
-    T sc = F / dd;
-#pragma unroll
-    for (int d = 0; d < D; ++d) acc[d] = acc[d] + sc * e[d];
-  };
-  auto diff = [&](const T* xj, T* e) {
-    e[0] = xi[0] - xj[0];
-    T s2 = e[0] * e[0];
-    if (D > 1) { e[1] = xi[1] - xj[1]; s2 = s2 + e[1] * e[1]; }
-    if (D > 2) { e[2] = xi[2] - xj[2]; s2 = s2 + e[2] * e[2]; }
-    return s2;
-  };
+  const PairCoef<T> coef = pair_coef<T>(P);
+  auto pair_e = [&](const T* e, T s2) { pair_term<T, D>(coef, e, s2, acc); };
+  auto diff = [&](const T* xj, T* e) { return pair_diff<T, D>(xi, xj, e); };
   auto pair = [&](const T* xj) {
     T e[3];
     T s2 = diff(xj, e);
@@ -784,14 +863,14 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
     // Two phases.  The walk over the 3^D cells only filters: candidates that
     // may be within the cutoff are queued, in visiting order, in this
     // thread's column of a shared buffer.  The force terms are then
-    // evaluated from the queue, where nearly every lane has work; the queue
-    // is drained early when full, so the summation order is unchanged.
+    // evaluated from the queue (and the partner list it spills to), where
+    // nearly every lane has work, in visiting order.
     //
     // For CLVD the grid is current, so the list the last rebuild defines
     // (candidates within `skin` of the committed positions, in cell order)
     // is this walk; the list is also written out when no birth or death this
     // step forces another rebuild.
-    __shared__ int queue[kQueue * kTile];
+    __shared__ __align__(16) int queue[kQueue * kTile];
     int nq = 0;
     // Queued pairs four at a time: loads and differences of four entries are
     // independent, their terms are then added in queue order.  The agent
@@ -828,15 +907,83 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
     if (!(clvd && (P.ctr->events == 0 || !P.force_in_list))) {
       // force-only walk (CellLinked, or a CLVD step that will rebuild anyway
       // and whose cutoff lies inside the list radius): four independent
-      // candidates per iteration, then an in-order enqueue
-      // The queue is drained by every active lane together when one of them
-      // may run out of room, so drains run converged.
+      // candidates per iteration, then an in-order enqueue.  Every active lane
+      // empties its queue when one of them may run out of room.
       auto push = [&](int q) {
         queue[nq * kTile + threadIdx.x] = q;
         ++nq;
       };
+      // With a partner list, a full queue is not evaluated but appended to the
+      // list in blocks of four (a remainder of up to three stays queued); the
+      // terms follow the walk, once every lane has all its partners.  Lanes
+      // find their partners in bursts that differ from lane to lane (in the
+      // rows near each agent), so evaluating whenever one lane's queue fills
+      // keeps few lanes busy; at the end each lane's loop is as long as its
+      // own partner count.
+      int nl4 = 0;  // blocks of four entries in the list
+      auto eval4 = [&](const int4 b) {
+        const int qq[4] = {b.x, b.y, b.z, b.w};
+        T xx[4][3], ee[4][3], ss[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) to3<T>(U[qq[u]], xx[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) ss[u] = diff(xx[u], ee[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (qq[u] != s) pair_e(ee[u], ss[u]);
+      };
+      // the stored blocks in order, fetched kListAhead blocks ahead into the
+      // queue, empty by then.  Ring position r of this lane is 16 bytes of the
+      // warp's own queue columns (rows 4r..4r+3, eight lanes a row), so only
+      // this warp touches it; the warp syncs before (here) and after (between
+      // slots) its lanes reuse the queue.
+      auto eval_list_staged = [&]() {
+        const int lane = threadIdx.x & 31;
+        int* const ring0 = queue + (lane >> 3) * kTile + (threadIdx.x & ~31) + (lane & 7) * 4;
+        auto ring = [&](int r) { return reinterpret_cast<int4*>(ring0 + r * 4 * kTile); };
+#pragma unroll
+        for (int j = 0; j < kListAhead; ++j) {
+          if (j < nl4) cp_async16(ring(j), list + (size_t)j * kTile);
+          cp_async_commit();
+        }
+        int r = 0, w = kListAhead;  // ring positions of block j and of block j + kListAhead
+        for (int j = 0; j < nl4; ++j) {
+          cp_async_wait<kListAhead - 1>();
+          const int4 b = *ring(r);
+          if (j + kListAhead < nl4) cp_async16(ring(w), list + (size_t)(j + kListAhead) * kTile);
+          cp_async_commit();
+          r = r + 1 == kListRing ? 0 : r + 1;
+          w = w + 1 == kListRing ? 0 : w + 1;
+          eval4(b);
+        }
+        cp_async_wait<0>();
+        nl4 = 0;
+      };
+      // whole blocks of the queue to the list; up to three entries stay queued,
+      // or, with `all`, the last block is padded with the agent itself
+      auto flush = [&](bool all) {
+        const int nb = all ? (nq + 3) >> 2 : nq >> 2;
+        if (nl4 + nb > P.pair_cap4) {  // list full: its terms now, in order
+          list_terms<T, D>(coef, U, list, nl4, s, xi, acc);
+          nl4 = 0;
+        }
+        for (int b = 0; b < nb; ++b) {
+          int e[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int k = 4 * b + u;
+            e[u] = k < nq ? queue[k * kTile + threadIdx.x] : s;
+          }
+          __stcg(list + (size_t)(nl4 + b) * kTile, make_int4(e[0], e[1], e[2], e[3]));
+        }
+        nl4 += nb;
+        const int r = all ? 0 : nq & 3;
+        for (int k = 0; k < r; ++k)
+          queue[k * kTile + threadIdx.x] = queue[(4 * nb + k) * kTile + threadIdx.x];
+        nq = r;
+      };
       auto room = [&](int k) {
-        if (__any_sync(__activemask(), nq > kQueue - k)) drain();
+        if (__any_sync(__activemask(), nq > kQueue - k)) flush(false);
       };
       // the slot's cell is the grid's assignment of the committed position,
       // which the walk starts from unless the rule reflected it off a wall
@@ -868,6 +1015,14 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
           if (diff(xj, e) < cut2) push(q);
         }
       }, own_cell);
+      // a warp with a stored list evaluates from the list, every entry of the
+      // queue appended first; otherwise the queue is drained below
+      __syncwarp(live);
+      if (__any_sync(live, nl4 > 0)) {
+        flush(true);
+        __syncwarp(live);  // every lane's queue is read before the rings overwrite it
+        eval_list_staged();
+      }
     } else {
       const bool write = !P.ctr->events;
       const T skin2 = P.skin2, skin2_lo = P.skin2_lo;
@@ -1013,6 +1168,36 @@ __global__ void __launch_bounds__(kTile) k_agent_de(Params<T> P) {
     T xo[3];
     to3<T>(P.POLD[s], xo);
     if (dist<T, D>(xn, xo) >= P.rebuild_thr) P.ctr->flag[p] = 1;
+  }
+}
+
+// One block per resident slot of the device; each warp takes runs of 32
+// slots from a ticket counter until the N slots are done, so each thread owns
+// one region of the partner-list scratch.  The last warp to finish resets the
+// counter for the next launch.
+template <typename T, int D>
+__global__ void __launch_bounds__(kTile, sizeof(T) == 4 ? 4 : 3) k_agent_de(Params<T> P) {
+  Counters* C = P.ctr;
+  const int N = (int)C->N[P.parity];
+  const int n_runs = (N + 31) >> 5;
+  const int lane = threadIdx.x & 31;
+  int4* const list =
+      P.pair_list ? P.pair_list + (size_t)blockIdx.x * P.pair_cap4 * kTile + threadIdx.x : nullptr;
+  while (true) {
+    int run = 0;
+    if (lane == 0) run = (int)atomicAdd(&C->de_ticket, 1u);
+    run = __shfl_sync(kFull, run, 0);
+    if (run >= n_runs) break;
+    const int slot = (run << 5) + lane;
+    agent_de<T, D>(P, N, slot, list, __ballot_sync(kFull, slot < N));
+    __syncwarp();
+  }
+  if (lane == 0) {
+    __threadfence();
+    if (atomicAdd(&C->de_done, 1u) == gridDim.x * (kTile / 32) - 1) {
+      C->de_ticket = 0u;
+      C->de_done = 0u;
+    }
   }
 }
 

@@ -182,8 +182,9 @@ def test_packed_colony_1m_bitexact(gpu_lib, abi):
 @pytest.mark.parametrize("alg", ["CellLinked", "CLVD"])
 def test_dense_colony_bitexact(gpu_lib, abi, prec, alg):
     """A compressed colony (4 agents per unit volume, the core density a colony
-    grown from 10^4 reaches): warps of the force kernel sit inside one cell and
-    take the sub-cell walk; still bit-exact, through divisions, with the grid."""
+    grown from 10^4 reaches): the force walk stores some 450 partners per
+    agent in its partner lists; still bit-exact, through divisions, with the
+    grid."""
     from scenarios import packed_colony_3d
     neigh = abi.NEIGH_CELL_LINKED if alg == "CellLinked" else abi.NEIGH_CLVD
     kw, st = packed_colony_3d(abi, N=6000, density=4.0, L=60.0, n_max=12000,
@@ -197,6 +198,23 @@ def test_dense_colony_bitexact(gpu_lib, abi, prec, alg):
     assert g.counters()["N"] > 6000
     if alg == "CellLinked":
         assert_same_grid(g, o)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_overcrowded_colony_bitexact(gpu_lib, abi, prec):
+    """24 agents per unit volume: agents have over 1024 partners, more than a
+    partner list holds, so lists fill in the middle of the walk and their
+    terms are added there; the sums keep the reference's order."""
+    from scenarios import packed_colony_3d
+    kw, st = packed_colony_3d(abi, N=3000, density=24.0, L=60.0, n_max=6000,
+                              precision=abi.F32 if prec == "f32" else abi.F64)
+    kw = dict(kw, neighbors=abi.NEIGH_CELL_LINKED)
+    g, o = both(abi, kw, st)
+    for _ in range(2):
+        g.step(4)
+        o.step(4)
+        assert_same_state(g.download(), o.download(), ["x", "y", "z", "v", "id", "parent"])
+    assert_same_grid(g, o)
 
 
 @pytest.mark.parametrize("alg", ["CellLinked", "CLVD"])
