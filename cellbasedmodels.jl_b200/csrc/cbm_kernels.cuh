@@ -22,6 +22,7 @@
 // graph without host round trips (the reference reads flagRecomputeNeighbors_
 // and NAdd_ on the host every step, src/neighbors.jl:548, update.jl:214).
 #pragma once
+#include <type_traits>
 
 #include "cbm_common.cuh"
 
@@ -762,9 +763,41 @@ __global__ void __launch_bounds__(kTile) k_agent_fate(Params<T> P) {
 // agentStepDE!: fused neighbor force + Euler / EM update, one thread per slot
 // (src/integrators.jl:465-505,683-734, functionDE.jl:13-117)
 // ---------------------------------------------------------------------------
+// Packed pairs of float operations (sm_100 f32x2): one instruction, and per
+// element the same IEEE rounding as the scalar operation.
+__device__ __forceinline__ float2 f2_sub(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;"
+      : "=l"(r)
+      : "l"(*reinterpret_cast<unsigned long long*>(&a)),
+        "l"(*reinterpret_cast<unsigned long long*>(&b)));
+  return *reinterpret_cast<float2*>(&r);
+}
+__device__ __forceinline__ float2 f2_mul(float2 a, float2 b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;"
+      : "=l"(r)
+      : "l"(*reinterpret_cast<unsigned long long*>(&a)),
+        "l"(*reinterpret_cast<unsigned long long*>(&b)));
+  return *reinterpret_cast<float2*>(&r);
+}
+
 // e = xi - xj and its squared norm, in the reference's order
+// ((e0 e0 + e1 e1) + e2 e2); in Float32 the x and y halves are packed pairs.
 template <typename T, int D>
 __device__ __forceinline__ T pair_diff(const T* xi, const T* xj, T* e) {
+  if constexpr (std::is_same<T, float>::value && D > 1) {
+    const float2 d = f2_sub(make_float2(xi[0], xi[1]), make_float2(xj[0], xj[1]));
+    const float2 q = f2_mul(d, d);
+    e[0] = d.x;
+    e[1] = d.y;
+    T s2 = q.x + q.y;
+    if (D > 2) {
+      e[2] = xi[2] - xj[2];
+      s2 = s2 + e[2] * e[2];
+    }
+    return s2;
+  }
   e[0] = xi[0] - xj[0];
   T s2 = e[0] * e[0];
   if (D > 1) {
