@@ -319,7 +319,7 @@ void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P) {
 template <typename T, int D>
 void enqueue_agent_de(cbm_ctx* c, const Params<T>& P) {
   PROF("k_agent_de");
-  k_agent_de<T, D><<<c->de_blocks, kTile, 0, c->stream>>>(P);
+  k_agent_de<T, D><<<kPartnerLists<D> ? c->de_blocks : c->n_blocks, kTile, 0, c->stream>>>(P);
 }
 
 template <typename T, int D>
@@ -706,7 +706,7 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     dispatch<DEOccupancy>(c, &bps);
     const long long resident = (long long)c->n_sm * bps;
     c->de_blocks = (int)(resident < c->n_blocks ? resident : c->n_blocks);
-    if (cells)
+    if (cells && k.dims == 3)
       c->pair_list = dalloc(c, (size_t)c->de_blocks * kTile * kPairCap4 * sizeof(int4), &ok);
   }
   if (list) {

@@ -241,6 +241,11 @@ constexpr int kQueue = CBM_FORCE_QUEUE;
 // fills is evaluated where it stands, so the capacity bounds memory, not
 // correctness.
 constexpr int kPairCap4 = 256;
+// Partner lists (and the persistent force grid that owns them) are used in
+// 3D; in 1D and 2D an agent's 3 or 9 cells hold few partners, and the
+// queue's drain serves them.
+template <int D>
+constexpr bool kPartnerLists = D == 3;
 static_assert(kPairCap4 >= kQueue / 4, "a flush must fit an empty list");
 
 // Asynchronous 16-byte copy global -> shared that bypasses L1 (each thread
@@ -1016,7 +1021,10 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
         nq = r;
       };
       auto room = [&](int k) {
-        if (__any_sync(__activemask(), nq > kQueue - k)) flush(false);
+        if (__any_sync(__activemask(), nq > kQueue - k)) {
+          if constexpr (kPartnerLists<D>) flush(false);
+          else drain();
+        }
       };
       // the slot's cell is the grid's assignment of the committed position,
       // which the walk starts from unless the rule reflected it off a wall
@@ -1050,11 +1058,13 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
       }, own_cell);
       // a warp with a stored list evaluates from the list, every entry of the
       // queue appended first; otherwise the queue is drained below
-      __syncwarp(live);
-      if (__any_sync(live, nl4 > 0)) {
-        flush(true);
-        __syncwarp(live);  // every lane's queue is read before the rings overwrite it
-        eval_list_staged();
+      if constexpr (kPartnerLists<D>) {
+        __syncwarp(live);
+        if (__any_sync(live, nl4 > 0)) {
+          flush(true);
+          __syncwarp(live);  // every lane's queue is read before the rings overwrite it
+          eval_list_staged();
+        }
       }
     } else {
       const bool write = !P.ctr->events;
@@ -1204,30 +1214,38 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
   }
 }
 
-// One block per resident slot of the device; each warp takes runs of 32
-// slots from a ticket counter until the N slots are done, so each thread owns
-// one region of the partner-list scratch.  The last warp to finish resets the
-// counter for the next launch.
+// One block per resident slot of the device, so each thread owns one region
+// of the partner-list scratch.  Warp w first takes run w of 32 slots, then
+// further runs from a ticket counter until the N slots are done (small
+// colonies need no ticket).  The last block to finish resets the counter for
+// the next launch.
 template <typename T, int D>
 __global__ void __launch_bounds__(kTile, sizeof(T) == 4 ? 4 : 3) k_agent_de(Params<T> P) {
   Counters* C = P.ctr;
   const int N = (int)C->N[P.parity];
+  if constexpr (!kPartnerLists<D>) {  // one thread per slot, grid over n_max
+    const int slot = (int)blockIdx.x * kTile + (int)threadIdx.x;
+    agent_de<T, D>(P, N, slot, nullptr, __ballot_sync(kFull, slot < N));
+    return;
+  }
   const int n_runs = (N + 31) >> 5;
   const int lane = threadIdx.x & 31;
+  const int n_warps = (int)gridDim.x * (kTile / 32);
   int4* const list =
       P.pair_list ? P.pair_list + (size_t)blockIdx.x * P.pair_cap4 * kTile + threadIdx.x : nullptr;
-  while (true) {
-    int run = 0;
-    if (lane == 0) run = (int)atomicAdd(&C->de_ticket, 1u);
-    run = __shfl_sync(kFull, run, 0);
-    if (run >= n_runs) break;
+  int run = (int)blockIdx.x * (kTile / 32) + (int)(threadIdx.x >> 5);
+  while (run < n_runs) {
     const int slot = (run << 5) + lane;
     agent_de<T, D>(P, N, slot, list, __ballot_sync(kFull, slot < N));
     __syncwarp();
+    int t = 0;
+    if (lane == 0) t = (int)atomicAdd(&C->de_ticket, 1u);
+    run = n_warps + __shfl_sync(kFull, t, 0);
   }
-  if (lane == 0) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
     __threadfence();
-    if (atomicAdd(&C->de_done, 1u) == gridDim.x * (kTile / 32) - 1) {
+    if (atomicAdd(&C->de_done, 1u) == gridDim.x - 1) {
       C->de_ticket = 0u;
       C->de_done = 0u;
     }
