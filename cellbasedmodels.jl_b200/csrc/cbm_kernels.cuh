@@ -299,6 +299,9 @@ __device__ __forceinline__ void walk_cells(const Params<T>& P, const typename V4
 
 // The pruned cell walk as a sequence of contiguous slot runs run(s0, s1).
 // `cell`, when given, is the linear cell of x (the grid's own assignment).
+// The decisions of the 3^(D-1) rows are taken first and kept as a mask
+// (three bits a row: visited, with the x-1 cell, with the x+1 cell), so the
+// walk itself holds only the mask, x's cell column and its first row.
 template <typename T, int D, typename F>
 __device__ __forceinline__ void walk_runs(const Params<T>& P, const T* x, T reach, F&& run,
                                           int cell) {
@@ -328,22 +331,34 @@ __device__ __forceinline__ void walk_runs(const Params<T>& P, const T* x, T reac
   const int nx = P.n_cells_d[0];
   constexpr int ny_rows = D > 1 ? 3 : 1;
   constexpr int nz_rows = D > 2 ? 3 : 1;
+  unsigned mask = 0u;
+#pragma unroll
   for (int dz = 0; dz < nz_rows; ++dz) {
-    const int pz = D > 2 ? q[2] + dz - 1 : 0;
-    if (D > 2 && (pz < 0 || pz >= P.n_cells_d[2])) continue;
-    const T gz = dz == 0 ? gm[2] : (dz == 2 ? gp[2] : (T)0);
+#pragma unroll
     for (int dy = 0; dy < ny_rows; ++dy) {
+      const int pz = D > 2 ? q[2] + dz - 1 : 0;
       const int py = D > 1 ? q[1] + dy - 1 : 0;
+      if (D > 2 && (pz < 0 || pz >= P.n_cells_d[2])) continue;
       if (D > 1 && (py < 0 || py >= P.n_cells_d[1])) continue;
+      const T gz = dz == 0 ? gm[2] : (dz == 2 ? gp[2] : (T)0);
       const T gy = dy == 0 ? gm[1] : (dy == 2 ? gp[1] : (T)0);
       const T gyz = (D > 1 ? gy * gy : (T)0) + (D > 2 ? gz * gz : (T)0);
       if (!(gyz < r2)) continue;
-      const int xa = (q[0] > 0 && gm[0] * gm[0] + gyz < r2) ? q[0] - 1 : q[0];
-      const int xb = (q[0] < nx - 1 && gp[0] * gp[0] + gyz < r2) ? q[0] + 1 : q[0];
-      const int row = nx * (py + P.n_cells_d[1] * pz);
-      run(ld(P.cell_start + row + xa), ld(P.cell_start + row + xb + 1));
+      const unsigned lo = (q[0] > 0 && gm[0] * gm[0] + gyz < r2) ? 2u : 0u;
+      const unsigned hi = (q[0] < nx - 1 && gp[0] * gp[0] + gyz < r2) ? 4u : 0u;
+      mask |= (1u | lo | hi) << (3 * (dz * ny_rows + dy));
     }
   }
+  const int x0 = q[0];
+  const int row0 = nx * ((D > 1 ? q[1] - 1 : 0) + P.n_cells_d[1] * (D > 2 ? q[2] - 1 : 0));
+  for (int dz = 0; dz < nz_rows; ++dz)
+    for (int dy = 0; dy < ny_rows; ++dy) {
+      const unsigned m = mask >> (3 * (dz * ny_rows + dy));
+      if (!(m & 1u)) continue;
+      const int row = row0 + nx * (dy + P.n_cells_d[1] * dz);
+      const int xa = x0 - (int)((m >> 1) & 1u), xb = x0 + (int)((m >> 2) & 1u);
+      run(ld(P.cell_start + row + xa), ld(P.cell_start + row + xb + 1));
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -872,7 +887,6 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
   if (s >= N) return;
   const bool reflect = P.walls == CBM_WALLS_REFLECT;
   const V4* U = reflect ? P.U : P.PA;
-  const int i = ld(P.IA + s);
   T xi[3];
   to3<T>(U[s], xi);
   T acc[3] = {(T)0, (T)0, (T)0};
@@ -891,7 +905,7 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
   const int alg = P.neighbors;
   if (alg == CBM_NEIGH_FULL) {
     for (int j = 0; j < N; ++j) {
-      if (j == i) continue;
+      if (j == ld(P.IA + s)) continue;
       T xj[3];
       to3<T>(U[ld(P.inv + j)], xj);
       pair(xj);
@@ -1186,6 +1200,7 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
 #pragma unroll
     for (int d = 0; d < D; ++d) dv[d] = dv[d] + (P.chemotaxis * gv[d]) / den;
   }
+  const int i = ld(P.IA + s);  // agent index of the slot
   T xn[3] = {(T)0, (T)0, (T)0};
   if (P.integrator == CBM_INT_EM) {
     T xi_n[3] = {(T)0, (T)0, (T)0};
