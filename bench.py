@@ -198,11 +198,13 @@ class SmiClocks:
 
 # DRAM bytes per agent of one launch, from one ncu capture each (dram__bytes_read.sum
 # + dram__bytes_write.sum) of k_agent_de in walk mode, Float32: the grown colony
-# (33.4 MB for about 1.02M agents, first timed step) and the packed snapshot
-# (35.0 MB for about 1.03M agents).  Traffic grows in proportion to the agents
-# of the launch, so it is scaled to the bench's agent count.
-MEASURED_TRAFFIC_PER_AGENT = {("k_agent_de", 4, True, "grown"): 32.7,
-                              ("k_agent_de", 4, True, "packed"): 34.0}
+# (5.34 GB for about 1.02M agents, first timed step: the partner lists, written
+# and read back, dominate; the compulsory state is 45 B/agent) and the packed
+# snapshot (35.5 MB for about 1.01M agents, whose partners rarely leave the
+# shared-memory queue).  Traffic grows in proportion to the agents of the
+# launch, so it is scaled to the bench's agent count.
+MEASURED_TRAFFIC_PER_AGENT = {("k_agent_de", 4, True, "grown"): 5230.0,
+                              ("k_agent_de", 4, True, "packed"): 35.1}
 
 
 def traffic_per_launch(name, s, walked, agents, workload):
