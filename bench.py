@@ -1,12 +1,16 @@
 #!/usr/bin/env python
 """Agent-steps/s of the per-step hot path on B200.
 
-Default workload (one GPU): a 3D growing colony snapshot of 10^6 agents in
-[0,400]^3 at packed density (0.15 agents per unit volume), Float32, soft-sphere
-repulsion/adhesion (k=10, a=1, r=1), Euler–Maruyama noise sigma=0.05, volume
-growth with division at v=2 and death probability 1e-4 (divisions occur every
-step), CLVD neighbors with list radius 3.3 and rebuild threshold 0.15,
-dt=0.005.  A "step" is one step! (rule, DE, update!, computeNeighbors!).
+Default workload (one GPU): the 3D growing colony as configured.  10^4 agents
+uniform in a radius-20 ball centred in [0,400]^3 grow by division on the GPU
+to 10^6 (1330 steps; about 4 agents per unit volume in the core, some 350
+partners inside the cutoff per agent), and the timed steps run on that state.
+Float32, soft-sphere repulsion/adhesion (k=10, a=1, r=1), Euler–Maruyama noise
+sigma=0.05, volume growth with division at v=2 and death probability 1e-4
+(divisions occur every step), CLVD neighbors with list radius 3.3 and rebuild
+threshold 0.15, dt=0.005.  `--workload packed` times a synthetic snapshot of
+10^6 agents at the packing density (0.15 per unit volume) instead.  A "step"
+is one step! (rule, DE, update!, computeNeighbors!).
 
   value  : device time (CUDA events on the library's stream, CUDA-graph replay),
            inputs resident in HBM, L2 flushed between timed steps
