@@ -437,6 +437,101 @@ class Batch:
 
 
 # ---- adjoint (cbm_adjoint_*) --------------------------------------------------
+# ---- implicit medium (cbm_medium_*, DGADI) ----------------------------------
+MEDIUM_MAX_FIELDS = 8
+
+
+class CbmMediumConfig(C.Structure):
+    _fields_ = [("dims", C.c_int32), ("precision", C.c_int32), ("n", C.c_int32 * 3),
+                ("n_fields", C.c_int32), ("box_lo", C.c_double * 3), ("box_hi", C.c_double * 3),
+                ("dt", C.c_double), ("diffusion", C.c_double * MEDIUM_MAX_FIELDS),
+                ("decay", C.c_double * MEDIUM_MAX_FIELDS), ("c_max", C.c_double)]
+
+
+def make_medium_config(dims, n, box_lo, box_hi, dt, diffusion, decay=None, c_max=0.0,
+                       precision=F32):
+    """A cbm_medium_config: `n` nodes per axis, one diffusion coefficient (and
+    optional decay) per field."""
+    k = CbmMediumConfig()
+    k.dims, k.precision = dims, precision
+    for d in range(3):
+        k.n[d] = int(n[d]) if d < dims else 1
+        k.box_lo[d] = float(box_lo[d]) if d < dims else 0.0
+        k.box_hi[d] = float(box_hi[d]) if d < dims else 1.0
+    k.n_fields = len(diffusion)
+    k.dt, k.c_max = float(dt), float(c_max)
+    for f, D in enumerate(diffusion):
+        k.diffusion[f] = float(D)
+        k.decay[f] = float(decay[f]) if decay is not None else 0.0
+    return k
+
+
+def _bind_medium(lib):
+    if getattr(lib, "_medium_bound", False):
+        return
+    vp, i32 = C.c_void_p, C.c_int32
+    sig = {
+        "cbm_medium_create": (C.c_int, [C.POINTER(vp), C.POINTER(CbmMediumConfig)]),
+        "cbm_medium_destroy": (None, [vp]),
+        "cbm_medium_last_error": (C.c_char_p, [vp]),
+        "cbm_medium_upload": (C.c_int, [vp, vp, vp]),
+        "cbm_medium_step": (C.c_int, [vp, i32, i32]),
+        "cbm_medium_download": (C.c_int, [vp, vp, C.POINTER(C.c_double)]),
+        "cbm_medium_stream": (vp, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    lib._medium_bound = True
+
+
+class Medium:
+    """A medium advanced by the implicit Douglas–Gunn ADI step (DGADI).
+    Fields are arrays of shape (n_fields, [n2, [n1,]] n0), x fastest."""
+
+    def __init__(self, cfg):
+        self.lib = load_library()
+        _bind_medium(self.lib)
+        h = C.c_void_p()
+        rc = self.lib.cbm_medium_create(C.byref(h), C.byref(cfg))
+        if rc != CBM_OK:
+            raise CbmError(rc, self.lib.cbm_medium_last_error(None).decode())
+        self.h = h
+        self.cfg = cfg
+        self.dtype = np.float64 if cfg.precision == F64 else np.float32
+        self.shape = (cfg.n_fields,) + tuple(int(cfg.n[d]) for d in reversed(range(cfg.dims)))
+
+    def _check(self, rc):
+        if rc != CBM_OK:
+            raise CbmError(rc, self.lib.cbm_medium_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cbm_medium_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def upload(self, fields, source=None):
+        f = np.ascontiguousarray(fields, dtype=self.dtype).reshape(self.shape)
+        s = None if source is None else np.ascontiguousarray(source, dtype=self.dtype)
+        self._check(self.lib.cbm_medium_upload(self.h, f.ctypes.data,
+                                               None if s is None else s.ctypes.data))
+
+    def step(self, n, flags=SYNC):
+        self._check(self.lib.cbm_medium_step(self.h, n, flags))
+
+    def download(self):
+        out = np.zeros(self.shape, self.dtype)
+        t = C.c_double()
+        self._check(self.lib.cbm_medium_download(self.h, out.ctypes.data, C.byref(t)))
+        return out, t.value
+
+    def stream(self):
+        return self.lib.cbm_medium_stream(self.h)
+
+
 class Adjoint:
     """Gradients of mean((x_T - target)^2) w.r.t. (k_rep, k_att, r_rep) and x0."""
 

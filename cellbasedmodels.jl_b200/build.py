@@ -13,7 +13,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libcbm_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("cbm_api.cu", "cbm_batch.cu", "cbm_adjoint.cu", "cbm_noalloc.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("cbm_api.cu", "cbm_batch.cu", "cbm_adjoint.cu", "cbm_noalloc.cu", "cbm_medium.cu")]
 DEPS = SOURCES + [
     os.path.join(HERE, "csrc", "cbm_kernels.cuh"),
     os.path.join(HERE, "csrc", "cbm_common.cuh"),

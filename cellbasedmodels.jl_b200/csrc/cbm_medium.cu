@@ -1,0 +1,349 @@
+// cbm_medium.cu — the implicit medium integrator DGADI on the device.
+//
+// CBMIntegrators.DGADI (src/integrators.jl:817-937) advances the medium by
+//   1. u .+= f(u)                        (the explicit part, no factor dt)
+//   2. a Thomas solve along every line of x, then y, then z
+//      (tridiagonal{1,2,3}D{x,y,z}{CPU,GPU}!, :141-428)
+// with the border nodes fixed at their initial values (the reference never
+// writes them into u_new, and copies u_new into u after each axis).
+//
+// Layout: field k, node (x, y, z) at k * nodes + x + n0 * (y + n1 * z).  Two
+// copies of every field: a step reads one and writes the interior of the
+// other, whose border nodes hold the uploaded values, so the copy back of the
+// reference is a swap.
+//
+// The line recurrence (0-based, nodes 0 and n-1 are the Dirichlet ends):
+//   c*_1 = sup / main                    d*_1 = (x_1 - sub x_0) / main
+//   m_j  = 1.0 / (main - sub c*_{j-1})   (Float64: Julia promotes 1.0 / x)
+//   c*_j = T(sup m_j)                    d*_j = T((x_j - sub d*_{j-1}) m_j)
+//   d*_{n-2} = T(((x_{n-2} - sup x_{n-1}) - sub d*_{n-3}) m_{n-2})
+//   x_{n-2} = d*_{n-2},  x_j = d*_j - c*_j x_{j+1}
+// c*_j and m_j depend only on the diagonals, so every line of a field and
+// axis shares one table of them (the same bits as recomputing them per line).
+// One thread walks one line: lines along y and z are coalesced across
+// threads; lines along x are served by L1 (each thread reads its own
+// contiguous row).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/cbm_b200.h"
+
+namespace {
+
+constexpr int kMedThreads = 256;
+constexpr int kSweepThreads = 128;
+
+template <typename T>
+struct FieldCoef {
+  T sub[CBM_MEDIUM_MAX_FIELDS], main[CBM_MEDIUM_MAX_FIELDS], sup[CBM_MEDIUM_MAX_FIELDS];
+  T decay[CBM_MEDIUM_MAX_FIELDS];
+};
+
+// Diagonals, c* and the pivots of every (field, axis): one thread each.
+// r = dt / (dims dx^2) with dx of the last axis for every axis (the
+// reference's column [l, dims]); the coefficients are formed in Float64 and
+// rounded to the field precision.
+template <typename T>
+__global__ void k_dgadi_tables(cbm_medium_config k, int nmax, FieldCoef<T>* coef, T* cstar,
+                               double* piv) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= k.n_fields * 3) return;
+  const int f = id / 3, a = id % 3;
+  const int D = k.dims;
+  const double dxl = (k.box_hi[D - 1] - k.box_lo[D - 1]) / (double)k.n[D - 1];
+  const double r = k.dt / ((double)D * (dxl * dxl));
+  const T sub = (T)(-k.diffusion[f] * r), sup = (T)(-k.diffusion[f] * r);
+  const T main = (T)(1.0 + 2.0 * k.diffusion[f] * r);
+  if (a == 0) {
+    coef->sub[f] = sub;
+    coef->main[f] = main;
+    coef->sup[f] = sup;
+    coef->decay[f] = (T)k.decay[f];
+  }
+  if (a >= D) return;
+  const int n = k.n[a];
+  T* cs = cstar + (size_t)id * nmax;
+  double* pv = piv + (size_t)id * nmax;
+  cs[1] = sup / main;
+  for (int j = 2; j <= n - 2; ++j) {
+    pv[j] = 1.0 / (double)(main - sub * cs[j - 1]);
+    if (j <= n - 3) cs[j] = (T)((double)sup * pv[j]);
+  }
+}
+
+// u .+= f(u) at interior nodes: f = s (c_max - u) - decay u
+template <typename T, int D>
+__global__ void k_dgadi_explicit(T* __restrict__ u, const T* __restrict__ src,
+                                 const FieldCoef<T>* __restrict__ coef, T cmax, int n0, int n1,
+                                 int n2, int nf) {
+  const long long nodes = (long long)n0 * n1 * n2;
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= nodes * nf) return;
+  const int f = (int)(id / nodes);
+  const long long i = id - (long long)f * nodes;
+  const int x = (int)(i % n0);
+  const int y = D > 1 ? (int)((i / n0) % n1) : 0;
+  const int z = D > 2 ? (int)(i / ((long long)n0 * n1)) : 0;
+  const bool in = x > 0 && x < n0 - 1 && (D < 2 || (y > 0 && y < n1 - 1)) &&
+                  (D < 3 || (z > 0 && z < n2 - 1));
+  if (!in) return;
+  const T ui = u[id];
+  const T du = src[i] * (cmax - ui) - coef->decay[f] * ui;
+  u[id] = ui + du;
+}
+
+// The Thomas solves of axis A: one thread per (field, line through interior
+// nodes of the other axes).  Reads xo, writes the line's interior of xn
+// (d* first, then the solution in place).
+template <typename T, int A, int D>
+__global__ void __launch_bounds__(kSweepThreads)
+    k_dgadi_sweep(const T* __restrict__ xo, T* __restrict__ xn, const FieldCoef<T>* __restrict__ coef,
+                  const T* __restrict__ cstar, const double* __restrict__ piv, int nmax, int n0,
+                  int n1, int n2, int nf) {
+  const int len[3] = {n0, n1, n2};
+  const long long stride[3] = {1, n0, (long long)n0 * n1};
+  constexpr int B = A == 0 ? 1 : 0;  // the line's position: (b, c) interior
+  constexpr int Cx = A == 2 ? 1 : 2;
+  const int nb = B < D ? len[B] - 2 : 1, nc = Cx < D ? len[Cx] - 2 : 1;
+  const long long lines = (long long)nb * nc;
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= lines * nf) return;
+  const int f = (int)(id / lines);
+  const long long l = id - (long long)f * lines;
+  const int ib = (int)(l % nb) + (B < D ? 1 : 0);
+  const int ic = (int)(l / nb) + (Cx < D ? 1 : 0);
+  const long long o =
+      (long long)f * n0 * n1 * n2 + (long long)ib * stride[B] + (long long)ic * stride[Cx];
+  const long long st = stride[A];
+  const int n = len[A];
+  const T sub = coef->sub[f], main = coef->main[f], sup = coef->sup[f];
+  const T* cs = cstar + (size_t)(f * 3 + A) * nmax;
+  const double* pv = piv + (size_t)(f * 3 + A) * nmax;
+  const T* X = xo + o;
+  T* Y = xn + o;
+  T d = (X[st] - sub * X[0]) / main;
+  Y[st] = d;
+  for (int j = 2; j <= n - 3; ++j) {
+    d = (T)((double)(X[j * st] - sub * d) * pv[j]);
+    Y[j * st] = d;
+  }
+  T x = (T)((double)((X[(n - 2) * st] - sup * X[(n - 1) * st]) - sub * d) * pv[n - 2]);
+  Y[(n - 2) * st] = x;
+  for (int j = n - 3; j >= 1; --j) {
+    x = Y[j * st] - cs[j] * x;
+    Y[j * st] = x;
+  }
+}
+
+}  // namespace
+
+struct cbm_medium {
+  cbm_medium_config cfg{};
+  int tsize = 4;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  long long nodes = 0;
+  int nmax = 0;
+  void* u[2] = {nullptr, nullptr};
+  void* src = nullptr;
+  void* coef = nullptr;
+  void* cstar = nullptr;
+  double* piv = nullptr;
+  int cur = 0;
+  long long steps = 0;
+  double t = 0;
+  bool loaded = false;
+  std::string err;
+};
+
+namespace {
+
+std::string g_medium_create_error;
+
+int mfail(cbm_medium* m, int code, const std::string& msg) {
+  if (m) m->err = msg;
+  else g_medium_create_error = msg;
+  return code;
+}
+
+#define MED_TRY(m, call)                                                                    \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return mfail(m, CBM_ERR_CUDA, std::string(#call) + " failed: " + cudaGetErrorString(e_)); \
+  } while (0)
+
+void mfree(cbm_medium* m) {
+  for (void* p : {m->u[0], m->u[1], m->src, m->coef, m->cstar, (void*)m->piv})
+    if (p) cudaFree(p);
+  m->u[0] = m->u[1] = m->src = m->coef = m->cstar = nullptr;
+  m->piv = nullptr;
+  if (m->stream) cudaStreamDestroy(m->stream);
+  m->stream = nullptr;
+}
+
+template <typename T, int D>
+int enqueue_step(cbm_medium* m) {
+  const cbm_medium_config& k = m->cfg;
+  const int n0 = k.n[0], n1 = D > 1 ? k.n[1] : 1, n2 = D > 2 ? k.n[2] : 1;
+  const int nf = k.n_fields;
+  T* u[2] = {(T*)m->u[0], (T*)m->u[1]};
+  const auto* coef = (const FieldCoef<T>*)m->coef;
+  const long long tot = m->nodes * nf;
+  k_dgadi_explicit<T, D><<<(unsigned)((tot + kMedThreads - 1) / kMedThreads), kMedThreads, 0,
+                           m->stream>>>(u[m->cur], (const T*)m->src, coef, (T)k.c_max, n0, n1,
+                                        n2, nf);
+  auto lines = [&](int a) {
+    const int len[3] = {n0, n1, n2};
+    long long l = 1;
+    for (int d = 0; d < D; ++d)
+      if (d != a) l *= len[d] - 2;
+    return l * nf;
+  };
+  auto grid = [&](long long n) { return (unsigned)((n + kSweepThreads - 1) / kSweepThreads); };
+  const T* cs = (const T*)m->cstar;
+  k_dgadi_sweep<T, 0, D><<<grid(lines(0)), kSweepThreads, 0, m->stream>>>(
+      u[m->cur], u[m->cur ^ 1], coef, cs, m->piv, m->nmax, n0, n1, n2, nf);
+  m->cur ^= 1;
+  if (D > 1) {
+    k_dgadi_sweep<T, 1, D><<<grid(lines(1)), kSweepThreads, 0, m->stream>>>(
+        u[m->cur], u[m->cur ^ 1], coef, cs, m->piv, m->nmax, n0, n1, n2, nf);
+    m->cur ^= 1;
+  }
+  if (D > 2) {
+    k_dgadi_sweep<T, 2, D><<<grid(lines(2)), kSweepThreads, 0, m->stream>>>(
+        u[m->cur], u[m->cur ^ 1], coef, cs, m->piv, m->nmax, n0, n1, n2, nf);
+    m->cur ^= 1;
+  }
+  MED_TRY(m, cudaGetLastError());
+  return CBM_OK;
+}
+
+template <typename T>
+int enqueue_step_t(cbm_medium* m) {
+  switch (m->cfg.dims) {
+    case 1: return enqueue_step<T, 1>(m);
+    case 2: return enqueue_step<T, 2>(m);
+    default: return enqueue_step<T, 3>(m);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int cbm_medium_create(cbm_medium** out, const cbm_medium_config* cfg) {
+  if (!out || !cfg) return mfail(nullptr, CBM_ERR_ARG, "null argument");
+  *out = nullptr;
+  const cbm_medium_config& k = *cfg;
+  if (k.dims < 1 || k.dims > 3) return mfail(nullptr, CBM_ERR_ARG, "dims must be 1, 2 or 3");
+  if (k.precision != CBM_F32 && k.precision != CBM_F64)
+    return mfail(nullptr, CBM_ERR_ARG, "precision must be CBM_F32 or CBM_F64");
+  if (k.n_fields < 1 || k.n_fields > CBM_MEDIUM_MAX_FIELDS)
+    return mfail(nullptr, CBM_ERR_ARG, "n_fields must be 1 .. CBM_MEDIUM_MAX_FIELDS");
+  long long nodes = 1;
+  int nmax = 0;
+  for (int d = 0; d < k.dims; ++d) {
+    if (k.n[d] < 4)
+      return mfail(nullptr, CBM_ERR_ARG, "every axis of a DGADI medium needs at least 4 nodes");
+    nodes *= k.n[d];
+    nmax = k.n[d] > nmax ? k.n[d] : nmax;
+  }
+  if (nodes * k.n_fields >= (1ll << 40)) return mfail(nullptr, CBM_ERR_ARG, "medium too large");
+  if (!(k.dt > 0) || !(k.box_hi[k.dims - 1] > k.box_lo[k.dims - 1]))
+    return mfail(nullptr, CBM_ERR_ARG, "dt and the last axis of the box must be positive");
+
+  cbm_medium* m = new cbm_medium;
+  m->cfg = k;
+  for (int d = k.dims; d < 3; ++d) m->cfg.n[d] = 1;
+  m->tsize = k.precision == CBM_F64 ? 8 : 4;
+  m->nodes = nodes;
+  m->nmax = nmax;
+  cudaGetDevice(&m->device);
+  const size_t fb = (size_t)nodes * k.n_fields * m->tsize;
+  bool ok = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && cudaMalloc(&m->u[0], fb) == cudaSuccess;
+  ok = ok && cudaMalloc(&m->u[1], fb) == cudaSuccess;
+  ok = ok && cudaMalloc(&m->src, (size_t)nodes * m->tsize) == cudaSuccess;
+  ok = ok && cudaMalloc(&m->coef, sizeof(FieldCoef<double>)) == cudaSuccess;
+  ok = ok && cudaMalloc(&m->cstar, (size_t)k.n_fields * 3 * nmax * m->tsize) == cudaSuccess;
+  ok = ok && cudaMalloc((void**)&m->piv, (size_t)k.n_fields * 3 * nmax * 8) == cudaSuccess;
+  if (!ok) {
+    mfree(m);
+    delete m;
+    return mfail(nullptr, CBM_ERR_NOMEM, "device allocation failed for the DGADI medium");
+  }
+  const unsigned tb = (unsigned)((k.n_fields * 3 + 63) / 64);
+  if (m->tsize == 8)
+    k_dgadi_tables<double><<<tb, 64, 0, m->stream>>>(m->cfg, nmax, (FieldCoef<double>*)m->coef,
+                                                     (double*)m->cstar, m->piv);
+  else
+    k_dgadi_tables<float><<<tb, 64, 0, m->stream>>>(m->cfg, nmax, (FieldCoef<float>*)m->coef,
+                                                    (float*)m->cstar, m->piv);
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(m->stream) != cudaSuccess) {
+    mfree(m);
+    delete m;
+    return mfail(nullptr, CBM_ERR_CUDA, "DGADI table set-up failed");
+  }
+  *out = m;
+  return CBM_OK;
+}
+
+void cbm_medium_destroy(cbm_medium* m) {
+  if (!m) return;
+  mfree(m);
+  delete m;
+}
+
+const char* cbm_medium_last_error(const cbm_medium* m) {
+  return m ? m->err.c_str() : g_medium_create_error.c_str();
+}
+
+int cbm_medium_upload(cbm_medium* m, const void* fields, const void* source) {
+  if (!m || !fields) return mfail(m, CBM_ERR_ARG, "null argument");
+  const size_t fb = (size_t)m->nodes * m->cfg.n_fields * m->tsize;
+  MED_TRY(m, cudaMemcpyAsync(m->u[0], fields, fb, cudaMemcpyHostToDevice, m->stream));
+  MED_TRY(m, cudaMemcpyAsync(m->u[1], m->u[0], fb, cudaMemcpyDeviceToDevice, m->stream));
+  if (source)
+    MED_TRY(m, cudaMemcpyAsync(m->src, source, (size_t)m->nodes * m->tsize,
+                               cudaMemcpyHostToDevice, m->stream));
+  else
+    MED_TRY(m, cudaMemsetAsync(m->src, 0, (size_t)m->nodes * m->tsize, m->stream));
+  MED_TRY(m, cudaStreamSynchronize(m->stream));
+  m->cur = 0;
+  m->steps = 0;
+  m->t = 0;
+  m->loaded = true;
+  return CBM_OK;
+}
+
+int cbm_medium_step(cbm_medium* m, int32_t nsteps, int32_t flags) {
+  if (!m) return mfail(m, CBM_ERR_ARG, "null medium");
+  if (!m->loaded) return mfail(m, CBM_ERR_STATE, "cbm_medium_step before cbm_medium_upload");
+  if (nsteps < 0) return mfail(m, CBM_ERR_ARG, "nsteps must be >= 0");
+  for (int s = 0; s < nsteps; ++s) {
+    const int rc = m->tsize == 8 ? enqueue_step_t<double>(m) : enqueue_step_t<float>(m);
+    if (rc != CBM_OK) return rc;
+    m->steps += 1;
+    m->t += m->cfg.dt;  // obj.t += dt
+  }
+  if (flags & CBM_SYNC) MED_TRY(m, cudaStreamSynchronize(m->stream));
+  return CBM_OK;
+}
+
+int cbm_medium_download(cbm_medium* m, void* fields, double* t) {
+  if (!m || !fields) return mfail(m, CBM_ERR_ARG, "null argument");
+  if (!m->loaded) return mfail(m, CBM_ERR_STATE, "cbm_medium_download before cbm_medium_upload");
+  const size_t fb = (size_t)m->nodes * m->cfg.n_fields * m->tsize;
+  MED_TRY(m, cudaMemcpyAsync(fields, m->u[m->cur], fb, cudaMemcpyDeviceToHost, m->stream));
+  MED_TRY(m, cudaStreamSynchronize(m->stream));
+  if (t) *t = m->t;
+  return CBM_OK;
+}
+
+void* cbm_medium_stream(cbm_medium* m) { return m ? (void*)m->stream : nullptr; }
+
+}  // extern "C"

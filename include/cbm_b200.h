@@ -317,6 +317,51 @@ int cbm_adjoint_forward(cbm_adjoint* a, int64_t n, const void* const* x0, int32_
                         void* const* xT);
 void* cbm_adjoint_stream(cbm_adjoint* a);
 
+/* ---- implicit medium: Douglas–Gunn ADI ------------------------------------
+ * CBMIntegrators.DGADI (src/integrators.jl:817-937) on a medium of n_fields
+ * fields over n[0] x n[1] x n[2] nodes (x fastest; unused axes have 1 node).
+ * One step, as DifferentialEquations.step!(::DGADI) (:875-933):
+ *   1. the explicit part is added to every field, u .+= f(u) (no factor dt,
+ *      as in the reference), with the medium model
+ *        f_k = s (c_max - u_k) - decay_k u_k   at interior nodes, 0 on the border
+ *      (s a static source field; the mediumODE of examples/Implementation.ipynb
+ *      is decay = 0);
+ *   2. one Thomas solve per axis, x then y then z, along the lines through
+ *      interior nodes (tridiagonal{1,2,3}D{x,y,z}, :141-428), with
+ *        sub = super = -D_k r,  main = 1 + 2 D_k r,
+ *        r = dt / (dims * dx^2), dx = (box_hi - box_lo) / n of the LAST axis
+ *      for every axis (the reference reads column [l, dims] of its table),
+ *      and the two border nodes of each line as Dirichlet values.  In Float32
+ *      the pivots 1.0 / (...) are Float64, as Julia promotes them.
+ * Border nodes keep their uploaded values (the reference never writes them).
+ * Every axis needs at least 4 nodes.  Each step enqueues 1 + dims kernels. */
+#define CBM_MEDIUM_MAX_FIELDS 8
+typedef struct cbm_medium_config {
+  int32_t dims;                           /* 1, 2 or 3 */
+  int32_t precision;                      /* CBM_F32 or CBM_F64 */
+  int32_t n[3];                           /* nodes per axis (NMedium) */
+  int32_t n_fields;                       /* 1 .. CBM_MEDIUM_MAX_FIELDS */
+  double box_lo[3], box_hi[3];            /* simBox */
+  double dt;
+  double diffusion[CBM_MEDIUM_MAX_FIELDS]; /* D_k (difussionCoefs) */
+  double decay[CBM_MEDIUM_MAX_FIELDS];     /* decay_k */
+  double c_max;                           /* target of the source term */
+} cbm_medium_config;
+
+typedef struct cbm_medium cbm_medium;
+int cbm_medium_create(cbm_medium** out, const cbm_medium_config* cfg);
+void cbm_medium_destroy(cbm_medium* m);
+const char* cbm_medium_last_error(const cbm_medium* m);
+/* fields: n_fields blocks of prod(n) reals (field k, then x fastest); source:
+ * prod(n) reals, or NULL for s = 0.  Host arrays of the configured precision.
+ * Sets t = 0. */
+int cbm_medium_upload(cbm_medium* m, const void* fields, const void* source);
+/* nsteps DGADI steps; flags & CBM_SYNC waits for them. */
+int cbm_medium_step(cbm_medium* m, int32_t nsteps, int32_t flags);
+/* fields as in upload; *t (if not NULL) = steps taken x dt since the upload. */
+int cbm_medium_download(cbm_medium* m, void* fields, double* t);
+void* cbm_medium_stream(cbm_medium* m);
+
 /* ---- allocation-free cell grid -------------------------------------------
  * This entry point has no counterpart in the reference.  It is for callers
  * that cannot allocate device memory when they need a grid: code running

@@ -21,6 +21,9 @@
  *   - computeNeighbors!: CellLinked serial assign / cumsum / sort, Verlet
  *     displacement check + rebuild, CLVD list over the cell grid
  *     (src/neighbors.jl:92-133,367-570,636-979,1071-1131).
+ *   - the implicit medium integrator DGADI: explicit part, then one Thomas
+ *     solve per axis with u_new/c_star/d_star as the reference keeps them
+ *     (src/integrators.jl:141-428,817-937).
  * Random draws come from the shared counter-based stream (include/cbm_rng.h)
  * so that the device path and this checker see the same numbers.
  *
@@ -732,6 +735,87 @@ struct Handle {
 template <typename T>
 Com<T>* as(Handle* h) { return (Com<T>*)h->p; }
 
+// ---- implicit medium: DGADI (src/integrators.jl:141-428, 817-937) ---------
+// The reference's arrays: u (the medium ODE state), u_new, c_star, d_star,
+// all copies of u0 (DGADI(problem, ...) :844-856), shape (field, x, y, z)
+// with x fastest inside a field here.
+template <typename T>
+struct Med {
+  cbm_medium_config cfg;
+  int64_t nodes = 0;
+  std::vector<T> u, u_new, c_star, d_star, src;
+  double t = 0;
+};
+
+// One line of tridiagonal{1,2,3}D{x,y,z}CPU! (:141-269), 0-based: nodes 0 and
+// n-1 are the Dirichlet ends.  1.0 / (...) is Float64 (Julia promotes the
+// Float32 denominator), so the pivots and the products with them are formed
+// in Float64 and rounded to T when stored.
+template <typename T>
+void thomasLine(const T* xo, T* xn, T* cs, T* ds, int64_t st, int n, T sub, T main, T sup) {
+  auto X = [&](int j) { return xo[(int64_t)j * st]; };
+  auto C = [&](int j) -> T& { return cs[(int64_t)j * st]; };
+  auto Dd = [&](int j) -> T& { return ds[(int64_t)j * st]; };
+  C(1) = sup / main;
+  Dd(1) = (X(1) - sub * X(0)) / main;
+  for (int j = 2; j <= n - 3; ++j) {
+    const double m = 1.0 / (double)(main - sub * C(j - 1));
+    C(j) = (T)((double)sup * m);
+    Dd(j) = (T)((double)(X(j) - sub * Dd(j - 1)) * m);
+  }
+  const double m = 1.0 / (double)(main - sub * C(n - 3));
+  Dd(n - 2) = (T)((double)((X(n - 2) - sup * X(n - 1)) - sub * Dd(n - 3)) * m);
+  xn[(int64_t)(n - 2) * st] = Dd(n - 2);
+  for (int j = n - 3; j >= 1; --j)
+    xn[(int64_t)j * st] = Dd(j) - C(j) * xn[(int64_t)(j + 1) * st];
+}
+
+// DifferentialEquations.step!(::DGADI) (:875-933)
+template <typename T>
+void medStep(Med<T>& M) {
+  const cbm_medium_config& k = M.cfg;
+  const int D = k.dims;
+  const int n0 = k.n[0], n1 = D > 1 ? k.n[1] : 1, n2 = D > 2 ? k.n[2] : 1;
+  const int64_t N = M.nodes;
+  // du = f(u) inside (@mediumInside), then u .+= du
+  for (int f = 0; f < k.n_fields; ++f) {
+    const T cmax = (T)k.c_max, dec = (T)k.decay[f];
+    T* u = M.u.data() + f * N;
+    for (int z = 0; z < n2; ++z)
+      for (int y = 0; y < n1; ++y)
+        for (int x = 0; x < n0; ++x) {
+          const bool in = x > 0 && x < n0 - 1 && (D < 2 || (y > 0 && y < n1 - 1)) &&
+                          (D < 3 || (z > 0 && z < n2 - 1));
+          if (!in) continue;
+          const int64_t i = x + (int64_t)n0 * (y + (int64_t)n1 * z);
+          const T du = M.src[i] * (cmax - u[i]) - dec * u[i];
+          u[i] = u[i] + du;
+        }
+  }
+  // r = dt / (dims dx^2) per axis; every axis reads the last one's
+  const double dxl = (k.box_hi[D - 1] - k.box_lo[D - 1]) / (double)k.n[D - 1];
+  const double r = k.dt / ((double)D * (dxl * dxl));
+  const int64_t stride[3] = {1, n0, (int64_t)n0 * n1};
+  const int len[3] = {n0, n1, n2};
+  for (int a = 0; a < D; ++a) {
+    // lines along axis a through interior nodes of the other axes
+    const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
+    const int lb = b < D ? len[b] : 1, lc = c < D ? len[c] : 1;
+    for (int f = 0; f < k.n_fields; ++f) {
+      const T sub = (T)(-k.diffusion[f] * r), sup = (T)(-k.diffusion[f] * r);
+      const T main = (T)(1.0 + 2.0 * k.diffusion[f] * r);
+      for (int ic = (c < D ? 1 : 0); ic < (c < D ? lc - 1 : 1); ++ic)
+        for (int ib = (b < D ? 1 : 0); ib < (b < D ? lb - 1 : 1); ++ib) {
+          const int64_t o = f * N + (int64_t)ib * stride[b] + (int64_t)ic * stride[c];
+          thomasLine<T>(M.u.data() + o, M.u_new.data() + o, M.c_star.data() + o,
+                        M.d_star.data() + o, stride[a], len[a], sub, main, sup);
+        }
+    }
+    M.u = M.u_new;  // obj.u .= obj.u_new
+  }
+  M.t += k.dt;
+}
+
 }  // namespace
 
 #define DISPATCH(h, expr)                          \
@@ -908,6 +992,92 @@ int oracle_rng_fill(int precision, uint64_t seed, uint32_t community, int kind, 
 }
 
 /* own log / cos-sin, exposed for accuracy tests */
+struct MedHandle {
+  int prec;
+  void* p;
+};
+
+void* oracle_medium_create(const cbm_medium_config* cfg) {
+  if (!cfg || cfg->dims < 1 || cfg->dims > 3 || cfg->n_fields < 1 ||
+      cfg->n_fields > CBM_MEDIUM_MAX_FIELDS)
+    return nullptr;
+  int64_t nodes = 1;
+  for (int d = 0; d < cfg->dims; ++d) {
+    if (cfg->n[d] < 4) return nullptr;
+    nodes *= cfg->n[d];
+  }
+  MedHandle* h = new MedHandle;
+  h->prec = cfg->precision;
+  auto init = [&](auto* M) {
+    M->cfg = *cfg;
+    for (int d = cfg->dims; d < 3; ++d) M->cfg.n[d] = 1;
+    M->nodes = nodes;
+    const size_t tot = (size_t)nodes * cfg->n_fields;
+    M->u.assign(tot, 0);
+    M->u_new.assign(tot, 0);
+    M->c_star.assign(tot, 0);
+    M->d_star.assign(tot, 0);
+    M->src.assign((size_t)nodes, 0);
+  };
+  if (h->prec == CBM_F64) {
+    auto* M = new Med<double>;
+    init(M);
+    h->p = M;
+  } else {
+    auto* M = new Med<float>;
+    init(M);
+    h->p = M;
+  }
+  return h;
+}
+
+void oracle_medium_destroy(void* vh) {
+  MedHandle* h = (MedHandle*)vh;
+  if (!h) return;
+  if (h->prec == CBM_F64) delete (Med<double>*)h->p;
+  else delete (Med<float>*)h->p;
+  delete h;
+}
+
+int oracle_medium_upload(void* vh, const void* fields, const void* source) {
+  MedHandle* h = (MedHandle*)vh;
+  auto up = [&](auto* M) {
+    using T = typename std::remove_reference<decltype(M->u[0])>::type;
+    const T* f = (const T*)fields;
+    std::copy(f, f + M->u.size(), M->u.begin());
+    M->u_new = M->u;
+    M->c_star = M->u;
+    M->d_star = M->u;
+    if (source) std::copy((const T*)source, (const T*)source + M->nodes, M->src.begin());
+    else std::fill(M->src.begin(), M->src.end(), (T)0);
+    M->t = 0;
+  };
+  if (h->prec == CBM_F64) up((Med<double>*)h->p);
+  else up((Med<float>*)h->p);
+  return CBM_OK;
+}
+
+int oracle_medium_step(void* vh, int nsteps) {
+  MedHandle* h = (MedHandle*)vh;
+  for (int s = 0; s < nsteps; ++s) {
+    if (h->prec == CBM_F64) medStep(*(Med<double>*)h->p);
+    else medStep(*(Med<float>*)h->p);
+  }
+  return CBM_OK;
+}
+
+int oracle_medium_download(void* vh, void* fields, double* t) {
+  MedHandle* h = (MedHandle*)vh;
+  auto down = [&](auto* M) {
+    using T = typename std::remove_reference<decltype(M->u[0])>::type;
+    std::copy(M->u.begin(), M->u.end(), (T*)fields);
+    if (t) *t = M->t;
+  };
+  if (h->prec == CBM_F64) down((Med<double>*)h->p);
+  else down((Med<float>*)h->p);
+  return CBM_OK;
+}
+
 double oracle_log_f64(double x) { return cbm_log_f64(x); }
 float oracle_log_f32(float x) { return cbm_log_f32(x); }
 void oracle_cossin_f64(double w, double* c, double* s) { cbm_cossin_turns_f64(w, c, s); }

@@ -49,6 +49,11 @@ def load_oracle(abi):
         "oracle_cossin_f64": (None, [dbl, C.POINTER(dbl), C.POINTER(dbl)]),
         "oracle_cossin_f32": (None, [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
         "oracle_philox": (None, [u32, u32, u32, u32, u32, u32, C.POINTER(u32)]),
+        "oracle_medium_create": (vp, [C.POINTER(abi.CbmMediumConfig)]),
+        "oracle_medium_destroy": (None, [vp]),
+        "oracle_medium_upload": (C.c_int, [vp, vp, vp]),
+        "oracle_medium_step": (C.c_int, [vp, C.c_int]),
+        "oracle_medium_download": (C.c_int, [vp, vp, C.POINTER(dbl)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -184,3 +189,36 @@ def oracle_adjoint_dual(abi, cfg, x0, target, nsteps, seeds=()):
     rc = f(C.byref(cfg), len(xs[0]), xp, nsteps, tp, ns, sa, sx, C.byref(loss), g, dx)
     assert rc == 0
     return loss.value, np.array(list(g)), np.array(list(dx)[:ns])
+
+
+class OracleMedium:
+    """The DGADI medium of the checker, with cbm_b200.Medium's methods."""
+
+    def __init__(self, abi, cfg):
+        self.lib = load_oracle(abi)
+        self.h = self.lib.oracle_medium_create(C.byref(cfg))
+        if not self.h:
+            raise ValueError("invalid medium configuration")
+        self.dtype = np.float64 if cfg.precision == abi.F64 else np.float32
+        self.shape = (cfg.n_fields,) + tuple(int(cfg.n[d]) for d in reversed(range(cfg.dims)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.oracle_medium_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def upload(self, fields, source=None):
+        f = np.ascontiguousarray(fields, dtype=self.dtype).reshape(self.shape)
+        s = None if source is None else np.ascontiguousarray(source, dtype=self.dtype)
+        self.lib.oracle_medium_upload(self.h, f.ctypes.data, None if s is None else s.ctypes.data)
+
+    def step(self, n):
+        self.lib.oracle_medium_step(self.h, n)
+
+    def download(self):
+        out = np.zeros(self.shape, self.dtype)
+        t = C.c_double()
+        self.lib.oracle_medium_download(self.h, out.ctypes.data, C.byref(t))
+        return out, t.value
