@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -74,25 +75,60 @@ __global__ void k_dgadi_tables(cbm_medium_config k, int nmax, FieldCoef<T>* coef
   }
 }
 
-// u .+= f(u) at interior nodes: f = s (c_max - u) - decay u
+// u .+= f(u) at interior nodes: f = s (c_max - u) - decay u.  Grid: x in
+// blocks of kMedThreads, (y, z) pairs, fields.
 template <typename T, int D>
 __global__ void k_dgadi_explicit(T* __restrict__ u, const T* __restrict__ src,
                                  const FieldCoef<T>* __restrict__ coef, T cmax, int n0, int n1,
-                                 int n2, int nf) {
-  const long long nodes = (long long)n0 * n1 * n2;
-  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= nodes * nf) return;
-  const int f = (int)(id / nodes);
-  const long long i = id - (long long)f * nodes;
-  const int x = (int)(i % n0);
-  const int y = D > 1 ? (int)((i / n0) % n1) : 0;
-  const int z = D > 2 ? (int)(i / ((long long)n0 * n1)) : 0;
+                                 int n2) {
+  const int x = blockIdx.x * kMedThreads + threadIdx.x;
+  const int yz = blockIdx.y;
+  const int y = D > 1 ? yz % n1 : 0;
+  const int z = D > 2 ? yz / n1 : 0;
+  const int f = blockIdx.z;
   const bool in = x > 0 && x < n0 - 1 && (D < 2 || (y > 0 && y < n1 - 1)) &&
                   (D < 3 || (z > 0 && z < n2 - 1));
   if (!in) return;
+  const long long i = x + (long long)n0 * yz;
+  const long long id = i + (long long)f * n0 * n1 * n2;
   const T ui = u[id];
   const T du = src[i] * (cmax - ui) - coef->decay[f] * ui;
   u[id] = ui + du;
+}
+
+constexpr unsigned kFullMask = 0xffffffffu;
+
+// One line's solve in place: X(j) is node j of the line (ends 0 and n-1).
+// The table entries and nodes of the next iteration are loaded one step
+// ahead, so that only the arithmetic stays on the recurrence's chain.
+template <typename T, typename F>
+__device__ __forceinline__ void line_solve(F&& X, int n, T sub, T main, T sup, const T* cs,
+                                           const double* pv) {
+  T d = (X(1) - sub * X(0)) / main;
+  X(1) = d;
+  double pn = pv[2];
+  T xn = X(2);
+  for (int j = 2; j <= n - 3; ++j) {
+    const double p = pn;
+    const T xj = xn;
+    pn = pv[j + 1];
+    xn = X(j + 1);
+    d = (T)((double)(xj - sub * d) * p);
+    X(j) = d;
+  }
+  T x = (T)((double)((xn - sup * X(n - 1)) - sub * d) * pn);
+  X(n - 2) = x;
+  T cn = n - 3 >= 1 ? cs[n - 3] : (T)0;
+  T dn = n - 3 >= 1 ? X(n - 3) : (T)0;
+  for (int j = n - 3; j >= 1; --j) {
+    const T c = cn, dj = dn;
+    if (j > 1) {
+      cn = cs[j - 1];
+      dn = X(j - 1);
+    }
+    x = dj - c * x;
+    X(j) = x;
+  }
 }
 
 // The Thomas solves of axis A: one thread per (field, line through interior
@@ -124,19 +160,161 @@ __global__ void __launch_bounds__(kSweepThreads)
   const double* pv = piv + (size_t)(f * 3 + A) * nmax;
   const T* X = xo + o;
   T* Y = xn + o;
-  T d = (X[st] - sub * X[0]) / main;
-  Y[st] = d;
-  for (int j = 2; j <= n - 3; ++j) {
-    d = (T)((double)(X[j * st] - sub * d) * pv[j]);
-    Y[j * st] = d;
+  // the ends and the interior to solve are copied to xn's line first (xn's
+  // ends are the uploaded border values, equal to xo's)
+  for (int j = 1; j < n - 1; ++j) Y[j * st] = X[j * st];
+  line_solve<T>([&](int j) -> T& { return Y[j * st]; }, n, sub, main, sup, cs, pv);
+}
+
+// The same solves with the lines of one warp staged in shared memory: 32
+// lines per block, copied in and out with coalesced accesses (rows along x
+// for axis 0; for axes 1 and 2, 32 consecutive lines at each position along
+// them) and solved in place there.  Row r of the tile is line r of the block:
+// at r * rowp + j for axis 0 (rowp odd, so the 32 rows fall in distinct
+// banks), at j * 32 + r otherwise.
+constexpr int kTileLines = 32;
+
+template <typename T, int A, int D>
+__global__ void __launch_bounds__(kTileLines)
+    k_dgadi_sweep_tiled(const T* __restrict__ xo, T* __restrict__ xn,
+                        const FieldCoef<T>* __restrict__ coef, const T* __restrict__ cstar,
+                        const double* __restrict__ piv, int nmax, int n0, int n1, int n2, int nf,
+                        int rowp) {
+  extern __shared__ __align__(16) unsigned char med_smem[];
+  T* tile = reinterpret_cast<T*>(med_smem);
+  const int len[3] = {n0, n1, n2};
+  const long long stride[3] = {1, n0, (long long)n0 * n1};
+  constexpr int B = A == 0 ? 1 : 0;
+  constexpr int Cx = A == 2 ? 1 : 2;
+  const int nb = B < D ? len[B] - 2 : 1, nc = Cx < D ? len[Cx] - 2 : 1;
+  const long long lines = (long long)nb * nc;
+  const int n = len[A];
+  const long long st = stride[A];
+  const int t = threadIdx.x;
+  // global offset of the first node of line (block base + r), or -1 past the end
+  auto line_base = [&](int r, int* field) -> long long {
+    const long long id = (long long)blockIdx.x * kTileLines + r;
+    if (id >= lines * nf) return -1;
+    const int f = (int)(id / lines);
+    const long long l = id - (long long)f * lines;
+    const int ib = (int)(l % nb) + (B < D ? 1 : 0);
+    const int ic = (int)(l / nb) + (Cx < D ? 1 : 0);
+    *field = f;
+    return (long long)f * n0 * n1 * n2 + (long long)ib * stride[B] + (long long)ic * stride[Cx];
+  };
+  int f = 0;
+  const long long o = line_base(t, &f);
+  auto at = [&](int r, int j) -> T& { return A == 0 ? tile[r * rowp + j] : tile[j * kTileLines + r]; };
+  if (A == 0) {
+    for (int r = 0; r < kTileLines; ++r) {
+      const long long orow = __shfl_sync(kFullMask, o, r);
+      if (orow < 0) break;
+      for (int j = t; j < n; j += kTileLines) at(r, j) = xo[orow + j];
+    }
+  } else if (o >= 0) {
+    for (int j = 0; j < n; ++j) at(t, j) = xo[o + j * st];
   }
-  T x = (T)((double)((X[(n - 2) * st] - sup * X[(n - 1) * st]) - sub * d) * pv[n - 2]);
-  Y[(n - 2) * st] = x;
-  for (int j = n - 3; j >= 1; --j) {
-    x = Y[j * st] - cs[j] * x;
-    Y[j * st] = x;
+  __syncwarp();
+  if (o >= 0) {
+    const T sub = coef->sub[f], main = coef->main[f], sup = coef->sup[f];
+    const T* cs = cstar + (size_t)(f * 3 + A) * nmax;
+    const double* pv = piv + (size_t)(f * 3 + A) * nmax;
+    line_solve<T>([&](int j) -> T& { return at(t, j); }, n, sub, main, sup, cs, pv);
+  }
+  __syncwarp();
+  if (A == 0) {
+    for (int r = 0; r < kTileLines; ++r) {
+      const long long orow = __shfl_sync(kFullMask, o, r);
+      if (orow < 0) break;
+      for (int j = 1 + t; j < n - 1; j += kTileLines) xn[orow + j] = at(r, j);
+    }
+  } else if (o >= 0) {
+    for (int j = 1; j < n - 1; ++j) xn[o + j * st] = at(t, j);
   }
 }
+
+// A whole field in one block's shared memory: nsteps complete steps in one
+// launch, one block per field (the fields do not interact).  Each step is the
+// explicit part, then the lines of x, y, z, one thread per line and in place
+// (the lines of one axis are disjoint and each writes only its interior),
+// with a block barrier between phases.  Rows are stored with an odd pitch px
+// so that the threads of the x phase fall in distinct banks; the source field
+// follows the medium field.  The global copy is read once and written back
+// once, in place.
+constexpr int kFusedThreads = 256;
+
+template <typename T, int D>
+__global__ void __launch_bounds__(kFusedThreads)
+    k_dgadi_fused(T* __restrict__ u, const T* __restrict__ src,
+                  const FieldCoef<T>* __restrict__ coef, const T* __restrict__ cstar,
+                  const double* __restrict__ piv, T cmax, int nmax, int n0, int n1, int n2,
+                  int px, int nsteps) {
+  extern __shared__ __align__(16) unsigned char med_smem[];
+  T* sh = reinterpret_cast<T*>(med_smem);
+  const int f = blockIdx.x;
+  const int nodes = n0 * n1 * n2;
+  const int snodes = px * n1 * n2;  // shared layout: x + px (y + n1 z)
+  T* ss = sh + snodes;
+  T* g = u + (size_t)f * nodes;
+  for (int i = threadIdx.x; i < nodes; i += kFusedThreads) {
+    const int x = i % n0, yz = i / n0;
+    sh[x + px * yz] = g[i];
+    ss[x + px * yz] = src[i];
+  }
+  __syncthreads();
+  const T sub = coef->sub[f], main = coef->main[f], sup = coef->sup[f], dec = coef->decay[f];
+  const int len[3] = {n0, n1, n2};
+  const int sst[3] = {1, px, px * n1};
+  for (int step = 0; step < nsteps; ++step) {
+    for (int i = threadIdx.x; i < nodes; i += kFusedThreads) {
+      const int x = i % n0;
+      const int y = D > 1 ? (i / n0) % n1 : 0;
+      const int z = D > 2 ? i / (n0 * n1) : 0;
+      const bool in = x > 0 && x < n0 - 1 && (D < 2 || (y > 0 && y < n1 - 1)) &&
+                      (D < 3 || (z > 0 && z < n2 - 1));
+      if (!in) continue;
+      const int k = x + px * (y + n1 * z);
+      const T ui = sh[k];
+      sh[k] = ui + (ss[k] * (cmax - ui) - dec * ui);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
+      const int nb = b < D ? len[b] - 2 : 1, nc = c < D ? len[c] - 2 : 1;
+      const int n = len[a], st = sst[a];
+      const T* cs = cstar + (size_t)(f * 3 + a) * nmax;
+      const double* pv = piv + (size_t)(f * 3 + a) * nmax;
+      for (int l = threadIdx.x; l < nb * nc; l += kFusedThreads) {
+        const int ib = l % nb + (b < D ? 1 : 0), ic = l / nb + (c < D ? 1 : 0);
+        T* X = sh + ib * sst[b] + ic * sst[c];
+        line_solve<T>([&](int j) -> T& { return X[j * st]; }, n, sub, main, sup, cs, pv);
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = threadIdx.x; i < nodes; i += kFusedThreads) {
+    const int x = i % n0, yz = i / n0;
+    g[i] = sh[x + px * yz];
+  }
+}
+
+// shared memory of the fused kernel (medium and source fields)
+template <typename T>
+size_t fused_bytes(const int* n, int dims) {
+  size_t nodes = (size_t)(n[0] | 1);
+  for (int d = 1; d < dims; ++d) nodes *= (size_t)n[d];
+  return 2 * nodes * sizeof(T);
+}
+constexpr size_t kFusedMaxBytes = 200 * 1024;
+
+// shared memory of one tiled sweep block along an axis of n nodes
+template <typename T>
+size_t tile_bytes(int axis, int n) {
+  const int rowp = axis == 0 ? (n | 1) : n;
+  return (size_t)kTileLines * rowp * sizeof(T);
+}
+constexpr size_t kTileMaxBytes = 96 * 1024;
 
 }  // namespace
 
@@ -153,6 +331,7 @@ struct cbm_medium {
   void* cstar = nullptr;
   double* piv = nullptr;
   int cur = 0;
+  bool fused = false;  // the whole field fits one block's shared memory
   long long steps = 0;
   double t = 0;
   bool loaded = false;
@@ -193,9 +372,11 @@ int enqueue_step(cbm_medium* m) {
   T* u[2] = {(T*)m->u[0], (T*)m->u[1]};
   const auto* coef = (const FieldCoef<T>*)m->coef;
   const long long tot = m->nodes * nf;
-  k_dgadi_explicit<T, D><<<(unsigned)((tot + kMedThreads - 1) / kMedThreads), kMedThreads, 0,
-                           m->stream>>>(u[m->cur], (const T*)m->src, coef, (T)k.c_max, n0, n1,
-                                        n2, nf);
+  (void)tot;
+  k_dgadi_explicit<T, D><<<dim3((unsigned)((n0 + kMedThreads - 1) / kMedThreads), (unsigned)(n1 * n2),
+                                (unsigned)nf),
+                           kMedThreads, 0, m->stream>>>(u[m->cur], (const T*)m->src, coef,
+                                                        (T)k.c_max, n0, n1, n2);
   auto lines = [&](int a) {
     const int len[3] = {n0, n1, n2};
     long long l = 1;
@@ -205,21 +386,70 @@ int enqueue_step(cbm_medium* m) {
   };
   auto grid = [&](long long n) { return (unsigned)((n + kSweepThreads - 1) / kSweepThreads); };
   const T* cs = (const T*)m->cstar;
-  k_dgadi_sweep<T, 0, D><<<grid(lines(0)), kSweepThreads, 0, m->stream>>>(
-      u[m->cur], u[m->cur ^ 1], coef, cs, m->piv, m->nmax, n0, n1, n2, nf);
-  m->cur ^= 1;
-  if (D > 1) {
-    k_dgadi_sweep<T, 1, D><<<grid(lines(1)), kSweepThreads, 0, m->stream>>>(
-        u[m->cur], u[m->cur ^ 1], coef, cs, m->piv, m->nmax, n0, n1, n2, nf);
+  const int len[3] = {n0, n1, n2};
+  auto sweep = [&](auto axis) {
+    constexpr int A = decltype(axis)::value;
+    const size_t tb = tile_bytes<T>(A, len[A]);
+    if (tb <= kTileMaxBytes) {
+      const long long nl = lines(A);
+      k_dgadi_sweep_tiled<T, A, D>
+          <<<(unsigned)((nl + kTileLines - 1) / kTileLines), kTileLines, tb, m->stream>>>(
+              u[m->cur], u[m->cur ^ 1], coef, cs, m->piv, m->nmax, n0, n1, n2, nf,
+              A == 0 ? (len[A] | 1) : len[A]);
+    } else {
+      k_dgadi_sweep<T, A, D><<<grid(lines(A)), kSweepThreads, 0, m->stream>>>(
+          u[m->cur], u[m->cur ^ 1], coef, cs, m->piv, m->nmax, n0, n1, n2, nf);
+    }
     m->cur ^= 1;
-  }
-  if (D > 2) {
-    k_dgadi_sweep<T, 2, D><<<grid(lines(2)), kSweepThreads, 0, m->stream>>>(
-        u[m->cur], u[m->cur ^ 1], coef, cs, m->piv, m->nmax, n0, n1, n2, nf);
-    m->cur ^= 1;
-  }
+  };
+  sweep(std::integral_constant<int, 0>());
+  if constexpr (D > 1) sweep(std::integral_constant<int, 1>());
+  if constexpr (D > 2) sweep(std::integral_constant<int, 2>());
   MED_TRY(m, cudaGetLastError());
   return CBM_OK;
+}
+
+template <typename T, int D>
+int enqueue_fused(cbm_medium* m, int nsteps) {
+  const cbm_medium_config& k = m->cfg;
+  const int n0 = k.n[0], n1 = D > 1 ? k.n[1] : 1, n2 = D > 2 ? k.n[2] : 1;
+  const size_t bytes = fused_bytes<T>(k.n, D);
+  k_dgadi_fused<T, D><<<k.n_fields, kFusedThreads, bytes, m->stream>>>(
+      (T*)m->u[m->cur], (const T*)m->src, (const FieldCoef<T>*)m->coef, (const T*)m->cstar,
+      m->piv, (T)k.c_max, m->nmax, n0, n1, n2, n0 | 1, nsteps);
+  MED_TRY(m, cudaGetLastError());
+  return CBM_OK;
+}
+template <typename T>
+int enqueue_fused_t(cbm_medium* m, int nsteps) {
+  switch (m->cfg.dims) {
+    case 1: return enqueue_fused<T, 1>(m, nsteps);
+    case 2: return enqueue_fused<T, 2>(m, nsteps);
+    default: return enqueue_fused<T, 3>(m, nsteps);
+  }
+}
+
+template <typename T, int D>
+bool set_tile_attrs_d(int bytes) {
+  bool ok = cudaFuncSetAttribute(k_dgadi_sweep_tiled<T, 0, D>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+  if (D > 1)
+    ok = ok && cudaFuncSetAttribute(k_dgadi_sweep_tiled<T, 1, D>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+  if (D > 2)
+    ok = ok && cudaFuncSetAttribute(k_dgadi_sweep_tiled<T, 2, D>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+  ok = ok && cudaFuncSetAttribute(k_dgadi_fused<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kFusedMaxBytes) == cudaSuccess;
+  return ok;
+}
+template <typename T>
+bool set_tile_attrs(int dims, int bytes) {
+  switch (dims) {
+    case 1: return set_tile_attrs_d<T, 1>(bytes);
+    case 2: return set_tile_attrs_d<T, 2>(bytes);
+    default: return set_tile_attrs_d<T, 3>(bytes);
+  }
 }
 
 template <typename T>
@@ -276,6 +506,18 @@ int cbm_medium_create(cbm_medium** out, const cbm_medium_config* cfg) {
     delete m;
     return mfail(nullptr, CBM_ERR_NOMEM, "device allocation failed for the DGADI medium");
   }
+  {
+    // tiled sweeps may use up to kTileMaxBytes of dynamic shared memory
+    const int big = (int)kTileMaxBytes;
+    bool attr = true;
+    if (m->tsize == 8) attr = set_tile_attrs<double>(k.dims, big);
+    else attr = set_tile_attrs<float>(k.dims, big);
+    if (!attr) {
+      mfree(m);
+      delete m;
+      return mfail(nullptr, CBM_ERR_CUDA, "cudaFuncSetAttribute failed for the DGADI sweeps");
+    }
+  }
   const unsigned tb = (unsigned)((k.n_fields * 3 + 63) / 64);
   if (m->tsize == 8)
     k_dgadi_tables<double><<<tb, 64, 0, m->stream>>>(m->cfg, nmax, (FieldCoef<double>*)m->coef,
@@ -288,6 +530,8 @@ int cbm_medium_create(cbm_medium** out, const cbm_medium_config* cfg) {
     delete m;
     return mfail(nullptr, CBM_ERR_CUDA, "DGADI table set-up failed");
   }
+  m->fused = (m->tsize == 8 ? fused_bytes<double>(m->cfg.n, k.dims)
+                            : fused_bytes<float>(m->cfg.n, k.dims)) <= kFusedMaxBytes;
   *out = m;
   return CBM_OK;
 }
@@ -324,11 +568,20 @@ int cbm_medium_step(cbm_medium* m, int32_t nsteps, int32_t flags) {
   if (!m) return mfail(m, CBM_ERR_ARG, "null medium");
   if (!m->loaded) return mfail(m, CBM_ERR_STATE, "cbm_medium_step before cbm_medium_upload");
   if (nsteps < 0) return mfail(m, CBM_ERR_ARG, "nsteps must be >= 0");
-  for (int s = 0; s < nsteps; ++s) {
-    const int rc = m->tsize == 8 ? enqueue_step_t<double>(m) : enqueue_step_t<float>(m);
+  if (m->fused && nsteps > 0) {
+    const int rc = m->tsize == 8 ? enqueue_fused_t<double>(m, nsteps) : enqueue_fused_t<float>(m, nsteps);
     if (rc != CBM_OK) return rc;
-    m->steps += 1;
-    m->t += m->cfg.dt;  // obj.t += dt
+    for (int s = 0; s < nsteps; ++s) {
+      m->steps += 1;
+      m->t += m->cfg.dt;  // obj.t += dt
+    }
+  } else {
+    for (int s = 0; s < nsteps; ++s) {
+      const int rc = m->tsize == 8 ? enqueue_step_t<double>(m) : enqueue_step_t<float>(m);
+      if (rc != CBM_OK) return rc;
+      m->steps += 1;
+      m->t += m->cfg.dt;  // obj.t += dt
+    }
   }
   if (flags & CBM_SYNC) MED_TRY(m, cudaStreamSynchronize(m->stream));
   return CBM_OK;

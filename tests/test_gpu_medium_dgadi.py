@@ -1,7 +1,9 @@
 """The device DGADI medium (cbm_medium_*) against the checker, bit for bit:
 1D/2D/3D, Float32 and Float64, several fields with their own diffusion and
 decay, a source field, unequal axes (the last axis's spacing sets r for every
-axis), and the two workloads of examples/Implementation.ipynb."""
+axis), and the two workloads of examples/Implementation.ipynb.  Small media
+run as one launch per call (a field per block, in shared memory); larger ones
+take one launch per axis, staged or from global memory."""
 import numpy as np
 import pytest
 
@@ -42,6 +44,24 @@ def test_dgadi_bitexact(gpu_lib, abi, dims, n, prec):
         assert a.dtype == b.dtype
         np.testing.assert_array_equal(a, b)
         assert ta == tb
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("dims,n", [(1, (30000, 1, 1)), (2, (900, 40, 1)), (3, (40, 30, 25))])
+def test_dgadi_large_media_bitexact(gpu_lib, abi, dims, n, prec):
+    """Media too large for one block's shared memory take one launch per axis:
+    lines too long for a 96 KB tile of 32 lines (1D, and x in 2D) are solved
+    from global memory, the others through shared-memory tiles."""
+    from conftest import cbm
+    rng = np.random.default_rng(60 + dims)
+    nodes = int(np.prod(n[:dims]))
+    cfg = abi.make_medium_config(dims, n, (0.0,) * 3, (3.0, 0.5, 1.0), 0.002, [0.8, 0.1],
+                                 [0.05, 0.0], c_max=1.0,
+                                 precision=abi.F32 if prec == "f32" else abi.F64)
+    u0 = rng.uniform(size=(2, nodes))
+    src = (rng.uniform(size=nodes) < 0.1).astype(float)
+    for a, b, ta, tb in _run_both(abi, cbm, cfg, u0, src, [3, 5]):
+        np.testing.assert_array_equal(a, b)
 
 
 @pytest.mark.parametrize("dims,n,steps", [(2, (101, 101, 1), 50), (3, (101, 101, 101), 4)])
