@@ -695,6 +695,50 @@ def run_configs(args):
                                    "value": round(n0 * args.config_f64_steps / (ms / 1e3), 1),
                                    "unit": UNIT}
 
+    # Implicit medium (DGADI): the two workloads of examples/Implementation.ipynb,
+    # co2 and co3 (D = 1 and 2) on [0,1]^d, dt 0.01, a source of strength 1 at
+    # the central node, Float32 as the reference's GPU platform runs them.
+    # The notebook's @time (2.45 s for 500 2D steps, 45.67 % of it compilation;
+    # 10.64 s for 200 3D steps; GPU model not stated) is wall time around the
+    # loop; wall_ms here is the same loop through the C ABI, synchronised.
+    from _oracle import OracleMedium
+    for name, dims, nn, steps, cpu_steps, published in (
+            ("medium_dgadi_2d_101", 2, (101, 101, 1), 500, 50, 2.45),
+            ("medium_dgadi_3d_101", 3, (101, 101, 101), 200, 2, 10.64)):
+        mcfg = abi.make_medium_config(dims, nn, (0.0,) * 3, (1.0,) * 3, 0.01, [1.0, 2.0],
+                                      c_max=1.0, precision=abi.F32)
+        nodes = int(np.prod(nn[:dims]))
+        src = np.zeros(tuple(reversed(nn[:dims])), np.float32)
+        src[tuple(round(k / 2) - 1 for k in reversed(nn[:dims]))] = 1.0
+        u0 = np.zeros((2, nodes), np.float32)
+        med = abi.Medium(mcfg)
+        med.upload(u0, src.reshape(-1))
+        med.step(10)
+        mst = torch.cuda.ExternalStream(med.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        e0.record(mst)
+        med.step(steps, 0)
+        e1.record(mst)
+        e1.synchronize()
+        wall = time.perf_counter() - w0
+        dev_ms = e0.elapsed_time(e1)
+        med.close()
+        o = OracleMedium(abi, mcfg)
+        o.upload(u0, src.reshape(-1))
+        c0 = time.perf_counter()
+        o.step(cpu_steps)
+        cpu_ms = 1e3 * (time.perf_counter() - c0) / cpu_steps
+        o.close()
+        out[name] = {"workload": f"examples/Implementation.ipynb {dims}D: 2 fields on "
+                                 f"{'x'.join(str(k) for k in nn[:dims])} nodes, {steps} DGADI steps",
+                     "dtype": "f32", "steps": steps, "device_ms": round(dev_ms, 3),
+                     "wall_ms": round(wall * 1e3, 3), "us_per_step": round(1e3 * dev_ms / steps, 2),
+                     "node_updates_per_s": round(2 * nodes * steps / (dev_ms / 1e3), 1),
+                     "reference_published_s": published,
+                     "cpu_oracle_ms_per_step": round(cpu_ms, 3), "cpu_oracle_threads": 1}
+
     # Error of the Float32 results against Float64 runs, 100 steps.  The noise
     # of an SDE run is drawn in the run's precision (Box-Muller in float or
     # double), so the two precisions follow different sample paths; the
