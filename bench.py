@@ -711,7 +711,7 @@ def run_configs(args):
         src = np.zeros(tuple(reversed(nn[:dims])), np.float32)
         src[tuple(round(k / 2) - 1 for k in reversed(nn[:dims]))] = 1.0
         u0 = np.zeros((2, nodes), np.float32)
-        med = abi.Medium(mcfg)
+        med = abi.DGADIMedium(mcfg)
         med.upload(u0, src.reshape(-1))
         med.step(10)
         mst = torch.cuda.ExternalStream(med.stream())

@@ -24,16 +24,17 @@ from types import SimpleNamespace
 
 import numpy as np
 
-from . import _abi, sweep  # noqa: F401
-from ._abi import (Adjoint, Batch, CbmConfig, CbmError, Context, load_library,  # noqa: F401
-                   make_config)
+from . import _abi, fitting, sweep  # noqa: F401
+from ._abi import (Adjoint, Batch, CbmConfig, CbmError, Context, DGADIMedium,  # noqa: F401
+                   load_library, make_config, make_medium_config)
 from .sweep import ShardedBatch, partition_communities  # noqa: F401
 
 __all__ = ["ABM", "Community", "evolve", "step", "loadToPlatform", "bringFromPlatform",
            "agentStepRule", "agentStepDE", "mediumStepRule", "mediumStepDE", "update",
            "computeNeighbors", "CBMNeighbors", "CBMIntegrators", "SoftSpheres", "Growth",
            "Medium", "B200", "Context", "Batch", "Adjoint", "ShardedBatch",
-           "partition_communities", "CbmError", "make_config", "load_library"]
+           "partition_communities", "CbmError", "make_config", "load_library",
+           "DGADIMedium", "make_medium_config", "fitting"]
 
 
 # ---- algorithm descriptors (src/neighbors.jl, src/integrators.jl) -------------

@@ -486,7 +486,7 @@ def _bind_medium(lib):
     lib._medium_bound = True
 
 
-class Medium:
+class DGADIMedium:
     """A medium advanced by the implicit Douglas–Gunn ADI step (DGADI).
     Fields are arrays of shape (n_fields, [n2, [n1,]] n0), x fastest."""
 

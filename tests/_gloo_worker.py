@@ -81,3 +81,34 @@ def run(rank, world, port, out_dir):
     finally:
         dist.barrier()
         dist.destroy_process_group()
+
+
+FIT_SEARCH = {"k_rep": [5.0, 10.0, 20.0], "sigma": [0.0, 0.1]}
+FIT_DEFAULTS = dict(r_rep=2.0, k_att=1.0, r_att=3.0)
+
+
+def fit_state(i, point):
+    rng = np.random.default_rng(100 + i)
+    n = 10 + 3 * i
+    return dict(x=rng.uniform(0, 1, n), y=rng.uniform(0, 1, n), z=rng.uniform(0, 1, n))
+
+
+def fit_loss(point, st):
+    return float(np.mean(st["x"])) + point["sigma"]
+
+
+def run_fit(rank, world, port, out_dir):
+    """batched_grid_search sharded over two gloo ranks with the host batch."""
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        cbm = load_package()
+        rows = cbm.fitting.batched_grid_search(
+            None, FIT_SEARCH, fit_state, fit_loss, 5, (0.0,) * 3, (1.0,) * 3, FIT_DEFAULTS,
+            return_all=True, rank=rank, world=world, dist=dist, factory=FakeBatch)
+        np.save(os.path.join(out_dir, f"fit{rank}.npy"),
+                np.array([[r["k_rep"], r["sigma"], r["_score_"]] for r in rows]))
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()

@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _run_both(abi, cbm, cfg, u0, src, steps):
-    g = cbm._abi.Medium(cfg)
+    g = cbm._abi.DGADIMedium(cfg)
     o = OracleMedium(abi, cfg)
     g.upload(u0, src)
     o.upload(u0, src)
@@ -84,8 +84,8 @@ def test_dgadi_implementation_notebook_workload(gpu_lib, abi, dims, n, steps):
 def test_dgadi_errors(gpu_lib, abi):
     from conftest import cbm
     with pytest.raises(cbm._abi.CbmError):
-        cbm._abi.Medium(abi.make_medium_config(2, (3, 8, 1), (0.0,) * 3, (1.0,) * 3, 0.01, [1.0]))
-    m = cbm._abi.Medium(abi.make_medium_config(1, (8, 1, 1), (0.0,) * 3, (1.0,) * 3, 0.01, [1.0]))
+        cbm._abi.DGADIMedium(abi.make_medium_config(2, (3, 8, 1), (0.0,) * 3, (1.0,) * 3, 0.01, [1.0]))
+    m = cbm._abi.DGADIMedium(abi.make_medium_config(1, (8, 1, 1), (0.0,) * 3, (1.0,) * 3, 0.01, [1.0]))
     with pytest.raises(cbm._abi.CbmError):
         m.step(1)
     m.close()
