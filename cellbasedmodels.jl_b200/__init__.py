@@ -55,6 +55,9 @@ class _Neighbors:
 class _Integrators:
     Euler = staticmethod(lambda: dict(integrator=_abi.INT_EULER))
     EM = staticmethod(lambda: dict(integrator=_abi.INT_EM))
+    # ODE integrators with 2 and 4 evaluations of f per step (integrators.jl:516-668)
+    Heun = staticmethod(lambda: dict(integrator=_abi.INT_HEUN))
+    RungeKutta4 = staticmethod(lambda: dict(integrator=_abi.INT_RK4))
 
 
 CBMNeighbors = _Neighbors()

@@ -73,6 +73,7 @@ struct cbm_ctx {
   int n_sm = 148;             // multiprocessors of the device (grid of the compaction)
   int de_blocks = 1;          // persistent grid of the force kernel
   void* pair_list = nullptr;  // its partner lists (cell walks only)
+  void* stage[3] = {nullptr, nullptr, nullptr};  // Heun / RK4: h, running sum, derivative
   int n_cells = 1;
   int n_cells_d[3] = {1, 1, 1};
   int n_scan_tiles = 1;
@@ -185,6 +186,9 @@ Params<T> params(const cbm_ctx* c, int parity) {
   P.IA = c->IA;
   P.IB = c->IB;
   P.U = (V4*)c->U;
+  P.stage_h = (V4*)c->stage[0];
+  P.stage_s = (V4*)c->stage[1];
+  P.stage_k = (V4*)c->stage[2];
   P.POLD = (V4*)c->POLD;
   P.inv = c->inv;
   P.cell_of_slot = c->cell_of_slot;
@@ -318,8 +322,38 @@ void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P) {
 
 template <typename T, int D>
 void enqueue_agent_de(cbm_ctx* c, const Params<T>& P) {
-  PROF("k_agent_de");
-  k_agent_de<T, D><<<kPartnerLists<D> ? c->de_blocks : c->n_blocks, kTile, 0, c->stream>>>(P);
+  const unsigned grid = kPartnerLists<D> ? c->de_blocks : c->n_blocks;
+  const int integ = c->cfg.integrator;
+  if (integ != CBM_INT_HEUN && integ != CBM_INT_RK4) {
+    PROF("k_agent_de");
+    k_agent_de<T, D><<<grid, kTile, 0, c->stream>>>(P);
+    return;
+  }
+  // multi-stage: f at u, then at each stage's positions (own cell from the
+  // position, no face pruning), each followed by its combination
+  auto stage = [&](bool at_h, int op) {
+    Params<T> Q = P;
+    Q.KOUT = Q.stage_k;
+    if (at_h) {
+      Q.XS = Q.stage_h;
+      Q.no_prune = 1;
+    }
+    {
+      PROF("k_agent_de");
+      k_agent_de<T, D><<<grid, kTile, 0, c->stream>>>(Q);
+    }
+    PROF("k_stage_combine");
+    k_stage_combine<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P, op);
+  };
+  if (integ == CBM_INT_HEUN) {
+    stage(false, kHeunStage);
+    stage(true, kHeunFinal);
+  } else {
+    stage(false, kRk1);
+    stage(true, kRk2);
+    stage(true, kRk3);
+    stage(true, kRkFinal);
+  }
 }
 
 template <typename T, int D>
@@ -598,8 +632,18 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
   if (!(k.dt > 0)) return fail(nullptr, CBM_ERR_ARG, "dt must be positive");
   if (k.neighbors < CBM_NEIGH_NONE || k.neighbors > CBM_NEIGH_CLVD)
     return fail(nullptr, CBM_ERR_ARG, "unknown neighbor algorithm %d", k.neighbors);
-  if (k.integrator != CBM_INT_EULER && k.integrator != CBM_INT_EM)
+  if (k.integrator < CBM_INT_EULER || k.integrator > CBM_INT_RK4)
     return fail(nullptr, CBM_ERR_ARG, "unknown integrator %d", k.integrator);
+  if (k.integrator == CBM_INT_HEUN || k.integrator == CBM_INT_RK4) {
+    if (k.sigma != 0)
+      return fail(nullptr, CBM_ERR_ARG, "Heun and RungeKutta4 integrate ODEs: sigma must be 0");
+    if (k.force_mode == CBM_FORCE_LAGGED)
+      return fail(nullptr, CBM_ERR_ARG, "Heun and RungeKutta4 need force_mode = CBM_FORCE_DIRECT");
+    if (k.neighbors != CBM_NEIGH_NONE && k.neighbors != CBM_NEIGH_FULL &&
+        k.neighbors != CBM_NEIGH_CELL_LINKED)
+      return fail(nullptr, CBM_ERR_ARG,
+                  "Heun and RungeKutta4 need neighbors NONE, FULL or CELL_LINKED");
+  }
   for (int d = 0; d < k.dims; ++d)
     if (!(k.box_hi[d] > k.box_lo[d])) return fail(nullptr, CBM_ERR_ARG, "empty simBox on axis %d", d);
   const bool cells = k.neighbors == CBM_NEIGH_CELL_LINKED || k.neighbors == CBM_NEIGH_CLVD;
@@ -679,6 +723,8 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
   c->IA = (int*)dalloc(c, n * 4, &ok);
   c->IB = (int*)dalloc(c, n * 4, &ok);
   if (k.walls == CBM_WALLS_REFLECT) c->U = dalloc(c, n * S4, &ok);
+  if (k.integrator == CBM_INT_HEUN || k.integrator == CBM_INT_RK4)
+    for (int q = 0; q < 3; ++q) c->stage[q] = dalloc(c, n * S4, &ok);
   if (list) c->POLD = dalloc(c, n * S4, &ok);
   c->inv = (int*)dalloc(c, n * 4, &ok);
   c->cell_of_slot = (int*)dalloc(c, n * 4, &ok);

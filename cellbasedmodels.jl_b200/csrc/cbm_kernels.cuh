@@ -52,6 +52,17 @@ struct Params {
   int* IA;              // slot -> agent index
   int* IB;              // working labels (relabelled by the compaction, -1 = dead)
   V4* U;                // positions after the rule's wall reflection (walls only)
+  // multi-stage integrators (Heun, RungeKutta4): stage positions, running sum
+  // and derivative of every slot, and per launch of k_agent_de the stage
+  // positions to read (XS) and where to store the derivative instead of
+  // integrating (KOUT); no_prune turns the cell walk's face pruning off
+  // (stage positions may lie outside the cells of the grid)
+  V4* stage_h;
+  V4* stage_s;
+  V4* stage_k;
+  const V4* XS;
+  V4* KOUT;
+  int no_prune;
   V4* POLD;             // positions at the last Verlet rebuild (slot order)
   int* inv;             // agent index -> slot of A
   int* cell_of_slot;    // cell of each A slot
@@ -317,7 +328,7 @@ __device__ __forceinline__ void walk_runs(const Params<T>& P, const T* x, T reac
     const int n = P.n_cells_d[d];
     const int c = cell >= 0 ? q[d] : cell_pos1<T>(P.edge, x[d], P.box_lo[d], P.box_hi[d], n);
     q[d] = c;
-    if (c >= 2 && c <= n - 3) {
+    if (c >= 2 && c <= n - 3 && !P.no_prune) {
       const T rel = x[d] - P.box_lo[d];
       const T k = (T)(c - 1);
       const T margin = (T)16 * Eps<T>::v * (fabs(rel) + (k + (T)1) * P.edge) + (T)1e-4 * reach;
@@ -886,7 +897,9 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
   const int p = P.parity;
   if (s >= N) return;
   const bool reflect = P.walls == CBM_WALLS_REFLECT;
-  const V4* U = reflect ? P.U : P.PA;
+  // positions read by this launch: a stage's, the rule's reflected ones, or
+  // the committed ones
+  const V4* U = P.XS ? P.XS : (reflect ? P.U : P.PA);
   T xi[3];
   to3<T>(U[s], xi);
   T acc[3] = {(T)0, (T)0, (T)0};
@@ -1042,7 +1055,7 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
       };
       // the slot's cell is the grid's assignment of the committed position,
       // which the walk starts from unless the rule reflected it off a wall
-      const int own_cell = reflect ? -1 : ld(P.cell_of_slot + s);
+      const int own_cell = (reflect || P.XS) ? -1 : ld(P.cell_of_slot + s);
       walk_runs<T, D>(P, xi, P.cut_reach, [&](int s0, int s1) {
         int q = s0;
         for (; q + 4 <= s1; q += 4) {
@@ -1200,6 +1213,10 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
 #pragma unroll
     for (int d = 0; d < D; ++d) dv[d] = dv[d] + (P.chemotaxis * gv[d]) / den;
   }
+  if (P.KOUT) {  // a stage of a multi-stage integrator: f(u) only
+    P.KOUT[s] = from3<T>(dv);
+    return;
+  }
   const int i = ld(P.IA + s);  // agent index of the slot
   T xn[3] = {(T)0, (T)0, (T)0};
   if (P.integrator == CBM_INT_EM) {
@@ -1265,6 +1282,75 @@ __global__ void __launch_bounds__(kTile, sizeof(T) == 4 ? 4 : 3) k_agent_de(Para
       C->de_done = 0u;
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// Stage combinations of the multi-stage agent integrators over the slots of
+// existing agents, with the reference's broadcast expressions element by
+// element (src/integrators.jl: Heun :541-571, RungeKutta4 :606-666):
+//   Heun  h1 = u + du dt;  u = (h1 + (u + du2 dt)) / 2
+//   RK4   h1 = u + (k1 dt)/2, u + (k2 dt)/2, u + k3 dt;
+//         u = u + ((((k1 + 2 k2) + 2 k3) + k4) dt) / 6
+// The volume v is a DE variable with dv = g when growth is on; its stage
+// values do not enter f, so only its final combination is formed.
+// ---------------------------------------------------------------------------
+enum { kHeunStage = 0, kHeunFinal = 1, kRk1 = 2, kRk2 = 3, kRk3 = 4, kRkFinal = 5 };
+
+template <typename T, int D>
+__global__ void __launch_bounds__(kTile) k_stage_combine(Params<T> P, int op) {
+  const int N = (int)P.ctr->N[P.parity];
+  const int s = blockIdx.x * kTile + threadIdx.x;
+  if (s >= N) return;
+  const bool reflect = P.walls == CBM_WALLS_REFLECT;
+  T u[3], k[3];
+  to3<T>((reflect ? P.U : P.PA)[s], u);
+  to3<T>(P.stage_k[s], k);
+  const T dt = P.dt;
+  T o[3] = {(T)0, (T)0, (T)0};
+  if (op == kHeunStage || op == kRk3) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) o[d] = u[d] + k[d] * dt;
+  } else if (op == kRk1 || op == kRk2) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) o[d] = u[d] + (k[d] * dt) / (T)2;
+  }
+  if (op == kRk1) {
+    P.stage_s[s] = P.stage_k[s];
+  } else if (op == kRk2 || op == kRk3 || op == kRkFinal) {
+    T a[3];
+    to3<T>(P.stage_s[s], a);
+#pragma unroll
+    for (int d = 0; d < D; ++d) a[d] = op == kRkFinal ? a[d] + k[d] : a[d] + (T)2 * k[d];
+    P.stage_s[s] = from3<T>(a);
+    if (op == kRkFinal) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) o[d] = u[d] + (a[d] * dt) / (T)6;
+    }
+  }
+  if (op != kHeunFinal && op != kRkFinal) {
+    P.stage_h[s] = from3<T>(o);
+    return;
+  }
+  const int i = ld(P.IA + s);
+  const T v = P.VA[s];
+  T vn = v;
+  if (op == kHeunFinal) {
+    T h[3];
+    to3<T>(P.stage_h[s], h);
+#pragma unroll
+    for (int d = 0; d < D; ++d) o[d] = (h[d] + (u[d] + k[d] * dt)) / (T)2;
+    if (P.growth) {
+      const T g = ld(P.G + i);
+      const T hv = v + g * dt;
+      vn = (hv + (v + g * dt)) / (T)2;
+    }
+  } else if (P.growth) {
+    const T g = ld(P.G + i);
+    vn = v + ((((g + (T)2 * g) + (T)2 * g) + g) * dt) / (T)6;
+  }
+  P.PB[s] = from3<T>(o);
+  P.VB[s] = vn;
+  P.IB[s] = i;
 }
 
 // ---------------------------------------------------------------------------

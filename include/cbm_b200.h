@@ -55,8 +55,11 @@ enum {
   CBM_NEIGH_CLVD = 4        /* list built over the cell grid, cell order (:997-1275) */
 };
 
-/* src/integrators.jl: Euler :465-505, EM :683-734 */
-enum { CBM_INT_EULER = 0, CBM_INT_EM = 1 };
+/* src/integrators.jl: Euler :465-505, EM :683-734, Heun :516-573,
+ * RungeKutta4 :583-668.  Heun and RungeKutta4 integrate ODEs (sigma = 0) and
+ * evaluate f at every stage over the neighbor structure of the last rebuild;
+ * they need neighbors NONE, FULL or CELL_LINKED and force_mode = CBM_FORCE_DIRECT. */
+enum { CBM_INT_EULER = 0, CBM_INT_EM = 1, CBM_INT_HEUN = 2, CBM_INT_RK4 = 3 };
 
 /* How the pair force enters dt(x).
  *  DIRECT: dt(x) += F(d)/d * (x - x[j]) inside @loopOverNeighbors.

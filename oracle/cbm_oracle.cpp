@@ -476,25 +476,27 @@ void sampleGrad(const Com<T>& C, const T* p, T* gv) {
   }
 }
 
+// f(du, u, p, t) of agentStepDE! for agents 0..N-1, with the positions of u
+// in X (the DE state, or a stage of a multi-stage integrator): the neighbor
+// loop's own cell is computed from X, its occupants are the last rebuild's.
 template <typename T>
-void agentStepDE(Com<T>& C) {
+void evalF(Com<T>& C, const std::vector<T>* X, std::vector<T>* out) {
   const cbm_config& k = C.cfg;
   const int D = C.dims;
   const int64_t N = C.N;
-  const T dt = (T)k.dt, krep = (T)k.k_rep, rrep = (T)k.r_rep, katt = (T)k.k_att,
-          ratt = (T)k.r_att;
+  const T krep = (T)k.k_rep, rrep = (T)k.r_rep, katt = (T)k.k_att, ratt = (T)k.r_att;
   const bool lagged = k.force_mode == CBM_FORCE_LAGGED;
 #pragma omp parallel for schedule(static) num_threads(g_threads)
   for (int64_t i = 0; i < N; ++i) {
     T acc[3] = {0, 0, 0};  // cleanArray: du = 0 (integrators.jl:442-450)
     T pi[3];
-    for (int d = 0; d < D; ++d) pi[d] = C.x_[d][i];
+    for (int d = 0; d < D; ++d) pi[d] = X[d][i];
     if (k.neighbors != CBM_NEIGH_NONE) {
-      forNeighbors(C, C.x_, i, N, [&](int64_t j) {
+      forNeighbors(C, X, i, N, [&](int64_t j) {
         T e[3];
         T s2 = 0;
         for (int d = 0; d < D; ++d) {
-          e[d] = pi[d] - C.x_[d][j];
+          e[d] = pi[d] - X[d][j];
           s2 = (d == 0) ? e[d] * e[d] : s2 + e[d] * e[d];
         }
         T dist = std::sqrt(s2);
@@ -529,8 +531,76 @@ void agentStepDE(Com<T>& C) {
       T den = (T)1 + std::sqrt(s);
       for (int d = 0; d < D; ++d) dv[d] = dv[d] + ((T)k.chemotaxis * gv[d]) / den;
     }
-    for (int d = 0; d < D; ++d) C.du[d][i] = dv[d];
+    for (int d = 0; d < D; ++d) out[d][i] = dv[d];
   }
+}
+
+// Heun (src/integrators.jl:541-571) and RungeKutta4 (:606-666) over 1:N,
+// each broadcast element by element.  The volume is a DE variable with
+// dt(v) = g when growth is on; f does not read it.
+template <typename T>
+void multiStage(Com<T>& C) {
+  const cbm_config& k = C.cfg;
+  const int D = C.dims;
+  const int64_t N = C.N;
+  const T dt = (T)k.dt;
+  std::vector<T> h[3], kk[3], acc[3];
+  for (int d = 0; d < 3; ++d) {
+    h[d].assign(C.x_[d].size(), 0);
+    kk[d].assign(C.x_[d].size(), 0);
+    acc[d].assign(C.x_[d].size(), 0);
+  }
+  if (k.integrator == CBM_INT_HEUN) {
+    evalF(C, C.x_, kk);
+    for (int64_t i = 0; i < N; ++i)
+      for (int d = 0; d < D; ++d) h[d][i] = C.x_[d][i] + kk[d][i] * dt;
+    evalF(C, h, kk);
+    for (int64_t i = 0; i < N; ++i) {
+      for (int d = 0; d < D; ++d) C.x_[d][i] = (h[d][i] + (C.x_[d][i] + kk[d][i] * dt)) / (T)2;
+      if (k.growth) {
+        const T v = C.v_[i], g = C.g[i];
+        const T hv = v + g * dt;
+        C.v_[i] = (hv + (v + g * dt)) / (T)2;
+      }
+    }
+    return;
+  }
+  // k1: h = u + (k1 dt)/2; k2: h = u + (k2 dt)/2; k3: h = u + k3 dt; k4
+  evalF(C, C.x_, kk);
+  for (int64_t i = 0; i < N; ++i)
+    for (int d = 0; d < D; ++d) {
+      acc[d][i] = kk[d][i];
+      h[d][i] = C.x_[d][i] + (kk[d][i] * dt) / (T)2;
+    }
+  for (int st = 2; st <= 4; ++st) {
+    evalF(C, h, kk);
+    for (int64_t i = 0; i < N; ++i)
+      for (int d = 0; d < D; ++d) {
+        acc[d][i] = st == 4 ? acc[d][i] + kk[d][i] : acc[d][i] + (T)2 * kk[d][i];
+        if (st == 2) h[d][i] = C.x_[d][i] + (kk[d][i] * dt) / (T)2;
+        if (st == 3) h[d][i] = C.x_[d][i] + kk[d][i] * dt;
+      }
+  }
+  for (int64_t i = 0; i < N; ++i) {
+    for (int d = 0; d < D; ++d) C.x_[d][i] = C.x_[d][i] + (acc[d][i] * dt) / (T)6;
+    if (k.growth) {
+      const T v = C.v_[i], g = C.g[i];
+      C.v_[i] = v + ((((g + (T)2 * g) + (T)2 * g) + g) * dt) / (T)6;
+    }
+  }
+}
+
+template <typename T>
+void agentStepDE(Com<T>& C) {
+  const cbm_config& k = C.cfg;
+  const int D = C.dims;
+  const int64_t N = C.N;
+  const T dt = (T)k.dt;
+  if (k.integrator == CBM_INT_HEUN || k.integrator == CBM_INT_RK4) {
+    multiStage(C);
+    return;
+  }
+  evalF(C, C.x_, C.du);
   // integrator update over 1:N (integrators.jl:495-496 / :720-721)
   const T sq = std::sqrt(dt);
   const T sig = (T)k.sigma;
