@@ -58,6 +58,8 @@ class _Integrators:
     # ODE integrators with 2 and 4 evaluations of f per step (integrators.jl:516-668)
     Heun = staticmethod(lambda: dict(integrator=_abi.INT_HEUN))
     RungeKutta4 = staticmethod(lambda: dict(integrator=_abi.INT_RK4))
+    # SDE integrator with 2 evaluations of f per step (integrators.jl:744-814)
+    EulerHeun = staticmethod(lambda: dict(integrator=_abi.INT_EULER_HEUN))
 
 
 CBMNeighbors = _Neighbors()

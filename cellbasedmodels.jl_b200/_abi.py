@@ -27,7 +27,7 @@ ERR_NAMES = {1: "CBM_ERR_ARG", 2: "CBM_ERR_CUDA", 3: "CBM_ERR_AGENT_OVERFLOW",
 
 F32, F64 = 0, 1
 NEIGH_NONE, NEIGH_FULL, NEIGH_CELL_LINKED, NEIGH_VERLET_DISPLACEMENT, NEIGH_CLVD = 0, 1, 2, 3, 4
-INT_EULER, INT_EM, INT_HEUN, INT_RK4 = 0, 1, 2, 3
+INT_EULER, INT_EM, INT_HEUN, INT_RK4, INT_EULER_HEUN = 0, 1, 2, 3, 4
 FORCE_DIRECT, FORCE_LAGGED = 0, 1
 ATT_FROM_REP, ATT_TO_ATT = 0, 1
 WALLS_NONE, WALLS_REFLECT, WALLS_PUSH = 0, 1, 2

@@ -324,7 +324,7 @@ template <typename T, int D>
 void enqueue_agent_de(cbm_ctx* c, const Params<T>& P) {
   const unsigned grid = kPartnerLists<D> ? c->de_blocks : c->n_blocks;
   const int integ = c->cfg.integrator;
-  if (integ != CBM_INT_HEUN && integ != CBM_INT_RK4) {
+  if (integ != CBM_INT_HEUN && integ != CBM_INT_RK4 && integ != CBM_INT_EULER_HEUN) {
     PROF("k_agent_de");
     k_agent_de<T, D><<<grid, kTile, 0, c->stream>>>(P);
     return;
@@ -348,6 +348,9 @@ void enqueue_agent_de(cbm_ctx* c, const Params<T>& P) {
   if (integ == CBM_INT_HEUN) {
     stage(false, kHeunStage);
     stage(true, kHeunFinal);
+  } else if (integ == CBM_INT_EULER_HEUN) {
+    stage(false, kEhStage);
+    stage(true, kEhFinal);
   } else {
     stage(false, kRk1);
     stage(true, kRk2);
@@ -632,17 +635,19 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
   if (!(k.dt > 0)) return fail(nullptr, CBM_ERR_ARG, "dt must be positive");
   if (k.neighbors < CBM_NEIGH_NONE || k.neighbors > CBM_NEIGH_CLVD)
     return fail(nullptr, CBM_ERR_ARG, "unknown neighbor algorithm %d", k.neighbors);
-  if (k.integrator < CBM_INT_EULER || k.integrator > CBM_INT_RK4)
+  if (k.integrator < CBM_INT_EULER || k.integrator > CBM_INT_EULER_HEUN)
     return fail(nullptr, CBM_ERR_ARG, "unknown integrator %d", k.integrator);
-  if (k.integrator == CBM_INT_HEUN || k.integrator == CBM_INT_RK4) {
-    if (k.sigma != 0)
+  const bool multistage = k.integrator == CBM_INT_HEUN || k.integrator == CBM_INT_RK4 ||
+                          k.integrator == CBM_INT_EULER_HEUN;
+  if (multistage) {
+    if (k.integrator != CBM_INT_EULER_HEUN && k.sigma != 0)
       return fail(nullptr, CBM_ERR_ARG, "Heun and RungeKutta4 integrate ODEs: sigma must be 0");
     if (k.force_mode == CBM_FORCE_LAGGED)
-      return fail(nullptr, CBM_ERR_ARG, "Heun and RungeKutta4 need force_mode = CBM_FORCE_DIRECT");
+      return fail(nullptr, CBM_ERR_ARG, "multi-stage integrators need force_mode = CBM_FORCE_DIRECT");
     if (k.neighbors != CBM_NEIGH_NONE && k.neighbors != CBM_NEIGH_FULL &&
         k.neighbors != CBM_NEIGH_CELL_LINKED)
       return fail(nullptr, CBM_ERR_ARG,
-                  "Heun and RungeKutta4 need neighbors NONE, FULL or CELL_LINKED");
+                  "multi-stage integrators need neighbors NONE, FULL or CELL_LINKED");
   }
   for (int d = 0; d < k.dims; ++d)
     if (!(k.box_hi[d] > k.box_lo[d])) return fail(nullptr, CBM_ERR_ARG, "empty simBox on axis %d", d);
@@ -723,7 +728,8 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
   c->IA = (int*)dalloc(c, n * 4, &ok);
   c->IB = (int*)dalloc(c, n * 4, &ok);
   if (k.walls == CBM_WALLS_REFLECT) c->U = dalloc(c, n * S4, &ok);
-  if (k.integrator == CBM_INT_HEUN || k.integrator == CBM_INT_RK4)
+  if (k.integrator == CBM_INT_HEUN || k.integrator == CBM_INT_RK4 ||
+      k.integrator == CBM_INT_EULER_HEUN)
     for (int q = 0; q < 3; ++q) c->stage[q] = dalloc(c, n * S4, &ok);
   if (list) c->POLD = dalloc(c, n * S4, &ok);
   c->inv = (int*)dalloc(c, n * 4, &ok);

@@ -1294,7 +1294,12 @@ __global__ void __launch_bounds__(kTile, sizeof(T) == 4 ? 4 : 3) k_agent_de(Para
 // The volume v is a DE variable with dv = g when growth is on; its stage
 // values do not enter f, so only its final combination is formed.
 // ---------------------------------------------------------------------------
-enum { kHeunStage = 0, kHeunFinal = 1, kRk1 = 2, kRk2 = 3, kRk3 = 4, kRkFinal = 5 };
+//   EulerHeun (:775-810, the CPU branch):
+//         h1 = (u + f1 dt) + (g xi1) sqrt(dt)
+//         u = u + (((f1 + f2) dt) + ((g + g) xi2) sqrt(dt)) / 2
+//         with g = sigma for positions, 0 for the volume, and xi2 a fresh draw
+enum { kHeunStage = 0, kHeunFinal = 1, kRk1 = 2, kRk2 = 3, kRk3 = 4, kRkFinal = 5, kEhStage = 6,
+       kEhFinal = 7 };
 
 template <typename T, int D>
 __global__ void __launch_bounds__(kTile) k_stage_combine(Params<T> P, int op) {
@@ -1313,6 +1318,29 @@ __global__ void __launch_bounds__(kTile) k_stage_combine(Params<T> P, int op) {
   } else if (op == kRk1 || op == kRk2) {
 #pragma unroll
     for (int d = 0; d < D; ++d) o[d] = u[d] + (k[d] * dt) / (T)2;
+  }
+  if (op == kEhStage || op == kEhFinal) {
+    const int i = ld(P.IA + s);
+    T xi[3] = {(T)0, (T)0, (T)0};
+    cbm_normals(P.seed, P.ctr->step[P.parity], (uint32_t)i,
+                op == kEhStage ? CBM_STREAM_NOISE : CBM_STREAM_NOISE_FINAL, P.community, D, xi);
+    if (op == kEhStage) {
+      P.stage_s[s] = P.stage_k[s];  // f1
+#pragma unroll
+      for (int d = 0; d < D; ++d) o[d] = (u[d] + k[d] * dt) + (P.sigma * xi[d]) * P.sqrt_dt;
+      P.stage_h[s] = from3<T>(o);
+      return;
+    }
+    T f1[3];
+    to3<T>(P.stage_s[s], f1);
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+      o[d] = u[d] + (((f1[d] + k[d]) * dt) + ((P.sigma + P.sigma) * xi[d]) * P.sqrt_dt) / (T)2;
+    const T v = P.VA[s];
+    P.PB[s] = from3<T>(o);
+    P.VB[s] = P.growth ? v + ((ld(P.G + i) + ld(P.G + i)) * dt) / (T)2 : v;
+    P.IB[s] = i;
+    return;
   }
   if (op == kRk1) {
     P.stage_s[s] = P.stage_k[s];

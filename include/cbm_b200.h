@@ -56,10 +56,12 @@ enum {
 };
 
 /* src/integrators.jl: Euler :465-505, EM :683-734, Heun :516-573,
- * RungeKutta4 :583-668.  Heun and RungeKutta4 integrate ODEs (sigma = 0) and
+ * RungeKutta4 :583-668, EulerHeun :744-814.  Heun and RungeKutta4 integrate
+ * ODEs (sigma = 0); EulerHeun integrates the SDE as the reference's CPU path
+ * does (the final update draws fresh noise).  The multi-stage integrators
  * evaluate f at every stage over the neighbor structure of the last rebuild;
  * they need neighbors NONE, FULL or CELL_LINKED and force_mode = CBM_FORCE_DIRECT. */
-enum { CBM_INT_EULER = 0, CBM_INT_EM = 1, CBM_INT_HEUN = 2, CBM_INT_RK4 = 3 };
+enum { CBM_INT_EULER = 0, CBM_INT_EM = 1, CBM_INT_HEUN = 2, CBM_INT_RK4 = 3, CBM_INT_EULER_HEUN = 4 };
 
 /* How the pair force enters dt(x).
  *  DIRECT: dt(x) += F(d)/d * (x - x[j]) inside @loopOverNeighbors.

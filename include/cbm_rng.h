@@ -43,6 +43,7 @@
 #define CBM_STREAM_DIVISION 1u /* normal(0,1) x dims for the division axis */
 #define CBM_STREAM_DEATH 2u    /* uniform(0,1) for the death branch */
 #define CBM_STREAM_USER 3u     /* cbm_rng_fill and tests */
+#define CBM_STREAM_NOISE_FINAL 4u /* EulerHeun: the fresh draw of its final update */
 
 /* ---- exactly rounded primitives that are never fused ------------------- */
 #if defined(__CUDA_ARCH__)

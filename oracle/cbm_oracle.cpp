@@ -550,6 +550,25 @@ void multiStage(Com<T>& C) {
     kk[d].assign(C.x_[d].size(), 0);
     acc[d].assign(C.x_[d].size(), 0);
   }
+  if (k.integrator == CBM_INT_EULER_HEUN) {
+    // EulerHeun (:775-810), the CPU branch; g = sigma for positions, 0 for v
+    const T sq = std::sqrt(dt), sig = (T)k.sigma;
+    evalF(C, C.x_, acc);  // f1
+    for (int64_t i = 0; i < N; ++i) {
+      T xi[3] = {0, 0, 0};
+      cbm_normals(k.seed, C.step, (uint32_t)i, CBM_STREAM_NOISE, k.community, D, xi);
+      for (int d = 0; d < D; ++d) h[d][i] = (C.x_[d][i] + acc[d][i] * dt) + (sig * xi[d]) * sq;
+    }
+    evalF(C, h, kk);  // f2
+    for (int64_t i = 0; i < N; ++i) {
+      T xi[3] = {0, 0, 0};
+      cbm_normals(k.seed, C.step, (uint32_t)i, CBM_STREAM_NOISE_FINAL, k.community, D, xi);
+      for (int d = 0; d < D; ++d)
+        C.x_[d][i] = C.x_[d][i] + (((acc[d][i] + kk[d][i]) * dt) + ((sig + sig) * xi[d]) * sq) / (T)2;
+      if (k.growth) C.v_[i] = C.v_[i] + ((C.g[i] + C.g[i]) * dt) / (T)2;
+    }
+    return;
+  }
   if (k.integrator == CBM_INT_HEUN) {
     evalF(C, C.x_, kk);
     for (int64_t i = 0; i < N; ++i)
@@ -596,7 +615,8 @@ void agentStepDE(Com<T>& C) {
   const int D = C.dims;
   const int64_t N = C.N;
   const T dt = (T)k.dt;
-  if (k.integrator == CBM_INT_HEUN || k.integrator == CBM_INT_RK4) {
+  if (k.integrator == CBM_INT_HEUN || k.integrator == CBM_INT_RK4 ||
+      k.integrator == CBM_INT_EULER_HEUN) {
     multiStage(C);
     return;
   }
@@ -1059,6 +1079,13 @@ int oracle_rng_fill(int precision, uint64_t seed, uint32_t community, int kind, 
     }
   }
   return CBM_OK;
+}
+
+/* the `dims` normals of one (step, agent, stream) of the shared stream */
+void oracle_normals(int precision, uint64_t seed, int64_t stepc, uint32_t agent, uint32_t stream,
+                    uint32_t community, int dims, void* out) {
+  if (precision == CBM_F64) cbm_normals(seed, stepc, agent, stream, community, dims, (double*)out);
+  else cbm_normals(seed, stepc, agent, stream, community, dims, (float*)out);
 }
 
 /* own log / cos-sin, exposed for accuracy tests */

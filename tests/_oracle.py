@@ -49,6 +49,7 @@ def load_oracle(abi):
         "oracle_cossin_f64": (None, [dbl, C.POINTER(dbl), C.POINTER(dbl)]),
         "oracle_cossin_f32": (None, [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
         "oracle_philox": (None, [u32, u32, u32, u32, u32, u32, C.POINTER(u32)]),
+        "oracle_normals": (None, [C.c_int, u64, i64, u32, u32, u32, C.c_int, vp]),
         "oracle_medium_create": (vp, [C.POINTER(abi.CbmMediumConfig)]),
         "oracle_medium_destroy": (None, [vp]),
         "oracle_medium_upload": (C.c_int, [vp, vp, vp]),

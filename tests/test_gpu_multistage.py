@@ -1,7 +1,8 @@
-"""Heun and RungeKutta4 agent integrators (src/integrators.jl:516-668) on the
-device against the checker, bit for bit: every stage evaluates f over the
-cell grid of the last rebuild at the stage's positions (own cell from the
-position, no face pruning), with the reference's combination expressions."""
+"""Heun, RungeKutta4 and EulerHeun agent integrators (src/integrators.jl:
+516-668,744-814) on the device against the checker, bit for bit: every stage
+evaluates f over the cell grid of the last rebuild at the stage's positions
+(own cell from the position, no face pruning), with the reference's
+combination expressions; EulerHeun with noise (sigma > 0)."""
 import numpy as np
 import pytest
 
@@ -12,14 +13,16 @@ from test_gpu_parity import assert_same_grid, assert_same_state, both
 cbm = conftest.cbm
 pytestmark = pytest.mark.gpu
 
-INTEGRATORS = {"heun": "INT_HEUN", "rk4": "INT_RK4"}
+INTEGRATORS = {"heun": "INT_HEUN", "rk4": "INT_RK4", "euler_heun": "INT_EULER_HEUN"}
+SIGMA = {"heun": 0.0, "rk4": 0.0, "euler_heun": 0.05}
+ALL = ["heun", "rk4", "euler_heun"]
 
 
-@pytest.mark.parametrize("integ", ["heun", "rk4"])
+@pytest.mark.parametrize("integ", ALL)
 def test_multistage_aggregation_2d(gpu_lib, abi, integ):
     """2D soft spheres, reflecting walls, Float64, CellLinked."""
     kw, st = aggregation_2d(abi, N=1500, L=60.0)
-    kw = dict(kw, integrator=getattr(abi, INTEGRATORS[integ]))
+    kw = dict(kw, integrator=getattr(abi, INTEGRATORS[integ]), sigma=SIGMA[integ])
     g, o = both(abi, kw, st)
     for _ in range(3):
         g.step(20)
@@ -29,10 +32,10 @@ def test_multistage_aggregation_2d(gpu_lib, abi, integ):
 
 
 @pytest.mark.parametrize("prec", ["f32", "f64"])
-@pytest.mark.parametrize("integ", ["heun", "rk4"])
+@pytest.mark.parametrize("integ", ALL)
 def test_multistage_colony_3d(gpu_lib, abi, integ, prec):
-    """3D colony with growth, division and death, CellLinked, sigma = 0."""
-    kw, st = colony_3d(abi, N=3000, L=60.0, n_max=12000, p_death=2e-3, sigma=0.0,
+    """3D colony with growth, division and death, CellLinked."""
+    kw, st = colony_3d(abi, N=3000, L=60.0, n_max=12000, p_death=2e-3, sigma=SIGMA[integ],
                        precision=abi.F32 if prec == "f32" else abi.F64,
                        neighbors=abi.NEIGH_CELL_LINKED)
     kw = dict(kw, integrator=getattr(abi, INTEGRATORS[integ]))
@@ -45,11 +48,11 @@ def test_multistage_colony_3d(gpu_lib, abi, integ, prec):
     assert a["id_max"] > 3000
 
 
-@pytest.mark.parametrize("integ", ["heun", "rk4"])
+@pytest.mark.parametrize("integ", ALL)
 def test_multistage_dense_colony(gpu_lib, abi, integ):
     """4 agents per unit volume: the stages' walks fill their partner lists."""
     kw, st = packed_colony_3d(abi, N=4000, density=4.0, L=60.0, n_max=8000)
-    kw = dict(kw, neighbors=abi.NEIGH_CELL_LINKED, sigma=0.0,
+    kw = dict(kw, neighbors=abi.NEIGH_CELL_LINKED, sigma=SIGMA[integ],
               integrator=getattr(abi, INTEGRATORS[integ]))
     g, o = both(abi, kw, st)
     for _ in range(2):
