@@ -888,6 +888,20 @@ __device__ __noinline__ void list_terms(const PairCoef<T> c, const typename V4T<
   }
 }
 
+// Squared distance for the candidate filter only: x and y packed, z fused.
+template <typename T, int D>
+__device__ __forceinline__ T filter_s2(const T* xi, const T* xj) {
+  if constexpr (std::is_same<T, float>::value && D > 2) {
+    const float2 d = f2_sub(make_float2(xi[0], xi[1]), make_float2(xj[0], xj[1]));
+    const float2 q = f2_mul(d, d);
+    const float dz = xi[2] - xj[2];
+    return __fmaf_rn(dz, dz, q.x + q.y);
+  } else {
+    T e[3];
+    return pair_diff<T, D>(xi, xj, e);
+  }
+}
+
 // Slot s of N; `list` is this thread's partner list (null: none); `live`
 // holds the lanes of this warp whose slot is below N.
 template <typename T, int D>
@@ -905,6 +919,9 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
   T acc[3] = {(T)0, (T)0, (T)0};
   const T krep = P.k_rep, rrep = P.r_rep, katt = P.k_att, ratt = P.r_att;
   const T cut2 = P.cut2;
+  // the filter's fused squared distance is within a few ulps of the
+  // evaluation's; 2^-20 above the bound keeps every pair the evaluation keeps
+  const T cut2f = cut2 * ((T)1 + (T)9.5367431640625e-07);
   const bool from_rep = P.att_form == CBM_ATT_FROM_REP;
   // pair term with the difference e = xi - xj and its squared norm s2
   const PairCoef<T> coef = pair_coef<T>(P);
@@ -1063,9 +1080,9 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
           T s2v[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            T xj[3], e[3];
+            T xj[3];
             to3<T>(U[q + u], xj);
-            s2v[u] = diff(xj, e);
+            s2v[u] = filter_s2<T, D>(xi, xj);
           }
           // every candidate is written at the queue's end and kept only when it
           // may be inside the cutoff (room() left space for four); the agent
@@ -1073,14 +1090,14 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             queue[nq * kTile + threadIdx.x] = q + u;
-            nq += s2v[u] < cut2 ? 1 : 0;
+            nq += s2v[u] < cut2f ? 1 : 0;
           }
         }
         for (; q < s1; ++q) {
           room(1);
-          T xj[3], e[3];
+          T xj[3];
           to3<T>(U[q], xj);
-          if (diff(xj, e) < cut2) push(q);
+          if (filter_s2<T, D>(xi, xj) < cut2f) push(q);
         }
       }, own_cell);
       // a warp with a stored list evaluates from the list, every entry of the
