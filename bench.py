@@ -571,6 +571,60 @@ def _rel_err(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)) if b.size else 0.0
 
 
+def run_dgadi(cpu=True):
+    """The implicit medium (DGADI) lines: {name: record}."""
+    import torch
+    from _oracle import OracleMedium
+    cbm = load_package()
+    abi = cbm._abi
+    out = {}
+    # Implicit medium (DGADI): the two workloads of examples/Implementation.ipynb,
+    # co2 and co3 (D = 1 and 2) on [0,1]^d, dt 0.01, a source of strength 1 at
+    # the central node, Float32 as the reference's GPU platform runs them.
+    # The notebook's @time (2.45 s for 500 2D steps, 45.67 % of it compilation;
+    # 10.64 s for 200 3D steps; GPU model not stated) is wall time around the
+    # loop; wall_ms here is the same loop through the C ABI, synchronised.
+    for name, dims, nn, steps, cpu_steps, published in (
+            ("medium_dgadi_2d_101", 2, (101, 101, 1), 500, 50, 2.45),
+            ("medium_dgadi_3d_101", 3, (101, 101, 101), 200, 2, 10.64)):
+        mcfg = abi.make_medium_config(dims, nn, (0.0,) * 3, (1.0,) * 3, 0.01, [1.0, 2.0],
+                                      c_max=1.0, precision=abi.F32)
+        nodes = int(np.prod(nn[:dims]))
+        src = np.zeros(tuple(reversed(nn[:dims])), np.float32)
+        src[tuple(round(k / 2) - 1 for k in reversed(nn[:dims]))] = 1.0
+        u0 = np.zeros((2, nodes), np.float32)
+        med = abi.DGADIMedium(mcfg)
+        med.upload(u0, src.reshape(-1))
+        med.step(10)
+        mst = torch.cuda.ExternalStream(med.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        e0.record(mst)
+        med.step(steps, 0)
+        e1.record(mst)
+        e1.synchronize()
+        wall = time.perf_counter() - w0
+        dev_ms = e0.elapsed_time(e1)
+        med.close()
+        cpu_ms = None
+        if cpu:
+            o = OracleMedium(abi, mcfg)
+            o.upload(u0, src.reshape(-1))
+            c0 = time.perf_counter()
+            o.step(cpu_steps)
+            cpu_ms = round(1e3 * (time.perf_counter() - c0) / cpu_steps, 3)
+            o.close()
+        out[name] = {"workload": f"examples/Implementation.ipynb {dims}D: 2 fields on "
+                                 f"{'x'.join(str(k) for k in nn[:dims])} nodes, {steps} DGADI steps",
+                     "dtype": "f32", "steps": steps, "device_ms": round(dev_ms, 3),
+                     "wall_ms": round(wall * 1e3, 3), "us_per_step": round(1e3 * dev_ms / steps, 2),
+                     "node_updates_per_s": round(2 * nodes * steps / (dev_ms / 1e3), 1),
+                     "reference_published_s": published,
+                     "cpu_oracle_ms_per_step": cpu_ms, "cpu_oracle_threads": 1}
+    return out
+
+
 def run_configs(args):
     """The other configurations of the path: the 2D aggregation (Float64,
     L2-resident, launch-bound: us/step) and 2D chemotaxis on a 1024^2 medium
@@ -695,49 +749,7 @@ def run_configs(args):
                                    "value": round(n0 * args.config_f64_steps / (ms / 1e3), 1),
                                    "unit": UNIT}
 
-    # Implicit medium (DGADI): the two workloads of examples/Implementation.ipynb,
-    # co2 and co3 (D = 1 and 2) on [0,1]^d, dt 0.01, a source of strength 1 at
-    # the central node, Float32 as the reference's GPU platform runs them.
-    # The notebook's @time (2.45 s for 500 2D steps, 45.67 % of it compilation;
-    # 10.64 s for 200 3D steps; GPU model not stated) is wall time around the
-    # loop; wall_ms here is the same loop through the C ABI, synchronised.
-    from _oracle import OracleMedium
-    for name, dims, nn, steps, cpu_steps, published in (
-            ("medium_dgadi_2d_101", 2, (101, 101, 1), 500, 50, 2.45),
-            ("medium_dgadi_3d_101", 3, (101, 101, 101), 200, 2, 10.64)):
-        mcfg = abi.make_medium_config(dims, nn, (0.0,) * 3, (1.0,) * 3, 0.01, [1.0, 2.0],
-                                      c_max=1.0, precision=abi.F32)
-        nodes = int(np.prod(nn[:dims]))
-        src = np.zeros(tuple(reversed(nn[:dims])), np.float32)
-        src[tuple(round(k / 2) - 1 for k in reversed(nn[:dims]))] = 1.0
-        u0 = np.zeros((2, nodes), np.float32)
-        med = abi.DGADIMedium(mcfg)
-        med.upload(u0, src.reshape(-1))
-        med.step(10)
-        mst = torch.cuda.ExternalStream(med.stream())
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        w0 = time.perf_counter()
-        e0.record(mst)
-        med.step(steps, 0)
-        e1.record(mst)
-        e1.synchronize()
-        wall = time.perf_counter() - w0
-        dev_ms = e0.elapsed_time(e1)
-        med.close()
-        o = OracleMedium(abi, mcfg)
-        o.upload(u0, src.reshape(-1))
-        c0 = time.perf_counter()
-        o.step(cpu_steps)
-        cpu_ms = 1e3 * (time.perf_counter() - c0) / cpu_steps
-        o.close()
-        out[name] = {"workload": f"examples/Implementation.ipynb {dims}D: 2 fields on "
-                                 f"{'x'.join(str(k) for k in nn[:dims])} nodes, {steps} DGADI steps",
-                     "dtype": "f32", "steps": steps, "device_ms": round(dev_ms, 3),
-                     "wall_ms": round(wall * 1e3, 3), "us_per_step": round(1e3 * dev_ms / steps, 2),
-                     "node_updates_per_s": round(2 * nodes * steps / (dev_ms / 1e3), 1),
-                     "reference_published_s": published,
-                     "cpu_oracle_ms_per_step": round(cpu_ms, 3), "cpu_oracle_threads": 1}
+    out.update(run_dgadi())
 
     # Error of the Float32 results against Float64 runs, 100 steps.  The noise
     # of an SDE run is drawn in the run's precision (Box-Muller in float or
@@ -843,6 +855,8 @@ def main():
                     help="keep the default tuning (for profiling one known launch)")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-configs", action="store_true")
+    ap.add_argument("--dgadi-only", action="store_true",
+                    help="print only the implicit-medium (DGADI) lines, without the CPU checker")
     ap.add_argument("--config-steps", type=int, default=200)
     ap.add_argument("--config-cpu-steps", type=int, default=5)
     ap.add_argument("--config-f64-steps", type=int, default=10)
@@ -850,6 +864,9 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--checkpoint-every", type=int, default=20)
     args = ap.parse_args()
+    if args.dgadi_only:
+        print(json.dumps({"dgadi": run_dgadi(cpu=False)}))
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

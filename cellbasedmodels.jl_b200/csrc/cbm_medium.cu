@@ -34,7 +34,6 @@
 
 namespace {
 
-constexpr int kMedThreads = 256;
 constexpr int kSweepThreads = 128;
 
 template <typename T>
@@ -75,28 +74,31 @@ __global__ void k_dgadi_tables(cbm_medium_config k, int nmax, FieldCoef<T>* coef
   }
 }
 
-// u .+= f(u) at interior nodes: f = s (c_max - u) - decay u.  Grid: x in
-// blocks of kMedThreads, (y, z) pairs, fields.
-template <typename T, int D>
-__global__ void k_dgadi_explicit(T* __restrict__ u, const T* __restrict__ src,
-                                 const FieldCoef<T>* __restrict__ coef, T cmax, int n0, int n1,
-                                 int n2) {
-  const int x = blockIdx.x * kMedThreads + threadIdx.x;
-  const int yz = blockIdx.y;
-  const int y = D > 1 ? yz % n1 : 0;
-  const int z = D > 2 ? yz / n1 : 0;
-  const int f = blockIdx.z;
-  const bool in = x > 0 && x < n0 - 1 && (D < 2 || (y > 0 && y < n1 - 1)) &&
-                  (D < 3 || (z > 0 && z < n2 - 1));
-  if (!in) return;
-  const long long i = x + (long long)n0 * yz;
-  const long long id = i + (long long)f * n0 * n1 * n2;
-  const T ui = u[id];
-  const T du = src[i] * (cmax - ui) - coef->decay[f] * ui;
-  u[id] = ui + du;
+// The explicit part u .+= f(u), f = s (c_max - u) - decay u, applies to the
+// nodes that are interior in every axis: exactly the interior nodes of the
+// lines along x through interior (y, z), whose solve reads nothing else.  So
+// it is applied while those lines are loaded, inside the x solves.
+template <typename T>
+__device__ __forceinline__ T explicit_part(T u, T s, T cmax, T decay) {
+  return u + (s * (cmax - u) - decay * u);
 }
 
 constexpr unsigned kFullMask = 0xffffffffu;
+
+// Asynchronous copy of one element global -> shared (no register round trip,
+// so a thread's copies are all in flight together); completed by
+// cp_async_wait_all, made visible to the warp by __syncwarp.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (sizeof(T) == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(a), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
 
 // One line's solve in place: X(j) is node j of the line (ends 0 and n-1).
 // The table entries and nodes of the next iteration are loaded one step
@@ -138,7 +140,7 @@ template <typename T, int A, int D>
 __global__ void __launch_bounds__(kSweepThreads)
     k_dgadi_sweep(const T* __restrict__ xo, T* __restrict__ xn, const FieldCoef<T>* __restrict__ coef,
                   const T* __restrict__ cstar, const double* __restrict__ piv, int nmax, int n0,
-                  int n1, int n2, int nf) {
+                  int n1, int n2, int nf, const T* __restrict__ src, T cmax) {
   const int len[3] = {n0, n1, n2};
   const long long stride[3] = {1, n0, (long long)n0 * n1};
   constexpr int B = A == 0 ? 1 : 0;  // the line's position: (b, c) interior
@@ -160,9 +162,15 @@ __global__ void __launch_bounds__(kSweepThreads)
   const double* pv = piv + (size_t)(f * 3 + A) * nmax;
   const T* X = xo + o;
   T* Y = xn + o;
-  // the ends and the interior to solve are copied to xn's line first (xn's
-  // ends are the uploaded border values, equal to xo's)
-  for (int j = 1; j < n - 1; ++j) Y[j * st] = X[j * st];
+  // the interior to solve is copied to xn's line first, with the explicit
+  // part along x (xn's ends are the uploaded border values, equal to xo's)
+  if (A == 0) {
+    const T* S = src + (o - (long long)f * n0 * n1 * n2);
+    const T dec = coef->decay[f];
+    for (int j = 1; j < n - 1; ++j) Y[j] = explicit_part(X[j], S[j], cmax, dec);
+  } else {
+    for (int j = 1; j < n - 1; ++j) Y[j * st] = X[j * st];
+  }
   line_solve<T>([&](int j) -> T& { return Y[j * st]; }, n, sub, main, sup, cs, pv);
 }
 
@@ -179,9 +187,10 @@ __global__ void __launch_bounds__(kTileLines)
     k_dgadi_sweep_tiled(const T* __restrict__ xo, T* __restrict__ xn,
                         const FieldCoef<T>* __restrict__ coef, const T* __restrict__ cstar,
                         const double* __restrict__ piv, int nmax, int n0, int n1, int n2, int nf,
-                        int rowp) {
+                        int rowp, const T* __restrict__ src, T cmax) {
   extern __shared__ __align__(16) unsigned char med_smem[];
   T* tile = reinterpret_cast<T*>(med_smem);
+  T* stile = tile + kTileLines * rowp;  // axis 0: the source rows
   const int len[3] = {n0, n1, n2};
   const long long stride[3] = {1, n0, (long long)n0 * n1};
   constexpr int B = A == 0 ? 1 : 0;
@@ -205,17 +214,28 @@ __global__ void __launch_bounds__(kTileLines)
   int f = 0;
   const long long o = line_base(t, &f);
   auto at = [&](int r, int j) -> T& { return A == 0 ? tile[r * rowp + j] : tile[j * kTileLines + r]; };
+  const long long fnodes = (long long)n0 * n1 * n2;
   if (A == 0) {
     for (int r = 0; r < kTileLines; ++r) {
       const long long orow = __shfl_sync(kFullMask, o, r);
+      const int frow = __shfl_sync(kFullMask, f, r);
       if (orow < 0) break;
-      for (int j = t; j < n; j += kTileLines) at(r, j) = xo[orow + j];
+      const long long srow = orow - (long long)frow * fnodes;
+      for (int j = t; j < n; j += kTileLines) {
+        cp_async_elem(&at(r, j), xo + orow + j);
+        cp_async_elem(&stile[r * rowp + j], src + srow + j);
+      }
     }
   } else if (o >= 0) {
-    for (int j = 0; j < n; ++j) at(t, j) = xo[o + j * st];
+    for (int j = 0; j < n; ++j) cp_async_elem(&at(t, j), xo + o + j * st);
   }
+  cp_async_wait_all();
   __syncwarp();
   if (o >= 0) {
+    if (A == 0) {
+      const T dec = coef->decay[f];
+      for (int j = 1; j < n - 1; ++j) at(t, j) = explicit_part(at(t, j), stile[t * rowp + j], cmax, dec);
+    }
     const T sub = coef->sub[f], main = coef->main[f], sup = coef->sup[f];
     const T* cs = cstar + (size_t)(f * 3 + A) * nmax;
     const double* pv = piv + (size_t)(f * 3 + A) * nmax;
@@ -274,8 +294,7 @@ __global__ void __launch_bounds__(kFusedThreads)
                       (D < 3 || (z > 0 && z < n2 - 1));
       if (!in) continue;
       const int k = x + px * (y + n1 * z);
-      const T ui = sh[k];
-      sh[k] = ui + (ss[k] * (cmax - ui) - dec * ui);
+      sh[k] = explicit_part(sh[k], ss[k], cmax, dec);
     }
     __syncthreads();
 #pragma unroll
@@ -312,7 +331,7 @@ constexpr size_t kFusedMaxBytes = 200 * 1024;
 template <typename T>
 size_t tile_bytes(int axis, int n) {
   const int rowp = axis == 0 ? (n | 1) : n;
-  return (size_t)kTileLines * rowp * sizeof(T);
+  return (axis == 0 ? 2 : 1) * (size_t)kTileLines * rowp * sizeof(T);
 }
 constexpr size_t kTileMaxBytes = 96 * 1024;
 
@@ -371,12 +390,8 @@ int enqueue_step(cbm_medium* m) {
   const int nf = k.n_fields;
   T* u[2] = {(T*)m->u[0], (T*)m->u[1]};
   const auto* coef = (const FieldCoef<T>*)m->coef;
-  const long long tot = m->nodes * nf;
-  (void)tot;
-  k_dgadi_explicit<T, D><<<dim3((unsigned)((n0 + kMedThreads - 1) / kMedThreads), (unsigned)(n1 * n2),
-                                (unsigned)nf),
-                           kMedThreads, 0, m->stream>>>(u[m->cur], (const T*)m->src, coef,
-                                                        (T)k.c_max, n0, n1, n2);
+  const T* src = (const T*)m->src;
+  const T cmax = (T)k.c_max;
   auto lines = [&](int a) {
     const int len[3] = {n0, n1, n2};
     long long l = 1;
@@ -395,10 +410,10 @@ int enqueue_step(cbm_medium* m) {
       k_dgadi_sweep_tiled<T, A, D>
           <<<(unsigned)((nl + kTileLines - 1) / kTileLines), kTileLines, tb, m->stream>>>(
               u[m->cur], u[m->cur ^ 1], coef, cs, m->piv, m->nmax, n0, n1, n2, nf,
-              A == 0 ? (len[A] | 1) : len[A]);
+              A == 0 ? (len[A] | 1) : len[A], src, cmax);
     } else {
       k_dgadi_sweep<T, A, D><<<grid(lines(A)), kSweepThreads, 0, m->stream>>>(
-          u[m->cur], u[m->cur ^ 1], coef, cs, m->piv, m->nmax, n0, n1, n2, nf);
+          u[m->cur], u[m->cur ^ 1], coef, cs, m->piv, m->nmax, n0, n1, n2, nf, src, cmax);
     }
     m->cur ^= 1;
   };

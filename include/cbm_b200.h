@@ -339,7 +339,9 @@ void* cbm_adjoint_stream(cbm_adjoint* a);
  *      and the two border nodes of each line as Dirichlet values.  In Float32
  *      the pivots 1.0 / (...) are Float64, as Julia promotes them.
  * Border nodes keep their uploaded values (the reference never writes them).
- * Every axis needs at least 4 nodes.  Each step enqueues 1 + dims kernels. */
+ * Every axis needs at least 4 nodes.  A medium whose field fits one SM's
+ * shared memory runs all steps of a call in one launch; a larger one enqueues
+ * one launch per axis and step. */
 #define CBM_MEDIUM_MAX_FIELDS 8
 typedef struct cbm_medium_config {
   int32_t dims;                           /* 1, 2 or 3 */
