@@ -644,10 +644,10 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
       return fail(nullptr, CBM_ERR_ARG, "Heun and RungeKutta4 integrate ODEs: sigma must be 0");
     if (k.force_mode == CBM_FORCE_LAGGED)
       return fail(nullptr, CBM_ERR_ARG, "multi-stage integrators need force_mode = CBM_FORCE_DIRECT");
-    if (k.neighbors != CBM_NEIGH_NONE && k.neighbors != CBM_NEIGH_FULL &&
-        k.neighbors != CBM_NEIGH_CELL_LINKED)
+    if (k.neighbors == CBM_NEIGH_CLVD)
       return fail(nullptr, CBM_ERR_ARG,
-                  "multi-stage integrators need neighbors NONE, FULL or CELL_LINKED");
+                  "multi-stage integrators need neighbors NONE, FULL, CELL_LINKED or "
+                  "VERLET_DISPLACEMENT");
   }
   for (int d = 0; d < k.dims; ++d)
     if (!(k.box_hi[d] > k.box_lo[d])) return fail(nullptr, CBM_ERR_ARG, "empty simBox on axis %d", d);

@@ -1318,6 +1318,17 @@ __global__ void __launch_bounds__(kTile, sizeof(T) == 4 ? 4 : 3) k_agent_de(Para
 enum { kHeunStage = 0, kHeunFinal = 1, kRk1 = 2, kRk2 = 3, kRk3 = 4, kRkFinal = 5, kEhStage = 6,
        kEhFinal = 7 };
 
+// verletDisplacement (neighbors.jl:367-391) on the new position xn of slot s,
+// as k_agent_de does it for the single-stage integrators
+template <typename T, int D>
+__device__ __forceinline__ void stage_displacement(const Params<T>& P, int s, const T* xn) {
+  if (is_verlet(P) && !P.ctr->events) {
+    T xo[3];
+    to3<T>(P.POLD[s], xo);
+    if (dist<T, D>(xn, xo) >= P.rebuild_thr) P.ctr->flag[P.parity] = 1;
+  }
+}
+
 template <typename T, int D>
 __global__ void __launch_bounds__(kTile) k_stage_combine(Params<T> P, int op) {
   const int N = (int)P.ctr->N[P.parity];
@@ -1357,6 +1368,7 @@ __global__ void __launch_bounds__(kTile) k_stage_combine(Params<T> P, int op) {
     P.PB[s] = from3<T>(o);
     P.VB[s] = P.growth ? v + ((ld(P.G + i) + ld(P.G + i)) * dt) / (T)2 : v;
     P.IB[s] = i;
+    stage_displacement<T, D>(P, s, o);
     return;
   }
   if (op == kRk1) {
@@ -1396,6 +1408,7 @@ __global__ void __launch_bounds__(kTile) k_stage_combine(Params<T> P, int op) {
   P.PB[s] = from3<T>(o);
   P.VB[s] = vn;
   P.IB[s] = i;
+  stage_displacement<T, D>(P, s, o);
 }
 
 // ---------------------------------------------------------------------------

@@ -60,7 +60,8 @@ enum {
  * ODEs (sigma = 0); EulerHeun integrates the SDE as the reference's CPU path
  * does (the final update draws fresh noise).  The multi-stage integrators
  * evaluate f at every stage over the neighbor structure of the last rebuild;
- * they need neighbors NONE, FULL or CELL_LINKED and force_mode = CBM_FORCE_DIRECT. */
+ * they need neighbors NONE, FULL, CELL_LINKED or VERLET_DISPLACEMENT and
+ * force_mode = CBM_FORCE_DIRECT. */
 enum { CBM_INT_EULER = 0, CBM_INT_EM = 1, CBM_INT_HEUN = 2, CBM_INT_RK4 = 3, CBM_INT_EULER_HEUN = 4 };
 
 /* How the pair force enters dt(x).

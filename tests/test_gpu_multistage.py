@@ -8,7 +8,7 @@ import pytest
 
 import conftest
 from scenarios import aggregation_2d, chemotaxis_2d, colony_3d, packed_colony_3d
-from test_gpu_parity import assert_same_grid, assert_same_state, both
+from test_gpu_parity import assert_same_grid, assert_same_lists, assert_same_state, both
 
 cbm = conftest.cbm
 pytestmark = pytest.mark.gpu
@@ -46,6 +46,21 @@ def test_multistage_colony_3d(gpu_lib, abi, integ, prec):
         a, b = g.download(), o.download()
         assert_same_state(a, b, ["x", "y", "z", "v", "g", "id", "parent"])
     assert a["id_max"] > 3000
+
+
+@pytest.mark.parametrize("integ", ALL)
+def test_multistage_verlet_displacement(gpu_lib, abi, integ):
+    """VerletDisplacement lists: every stage reads the list of the last
+    rebuild; the final combination checks the displacement for the rebuild."""
+    kw, st = colony_3d(abi, N=1500, L=60.0, n_max=6000, p_death=0.0, sigma=SIGMA[integ],
+                       neighbors=abi.NEIGH_VERLET_DISPLACEMENT)
+    kw = dict(kw, integrator=getattr(abi, INTEGRATORS[integ]), fate=abi.FATE_NONE, growth=0)
+    g, o = both(abi, kw, st)
+    for _ in range(3):
+        g.step(20)
+        o.step(20)
+        assert_same_state(g.download(), o.download(), ["x", "y", "z"])
+    assert_same_lists(g, o)
 
 
 @pytest.mark.parametrize("integ", ALL)
