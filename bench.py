@@ -28,6 +28,7 @@ scaling, no data-path collective); the time is the max over ranks.
 import argparse
 import datetime
 import json
+import math
 import os
 import subprocess
 import sys
@@ -625,6 +626,79 @@ def run_dgadi(cpu=True):
     return out
 
 
+def rod_disc(abi, n, seed=21):
+    """n rods of d = 1, l uniform in [2, 3], uniform in a disc at about one rod
+    per 3.8 units^2 (the colony's packing), small random velocities."""
+    rng = np.random.default_rng(seed)
+    radius = math.sqrt(n * 3.8 / math.pi)
+    r = radius * np.sqrt(rng.uniform(0, 1, n))
+    phi = rng.uniform(0, 2 * math.pi, n)
+    st = {k: np.zeros(n) for k in abi.ROD_FIELDS}
+    st["x"], st["y"] = r * np.cos(phi), r * np.sin(phi)
+    st["vx"], st["vy"] = rng.normal(0, 0.01, n), rng.normal(0, 0.01, n)
+    st["theta"] = rng.uniform(-math.pi, math.pi, n)
+    st["omega"] = rng.normal(0, 0.01, n)
+    st["d"], st["m"] = np.ones(n), np.ones(n)
+    st["l"] = rng.uniform(2.0, 3.0, n)
+    return st
+
+
+# Model constants of examples/Bacteries.ipynb in its natural units (m = 1/100,
+# g = 1/10000, d = 1): kn = 2e6 m g / d, gamma = 2.2e2 sqrt(g / d)
+ROD_PARAMS = dict(dt=0.1, kn=2.0e6 * (1e-2 * 1e-4), gamma_n=2.2e2 * math.sqrt(1e-4),
+                  gamma_t=2.2e2 * math.sqrt(1e-4), mu_cc=0.1, mu_cw=0.8, beta=0.8, beta_w=0.8)
+
+
+def run_rods(cpu=True, n=32768, steps=200, cpu_steps=3):
+    """The rods2D line: a colony of the size examples/Bacteries.ipynb times
+    (about 3.2e4 rods, Float64, CellLinked cellEdge 4, simBox [-300, 300]^2),
+    200 steps through the C ABI, with the CPU checker beside it."""
+    import torch
+    from _oracle import OracleRods
+    cbm = load_package()
+    abi = cbm._abi
+    st = rod_disc(abi, n)
+    cfg = abi.make_rods_config(n, (-300.0, -300.0), (300.0, 300.0), cell_edge=4.0,
+                               neighbors=abi.NEIGH_CELL_LINKED, precision=abi.F64, **ROD_PARAMS)
+    g = abi.Rods2D(cfg)
+    g.upload(st)
+    g.step(5)
+    rst = torch.cuda.ExternalStream(g.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(rst)
+    g.step(steps, 0)
+    e1.record(rst)
+    e1.synchronize()
+    dev_ms = e0.elapsed_time(e1)
+    # e2e: host state in, steps, host state out
+    w0 = time.perf_counter()
+    g.upload(st)
+    g.step(steps, 0)
+    out_state = g.download()
+    wall = time.perf_counter() - w0
+    g.close()
+    rec = {"workload": f"rods2D colony, {n} rods (d 1, l 2-3) in a disc at one rod per 3.8 "
+                       f"units^2, examples/Bacteries.ipynb constants, dt 0.1, CellLinked "
+                       f"cellEdge 4, simBox [-300,300]^2",
+           "dtype": "f64", "rods": n, "steps": steps, "device_ms": round(dev_ms, 3),
+           "ms_per_step": round(dev_ms / steps, 4),
+           "value": round(n * steps / (dev_ms / 1e3), 1), "unit": "rod-steps/s",
+           "e2e_rod_steps_per_s": round(n * steps / wall, 1),
+           "rods_in_contact": int(np.count_nonzero(out_state["pressure"]))}
+    if cpu:
+        o = OracleRods(abi, cfg)
+        o.upload(st)
+        c0 = time.perf_counter()
+        o.step(cpu_steps)
+        cpu_s = (time.perf_counter() - c0) / cpu_steps
+        o.close()
+        rec["cpu_oracle_ms_per_step"] = round(1e3 * cpu_s, 3)
+        rec["cpu_oracle_threads"] = os.cpu_count()
+        rec["cpu_value"] = round(n / cpu_s, 1)
+    return rec
+
+
 def run_configs(args):
     """The other configurations of the path: the 2D aggregation (Float64,
     L2-resident, launch-bound: us/step) and 2D chemotaxis on a 1024^2 medium
@@ -750,6 +824,7 @@ def run_configs(args):
                                    "unit": UNIT}
 
     out.update(run_dgadi())
+    out["rods2d_colony_32k_f64"] = run_rods()
 
     # Error of the Float32 results against Float64 runs, 100 steps.  The noise
     # of an SDE run is drawn in the run's precision (Box-Muller in float or
@@ -857,6 +932,8 @@ def main():
     ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--dgadi-only", action="store_true",
                     help="print only the implicit-medium (DGADI) lines, without the CPU checker")
+    ap.add_argument("--rods-only", action="store_true",
+                    help="print only the rods2D line, without the CPU checker")
     ap.add_argument("--config-steps", type=int, default=200)
     ap.add_argument("--config-cpu-steps", type=int, default=5)
     ap.add_argument("--config-f64-steps", type=int, default=10)
@@ -866,6 +943,9 @@ def main():
     args = ap.parse_args()
     if args.dgadi_only:
         print(json.dumps({"dgadi": run_dgadi(cpu=False)}))
+        return
+    if args.rods_only:
+        print(json.dumps({"rods": run_rods(cpu=False)}))
         return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

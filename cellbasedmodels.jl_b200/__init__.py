@@ -26,7 +26,7 @@ import numpy as np
 
 from . import _abi, fitting, sweep  # noqa: F401
 from ._abi import (Adjoint, Batch, CbmConfig, CbmError, Context, DGADIMedium,  # noqa: F401
-                   load_library, make_config, make_medium_config)
+                   Rods2D, load_library, make_config, make_medium_config, make_rods_config)
 from .sweep import ShardedBatch, partition_communities  # noqa: F401
 
 __all__ = ["ABM", "Community", "evolve", "step", "loadToPlatform", "bringFromPlatform",
@@ -34,7 +34,7 @@ __all__ = ["ABM", "Community", "evolve", "step", "loadToPlatform", "bringFromPla
            "computeNeighbors", "CBMNeighbors", "CBMIntegrators", "SoftSpheres", "Growth",
            "Medium", "B200", "Context", "Batch", "Adjoint", "ShardedBatch",
            "partition_communities", "CbmError", "make_config", "load_library",
-           "DGADIMedium", "make_medium_config", "fitting"]
+           "DGADIMedium", "make_medium_config", "Rods2D", "make_rods_config", "fitting"]
 
 
 # ---- algorithm descriptors (src/neighbors.jl, src/integrators.jl) -------------

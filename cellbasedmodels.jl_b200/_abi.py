@@ -532,6 +532,100 @@ class DGADIMedium:
         return self.lib.cbm_medium_stream(self.h)
 
 
+ROD_FIELDS = ("x", "y", "vx", "vy", "theta", "omega", "d", "l", "m", "fx", "fy", "W",
+              "pressure")
+
+
+class CbmRodsConfig(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("neighbors", C.c_int32), ("n_max", C.c_int64),
+                ("box_lo", C.c_double * 2), ("box_hi", C.c_double * 2), ("cell_edge", C.c_double),
+                ("dt", C.c_double), ("kn", C.c_double), ("gamma_n", C.c_double),
+                ("gamma_t", C.c_double), ("mu_cc", C.c_double), ("mu_cw", C.c_double),
+                ("beta", C.c_double), ("beta_w", C.c_double)]
+
+
+def make_rods_config(n_max, box_lo, box_hi, dt, kn, gamma_n, gamma_t, mu_cc, beta, beta_w,
+                     mu_cw=0.0, cell_edge=0.0, neighbors=NEIGH_CELL_LINKED, precision=F64):
+    """A cbm_rods_config: the model parameters of rods2D (kn, γn, γt, μcc, μcw,
+    β, βω), its simBox and the CellLinked cell edge."""
+    k = CbmRodsConfig()
+    k.precision, k.neighbors, k.n_max = precision, neighbors, int(n_max)
+    for d in range(2):
+        k.box_lo[d], k.box_hi[d] = float(box_lo[d]), float(box_hi[d])
+    k.cell_edge, k.dt = float(cell_edge), float(dt)
+    k.kn, k.gamma_n, k.gamma_t = float(kn), float(gamma_n), float(gamma_t)
+    k.mu_cc, k.mu_cw, k.beta, k.beta_w = float(mu_cc), float(mu_cw), float(beta), float(beta_w)
+    return k
+
+
+class Rods2D:
+    """The rods2D model (src/models/rods.jl) stepped with Euler on the device.
+    State is a dict of ROD_FIELDS arrays (or a (13, n) / (12, n) array in
+    that order); pressure is output only."""
+
+    def __init__(self, cfg):
+        self.lib = load_library()
+        lib = self.lib
+        if not getattr(lib, "_rods_bound", False):
+            vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
+            for name, res, args in (
+                    ("cbm_rods_create", C.c_int, [C.POINTER(vp), C.POINTER(CbmRodsConfig)]),
+                    ("cbm_rods_destroy", None, [vp]),
+                    ("cbm_rods_last_error", C.c_char_p, [vp]),
+                    ("cbm_rods_upload", C.c_int, [vp, i64, C.POINTER(vp)]),
+                    ("cbm_rods_step", C.c_int, [vp, i32, i32]),
+                    ("cbm_rods_download", C.c_int, [vp, C.POINTER(vp), C.POINTER(i64)]),
+                    ("cbm_rods_stream", vp, [vp])):
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            lib._rods_bound = True
+        h = C.c_void_p()
+        rc = lib.cbm_rods_create(C.byref(h), C.byref(cfg))
+        if rc != CBM_OK:
+            raise CbmError(rc, lib.cbm_rods_last_error(None).decode())
+        self.h = h
+        self.cfg = cfg
+        self.dtype = np.float64 if cfg.precision == F64 else np.float32
+        self.n = 0
+
+    def _check(self, rc):
+        if rc != CBM_OK:
+            raise CbmError(rc, self.lib.cbm_rods_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cbm_rods_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def upload(self, state):
+        if isinstance(state, dict):
+            cols = [state[k] for k in ROD_FIELDS[:12]]
+        else:
+            cols = list(np.asarray(state)[:12])
+        arrs = [np.ascontiguousarray(c, dtype=self.dtype) for c in cols]
+        n = len(arrs[0]) if arrs else 0
+        ptrs = (C.c_void_p * 13)(*([a.ctypes.data for a in arrs] + [None]))
+        self._keep = arrs
+        self._check(self.lib.cbm_rods_upload(self.h, n, ptrs))
+        self.n = n
+
+    def step(self, n, flags=SYNC):
+        self._check(self.lib.cbm_rods_step(self.h, n, flags))
+
+    def download(self):
+        out = np.zeros((13, self.n), self.dtype)
+        ptrs = (C.c_void_p * 13)(*[out[q].ctypes.data for q in range(13)])
+        n = C.c_int64()
+        self._check(self.lib.cbm_rods_download(self.h, ptrs, C.byref(n)))
+        return {k: out[q] for q, k in enumerate(ROD_FIELDS)}
+
+    def stream(self):
+        return self.lib.cbm_rods_stream(self.h)
+
+
 class Adjoint:
     """Gradients of mean((x_T - target)^2) w.r.t. (k_rep, k_att, r_rep) and x0."""
 

@@ -13,13 +13,14 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libcbm_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("cbm_api.cu", "cbm_batch.cu", "cbm_adjoint.cu", "cbm_noalloc.cu", "cbm_medium.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("cbm_api.cu", "cbm_batch.cu", "cbm_adjoint.cu", "cbm_noalloc.cu", "cbm_medium.cu", "cbm_rods.cu")]
 DEPS = SOURCES + [
     os.path.join(HERE, "csrc", "cbm_kernels.cuh"),
     os.path.join(HERE, "csrc", "cbm_common.cuh"),
     os.path.join(HERE, "csrc", "cbm_grid.cuh"),
     os.path.join(HERE, "..", "include", "cbm_b200.h"),
     os.path.join(HERE, "..", "include", "cbm_rng.h"),
+    os.path.join(HERE, "..", "include", "cbm_rods_math.h"),
 ]
 
 

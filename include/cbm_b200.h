@@ -370,6 +370,47 @@ int cbm_medium_step(cbm_medium* m, int32_t nsteps, int32_t flags);
 int cbm_medium_download(cbm_medium* m, void* fields, double* t);
 void* cbm_medium_stream(cbm_medium* m);
 
+/* ---- rods: the rods2D model (src/models/rods.jl) ---------------------------
+ * 2D rods of diameter d, length l and mass m, after Volfson et al.  The ODE
+ * of rods2D (rods.jl:86-118), integrated by Euler:
+ *   dt(x) = vx, dt(y) = vy, dt(vx) = -beta vx + fx/m, dt(vy) = -beta vy + fy/m,
+ *   dt(theta) = omega, dt(omega) = W/(m (d+l)^2/12 + m d^2) - beta_w omega,
+ * where fx, fy, W (and pressure) are summed over the neighbors with
+ * rodForces (:21-59) and CBMMetrics.rodIntersection (src/metrics.jl:128-246).
+ * Assigned inside the ODE, they are written to the new copy and read lagged:
+ * dt(vx) uses the fx committed by the previous step, as the reference's code
+ * generator has it.  Neighbors: the CellLinked grid over the committed
+ * positions (cell_edge), in the reference's order, or all pairs (FULL).
+ * cos and sin are the library's own series (the same bits on host and
+ * device); delta^1.5 = delta sqrt(delta), delta^0.5 = sqrt(delta). */
+typedef struct cbm_rods_config {
+  int32_t precision;        /* CBM_F32 or CBM_F64 */
+  int32_t neighbors;        /* CBM_NEIGH_FULL or CBM_NEIGH_CELL_LINKED */
+  int64_t n_max;            /* rod capacity */
+  double box_lo[2], box_hi[2];
+  double cell_edge;
+  double dt;
+  double kn, gamma_n, gamma_t, mu_cc, mu_cw, beta, beta_w;
+} cbm_rods_config;
+
+typedef struct cbm_rods cbm_rods;
+int cbm_rods_create(cbm_rods** out, const cbm_rods_config* cfg);
+void cbm_rods_destroy(cbm_rods* r);
+const char* cbm_rods_last_error(const cbm_rods* r);
+/* The per-rod fields, each an array of n reals of the configured precision,
+ * in this order (CBM_RODS_FIELDS of them; pressure is read by download only). */
+#define CBM_RODS_FIELDS 13
+enum {
+  CBM_ROD_X = 0, CBM_ROD_Y, CBM_ROD_VX, CBM_ROD_VY, CBM_ROD_THETA, CBM_ROD_OMEGA, CBM_ROD_D,
+  CBM_ROD_L, CBM_ROD_M, CBM_ROD_FX, CBM_ROD_FY, CBM_ROD_W, CBM_ROD_PRESSURE
+};
+/* fields[k] for k < CBM_ROD_PRESSURE are read (host arrays); sets the step to 0 */
+int cbm_rods_upload(cbm_rods* r, int64_t n, const void* const* fields);
+int cbm_rods_step(cbm_rods* r, int32_t nsteps, int32_t flags);
+/* fields[k] (host arrays of at least n reals) receive every field; *n_out = n */
+int cbm_rods_download(cbm_rods* r, void* const* fields, int64_t* n_out);
+void* cbm_rods_stream(cbm_rods* r);
+
 /* ---- allocation-free cell grid -------------------------------------------
  * This entry point has no counterpart in the reference.  It is for callers
  * that cannot allocate device memory when they need a grid: code running

@@ -1315,3 +1315,328 @@ extern "C" int oracle_adjoint_dual(const cbm_config* cfg, int64_t n, const doubl
   for (int s = 0; s < n_seed; ++s) dx0_seeded[s] = L.d[3 + s];
   return CBM_OK;
 }
+
+/* ---------------------------------------------------------------------------
+ * rods2D (src/models/rods.jl:61-121) with the Euler integrator: rodForces
+ * (rods.jl:21-59) over @loopOverNeighbors, fx/fy/W/pressure written to their
+ * "__" copies while du reads the committed (lagged) fx, fy, W, then update!
+ * and computeNeighbors! (CellLinked, or all pairs).  The geometry follows
+ * CBMMetrics (src/metrics.jl:137-246) statement by statement.  cos/sin of
+ * theta are the shared series of include/cbm_rng.h on theta/(2 pi) reduced to
+ * [0, 1); x^1.5 is x*sqrt(x) and x^.5 is sqrt(x); in Float32 every constant
+ * is Float32.
+ * ------------------------------------------------------------------------- */
+namespace {
+
+template <typename T>
+T jlMin(T a, T b) {
+  if (std::isnan(a) || std::isnan(b)) return a + b;
+  if (a == b) return std::signbit(b) ? b : a;
+  return b < a ? b : a;
+}
+template <typename T>
+T jlMax(T a, T b) {
+  if (std::isnan(a) || std::isnan(b)) return a + b;
+  if (a == b) return std::signbit(a) ? b : a;
+  return b > a ? b : a;
+}
+
+template <typename T>
+void rodCosSin(T theta, T& c, T& s) {
+  T w = theta * (T)0.15915494309189535;
+  w = w - std::floor(w);
+  if (w >= (T)1) w = w - (T)1;
+  if constexpr (std::is_same<T, double>::value) cbm_cossin_turns_f64(w, &c, &s);
+  else cbm_cossin_turns_f32(w, &c, &s);
+}
+
+/* point2line: projection of (x1, y1) on the line through (x2, y2) at theta2 */
+template <typename T>
+void point2line(T x1, T y1, T x2, T y2, T c2, T s2, T& px, T& py) {
+  T cx = x2 - x1;
+  T cy = y2 - y1;
+  T t = s2 * cx - c2 * cy;
+  px = t * s2 + x1;
+  py = -t * c2 + y1;
+}
+
+/* pointInsideRod: the point clamped to the rod's segment, scaled by sep */
+template <typename T>
+void pointInsideRod(T x1, T y1, T l1, T px, T py, T sep, T& ox, T& oy) {
+  T ex = x1 - px, ey = y1 - py;
+  T d = jlMax(std::sqrt(ex * ex + ey * ey), (T)0.00000001);
+  T ux = (px - x1) / d;
+  T uy = (py - y1) / d;
+  T a = sep * jlMin(d, l1 / (T)2);
+  ox = a * ux + x1;
+  oy = a * uy + y1;
+}
+
+template <typename T>
+void intersection2lines(T x1, T y1, T c1, T s1, T x2, T y2, T c2, T s2, T& px, T& py) {
+  T cx = x1 - x2, cy = y1 - y2;
+  T nrm = c1 * s2 - s1 * c2;
+  if (std::fabs(nrm) > (T)0.0000001) {
+    T sc = (-s2 * cx + c2 * cy) / nrm;
+    px = sc * c1 + x1;
+    py = sc * s1 + y1;
+  } else {
+    px = (x1 + x2) / (T)2;
+    py = (y1 + y2) / (T)2;
+  }
+}
+
+template <typename T>
+void rodIntersection(T x1, T y1, T l1, T c1, T s1, T x2, T y2, T l2, T c2, T s2, T& xa, T& ya,
+                     T& xb, T& yb) {
+  const T sep = (T)0.99;
+  xa = x1; ya = y1; xb = x2; yb = y2;
+  T px, py;
+  intersection2lines(x1, y1, c1, s1, x2, y2, c2, s2, px, py);
+  T e0 = x1 - px, e1 = y1 - py;
+  T d1 = std::sqrt(e0 * e0 + e1 * e1);
+  e0 = x2 - px; e1 = y2 - py;
+  T d2 = std::sqrt(e0 * e0 + e1 * e1);
+  T nrm = c1 * s2 - s1 * c2;
+  if (std::fabs(nrm) < (T)0.000001) {
+    T qx, qy;
+    point2line(px, py, x1, y1, c1, s1, qx, qy);
+    pointInsideRod(x1, y1, l1, qx, qy, sep, xa, ya);
+    point2line(px, py, x2, y2, c2, s2, qx, qy);
+    pointInsideRod(x2, y2, l2, qx, qy, sep, xb, yb);
+  } else if (d1 <= l1 / (T)2 && d2 <= l2 / (T)2) {
+    pointInsideRod(x1, y1, l1, px, py, sep, xa, ya);
+    pointInsideRod(x2, y2, l2, px, py, sep, xb, yb);
+  } else if (d1 <= l1 / (T)2 && d2 > l2 / (T)2) {
+    pointInsideRod(x2, y2, l2, px, py, sep, xb, yb);
+    point2line(xb, yb, x1, y1, c1, s1, xa, ya);
+  } else if (d1 > l1 / (T)2 && d2 <= l2 / (T)2) {
+    pointInsideRod(x1, y1, l1, px, py, sep, xa, ya);
+    point2line(xa, ya, x2, y2, c2, s2, xb, yb);
+  } else {
+    pointInsideRod(x2, y2, l2, px, py, sep, xb, yb);
+    point2line(xb, yb, x1, y1, c1, s1, xa, ya);
+    e0 = x1 - xa; e1 = y1 - ya;
+    d2 = std::sqrt(e0 * e0 + e1 * e1);
+    if (d2 > l1 / (T)2) {
+      pointInsideRod(x1, y1, l1, px, py, sep, xa, ya);
+      T qx, qy;
+      point2line(xa, ya, x2, y2, c2, s2, qx, qy);
+      e0 = x2 - qx; e1 = y2 - qy;
+      d2 = std::sqrt(e0 * e0 + e1 * e1);
+      if (d2 < l2 / (T)2) { xb = qx; yb = qy; }
+    }
+  }
+}
+
+template <typename T>
+struct Rods {
+  cbm_rods_config cfg;
+  int64_t n = 0;
+  std::vector<T> f[CBM_RODS_FIELDS];
+  std::vector<T> cosT, sinT, fx_, fy_, w_, p_;
+  int64_t nc[2] = {1, 1};
+  std::vector<int64_t> cellCount, cellStart, cellAgents;
+};
+
+template <typename T>
+int64_t rodCell(const Rods<T>& R, int64_t i) {
+  const T edge = (T)R.cfg.cell_edge;
+  int64_t px = cellPos1<T>(edge, R.f[CBM_ROD_X][i], (T)R.cfg.box_lo[0], (T)R.cfg.box_hi[0], R.nc[0]);
+  int64_t py = cellPos1<T>(edge, R.f[CBM_ROD_Y][i], (T)R.cfg.box_lo[1], (T)R.cfg.box_hi[1], R.nc[1]);
+  return px + R.nc[0] * py;
+}
+
+/* computeNeighbors! (CellLinked): counts, cumulative sum, rods in index order
+ * inside each cell */
+template <typename T>
+void rodGrid(Rods<T>& R) {
+  if (R.cfg.neighbors != CBM_NEIGH_CELL_LINKED) return;
+  const int64_t ncell = R.nc[0] * R.nc[1];
+  R.cellCount.assign((size_t)ncell, 0);
+  R.cellStart.assign((size_t)ncell + 1, 0);
+  R.cellAgents.assign((size_t)R.n, 0);
+  std::vector<int64_t> cell((size_t)R.n);
+  for (int64_t i = 0; i < R.n; ++i) R.cellCount[cell[i] = rodCell(R, i)]++;
+  for (int64_t c = 0; c < ncell; ++c) R.cellStart[c + 1] = R.cellStart[c] + R.cellCount[c];
+  std::vector<int64_t> fill(R.cellStart.begin(), R.cellStart.end() - 1);
+  for (int64_t i = 0; i < R.n; ++i) R.cellAgents[fill[cell[i]]++] = i;
+}
+
+template <typename T>
+void rodStep(Rods<T>& R) {
+  const int64_t N = R.n;
+  const T kn = (T)R.cfg.kn, gn = (T)R.cfg.gamma_n, gt = (T)R.cfg.gamma_t, mucc = (T)R.cfg.mu_cc;
+  std::vector<T>* F = R.f;
+  for (int64_t i = 0; i < N; ++i) rodCosSin(F[CBM_ROD_THETA][i], R.cosT[i], R.sinT[i]);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < N; ++i) {
+    T sfx = 0, sfy = 0, sw = 0, sp = 0;
+    const T x = F[CBM_ROD_X][i], y = F[CBM_ROD_Y][i], d = F[CBM_ROD_D][i], l = F[CBM_ROD_L][i];
+    const T vx = F[CBM_ROD_VX][i], vy = F[CBM_ROD_VY][i], m = F[CBM_ROD_M][i];
+    auto pair = [&](int64_t j) {
+      if (j == i) return;
+      T xa, ya, xb, yb;
+      rodIntersection(x, y, l, R.cosT[i], R.sinT[i], F[CBM_ROD_X][j], F[CBM_ROD_Y][j],
+                      F[CBM_ROD_L][j], R.cosT[j], R.sinT[j], xa, ya, xb, yb);
+      T rij = std::sqrt((xa - xb) * (xa - xb) + (ya - yb) * (ya - yb));
+      if (!(rij > (T)0 && rij < (d + F[CBM_ROD_D][j]) / (T)2)) return;  // Fij = 0: adds +0
+      T dl = d - rij;
+      T me = m / (T)2;
+      T nx = (xa - xb) / rij;
+      T ny = (ya - yb) / rij;
+      T wx = vx - F[CBM_ROD_VX][j];
+      T wy = vy - F[CBM_ROD_VY][j];
+      T vn = nx * wx + ny * wy;
+      T fn = kn * (dl * std::sqrt(dl)) - gn * me * dl * vn;
+      T ft = -jlMin(gt * me * std::sqrt(dl), mucc * fn);
+      T fx = fn * nx + ft * (wx - vn * nx);
+      T fy = fn * ny + ft * (wy - vn * ny);
+      T w = (xa - x) * fy - (ya - y) * fx;
+      sfx += fx;
+      sfy += fy;
+      sw += w;
+      sp += std::sqrt(fx * fx + fy * fy);
+    };
+    if (R.cfg.neighbors == CBM_NEIGH_FULL) {
+      for (int64_t j = 0; j < N; ++j) pair(j);
+    } else {
+      const int64_t c = rodCell(R, i);
+      const int64_t cx = c % R.nc[0], cy = c / R.nc[0];
+      for (int k = 0; k < 9; ++k) {
+        const int64_t qx = cx + k % 3 - 1, qy = cy + k / 3 - 1;
+        if (qx < 0 || qx >= R.nc[0] || qy < 0 || qy >= R.nc[1]) continue;
+        const int64_t cc = qx + R.nc[0] * qy;
+        for (int64_t s = R.cellStart[cc]; s < R.cellStart[cc + 1]; ++s) pair(R.cellAgents[s]);
+      }
+    }
+    R.fx_[i] = sfx;
+    R.fy_[i] = sfy;
+    R.w_[i] = sw;
+    R.p_[i] = sp;
+  }
+  const T dt = (T)R.cfg.dt, beta = (T)R.cfg.beta, bw = (T)R.cfg.beta_w;
+  for (int64_t i = 0; i < N; ++i) {
+    const T vx = F[CBM_ROD_VX][i], vy = F[CBM_ROD_VY][i], om = F[CBM_ROD_OMEGA][i];
+    const T d = F[CBM_ROD_D][i], l = F[CBM_ROD_L][i], m = F[CBM_ROD_M][i];
+    // du of rods.jl:111-116, then Euler u + dt du (integrators.jl Euler)
+    T ax = -beta * vx + F[CBM_ROD_FX][i] / m;
+    T ay = -beta * vy + F[CBM_ROD_FY][i] / m;
+    T aw = F[CBM_ROD_W][i] / (m * ((d + l) * (d + l)) / (T)12 + m * (d * d)) - bw * om;
+    F[CBM_ROD_X][i] += vx * dt;
+    F[CBM_ROD_Y][i] += vy * dt;
+    F[CBM_ROD_VX][i] = vx + ax * dt;
+    F[CBM_ROD_VY][i] = vy + ay * dt;
+    F[CBM_ROD_THETA][i] += om * dt;
+    F[CBM_ROD_OMEGA][i] = om + aw * dt;
+  }
+  // update!: commit the "__" copies
+  F[CBM_ROD_FX] = R.fx_;
+  F[CBM_ROD_FY] = R.fy_;
+  F[CBM_ROD_W] = R.w_;
+  F[CBM_ROD_PRESSURE] = R.p_;
+  rodGrid(R);
+}
+
+struct RodHandle {
+  int prec;
+  void* p;
+};
+
+}  // namespace
+
+extern "C" {
+
+void* oracle_rods_create(const cbm_rods_config* cfg) {
+  if (!cfg) return nullptr;
+  RodHandle* h = new RodHandle;
+  h->prec = cfg->precision;
+  auto init = [&](auto* R) {
+    R->cfg = *cfg;
+    if (cfg->neighbors == CBM_NEIGH_CELL_LINKED)
+      for (int d = 0; d < 2; ++d)
+        R->nc[d] = (int64_t)std::ceil((cfg->box_hi[d] - cfg->box_lo[d]) / cfg->cell_edge + 2.0);
+  };
+  if (h->prec == CBM_F64) {
+    auto* R = new Rods<double>;
+    init(R);
+    h->p = R;
+  } else {
+    auto* R = new Rods<float>;
+    init(R);
+    h->p = R;
+  }
+  return h;
+}
+
+void oracle_rods_destroy(void* vh) {
+  RodHandle* h = (RodHandle*)vh;
+  if (!h) return;
+  if (h->prec == CBM_F64) delete (Rods<double>*)h->p;
+  else delete (Rods<float>*)h->p;
+  delete h;
+}
+
+/* fields: CBM_ROD_PRESSURE arrays of n (pressure starts at zero) */
+int oracle_rods_upload(void* vh, int64_t n, const void* const* fields) {
+  RodHandle* h = (RodHandle*)vh;
+  auto up = [&](auto* R) {
+    using T = typename std::remove_reference<decltype(R->cosT[0])>::type;
+    R->n = n;
+    for (int q = 0; q < CBM_RODS_FIELDS; ++q) {
+      R->f[q].assign((size_t)n, (T)0);
+      if (q < CBM_ROD_PRESSURE) std::copy((const T*)fields[q], (const T*)fields[q] + n, R->f[q].begin());
+    }
+    for (auto* v : {&R->cosT, &R->sinT, &R->fx_, &R->fy_, &R->w_, &R->p_}) v->assign((size_t)n, (T)0);
+    rodGrid(*R);
+  };
+  if (h->prec == CBM_F64) up((Rods<double>*)h->p);
+  else up((Rods<float>*)h->p);
+  return CBM_OK;
+}
+
+int oracle_rods_step(void* vh, int nsteps) {
+  RodHandle* h = (RodHandle*)vh;
+  for (int s = 0; s < nsteps; ++s) {
+    if (h->prec == CBM_F64) rodStep(*(Rods<double>*)h->p);
+    else rodStep(*(Rods<float>*)h->p);
+  }
+  return CBM_OK;
+}
+
+int oracle_rods_download(void* vh, void* const* fields) {
+  RodHandle* h = (RodHandle*)vh;
+  auto down = [&](auto* R) {
+    using T = typename std::remove_reference<decltype(R->cosT[0])>::type;
+    for (int q = 0; q < CBM_RODS_FIELDS; ++q)
+      if (fields[q]) std::copy(R->f[q].begin(), R->f[q].end(), (T*)fields[q]);
+  };
+  if (h->prec == CBM_F64) down((Rods<double>*)h->p);
+  else down((Rods<float>*)h->p);
+  return CBM_OK;
+}
+
+/* rodForces of one pair, for the pin against a transcription of rods.jl */
+int oracle_rod_pair_f64(const double* a, const double* b, const double* k, double* out) {
+  double c1, s1, c2, s2;
+  rodCosSin(a[4], c1, s1);
+  rodCosSin(b[4], c2, s2);
+  double xa, ya, xb, yb;
+  rodIntersection(a[0], a[1], a[3], c1, s1, b[0], b[1], b[3], c2, s2, xa, ya, xb, yb);
+  out[3] = xa; out[4] = ya; out[5] = xb; out[6] = yb;
+  out[0] = out[1] = out[2] = 0.0;
+  double rij = std::sqrt((xa - xb) * (xa - xb) + (ya - yb) * (ya - yb));
+  if (!(rij > 0.0 && rij < (a[2] + b[2]) / 2.0)) return 0;
+  double dl = a[2] - rij, me = a[7] / 2.0;
+  double nx = (xa - xb) / rij, ny = (ya - yb) / rij;
+  double wx = a[5] - b[5], wy = a[6] - b[6];
+  double vn = nx * wx + ny * wy;
+  double fn = k[0] * (dl * std::sqrt(dl)) - k[1] * me * dl * vn;
+  double ft = -jlMin(k[2] * me * std::sqrt(dl), k[3] * fn);
+  out[0] = fn * nx + ft * (wx - vn * nx);
+  out[1] = fn * ny + ft * (wy - vn * ny);
+  out[2] = (xa - a[0]) * out[1] - (ya - a[1]) * out[0];
+  return 1;
+}
+
+}  // extern "C"

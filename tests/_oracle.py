@@ -55,6 +55,12 @@ def load_oracle(abi):
         "oracle_medium_upload": (C.c_int, [vp, vp, vp]),
         "oracle_medium_step": (C.c_int, [vp, C.c_int]),
         "oracle_medium_download": (C.c_int, [vp, vp, C.POINTER(dbl)]),
+        "oracle_rods_create": (vp, [C.POINTER(abi.CbmRodsConfig)]),
+        "oracle_rods_destroy": (None, [vp]),
+        "oracle_rods_upload": (C.c_int, [vp, C.c_int64, C.POINTER(vp)]),
+        "oracle_rods_step": (C.c_int, [vp, C.c_int]),
+        "oracle_rods_download": (C.c_int, [vp, C.POINTER(vp)]),
+        "oracle_rod_pair_f64": (C.c_int, [C.POINTER(dbl)] * 4),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -223,3 +229,48 @@ class OracleMedium:
         t = C.c_double()
         self.lib.oracle_medium_download(self.h, out.ctypes.data, C.byref(t))
         return out, t.value
+
+
+class OracleRods:
+    """The rods2D Euler step of the checker, with Rods2D's methods."""
+
+    def __init__(self, abi, cfg):
+        self.abi = abi
+        self.lib = load_oracle(abi)
+        self.h = self.lib.oracle_rods_create(C.byref(cfg))
+        self.dtype = np.float64 if cfg.precision == abi.F64 else np.float32
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.oracle_rods_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def upload(self, state):
+        cols = [state[k] for k in self.abi.ROD_FIELDS[:12]]
+        arrs = [np.ascontiguousarray(c, dtype=self.dtype) for c in cols]
+        self.n = len(arrs[0])
+        ptrs = (C.c_void_p * 13)(*([a.ctypes.data for a in arrs] + [None]))
+        self.lib.oracle_rods_upload(self.h, self.n, ptrs)
+
+    def step(self, n):
+        self.lib.oracle_rods_step(self.h, n)
+
+    def download(self):
+        out = np.zeros((13, self.n), self.dtype)
+        ptrs = (C.c_void_p * 13)(*[out[q].ctypes.data for q in range(13)])
+        self.lib.oracle_rods_download(self.h, ptrs)
+        return {k: out[q] for q, k in enumerate(self.abi.ROD_FIELDS)}
+
+
+def oracle_rod_pair(abi, a, b, k):
+    """rodForces of one pair (a, b: x, y, d, l, theta, vx, vy, m; k: kn, γn,
+    γt, μcc) in Float64: (contact, [Fx, Fy, W, xi, yi, xj, yj])."""
+    lib = load_oracle(abi)
+    arr = [np.ascontiguousarray(v, dtype=np.float64) for v in (a, b, k)]
+    out = np.zeros(7)
+    dp = C.POINTER(C.c_double)
+    c = lib.oracle_rod_pair_f64(*(v.ctypes.data_as(dp) for v in arr), out.ctypes.data_as(dp))
+    return bool(c), out

@@ -60,3 +60,19 @@ def test_create_rejects_capacities_beyond_the_fate_scan():
     rc = lib.cbm_create(C2.byref(h), C2.byref(cfg))
     assert rc == 1  # CBM_ERR_ARG
     assert b"2^28" in lib.cbm_last_error(None)
+
+
+def test_rods_create_rejects_bad_configurations():
+    """cbm_rods_create checks its configuration before any CUDA call."""
+    import pytest
+    abi = conftest.cbm._abi
+    base = dict(n_max=8, box_lo=(-5.0, -5.0), box_hi=(5.0, 5.0), dt=1e-4, kn=1.0, gamma_n=1.0,
+                gamma_t=1.0, mu_cc=0.1, beta=0.8, beta_w=0.8, cell_edge=3.0)
+    bad = [dict(neighbors=abi.NEIGH_VERLET_DISPLACEMENT), dict(neighbors=abi.NEIGH_NONE),
+           dict(cell_edge=0.0), dict(dt=0.0), dict(n_max=0), dict(box_hi=(-5.0, 5.0)),
+           dict(precision=7)]
+    for change in bad:
+        kw = dict(base, **change)
+        with pytest.raises(abi.CbmError) as e:
+            abi.Rods2D(abi.make_rods_config(**kw))
+        assert e.value.code == abi.CBM_ERR_ARG, change

@@ -1,0 +1,287 @@
+"""The checker's rods2D restatement against a plain-Python transcription of the
+reference's rod model, statement by statement:
+rodForces (src/models/rods.jl:21-59), the rods2D agentODE (rods.jl:86-118)
+and CBMMetrics' geometry (src/metrics.jl:137-246).
+
+The reference ships no rod tests or fixtures, so this transcription is the pin.
+The transcription follows the Julia text with this build's definitions:
+cos and sin come from the shared series on theta / (2 pi) reduced to [0, 1),
+and x^1.5 is x * sqrt(x).  Python floats are IEEE doubles and Python does no
+contraction, so the Float64 comparisons are bit-exact.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from conftest import cbm
+from _oracle import OracleRods, load_oracle, oracle_rod_pair
+
+abi = cbm._abi
+
+
+def _cossin(theta):
+    lib = load_oracle(abi)
+    w = theta * 0.15915494309189535
+    w = w - math.floor(w)
+    if w >= 1.0:
+        w = w - 1.0
+    c, s = C.c_double(), C.c_double()
+    lib.oracle_cossin_f64(w, C.byref(c), C.byref(s))
+    return c.value, s.value
+
+
+def jl_min(a, b):
+    if a != a or b != b:
+        return a + b
+    if a == b:
+        return b if math.copysign(1.0, b) < 0 else a
+    return b if b < a else a
+
+
+def jl_max(a, b):
+    if a != a or b != b:
+        return a + b
+    if a == b:
+        return b if math.copysign(1.0, a) < 0 else a
+    return b if b > a else a
+
+
+# --- CBMMetrics (src/metrics.jl) ------------------------------------------------
+def intersection2lines(x1, y1, t1, x2, y2, t2):
+    c1, s1 = _cossin(t1)
+    c2, s2 = _cossin(t2)
+    cx = x1 - x2
+    cy = y1 - y2
+    norm = c1 * s2 - s1 * c2
+    if abs(norm) > 0.0000001:
+        scale = (-s2 * cx + c2 * cy) / norm
+        return scale * c1 + x1, scale * s1 + y1
+    return (x1 + x2) / 2, (y1 + y2) / 2
+
+
+def point2line(x1, y1, x2, y2, t2):
+    c2, s2 = _cossin(t2)
+    cx = x2 - x1
+    cy = y2 - y1
+    return (s2 * cx - c2 * cy) * s2 + x1, -(s2 * cx - c2 * cy) * c2 + y1
+
+
+def point_inside_rod(x1, y1, l1, t1, px, py, sep):
+    di = jl_max(math.sqrt((x1 - px) * (x1 - px) + (y1 - py) * (y1 - py)), 0.00000001)
+    dxi = (px - x1) / di
+    dyi = (py - y1) / di
+    return sep * jl_min(di, l1 / 2) * dxi + x1, sep * jl_min(di, l1 / 2) * dyi + y1
+
+
+def rod_intersection(x1, y1, l1, t1, x2, y2, l2, t2, sep=0.99):
+    x1a, y1a, x2a, y2a = x1, y1, x2, y2
+    px, py = intersection2lines(x1, y1, t1, x2, y2, t2)
+    di = math.sqrt((x1 - px) * (x1 - px) + (y1 - py) * (y1 - py))
+    dj = math.sqrt((x2 - px) * (x2 - px) + (y2 - py) * (y2 - py))
+    c1, s1 = _cossin(t1)
+    c2, s2 = _cossin(t2)
+    norm = c1 * s2 - s1 * c2
+    if abs(norm) < 0.000001:
+        x1a, y1a = point2line(px, py, x1, y1, t1)
+        x1a, y1a = point_inside_rod(x1, y1, l1, t1, x1a, y1a, sep)
+        x2a, y2a = point2line(px, py, x2, y2, t2)
+        x2a, y2a = point_inside_rod(x2, y2, l2, t2, x2a, y2a, sep)
+    elif di <= l1 / 2 and dj <= l2 / 2:
+        x1a, y1a = point_inside_rod(x1, y1, l1, t1, px, py, sep)
+        x2a, y2a = point_inside_rod(x2, y2, l2, t2, px, py, sep)
+    elif di <= l1 / 2 and dj > l2 / 2:
+        x2a, y2a = point_inside_rod(x2, y2, l2, t2, px, py, sep)
+        x1a, y1a = point2line(x2a, y2a, x1, y1, t1)
+    elif di > l1 / 2 and dj <= l2 / 2:
+        x1a, y1a = point_inside_rod(x1, y1, l1, t1, px, py, sep)
+        x2a, y2a = point2line(x1a, y1a, x2, y2, t2)
+    else:
+        x2a, y2a = point_inside_rod(x2, y2, l2, t2, px, py, sep)
+        x1a, y1a = point2line(x2a, y2a, x1, y1, t1)
+        dj = math.sqrt((x1 - x1a) * (x1 - x1a) + (y1 - y1a) * (y1 - y1a))
+        if dj > l1 / 2:
+            x1a, y1a = point_inside_rod(x1, y1, l1, t1, px, py, sep)
+            x2b, y2b = point2line(x1a, y1a, x2, y2, t2)
+            dj = math.sqrt((x2 - x2b) * (x2 - x2b) + (y2 - y2b) * (y2 - y2b))
+            if dj < l2 / 2:
+                x2a, y2a = x2b, y2b
+    return x1a, y1a, x2a, y2a
+
+
+# --- rodForces (src/models/rods.jl:21-59) ----------------------------------------
+def rod_forces(x, y, d, l, th, vx, vy, m, x2, y2, d2, l2, th2, vx2, vy2, kn, gn, gt, mucc,
+               pow15=lambda v: v * math.sqrt(v)):
+    fx = fy = w = 0.0
+    xi, yi, xj, yj = rod_intersection(x, y, l, th, x2, y2, l2, th2)
+    rij = math.sqrt((xi - xj) * (xi - xj) + (yi - yj) * (yi - yj))
+    if rij > 0.0 and rij < (d + d2) / 2:
+        delta = d - rij
+        me = m / 2
+        nx = (xi - xj) / rij
+        ny = (yi - yj) / rij
+        vijx = vx - vx2
+        vijy = vy - vy2
+        vn = nx * vijx + ny * vijy
+        fn = kn * pow15(delta) - gn * me * delta * vn
+        ft = -jl_min(gt * me * math.sqrt(delta), mucc * fn)
+        fx = fn * nx + ft * (vijx - vn * nx)
+        fy = fn * ny + ft * (vijy - vn * ny)
+        w = (xi - x) * fy - (yi - y) * fx
+    return fx, fy, w, (xi, yi, xj, yj)
+
+
+K = dict(kn=2.0e6, gn=100.0, gt=20.0, mucc=0.1)
+
+
+def _pairs(seed, n):
+    """Pairs of rods at contact range in all the geometric cases: crossing,
+    T-shaped, end to end, side by side, exactly and nearly parallel."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        d, l = rng.uniform(0.8, 1.2), rng.uniform(1.0, 4.0)
+        # d2 <= d: with d2 > d a contact can have delta = d - rij < 0, where
+        # Julia's delta^1.5 raises a DomainError
+        d2, l2 = rng.uniform(0.8, 1.0) * d, rng.uniform(1.0, 4.0)
+        th = rng.uniform(-7.0, 7.0)
+        kind = q % 5
+        if kind == 3:
+            th2 = th
+        elif kind == 4:
+            th2 = th + rng.uniform(-1e-6, 1e-6)
+        else:
+            th2 = rng.uniform(-7.0, 7.0)
+        r = rng.uniform(0.0, (l + l2) / 2 + 1.0)
+        phi = rng.uniform(0, 2 * math.pi)
+        a = [0.3, -0.2, d, l, th, rng.normal(), rng.normal(), rng.uniform(0.5, 2.0)]
+        b = [0.3 + r * math.cos(phi), -0.2 + r * math.sin(phi), d2, l2, th2, rng.normal(),
+             rng.normal(), rng.uniform(0.5, 2.0)]
+        out.append((a, b))
+    return out
+
+
+def test_rod_pair_matches_transcription():
+    k = [K["kn"], K["gn"], K["gt"], K["mucc"]]
+    contacts = 0
+    for a, b in _pairs(7, 600):
+        hit, got = oracle_rod_pair(abi, a, b, k)
+        fx, fy, w, pts = rod_forces(*a, *b[:7], **K)
+        assert list(got[3:]) == list(pts), (a, b)
+        assert (got[0], got[1], got[2]) == (fx, fy, w), (a, b)
+        contacts += hit
+    assert contacts > 100  # the cases reach contact
+
+
+def test_pow15_definition_close_to_julia_pow():
+    """x^1.5 as x*sqrt(x) differs from a correctly rounded pow by an ulp or so."""
+    for a, b in _pairs(8, 300):
+        f1 = rod_forces(*a, *b[:7], **K)
+        f2 = rod_forces(*a, *b[:7], **K, pow15=lambda v: v ** 1.5)
+        for u, v in zip(f1[:3], f2[:3]):
+            assert u == pytest.approx(v, rel=1e-12, abs=1e-9)
+
+
+def _colony(n, seed, box=12.0):
+    rng = np.random.default_rng(seed)
+    st = {k: np.zeros(n) for k in abi.ROD_FIELDS}
+    st["x"] = rng.uniform(-box, box, n)
+    st["y"] = rng.uniform(-box, box, n)
+    st["vx"] = rng.normal(0, 0.1, n)
+    st["vy"] = rng.normal(0, 0.1, n)
+    st["theta"] = rng.uniform(-math.pi, math.pi, n)
+    st["omega"] = rng.normal(0, 0.1, n)
+    st["d"] = np.full(n, 1.0)
+    st["l"] = rng.uniform(1.0, 3.0, n)
+    st["m"] = rng.uniform(0.8, 1.2, n)
+    return st
+
+
+PARAMS = dict(dt=1e-4, kn=2.0e6, gamma_n=100.0, gamma_t=20.0, mu_cc=0.1, beta=0.8, beta_w=0.8)
+BOX_LO, BOX_HI = (-14.0, -14.0), (14.0, 14.0)
+
+
+def _cell_of(x, lo, hi, edge, n):
+    # cellPos (src/neighbors.jl:636-638), 0-based, with Julia's float ÷
+    if x > hi:
+        return n - 1
+    if not (x >= lo):
+        return 0
+    a = x - lo
+    p = int(round((a - math.fmod(a, edge)) / edge)) + 1
+    return min(p, n - 1)
+
+
+def _py_step(st, neighbors, edge):
+    """One step!: agentStepDE! (Euler over rods2D's agentODE), update!,
+    with neighbors walked as @loopOverNeighbors does."""
+    n = len(st["x"])
+    f = {k: list(map(float, v)) for k, v in st.items()}
+    order = list(range(n))
+    if neighbors == abi.NEIGH_CELL_LINKED:
+        nc = [math.ceil((BOX_HI[d] - BOX_LO[d]) / edge + 2) for d in range(2)]
+        cell = [_cell_of(f["x"][i], BOX_LO[0], BOX_HI[0], edge, nc[0])
+                + nc[0] * _cell_of(f["y"][i], BOX_LO[1], BOX_HI[1], edge, nc[1]) for i in range(n)]
+        members = {}
+        for i in range(n):
+            members.setdefault(cell[i], []).append(i)
+    new = {k: [0.0] * n for k in ("fx", "fy", "W", "pressure")}
+    for i in range(n):
+        if neighbors == abi.NEIGH_FULL:
+            cand = order
+        else:
+            cx, cy = cell[i] % nc[0], cell[i] // nc[0]
+            cand = []
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    qx, qy = cx + dx, cy + dy
+                    if 0 <= qx < nc[0] and 0 <= qy < nc[1]:
+                        cand += members.get(qx + nc[0] * qy, [])
+        fx = fy = w = p = 0
+        for j in cand:
+            if j == i:
+                continue
+            a, b, c, _ = rod_forces(f["x"][i], f["y"][i], f["d"][i], f["l"][i], f["theta"][i],
+                                    f["vx"][i], f["vy"][i], f["m"][i], f["x"][j], f["y"][j],
+                                    f["d"][j], f["l"][j], f["theta"][j], f["vx"][j], f["vy"][j],
+                                    PARAMS["kn"], PARAMS["gamma_n"], PARAMS["gamma_t"],
+                                    PARAMS["mu_cc"])
+            fx += a
+            fy += b
+            w += c
+            p += math.sqrt(a * a + b * b)
+        new["fx"][i], new["fy"][i], new["W"][i], new["pressure"][i] = fx, fy, w, p
+    dt, beta, bw = PARAMS["dt"], PARAMS["beta"], PARAMS["beta_w"]
+    out = {k: list(v) for k, v in f.items()}
+    for i in range(n):
+        vx, vy, om = f["vx"][i], f["vy"][i], f["omega"][i]
+        d, l, m = f["d"][i], f["l"][i], f["m"][i]
+        out["x"][i] = f["x"][i] + vx * dt
+        out["y"][i] = f["y"][i] + vy * dt
+        out["vx"][i] = vx + (-beta * vx + f["fx"][i] / m) * dt
+        out["vy"][i] = vy + (-beta * vy + f["fy"][i] / m) * dt
+        out["theta"][i] = f["theta"][i] + om * dt
+        out["omega"][i] = om + (f["W"][i] / (m * ((d + l) * (d + l)) / 12 + m * (d * d)) - bw * om) * dt
+    for k in new:
+        out[k] = new[k]
+    return {k: np.array(v) for k, v in out.items()}
+
+
+@pytest.mark.parametrize("neighbors", ["full", "cell_linked"])
+def test_rods_step_matches_transcription(neighbors):
+    nb = abi.NEIGH_FULL if neighbors == "full" else abi.NEIGH_CELL_LINKED
+    edge = 4.0
+    st = _colony(60, 3, box=6.0)
+    cfg = abi.make_rods_config(60, BOX_LO, BOX_HI, cell_edge=edge, neighbors=nb,
+                               precision=abi.F64, **PARAMS)
+    orc = OracleRods(abi, cfg)
+    orc.upload(st)
+    ref = {k: np.asarray(v, dtype=float) for k, v in st.items()}
+    for _ in range(3):
+        ref = _py_step(ref, nb, edge)
+        orc.step(1)
+        got = orc.download()
+        for k in abi.ROD_FIELDS:
+            np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+    assert np.count_nonzero(ref["pressure"]) > 10  # rods are in contact
