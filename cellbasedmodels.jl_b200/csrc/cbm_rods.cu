@@ -2,15 +2,26 @@
 //
 // One step, as step! runs rods2D with the Euler integrator:
 //   1. agentStepDE!: every rod sums rodForces over its neighbors (the
-//      CellLinked grid of the committed positions, 9 cells x fastest, rods
+//      CellLinked grid of the committed positions: 9 cells x fastest, rods
 //      ascending inside a cell; or all rods) into the new copies fx__, fy__,
-//      W__, pressure__, then u += du dt with du from the committed (lagged)
-//      fx, fy, W (k_rod_forces, then k_rod_update);
-//   2. update!: the new copies are committed (k_rod_update);
-//   3. computeNeighbors!: the grid is rebuilt on the new positions
-//      (the stable counting sort of cbm_grid.cuh).
-// Rods stay in index order (no division or death in rods2D).  The force
+//      W__, pressure__, while u += du dt takes du from the committed (lagged)
+//      fx, fy, W;
+//   2. update!: the new copies are committed;
+//   3. computeNeighbors!: the grid is rebuilt on the new positions.
+// Rods stay in index order (rods2D has no division or death).  The force
 // arithmetic is cbm_rods_math.h.
+//
+// The state is double-buffered: k_rod_step reads buffer a (committed) and
+// writes buffer b, so 1 and 2 are one launch and the commit is a swap.  The
+// same launch computes the cell of each new position and its atomic rank
+// (assignCells); the scan, scatter and stable passes of cbm_grid.cuh finish
+// the grid.  Four launches per step, replayed from a CUDA graph of two steps.
+//
+// A rod's candidates are spread over a group of kRodLanes lanes: lane k takes
+// candidates k, k + G, ...; after each chunk of G the group's terms are
+// broadcast by shuffles and every lane adds them in candidate order, so the
+// sums have the reference's order.  Only contacts add (a pair without contact
+// contributes +0.0, which leaves a sum started at +0.0 unchanged).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -25,104 +36,158 @@ using namespace cbm;
 
 namespace {
 
+constexpr int kRodBlock = 128;
+#ifndef CBM_ROD_LANES
+#define CBM_ROD_LANES 8
+#endif
+constexpr int kRodLanes = CBM_ROD_LANES;  // lanes per rod
+static_assert(kRodLanes == 4 || kRodLanes == 8 || kRodLanes == 16, "lanes per rod");
+
+// the per-rod arrays that a step rewrites (the rest, d, l, m, are constant)
+enum { kSX = 0, kSY, kSVX, kSVY, kSTH, kSOM, kSFX, kSFY, kSW, kSP, kSCOS, kSSIN, kStateArrays };
+
 template <typename T>
-struct RodParams {
-  T* f[CBM_RODS_FIELDS];     // committed fields, index order
-  T* fnew[4];                // fx__, fy__, W__, pressure__
-  T* cs[2];                  // cos, sin of theta
-  const int* cell_start;     // n_cells + 1
+struct RodStep {
+  T* a[kStateArrays];  // committed
+  T* b[kStateArrays];  // written
+  const T* d;
+  const T* l;
+  const T* m;
+  const int* cell_start;  // grid of a
   const int* cell_agents;
+  int* cell_count;        // zero on entry (the scan clears it)
+  int* agent_cell;        // cell and rank of b's positions
+  int* agent_rank;
+  Counters* ctr;
   int n;
-  int full;                  // all pairs instead of the grid
+  int full;               // all pairs instead of the grid
   T box_lo[2], box_hi[2], edge;
   int n_cells_d[3];
   T dt, beta, beta_w;
   CbmRodCoef<T> k;
 };
 
+// cos and sin of the uploaded angles
 template <typename T>
-__global__ void __launch_bounds__(kTile) k_rod_geom(RodParams<T> R) {
+__global__ void __launch_bounds__(kTile) k_rod_geom(T* const* a, int n) {
   const int i = blockIdx.x * kTile + threadIdx.x;
-  if (i >= R.n) return;
+  if (i >= n) return;
   T c, s;
-  cbm_rod_cossin<T>(R.f[CBM_ROD_THETA][i], &c, &s);
-  R.cs[0][i] = c;
-  R.cs[1][i] = s;
+  cbm_rod_cossin<T>(a[kSTH][i], &c, &s);
+  a[kSCOS][i] = c;
+  a[kSSIN][i] = s;
 }
 
-// the neighbor sum of rod i (@loopOverNeighbors with rodForces, rods.jl:94-111)
 template <typename T>
-__global__ void __launch_bounds__(kTile) k_rod_forces(RodParams<T> R) {
-  const int i = blockIdx.x * kTile + threadIdx.x;
-  if (i >= R.n) return;
-  const CbmRodGeom<T> a{R.f[CBM_ROD_X][i], R.f[CBM_ROD_Y][i], R.cs[0][i], R.cs[1][i],
-                        R.f[CBM_ROD_L][i]};
-  const T d1 = R.f[CBM_ROD_D][i], m1 = R.f[CBM_ROD_M][i];
-  const T vx1 = R.f[CBM_ROD_VX][i], vy1 = R.f[CBM_ROD_VY][i];
-  T fx = (T)0, fy = (T)0, w = (T)0, p = (T)0;
-  auto pair = [&](int j) {
-    if (j == i) return;
-    const CbmRodGeom<T> b{R.f[CBM_ROD_X][j], R.f[CBM_ROD_Y][j], R.cs[0][j], R.cs[1][j],
-                          R.f[CBM_ROD_L][j]};
-    T gx, gy, gw;
-    if (!cbm_rod_forces<T>(a, d1, vx1, vy1, m1, b, R.f[CBM_ROD_D][j], R.f[CBM_ROD_VX][j],
-                           R.f[CBM_ROD_VY][j], R.k, &gx, &gy, &gw))
-      return;
-    fx = fx + gx;
-    fy = fy + gy;
-    w = w + gw;
-    p = p + sqrt(gx * gx + gy * gy);
-  };
-  if (R.full) {
-    for (int j = 0; j < R.n; ++j) pair(j);
-  } else {
-    const T x[2] = {a.x, a.y};
-    const int c = cell_of<T, 2>(R.edge, R.box_lo, R.box_hi, R.n_cells_d, x);
-    const int nx = R.n_cells_d[0], ny = R.n_cells_d[1];
-    const int qx = c % nx, qy = c / nx;
-    for (int dy = -1; dy <= 1; ++dy) {
-      const int py = qy + dy;
-      if (py < 0 || py >= ny) continue;
-      for (int dx = -1; dx <= 1; ++dx) {
-        const int px = qx + dx;
-        if (px < 0 || px >= nx) continue;
-        const int cell = px + nx * py;
-        const int s1 = R.cell_start[cell + 1];
-        for (int s = R.cell_start[cell]; s < s1; ++s) pair(R.cell_agents[s]);
+__device__ __forceinline__ T shfl_group(T v, int q) {
+  return __shfl_sync(0xffffffffu, v, q, kRodLanes);
+}
+
+// Steps 1 and 2 of one step (rods.jl:86-118 with rodForces, :21-59), and the
+// cell assignment of step 3 (assignCells, neighbors.jl:763-821)
+template <typename T>
+__global__ void __launch_bounds__(kRodBlock) k_rod_step(RodStep<T> R) {
+  const int t = blockIdx.x * kRodBlock + threadIdx.x;
+  const int i = t / kRodLanes, lane = t % kRodLanes;
+  const bool live = i < R.n;
+  if (t == 0 && !R.full) {
+    R.ctr->scan_ticket = 0u;  // fresh tickets and tile-state generation for the scan
+    R.ctr->scan_epoch = R.ctr->scan_epoch + 1u;
+  }
+  CbmRodGeom<T> g{(T)0, (T)0, (T)1, (T)0, (T)0};
+  T d1 = (T)0, m1 = (T)1, vx1 = (T)0, vy1 = (T)0;
+  if (live) {
+    g = CbmRodGeom<T>{R.a[kSX][i], R.a[kSY][i], R.a[kSCOS][i], R.a[kSSIN][i], R.l[i]};
+    d1 = R.d[i];
+    m1 = R.m[i];
+    vx1 = R.a[kSVX][i];
+    vy1 = R.a[kSVY][i];
+  }
+  // candidate runs: all rods, or the three rows of x-neighbor cells
+  int rs[3] = {0, 0, 0}, re[3] = {0, 0, 0};
+  if (live) {
+    if (R.full) {
+      re[0] = R.n;
+    } else {
+      const T x[2] = {g.x, g.y};
+      const int c = cell_of<T, 2>(R.edge, R.box_lo, R.box_hi, R.n_cells_d, x);
+      const int nx = R.n_cells_d[0], ny = R.n_cells_d[1];
+      const int qx = c % nx, qy = c / nx;
+      const int x0 = qx > 0 ? qx - 1 : 0, x1 = qx < nx - 1 ? qx + 1 : nx - 1;
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const int py = qy + r - 1;
+        if (py < 0 || py >= ny) continue;
+        rs[r] = R.cell_start[nx * py + x0];
+        re[r] = R.cell_start[nx * py + x1 + 1];
       }
     }
   }
-  R.fnew[0][i] = fx;
-  R.fnew[1][i] = fy;
-  R.fnew[2][i] = w;
-  R.fnew[3][i] = p;
-}
-
-// Euler over the ODE of rods2D (rods.jl:113-118) with the committed forces,
-// then update!: the new copies become the committed fx, fy, W, pressure
-template <typename T>
-__global__ void __launch_bounds__(kTile) k_rod_update(RodParams<T> R) {
-  const int i = blockIdx.x * kTile + threadIdx.x;
-  if (i >= R.n) return;
+  const int group_shift = (threadIdx.x & 31) & ~(kRodLanes - 1);
+  T fx = (T)0, fy = (T)0, w = (T)0, p = (T)0;
+#pragma unroll 1
+  for (int r = 0; r < 3; ++r) {
+    const int chunks = __reduce_max_sync(0xffffffffu, (re[r] - rs[r] + kRodLanes - 1) / kRodLanes);
+#pragma unroll 1
+    for (int c = 0; c < chunks; ++c) {
+      const int s = rs[r] + c * kRodLanes + lane;
+      bool hit = false;
+      T gx = (T)0, gy = (T)0, gw = (T)0, gp = (T)0;
+      if (s < re[r]) {
+        const int j = R.full ? s : R.cell_agents[s];
+        if (j != i) {
+          const CbmRodGeom<T> h{R.a[kSX][j], R.a[kSY][j], R.a[kSCOS][j], R.a[kSSIN][j], R.l[j]};
+          hit = cbm_rod_forces<T>(g, d1, vx1, vy1, m1, h, R.d[j], R.a[kSVX][j], R.a[kSVY][j], R.k,
+                                  &gx, &gy, &gw);
+          if (hit) gp = sqrt(gx * gx + gy * gy);
+        }
+      }
+      const unsigned hits = __ballot_sync(0xffffffffu, hit);
+      if (hits == 0u) continue;
+      const unsigned mine = (hits >> group_shift) & ((1u << kRodLanes) - 1u);
+#pragma unroll
+      for (int q = 0; q < kRodLanes; ++q) {
+        const T ax = shfl_group(gx, q), ay = shfl_group(gy, q);
+        const T aw = shfl_group(gw, q), ap = shfl_group(gp, q);
+        if (mine & (1u << q)) {
+          fx = fx + ax;
+          fy = fy + ay;
+          w = w + aw;
+          p = p + ap;
+        }
+      }
+    }
+  }
+  if (!live || lane != 0) return;
+  // Euler: u + du dt with the committed forces, then the commit of the sums
   const T dt = R.dt;
-  const T x = R.f[CBM_ROD_X][i], y = R.f[CBM_ROD_Y][i];
-  const T vx = R.f[CBM_ROD_VX][i], vy = R.f[CBM_ROD_VY][i];
-  const T th = R.f[CBM_ROD_THETA][i], om = R.f[CBM_ROD_OMEGA][i];
-  const T d = R.f[CBM_ROD_D][i], l = R.f[CBM_ROD_L][i], m = R.f[CBM_ROD_M][i];
-  const T dvx = -R.beta * vx + R.f[CBM_ROD_FX][i] / m;
-  const T dvy = -R.beta * vy + R.f[CBM_ROD_FY][i] / m;
+  const T vx = vx1, vy = vy1, om = R.a[kSOM][i], th = R.a[kSTH][i];
+  const T d = d1, l = g.l, m = m1;
+  const T dvx = -R.beta * vx + R.a[kSFX][i] / m;
+  const T dvy = -R.beta * vy + R.a[kSFY][i] / m;
   const T den = (m * ((d + l) * (d + l))) / (T)12 + m * (d * d);
-  const T dom = R.f[CBM_ROD_W][i] / den - R.beta_w * om;
-  R.f[CBM_ROD_X][i] = x + vx * dt;
-  R.f[CBM_ROD_Y][i] = y + vy * dt;
-  R.f[CBM_ROD_VX][i] = vx + dvx * dt;
-  R.f[CBM_ROD_VY][i] = vy + dvy * dt;
-  R.f[CBM_ROD_THETA][i] = th + om * dt;
-  R.f[CBM_ROD_OMEGA][i] = om + dom * dt;
-  R.f[CBM_ROD_FX][i] = R.fnew[0][i];
-  R.f[CBM_ROD_FY][i] = R.fnew[1][i];
-  R.f[CBM_ROD_W][i] = R.fnew[2][i];
-  R.f[CBM_ROD_PRESSURE][i] = R.fnew[3][i];
+  const T dom = R.a[kSW][i] / den - R.beta_w * om;
+  const T xn = g.x + vx * dt, yn = g.y + vy * dt, thn = th + om * dt;
+  R.b[kSX][i] = xn;
+  R.b[kSY][i] = yn;
+  R.b[kSVX][i] = vx + dvx * dt;
+  R.b[kSVY][i] = vy + dvy * dt;
+  R.b[kSTH][i] = thn;
+  R.b[kSOM][i] = om + dom * dt;
+  R.b[kSFX][i] = fx;
+  R.b[kSFY][i] = fy;
+  R.b[kSW][i] = w;
+  R.b[kSP][i] = p;
+  T cn, sn;
+  cbm_rod_cossin<T>(thn, &cn, &sn);
+  R.b[kSCOS][i] = cn;
+  R.b[kSSIN][i] = sn;
+  if (!R.full) {
+    const T x[2] = {xn, yn};
+    const int c = cell_of<T, 2>(R.edge, R.box_lo, R.box_hi, R.n_cells_d, x);
+    R.agent_cell[i] = c;
+    R.agent_rank[i] = atomicAdd(R.cell_count + c, 1);
+  }
 }
 
 }  // namespace
@@ -132,9 +197,10 @@ struct cbm_rods {
   int tsize = 4;
   cudaStream_t stream = nullptr;
   int n = 0;
-  void* f[CBM_RODS_FIELDS] = {};
-  void* fnew[4] = {};
-  void* cs[2] = {};
+  int cur = 0;                       // buffer holding the committed state
+  void* st[2][kStateArrays] = {};    // double-buffered per-rod arrays
+  void* dlm[3] = {};                 // d, l, m
+  void** ptrs = nullptr;             // device copy of st (for k_rod_geom)
   // grid (CellLinked)
   int n_cells_d[3] = {1, 1, 1};
   int n_cells = 1;
@@ -146,6 +212,7 @@ struct cbm_rods {
   int* cell_tmp = nullptr;
   int* cell_agents = nullptr;
   unsigned long long* scan_state = nullptr;
+  cudaGraphExec_t pair_graph[2] = {nullptr, nullptr};  // two steps starting at cur = 0 / 1
   bool loaded = false;
   std::string err;
 };
@@ -167,56 +234,53 @@ int rfail(cbm_rods* r, int code, const std::string& msg) {
       return rfail(r, CBM_ERR_CUDA, std::string(#call) + " failed: " + cudaGetErrorString(e_)); \
   } while (0)
 
+void drop_graphs(cbm_rods* r) {
+  for (cudaGraphExec_t& g : r->pair_graph)
+    if (g) cudaGraphExecDestroy(g), g = nullptr;
+}
+
 void rfree(cbm_rods* r) {
-  for (void*& p : r->f)
+  drop_graphs(r);
+  for (auto& b : r->st)
+    for (void*& p : b)
+      if (p) cudaFree(p), p = nullptr;
+  for (void*& p : r->dlm)
     if (p) cudaFree(p), p = nullptr;
-  for (void*& p : r->fnew)
-    if (p) cudaFree(p), p = nullptr;
-  for (void*& p : r->cs)
-    if (p) cudaFree(p), p = nullptr;
-  for (void* p : {(void*)r->ctr, (void*)r->cell_count, (void*)r->cell_start, (void*)r->agent_cell,
-                  (void*)r->agent_rank, (void*)r->cell_tmp, (void*)r->cell_agents,
-                  (void*)r->scan_state})
+  for (void* p : {(void*)r->ptrs, (void*)r->ctr, (void*)r->cell_count, (void*)r->cell_start,
+                  (void*)r->agent_cell, (void*)r->agent_rank, (void*)r->cell_tmp,
+                  (void*)r->cell_agents, (void*)r->scan_state})
     if (p) cudaFree(p);
+  r->ptrs = nullptr;
   r->ctr = nullptr;
   if (r->stream) cudaStreamDestroy(r->stream);
   r->stream = nullptr;
 }
 
-template <typename T>
-RodParams<T> rod_params(const cbm_rods* r) {
-  RodParams<T> R;
-  memset(&R, 0, sizeof R);
-  const cbm_rods_config& k = r->cfg;
-  for (int q = 0; q < CBM_RODS_FIELDS; ++q) R.f[q] = (T*)r->f[q];
-  for (int q = 0; q < 4; ++q) R.fnew[q] = (T*)r->fnew[q];
-  R.cs[0] = (T*)r->cs[0];
-  R.cs[1] = (T*)r->cs[1];
-  R.cell_start = r->cell_start;
-  R.cell_agents = r->cell_agents;
-  R.n = r->n;
-  R.full = k.neighbors == CBM_NEIGH_FULL;
-  for (int d = 0; d < 2; ++d) {
-    R.box_lo[d] = (T)k.box_lo[d];
-    R.box_hi[d] = (T)k.box_hi[d];
+// field k of the C ABI (CBM_ROD_*) in buffer `buf`
+void* field_ptr(cbm_rods* r, int buf, int k) {
+  switch (k) {
+    case CBM_ROD_X: return r->st[buf][kSX];
+    case CBM_ROD_Y: return r->st[buf][kSY];
+    case CBM_ROD_VX: return r->st[buf][kSVX];
+    case CBM_ROD_VY: return r->st[buf][kSVY];
+    case CBM_ROD_THETA: return r->st[buf][kSTH];
+    case CBM_ROD_OMEGA: return r->st[buf][kSOM];
+    case CBM_ROD_D: return r->dlm[0];
+    case CBM_ROD_L: return r->dlm[1];
+    case CBM_ROD_M: return r->dlm[2];
+    case CBM_ROD_FX: return r->st[buf][kSFX];
+    case CBM_ROD_FY: return r->st[buf][kSFY];
+    case CBM_ROD_W: return r->st[buf][kSW];
+    default: return r->st[buf][kSP];
   }
-  R.edge = (T)k.cell_edge;
-  for (int d = 0; d < 3; ++d) R.n_cells_d[d] = r->n_cells_d[d];
-  R.dt = (T)k.dt;
-  R.beta = (T)k.beta;
-  R.beta_w = (T)k.beta_w;
-  R.k = CbmRodCoef<T>{(T)k.kn, (T)k.gamma_n, (T)k.gamma_t, (T)k.mu_cc};
-  return R;
 }
 
-// computeNeighbors!: the CellLinked grid of the committed positions
 template <typename T>
-void enqueue_grid(cbm_rods* r) {
-  if (r->cfg.neighbors != CBM_NEIGH_CELL_LINKED) return;
+GridParams<T> grid_params(const cbm_rods* r) {
   GridParams<T> G;
   memset(&G, 0, sizeof G);
-  G.pos[0] = (const T*)r->f[CBM_ROD_X];
-  G.pos[1] = (const T*)r->f[CBM_ROD_Y];
+  G.pos[0] = (const T*)r->st[r->cur][kSX];
+  G.pos[1] = (const T*)r->st[r->cur][kSY];
   for (int d = 0; d < 2; ++d) {
     G.box_lo[d] = (T)r->cfg.box_lo[d];
     G.box_hi[d] = (T)r->cfg.box_hi[d];
@@ -234,8 +298,14 @@ void enqueue_grid(cbm_rods* r) {
   G.agent_rank = r->agent_rank;
   G.cell_tmp = r->cell_tmp;
   G.cell_agents = r->cell_agents;
+  return G;
+}
+
+// computeNeighbors! from scratch on the committed positions (after upload)
+template <typename T>
+void enqueue_full_grid(cbm_rods* r) {
+  const GridParams<T> G = grid_params<T>(r);
   const unsigned nb = (unsigned)(r->n > 0 ? (r->n + kTile - 1) / kTile : 1);
-  cudaMemsetAsync(G.cell_count, 0, (size_t)r->n_cells * 4, r->stream);
   k_grid_hist<T, 2><<<nb, kTile, 0, r->stream>>>(G);
   k_scan_cells<<<G.n_scan_tiles, kTile, 0, r->stream>>>(grid_scan_args(G));
   k_grid_scatter<T><<<nb, kTile, 0, r->stream>>>(G);
@@ -243,14 +313,74 @@ void enqueue_grid(cbm_rods* r) {
 }
 
 template <typename T>
-int enqueue_rod_step(cbm_rods* r) {
-  const RodParams<T> R = rod_params<T>(r);
-  const unsigned nb = (unsigned)(r->n > 0 ? (r->n + kTile - 1) / kTile : 1);
-  k_rod_geom<T><<<nb, kTile, 0, r->stream>>>(R);
-  k_rod_forces<T><<<nb, kTile, 0, r->stream>>>(R);
-  k_rod_update<T><<<nb, kTile, 0, r->stream>>>(R);
-  enqueue_grid<T>(r);
-  ROD_TRY(r, cudaGetLastError());
+void enqueue_rod_step(cbm_rods* r) {
+  RodStep<T> R;
+  memset(&R, 0, sizeof R);
+  const cbm_rods_config& k = r->cfg;
+  for (int q = 0; q < kStateArrays; ++q) {
+    R.a[q] = (T*)r->st[r->cur][q];
+    R.b[q] = (T*)r->st[1 - r->cur][q];
+  }
+  R.d = (const T*)r->dlm[0];
+  R.l = (const T*)r->dlm[1];
+  R.m = (const T*)r->dlm[2];
+  R.cell_start = r->cell_start;
+  R.cell_agents = r->cell_agents;
+  R.cell_count = r->cell_count;
+  R.agent_cell = r->agent_cell;
+  R.agent_rank = r->agent_rank;
+  R.ctr = r->ctr;
+  R.n = r->n;
+  R.full = k.neighbors == CBM_NEIGH_FULL;
+  for (int d = 0; d < 2; ++d) {
+    R.box_lo[d] = (T)k.box_lo[d];
+    R.box_hi[d] = (T)k.box_hi[d];
+  }
+  R.edge = (T)k.cell_edge;
+  for (int d = 0; d < 3; ++d) R.n_cells_d[d] = r->n_cells_d[d];
+  R.dt = (T)k.dt;
+  R.beta = (T)k.beta;
+  R.beta_w = (T)k.beta_w;
+  R.k = CbmRodCoef<T>{(T)k.kn, (T)k.gamma_n, (T)k.gamma_t, (T)k.mu_cc};
+  const long long threads = (long long)(r->n > 0 ? r->n : 1) * kRodLanes;
+  const unsigned nb = (unsigned)((threads + kRodBlock - 1) / kRodBlock);
+  k_rod_step<T><<<nb, kRodBlock, 0, r->stream>>>(R);
+  r->cur = 1 - r->cur;
+  if (!R.full) {
+    // the rest of computeNeighbors! on the new positions
+    const GridParams<T> G = grid_params<T>(r);
+    const unsigned ng = (unsigned)(r->n > 0 ? (r->n + kTile - 1) / kTile : 1);
+    k_scan_cells<<<G.n_scan_tiles, kTile, 0, r->stream>>>(grid_scan_args(G));
+    k_grid_scatter<T><<<ng, kTile, 0, r->stream>>>(G);
+    k_grid_stable<T><<<ng, kTile, 0, r->stream>>>(G);
+  }
+}
+
+void enqueue_one(cbm_rods* r) {
+  if (r->tsize == 8) enqueue_rod_step<double>(r);
+  else enqueue_rod_step<float>(r);
+}
+
+// a graph of two steps starting at the current buffer (which it leaves current)
+int pair_graph(cbm_rods* r, cudaGraphExec_t* out) {
+  cudaGraphExec_t& g = r->pair_graph[r->cur];
+  if (!g) {
+    cudaGraph_t graph = nullptr;
+    ROD_TRY(r, cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_one(r);
+    enqueue_one(r);
+    const cudaError_t e = cudaStreamEndCapture(r->stream, &graph);
+    if (e != cudaSuccess)
+      return rfail(r, CBM_ERR_CUDA, std::string("rods graph capture failed: ") + cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(&g, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+      g = nullptr;
+      return rfail(r, CBM_ERR_CUDA,
+                   std::string("rods graph instantiation failed: ") + cudaGetErrorString(ei));
+    }
+  }
+  *out = g;
   return CBM_OK;
 }
 
@@ -266,7 +396,8 @@ int cbm_rods_create(cbm_rods** out, const cbm_rods_config* cfg) {
     return rfail(nullptr, CBM_ERR_ARG, "precision must be CBM_F32 or CBM_F64");
   if (k.neighbors != CBM_NEIGH_FULL && k.neighbors != CBM_NEIGH_CELL_LINKED)
     return rfail(nullptr, CBM_ERR_ARG, "rods need neighbors CBM_NEIGH_FULL or CBM_NEIGH_CELL_LINKED");
-  if (k.n_max < 1 || k.n_max >= (1ll << 30)) return rfail(nullptr, CBM_ERR_ARG, "n_max must be in [1, 2^30)");
+  if (k.n_max < 1 || k.n_max >= (1ll << 27))
+    return rfail(nullptr, CBM_ERR_ARG, "n_max must be in [1, 2^27)");
   if (!(k.dt > 0)) return rfail(nullptr, CBM_ERR_ARG, "dt must be positive");
   for (int d = 0; d < 2; ++d)
     if (!(k.box_hi[d] > k.box_lo[d])) return rfail(nullptr, CBM_ERR_ARG, "empty simBox");
@@ -280,7 +411,7 @@ int cbm_rods_create(cbm_rods** out, const cbm_rods_config* cfg) {
     }
     long long nc = 1;
     for (int d = 0; d < 2; ++d) {
-      // nCells_ = ceil((hi - lo) / edge + 2), neighbors.jl:605
+      // nCells = ceil((hi - lo) / edge + 2), neighbors.jl:605
       const double v = std::ceil((k.box_hi[d] - k.box_lo[d]) / k.cell_edge + 2.0);
       if (!(v >= 1 && v < 1.0e8)) {
         delete r;
@@ -297,19 +428,28 @@ int cbm_rods_create(cbm_rods** out, const cbm_rods_config* cfg) {
   }
   const size_t n = (size_t)k.n_max, S = (size_t)r->tsize;
   bool ok = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) == cudaSuccess;
-  for (int q = 0; q < CBM_RODS_FIELDS; ++q) ok = ok && cudaMalloc(&r->f[q], n * S) == cudaSuccess;
-  for (int q = 0; q < 4; ++q) ok = ok && cudaMalloc(&r->fnew[q], n * S) == cudaSuccess;
-  for (int q = 0; q < 2; ++q) ok = ok && cudaMalloc(&r->cs[q], n * S) == cudaSuccess;
+  for (auto& b : r->st)
+    for (void*& p : b) ok = ok && cudaMalloc(&p, n * S) == cudaSuccess;
+  for (void*& p : r->dlm) ok = ok && cudaMalloc(&p, n * S) == cudaSuccess;
+  ok = ok && cudaMalloc((void**)&r->ptrs, 2 * kStateArrays * sizeof(void*)) == cudaSuccess;
   const int tiles = (r->n_cells + kScanTile - 1) / kScanTile;
+  // whole scan tiles of counts: the scan loads and clears them as int4
+  const size_t count_ints = (size_t)tiles * kScanTile;
   ok = ok && cudaMalloc((void**)&r->ctr, sizeof(Counters)) == cudaSuccess;
-  ok = ok && cudaMalloc((void**)&r->cell_count, (size_t)r->n_cells * 4) == cudaSuccess;
+  ok = ok && cudaMalloc((void**)&r->cell_count, count_ints * 4) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&r->cell_start, ((size_t)r->n_cells + 1) * 4) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&r->agent_cell, n * 4) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&r->agent_rank, n * 4) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&r->cell_tmp, n * 4) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&r->cell_agents, n * 4) == cudaSuccess;
   ok = ok && cudaMalloc((void**)&r->scan_state, (size_t)tiles * 8) == cudaSuccess;
+  void* host_ptrs[2 * kStateArrays];
+  for (int b = 0; b < 2; ++b)
+    for (int q = 0; q < kStateArrays; ++q) host_ptrs[b * kStateArrays + q] = r->st[b][q];
+  ok = ok && cudaMemcpyAsync(r->ptrs, host_ptrs, sizeof host_ptrs, cudaMemcpyHostToDevice,
+                             r->stream) == cudaSuccess;
   ok = ok && cudaMemsetAsync(r->ctr, 0, sizeof(Counters), r->stream) == cudaSuccess;
+  ok = ok && cudaMemsetAsync(r->cell_count, 0, count_ints * 4, r->stream) == cudaSuccess;
   ok = ok && cudaMemsetAsync(r->scan_state, 0, (size_t)tiles * 8, r->stream) == cudaSuccess;
   ok = ok && cudaStreamSynchronize(r->stream) == cudaSuccess;
   if (!ok) {
@@ -336,13 +476,25 @@ int cbm_rods_upload(cbm_rods* r, int64_t n, const void* const* fields) {
   if (n < 0 || n > r->cfg.n_max) return rfail(r, CBM_ERR_ARG, "n must be in [0, n_max]");
   for (int q = 0; q < CBM_ROD_PRESSURE; ++q)
     if (!fields[q]) return rfail(r, CBM_ERR_ARG, "a rod field is missing");
+  ROD_TRY(r, cudaStreamSynchronize(r->stream));
+  if ((int)n != r->n) drop_graphs(r);  // the graphs hold n in their launch shapes
   r->n = (int)n;
+  r->cur = 0;
   const size_t b = (size_t)n * r->tsize;
-  for (int q = 0; q < CBM_ROD_PRESSURE; ++q)
-    if (b) ROD_TRY(r, cudaMemcpyAsync(r->f[q], fields[q], b, cudaMemcpyHostToDevice, r->stream));
-  if (b) ROD_TRY(r, cudaMemsetAsync(r->f[CBM_ROD_PRESSURE], 0, b, r->stream));
-  if (r->tsize == 8) enqueue_grid<double>(r);
-  else enqueue_grid<float>(r);
+  if (b) {
+    for (int q = 0; q < CBM_ROD_PRESSURE; ++q)
+      ROD_TRY(r, cudaMemcpyAsync(field_ptr(r, 0, q), fields[q], b, cudaMemcpyHostToDevice,
+                                 r->stream));
+    ROD_TRY(r, cudaMemsetAsync(field_ptr(r, 0, CBM_ROD_PRESSURE), 0, b, r->stream));
+  }
+  const unsigned nb = (unsigned)(n > 0 ? (n + kTile - 1) / kTile : 1);
+  if (r->tsize == 8) {
+    k_rod_geom<double><<<nb, kTile, 0, r->stream>>>((double* const*)r->ptrs, (int)n);
+    if (r->cfg.neighbors == CBM_NEIGH_CELL_LINKED) enqueue_full_grid<double>(r);
+  } else {
+    k_rod_geom<float><<<nb, kTile, 0, r->stream>>>((float* const*)r->ptrs, (int)n);
+    if (r->cfg.neighbors == CBM_NEIGH_CELL_LINKED) enqueue_full_grid<float>(r);
+  }
   ROD_TRY(r, cudaGetLastError());
   ROD_TRY(r, cudaStreamSynchronize(r->stream));
   r->loaded = true;
@@ -353,10 +505,17 @@ int cbm_rods_step(cbm_rods* r, int32_t nsteps, int32_t flags) {
   if (!r) return rfail(r, CBM_ERR_ARG, "null rods");
   if (!r->loaded) return rfail(r, CBM_ERR_STATE, "cbm_rods_step before cbm_rods_upload");
   if (nsteps < 0) return rfail(r, CBM_ERR_ARG, "nsteps must be >= 0");
-  for (int s = 0; s < nsteps; ++s) {
-    const int rc = r->tsize == 8 ? enqueue_rod_step<double>(r) : enqueue_rod_step<float>(r);
-    if (rc != CBM_OK) return rc;
+  int s = 0;
+  if (!(flags & CBM_NO_GRAPH)) {
+    for (; s + 2 <= nsteps; s += 2) {
+      cudaGraphExec_t g = nullptr;
+      const int rc = pair_graph(r, &g);
+      if (rc != CBM_OK) return rc;
+      ROD_TRY(r, cudaGraphLaunch(g, r->stream));
+    }
   }
+  for (; s < nsteps; ++s) enqueue_one(r);
+  ROD_TRY(r, cudaGetLastError());
   if (flags & CBM_SYNC) ROD_TRY(r, cudaStreamSynchronize(r->stream));
   return CBM_OK;
 }
@@ -367,7 +526,8 @@ int cbm_rods_download(cbm_rods* r, void* const* fields, int64_t* n_out) {
   const size_t b = (size_t)r->n * r->tsize;
   for (int q = 0; q < CBM_RODS_FIELDS; ++q)
     if (fields[q] && b)
-      ROD_TRY(r, cudaMemcpyAsync(fields[q], r->f[q], b, cudaMemcpyDeviceToHost, r->stream));
+      ROD_TRY(r, cudaMemcpyAsync(fields[q], field_ptr(r, r->cur, q), b, cudaMemcpyDeviceToHost,
+                                 r->stream));
   ROD_TRY(r, cudaStreamSynchronize(r->stream));
   if (n_out) *n_out = r->n;
   return CBM_OK;

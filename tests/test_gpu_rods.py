@@ -30,14 +30,14 @@ def _colony(abi, n, seed, half, spread_out=0.0):
     return st
 
 
-def _compare(abi, cbm, cfg, st, steps):
+def _compare(abi, cbm, cfg, st, steps, flags=None):
     g = cbm._abi.Rods2D(cfg)
     o = OracleRods(abi, cfg)
     g.upload(st)
     o.upload(st)
     contacts = 0
     for s in steps:
-        g.step(s)
+        g.step(s, abi.SYNC if flags is None else flags)
         o.step(s)
         a = g.download()
         b = o.download()
@@ -64,15 +64,17 @@ def test_rods_bitexact(gpu_lib, abi, prec, neighbors):
     assert contacts > n // 3
 
 
+@pytest.mark.parametrize("graph", [True, False])
 @pytest.mark.parametrize("prec", ["f32", "f64"])
-def test_rods_outside_box(gpu_lib, abi, prec):
-    """Rods beyond the simBox fall in the border cells (cellPos clamps)."""
+def test_rods_outside_box(gpu_lib, abi, prec, graph):
+    """Rods beyond the simBox fall in the border cells (cellPos clamps); the
+    steps replayed from the two-step graphs and launched one by one agree."""
     from conftest import cbm
     n = 600
     st = _colony(abi, n, 12, 10.0, spread_out=6.0)
     cfg = abi.make_rods_config(n, (-10.0, -10.0), (10.0, 10.0), cell_edge=3.5,
                                precision=abi.F32 if prec == "f32" else abi.F64, **PARAMS)
-    _compare(abi, cbm, cfg, st, [3, 4])
+    _compare(abi, cbm, cfg, st, [3, 4], flags=abi.SYNC | (0 if graph else abi.NO_GRAPH))
 
 
 def test_rods_large_grid_f32(gpu_lib, abi):

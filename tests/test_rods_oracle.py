@@ -285,3 +285,4 @@ def test_rods_step_matches_transcription(neighbors):
         for k in abi.ROD_FIELDS:
             np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
     assert np.count_nonzero(ref["pressure"]) > 10  # rods are in contact
+
