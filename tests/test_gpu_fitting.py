@@ -41,3 +41,33 @@ def test_batched_grid_search_matches_plain_runs(gpu_lib, abi):
     i = int(np.argmin([r["_score_"] for r in rows]))
     assert (best["k_rep"], best["sigma"], best["_score_"]) == \
         (rows[i]["k_rep"], rows[i]["sigma"], rows[i]["_score_"])
+
+
+def test_swarm_on_batched_evaluator_matches_plain_runs(gpu_lib, abi):
+    """Two generations of swarmAlgorithm, each one batch: every score equals
+    the loss of a plain-path run of that point with the community index the
+    evaluator gave it (generation g, individual i -> g * population + i)."""
+    base, descs, states = batched_sweep(abi, n_comm=1, n_lo=300, n_hi=300, seed=22)
+    st = states[0]
+    L = descs[0]["box_hi"][0]
+    x0 = np.asarray(st["x"], np.float32)
+    defaults = dict(r_rep=2.0, k_att=1.0, r_att=3.0)
+
+    def loss(point, s):
+        return float(np.mean((s["x"] - x0) ** 2))
+
+    ev = cbm.fitting.BatchedEvaluator(abi.make_config(**base), st, loss, 30, (0.0,) * 3,
+                                      (L,) * 3, defaults, tuning=TUNING)
+    rows = cbm.fitting.swarm_algorithm(None, {"k_rep": (5.0, 30.0), "sigma": (0.0, 0.08)},
+                                       population=4, stop_max_generations=2,
+                                       rng=np.random.default_rng(5), evaluate_population=ev,
+                                       return_all=True)
+    assert len(rows) == 8 and ev.calls == 2
+    for c, r in enumerate(rows):
+        desc = dict(n=len(x0), box_lo=(0.0,) * 3, box_hi=(L,) * 3, k_rep=r["k_rep"],
+                    sigma=r["sigma"], community=c, **defaults)
+        g = cbm.Context(abi.make_config(**plain_config_for(abi, base, desc, TUNING)))
+        g.upload(st)
+        g.step(30)
+        assert r["_score_"] == loss(r, g.download()), f"row {c}"
+        g.close()
