@@ -699,6 +699,46 @@ def run_rods(cpu=True, n=32768, steps=200, cpu_steps=3):
     return rec
 
 
+# rods2dGrowth constants of examples/Bacteries.ipynb: growth = 1e-6 sqrt(g d) 1e5,
+# lMax 3, sigma_lTarget 0.2, alpha 50
+ROD_GROWTH = dict(growth=1e-6 * math.sqrt(1e-4) * 1e5, alpha=50.0, sigma_l_target=0.2,
+                  l_max=3.0, seed=2024)
+
+
+def run_rods_growth(n=32768, steps=200):
+    """The rods2dGrowth line: the disc of run_rods with lTarget = l + U(0, 0.02),
+    so that rods divide throughout the timed steps (the notebook's scaling loop
+    times 200 steps of a growing colony at about this size)."""
+    import torch
+    cbm = load_package()
+    abi = cbm._abi
+    st = rod_disc(abi, n)
+    st["l_target"] = st["l"] + np.random.default_rng(5).uniform(0.0, 0.02, n)
+    cfg = abi.make_rods_config(2 * n, (-300.0, -300.0), (300.0, 300.0), cell_edge=4.0,
+                               neighbors=abi.NEIGH_CELL_LINKED, precision=abi.F64,
+                               **ROD_PARAMS, **ROD_GROWTH)
+    g = abi.Rods2D(cfg)
+    g.upload(st)
+    g.step(2)
+    n0 = len(g.download()["x"])
+    rst = torch.cuda.ExternalStream(g.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(rst)
+    g.step(steps, 0)
+    e1.record(rst)
+    e1.synchronize()
+    dev_ms = e0.elapsed_time(e1)
+    n1 = len(g.download()["x"])
+    g.close()
+    return {"workload": f"rods2dGrowth colony, {n} rods at start (the rods2d line's disc), "
+                        f"lTarget = l + U(0, 0.02), examples/Bacteries.ipynb constants, dt 0.1, "
+                        f"CellLinked cellEdge 4, n_max {2 * n}",
+            "dtype": "f64", "rods_start": n0, "rods_end": n1, "steps": steps,
+            "device_ms": round(dev_ms, 3), "ms_per_step": round(dev_ms / steps, 4),
+            "value": round(0.5 * (n0 + n1) * steps / (dev_ms / 1e3), 1), "unit": "rod-steps/s"}
+
+
 def run_configs(args):
     """The other configurations of the path: the 2D aggregation (Float64,
     L2-resident, launch-bound: us/step) and 2D chemotaxis on a 1024^2 medium
@@ -825,6 +865,7 @@ def run_configs(args):
 
     out.update(run_dgadi())
     out["rods2d_colony_32k_f64"] = run_rods()
+    out["rods2d_growth_32k_f64"] = run_rods_growth()
 
     # Error of the Float32 results against Float64 runs, 100 steps.  The noise
     # of an SDE run is drawn in the run's precision (Box-Muller in float or
@@ -945,7 +986,7 @@ def main():
         print(json.dumps({"dgadi": run_dgadi(cpu=False)}))
         return
     if args.rods_only:
-        print(json.dumps({"rods": run_rods(cpu=False)}))
+        print(json.dumps({"rods": run_rods(cpu=False), "rods_growth": run_rods_growth()}))
         return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

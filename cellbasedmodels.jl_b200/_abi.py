@@ -533,7 +533,7 @@ class DGADIMedium:
 
 
 ROD_FIELDS = ("x", "y", "vx", "vy", "theta", "omega", "d", "l", "m", "fx", "fy", "W",
-              "pressure")
+              "pressure", "l_target")
 
 
 class CbmRodsConfig(C.Structure):
@@ -541,14 +541,21 @@ class CbmRodsConfig(C.Structure):
                 ("box_lo", C.c_double * 2), ("box_hi", C.c_double * 2), ("cell_edge", C.c_double),
                 ("dt", C.c_double), ("kn", C.c_double), ("gamma_n", C.c_double),
                 ("gamma_t", C.c_double), ("mu_cc", C.c_double), ("mu_cw", C.c_double),
-                ("beta", C.c_double), ("beta_w", C.c_double)]
+                ("beta", C.c_double), ("beta_w", C.c_double), ("growth_model", C.c_int32),
+                ("pad0", C.c_int32), ("growth", C.c_double), ("alpha", C.c_double),
+                ("sigma_l_target", C.c_double), ("l_max", C.c_double), ("seed", C.c_uint64)]
 
 
 def make_rods_config(n_max, box_lo, box_hi, dt, kn, gamma_n, gamma_t, mu_cc, beta, beta_w,
-                     mu_cw=0.0, cell_edge=0.0, neighbors=NEIGH_CELL_LINKED, precision=F64):
+                     mu_cw=0.0, cell_edge=0.0, neighbors=NEIGH_CELL_LINKED, precision=F64,
+                     growth=None, alpha=0.0, sigma_l_target=0.0, l_max=0.0, seed=0):
     """A cbm_rods_config: the model parameters of rods2D (kn, γn, γt, μcc, μcw,
-    β, βω), its simBox and the CellLinked cell edge."""
+    β, βω), its simBox and the CellLinked cell edge; with `growth` given, the
+    rods2dGrowth model (growth, α, σlTarget, lMax) and the seed of its draws."""
     k = CbmRodsConfig()
+    if growth is not None:
+        k.growth_model, k.growth, k.alpha = 1, float(growth), float(alpha)
+        k.sigma_l_target, k.l_max, k.seed = float(sigma_l_target), float(l_max), int(seed)
     k.precision, k.neighbors, k.n_max = precision, neighbors, int(n_max)
     for d in range(2):
         k.box_lo[d], k.box_hi[d] = float(box_lo[d]), float(box_hi[d])
@@ -559,9 +566,9 @@ def make_rods_config(n_max, box_lo, box_hi, dt, kn, gamma_n, gamma_t, mu_cc, bet
 
 
 class Rods2D:
-    """The rods2D model (src/models/rods.jl) stepped with Euler on the device.
-    State is a dict of ROD_FIELDS arrays (or a (13, n) / (12, n) array in
-    that order); pressure is output only."""
+    """The rods2D / rods2dGrowth model (src/models/rods.jl) stepped with Euler
+    on the device.  State is a dict of ROD_FIELDS arrays; pressure is output
+    only and l_target is used by rods2dGrowth only."""
 
     def __init__(self, cfg):
         self.lib = load_library()
@@ -601,14 +608,14 @@ class Rods2D:
     __del__ = close
 
     def upload(self, state):
-        if isinstance(state, dict):
-            cols = [state[k] for k in ROD_FIELDS[:12]]
-        else:
-            cols = list(np.asarray(state)[:12])
-        arrs = [np.ascontiguousarray(c, dtype=self.dtype) for c in cols]
+        nf = len(ROD_FIELDS)
+        arrs = [np.ascontiguousarray(state[k], dtype=self.dtype) for k in ROD_FIELDS[:12]]
         n = len(arrs[0]) if arrs else 0
-        ptrs = (C.c_void_p * 13)(*([a.ctypes.data for a in arrs] + [None]))
-        self._keep = arrs
+        lt = state.get("l_target")
+        lt = None if lt is None else np.ascontiguousarray(lt, dtype=self.dtype)
+        ptrs = (C.c_void_p * nf)(*([a.ctypes.data for a in arrs]
+                                   + [None, None if lt is None else lt.ctypes.data]))
+        self._keep = arrs + [lt]
         self._check(self.lib.cbm_rods_upload(self.h, n, ptrs))
         self.n = n
 
@@ -616,9 +623,13 @@ class Rods2D:
         self._check(self.lib.cbm_rods_step(self.h, n, flags))
 
     def download(self):
-        out = np.zeros((13, self.n), self.dtype)
-        ptrs = (C.c_void_p * 13)(*[out[q].ctypes.data for q in range(13)])
+        nf = len(ROD_FIELDS)
         n = C.c_int64()
+        none = (C.c_void_p * nf)()
+        self._check(self.lib.cbm_rods_download(self.h, none, C.byref(n)))  # the count only
+        self.n = int(n.value)
+        out = np.zeros((nf, self.n), self.dtype)
+        ptrs = (C.c_void_p * nf)(*[out[q].ctypes.data for q in range(nf)])
         self._check(self.lib.cbm_rods_download(self.h, ptrs, C.byref(n)))
         return {k: out[q] for q, k in enumerate(ROD_FIELDS)}
 

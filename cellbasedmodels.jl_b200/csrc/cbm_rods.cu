@@ -43,8 +43,14 @@ constexpr int kRodBlock = 128;
 constexpr int kRodLanes = CBM_ROD_LANES;  // lanes per rod
 static_assert(kRodLanes == 4 || kRodLanes == 8 || kRodLanes == 16, "lanes per rod");
 
-// the per-rod arrays that a step rewrites (the rest, d, l, m, are constant)
-enum { kSX = 0, kSY, kSVX, kSVY, kSTH, kSOM, kSFX, kSFY, kSW, kSP, kSCOS, kSSIN, kStateArrays };
+// the per-rod arrays that a step rewrites; d, l, m are constant in rods2D and
+// single arrays, while rods2dGrowth rewrites (moves) every field, so there
+// l, lTarget, d and m are double-buffered too
+enum {
+  kSX = 0, kSY, kSVX, kSVY, kSTH, kSOM, kSFX, kSFY, kSW, kSP, kSCOS, kSSIN,
+  kSL, kSLT, kSD, kSM, kStateArrays
+};
+constexpr int kPlainArrays = kSL;  // arrays of the rods2D state
 
 template <typename T>
 struct RodStep {
@@ -65,6 +71,14 @@ struct RodStep {
   int n_cells_d[3];
   T dt, beta, beta_w;
   CbmRodCoef<T> k;
+  // rods2dGrowth
+  const long long* cnt_a;  // {n, step} of a
+  long long* cnt_b;        // {n, step} of b
+  const int* div_rank;     // exclusive prefix of the division flags (n_max + 1)
+  const int* holes;        // index of the k-th dividing rod
+  int n_max;
+  T growth, alpha, lt_lo, lt_hi;
+  unsigned long long seed;
 };
 
 // cos and sin of the uploaded angles
@@ -83,13 +97,70 @@ __device__ __forceinline__ T shfl_group(T v, int q) {
   return __shfl_sync(0xffffffffu, v, q, kRodLanes);
 }
 
+// assignCells for a row of b (neighbors.jl:763-821)
+template <typename T>
+__device__ __forceinline__ void rod_assign_cell(const RodStep<T>& R, int row, T x0, T y0) {
+  const T x[2] = {x0, y0};
+  const int c = cell_of<T, 2>(R.edge, R.box_lo, R.box_hi, R.n_cells_d, x);
+  R.agent_cell[row] = c;
+  R.agent_rank[row] = atomicAdd(R.cell_count + c, 1);
+}
+
+// rods2dGrowth's rule for a rod with l > lTarget (rods.jl:141-161), with the
+// bookkeeping of @addAgent / @removeAgent and update! folded in.  The k-th
+// dividing rod (index order) adds rows n + 2k and n + 2k + 1 and leaves a
+// hole at its own row.  update! then moves the last D of the n + 2D rows, in
+// reverse order, into the holes in ascending order
+// (kernelListSurvived / kernelFillHolesParameters, update.jl:15-84).  So
+// row s >= n + D lands at holes[n + 2D - 1 - s], and every other row stays.
+// Fields not given to @addAgent are the parent's committed values.
+template <typename T>
+__device__ void rod_divide(const RodStep<T>& R, int i, int n) {
+  const int D = R.div_rank[n], k = R.div_rank[i];
+  const long long step = R.cnt_a[1];
+  const T x = R.a[kSX][i], y = R.a[kSY][i], c = R.a[kSCOS][i], s = R.a[kSSIN][i];
+  const T l = R.a[kSL][i], d = R.a[kSD][i], om = R.a[kSOM][i];
+  // CBMDistributions.uniform(a, b) = (b - a) rand() + a (src/random.jl:15)
+  const T ww = ((T)0.1 - (T)-0.1) * cbm_uniform<T>(R.seed, step, (uint32_t)i, CBM_STREAM_ROD_TORQUE, 0u) +
+               (T)-0.1;
+  const T q = (l + d) / (T)4;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int slot = n + 2 * k + h;  // < n_max: the caller checked n + 2 D <= n_max
+    const int row = slot < n + D ? slot : R.holes[n + 2 * D - 1 - slot];
+    const T xs = h == 0 ? q * c + x : (-(l + d) / (T)4) * c + x;
+    const T ys = h == 0 ? q * s + y : (-(l + d) / (T)4) * s + y;
+    const T lt = (R.lt_hi - R.lt_lo) *
+                     cbm_uniform<T>(R.seed, step, (uint32_t)i, CBM_STREAM_ROD_TARGET + (uint32_t)h, 0u) +
+                 R.lt_lo;
+    R.b[kSX][row] = xs;
+    R.b[kSY][row] = ys;
+    R.b[kSVX][row] = R.a[kSVX][i];
+    R.b[kSVY][row] = R.a[kSVY][i];
+    R.b[kSTH][row] = R.a[kSTH][i];
+    R.b[kSOM][row] = h == 0 ? om + ww : om - ww;
+    R.b[kSFX][row] = R.a[kSFX][i];
+    R.b[kSFY][row] = R.a[kSFY][i];
+    R.b[kSW][row] = R.a[kSW][i];
+    R.b[kSP][row] = R.a[kSP][i];
+    R.b[kSCOS][row] = c;
+    R.b[kSSIN][row] = s;
+    R.b[kSL][row] = (l - d) / (T)2;
+    R.b[kSLT][row] = lt;
+    R.b[kSD][row] = d;
+    R.b[kSM][row] = R.a[kSM][i];
+    if (!R.full) rod_assign_cell<T>(R, row, xs, ys);
+  }
+}
+
 // Steps 1 and 2 of one step (rods.jl:86-118 with rodForces, :21-59), and the
 // cell assignment of step 3 (assignCells, neighbors.jl:763-821)
-template <typename T>
+template <typename T, bool GROW>
 __global__ void __launch_bounds__(kRodBlock) k_rod_step(RodStep<T> R) {
   const int t = blockIdx.x * kRodBlock + threadIdx.x;
   const int i = t / kRodLanes, lane = t % kRodLanes;
-  const bool live = i < R.n;
+  const int n = GROW ? (int)R.cnt_a[0] : R.n;
+  const bool live = i < n;
   if (t == 0 && !R.full) {
     R.ctr->scan_ticket = 0u;  // fresh tickets and tile-state generation for the scan
     R.ctr->scan_epoch = R.ctr->scan_epoch + 1u;
@@ -107,7 +178,7 @@ __global__ void __launch_bounds__(kRodBlock) k_rod_step(RodStep<T> R) {
   int rs[3] = {0, 0, 0}, re[3] = {0, 0, 0};
   if (live) {
     if (R.full) {
-      re[0] = R.n;
+      re[0] = n;
     } else {
       const T x[2] = {g.x, g.y};
       const int c = cell_of<T, 2>(R.edge, R.box_lo, R.box_hi, R.n_cells_d, x);
@@ -159,6 +230,14 @@ __global__ void __launch_bounds__(kRodBlock) k_rod_step(RodStep<T> R) {
     }
   }
   if (!live || lane != 0) return;
+  if constexpr (GROW) {
+    // without room for every birth the step divides nothing and reports the
+    // overflow (k_rod_holes), so the rows stay well formed
+    if (R.div_rank[i + 1] != R.div_rank[i] && n + 2 * R.div_rank[n] <= R.n_max) {
+      rod_divide<T>(R, i, n);
+      return;
+    }
+  }
   // Euler: u + du dt with the committed forces, then the commit of the sums
   const T dt = R.dt;
   const T vx = vx1, vy = vy1, om = R.a[kSOM][i], th = R.a[kSTH][i];
@@ -182,12 +261,62 @@ __global__ void __launch_bounds__(kRodBlock) k_rod_step(RodStep<T> R) {
   cbm_rod_cossin<T>(thn, &cn, &sn);
   R.b[kSCOS][i] = cn;
   R.b[kSSIN][i] = sn;
-  if (!R.full) {
-    const T x[2] = {xn, yn};
-    const int c = cell_of<T, 2>(R.edge, R.box_lo, R.box_hi, R.n_cells_d, x);
-    R.agent_cell[i] = c;
-    R.agent_rank[i] = atomicAdd(R.cell_count + c, 1);
+  if constexpr (GROW) {
+    // dt(l) = growth/(1 + alpha pressure), the committed pressure (rods.jl:137-139)
+    R.b[kSL][i] = l + (R.growth / ((T)1 + R.alpha * R.a[kSP][i])) * dt;
+    R.b[kSLT][i] = R.a[kSLT][i];
+    R.b[kSD][i] = d;
+    R.b[kSM][i] = m;
   }
+  if (!R.full) rod_assign_cell<T>(R, i, xn, yn);
+}
+
+// rods2dGrowth, before the step: the division flags l > lTarget of the
+// committed rods (rods.jl:143), as counts for the scan that ranks them
+template <typename T>
+__global__ void __launch_bounds__(kTile) k_rod_flags(RodStep<T> R, int* flags, Counters* dctr) {
+  const int i = blockIdx.x * kTile + threadIdx.x;
+  if (i == 0) {
+    dctr->scan_ticket = 0u;  // fresh tickets and tile-state generation for the scan
+    dctr->scan_epoch = dctr->scan_epoch + 1u;
+  }
+  if (i >= (int)R.cnt_a[0]) return;
+  flags[i] = R.a[kSL][i] > R.a[kSLT][i] ? 1 : 0;
+}
+
+// holes[k] = index of the k-th dividing rod; the step's count and counter
+template <typename T>
+__global__ void __launch_bounds__(kTile) k_rod_holes(RodStep<T> R, int* holes, Counters* ctr) {
+  const int i = blockIdx.x * kTile + threadIdx.x;
+  const int n = (int)R.cnt_a[0];
+  if (i == 0) {
+    const long long D = R.div_rank[n];
+    const bool room = n + 2 * D <= R.n_max;
+    R.cnt_b[0] = room ? n + D : n;
+    R.cnt_b[1] = R.cnt_a[1] + 1;
+    if (!room) atomicOr(&ctr->err, kErrAgentOverflow);
+  }
+  if (i >= n) return;
+  if (R.div_rank[i + 1] != R.div_rank[i]) holes[R.div_rank[i]] = i;
+}
+
+// k_grid_scatter / k_grid_stable of cbm_grid.cuh with the rod count on the device
+template <typename T>
+__global__ void __launch_bounds__(kTile) k_rod_scatter(GridParams<T> G, const long long* cnt) {
+  const int i = blockIdx.x * kTile + threadIdx.x;
+  if (i >= (int)cnt[0]) return;
+  G.cell_tmp[G.cell_start[G.agent_cell[i]] + G.agent_rank[i]] = i;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTile) k_rod_stable(GridParams<T> G, const long long* cnt) {
+  const int i = blockIdx.x * kTile + threadIdx.x;
+  if (i >= (int)cnt[0]) return;
+  const int c = G.agent_cell[i];
+  const int s0 = G.cell_start[c], s1 = G.cell_start[c + 1];
+  int r = 0;
+  for (int s = s0; s < s1; ++s) r += ld(G.cell_tmp + s) < i;
+  G.cell_agents[s0 + r] = i;
 }
 
 }  // namespace
@@ -212,6 +341,16 @@ struct cbm_rods {
   int* cell_tmp = nullptr;
   int* cell_agents = nullptr;
   unsigned long long* scan_state = nullptr;
+  // rods2dGrowth: {n, step} per buffer on the device, the division ranks
+  bool grow = false;
+  long long* cnt = nullptr;          // cnt[2 * buf + 0] = n, cnt[2 * buf + 1] = step
+  int* div_flags = nullptr;          // whole scan tiles, zero between steps
+  int* div_rank = nullptr;           // n_max + 1
+  int* holes = nullptr;              // n_max
+  Counters* div_ctr = nullptr;
+  unsigned long long* div_state = nullptr;
+  int div_tiles = 0;
+  long long cnt_host[4] = {0, 0, 0, 0};
   cudaGraphExec_t pair_graph[2] = {nullptr, nullptr};  // two steps starting at cur = 0 / 1
   bool loaded = false;
   std::string err;
@@ -248,7 +387,9 @@ void rfree(cbm_rods* r) {
     if (p) cudaFree(p), p = nullptr;
   for (void* p : {(void*)r->ptrs, (void*)r->ctr, (void*)r->cell_count, (void*)r->cell_start,
                   (void*)r->agent_cell, (void*)r->agent_rank, (void*)r->cell_tmp,
-                  (void*)r->cell_agents, (void*)r->scan_state})
+                  (void*)r->cell_agents, (void*)r->scan_state, (void*)r->cnt,
+                  (void*)r->div_flags, (void*)r->div_rank, (void*)r->holes, (void*)r->div_ctr,
+                  (void*)r->div_state})
     if (p) cudaFree(p);
   r->ptrs = nullptr;
   r->ctr = nullptr;
@@ -265,12 +406,13 @@ void* field_ptr(cbm_rods* r, int buf, int k) {
     case CBM_ROD_VY: return r->st[buf][kSVY];
     case CBM_ROD_THETA: return r->st[buf][kSTH];
     case CBM_ROD_OMEGA: return r->st[buf][kSOM];
-    case CBM_ROD_D: return r->dlm[0];
-    case CBM_ROD_L: return r->dlm[1];
-    case CBM_ROD_M: return r->dlm[2];
+    case CBM_ROD_D: return r->grow ? r->st[buf][kSD] : r->dlm[0];
+    case CBM_ROD_L: return r->grow ? r->st[buf][kSL] : r->dlm[1];
+    case CBM_ROD_M: return r->grow ? r->st[buf][kSM] : r->dlm[2];
     case CBM_ROD_FX: return r->st[buf][kSFX];
     case CBM_ROD_FY: return r->st[buf][kSFY];
     case CBM_ROD_W: return r->st[buf][kSW];
+    case CBM_ROD_L_TARGET: return r->grow ? r->st[buf][kSLT] : nullptr;
     default: return r->st[buf][kSP];
   }
 }
@@ -321,9 +463,9 @@ void enqueue_rod_step(cbm_rods* r) {
     R.a[q] = (T*)r->st[r->cur][q];
     R.b[q] = (T*)r->st[1 - r->cur][q];
   }
-  R.d = (const T*)r->dlm[0];
-  R.l = (const T*)r->dlm[1];
-  R.m = (const T*)r->dlm[2];
+  R.d = (const T*)(r->grow ? r->st[r->cur][kSD] : r->dlm[0]);
+  R.l = (const T*)(r->grow ? r->st[r->cur][kSL] : r->dlm[1]);
+  R.m = (const T*)(r->grow ? r->st[r->cur][kSM] : r->dlm[2]);
   R.cell_start = r->cell_start;
   R.cell_agents = r->cell_agents;
   R.cell_count = r->cell_count;
@@ -342,17 +484,54 @@ void enqueue_rod_step(cbm_rods* r) {
   R.beta = (T)k.beta;
   R.beta_w = (T)k.beta_w;
   R.k = CbmRodCoef<T>{(T)k.kn, (T)k.gamma_n, (T)k.gamma_t, (T)k.mu_cc};
-  const long long threads = (long long)(r->n > 0 ? r->n : 1) * kRodLanes;
+  if (!r->grow) {
+    const long long threads = (long long)(r->n > 0 ? r->n : 1) * kRodLanes;
+    const unsigned nb = (unsigned)((threads + kRodBlock - 1) / kRodBlock);
+    k_rod_step<T, false><<<nb, kRodBlock, 0, r->stream>>>(R);
+    r->cur = 1 - r->cur;
+    if (!R.full) {
+      // the rest of computeNeighbors! on the new positions
+      const GridParams<T> G = grid_params<T>(r);
+      const unsigned ng = (unsigned)(r->n > 0 ? (r->n + kTile - 1) / kTile : 1);
+      k_scan_cells<<<G.n_scan_tiles, kTile, 0, r->stream>>>(grid_scan_args(G));
+      k_grid_scatter<T><<<ng, kTile, 0, r->stream>>>(G);
+      k_grid_stable<T><<<ng, kTile, 0, r->stream>>>(G);
+    }
+    return;
+  }
+  // rods2dGrowth: the count lives on the device, launches cover n_max
+  R.cnt_a = r->cnt + 2 * r->cur;
+  R.cnt_b = r->cnt + 2 * (1 - r->cur);
+  R.div_rank = r->div_rank;
+  R.holes = r->holes;
+  R.n_max = (int)k.n_max;
+  R.growth = (T)k.growth;
+  R.alpha = (T)k.alpha;
+  R.lt_lo = (T)k.l_max - (T)k.sigma_l_target;
+  R.lt_hi = (T)k.l_max + (T)k.sigma_l_target;
+  R.seed = k.seed;
+  const unsigned nt = (unsigned)((k.n_max + kTile - 1) / kTile);
+  k_rod_flags<T><<<nt, kTile, 0, r->stream>>>(R, r->div_flags, r->div_ctr);
+  ScanArgs A;
+  A.count = r->div_flags;
+  A.start = r->div_rank;
+  A.state = r->div_state;
+  A.n = (int)k.n_max;
+  A.n_tiles = r->div_tiles;
+  A.ctr = r->div_ctr;
+  A.due = nullptr;
+  k_scan_cells<<<A.n_tiles, kTile, 0, r->stream>>>(A);
+  k_rod_holes<T><<<nt, kTile, 0, r->stream>>>(R, r->holes, r->ctr);
+  const long long threads = (long long)k.n_max * kRodLanes;
   const unsigned nb = (unsigned)((threads + kRodBlock - 1) / kRodBlock);
-  k_rod_step<T><<<nb, kRodBlock, 0, r->stream>>>(R);
+  k_rod_step<T, true><<<nb, kRodBlock, 0, r->stream>>>(R);
   r->cur = 1 - r->cur;
   if (!R.full) {
-    // the rest of computeNeighbors! on the new positions
     const GridParams<T> G = grid_params<T>(r);
-    const unsigned ng = (unsigned)(r->n > 0 ? (r->n + kTile - 1) / kTile : 1);
+    const long long* cnt = r->cnt + 2 * r->cur;
     k_scan_cells<<<G.n_scan_tiles, kTile, 0, r->stream>>>(grid_scan_args(G));
-    k_grid_scatter<T><<<ng, kTile, 0, r->stream>>>(G);
-    k_grid_stable<T><<<ng, kTile, 0, r->stream>>>(G);
+    k_rod_scatter<T><<<nt, kTile, 0, r->stream>>>(G, cnt);
+    k_rod_stable<T><<<nt, kTile, 0, r->stream>>>(G, cnt);
   }
 }
 
@@ -401,8 +580,14 @@ int cbm_rods_create(cbm_rods** out, const cbm_rods_config* cfg) {
   if (!(k.dt > 0)) return rfail(nullptr, CBM_ERR_ARG, "dt must be positive");
   for (int d = 0; d < 2; ++d)
     if (!(k.box_hi[d] > k.box_lo[d])) return rfail(nullptr, CBM_ERR_ARG, "empty simBox");
+  if (k.growth_model != 0 && k.growth_model != 1)
+    return rfail(nullptr, CBM_ERR_ARG, "growth_model must be 0 (rods2D) or 1 (rods2dGrowth)");
+  if (k.growth_model && !(std::isfinite(k.growth) && std::isfinite(k.alpha) &&
+                          std::isfinite(k.l_max) && std::isfinite(k.sigma_l_target)))
+    return rfail(nullptr, CBM_ERR_ARG, "growth, alpha, l_max and sigma_l_target must be finite");
   cbm_rods* r = new cbm_rods;
   r->cfg = k;
+  r->grow = k.growth_model != 0;
   r->tsize = k.precision == CBM_F64 ? 8 : 4;
   if (k.neighbors == CBM_NEIGH_CELL_LINKED) {
     if (!(k.cell_edge > 0)) {
@@ -428,9 +613,25 @@ int cbm_rods_create(cbm_rods** out, const cbm_rods_config* cfg) {
   }
   const size_t n = (size_t)k.n_max, S = (size_t)r->tsize;
   bool ok = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) == cudaSuccess;
+  const int arrays = r->grow ? kStateArrays : kPlainArrays;
   for (auto& b : r->st)
-    for (void*& p : b) ok = ok && cudaMalloc(&p, n * S) == cudaSuccess;
-  for (void*& p : r->dlm) ok = ok && cudaMalloc(&p, n * S) == cudaSuccess;
+    for (int q = 0; q < arrays; ++q) ok = ok && cudaMalloc(&b[q], n * S) == cudaSuccess;
+  if (!r->grow)
+    for (void*& p : r->dlm) ok = ok && cudaMalloc(&p, n * S) == cudaSuccess;
+  if (r->grow) {
+    r->div_tiles = (int)((k.n_max + kScanTile - 1) / kScanTile);
+    const size_t flag_ints = (size_t)r->div_tiles * kScanTile;
+    ok = ok && cudaMalloc((void**)&r->cnt, 4 * sizeof(long long)) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&r->div_flags, flag_ints * 4) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&r->div_rank, (n + 1) * 4) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&r->holes, n * 4) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&r->div_ctr, sizeof(Counters)) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&r->div_state, (size_t)r->div_tiles * 8) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(r->cnt, 0, 4 * sizeof(long long), r->stream) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(r->div_flags, 0, flag_ints * 4, r->stream) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(r->div_ctr, 0, sizeof(Counters), r->stream) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(r->div_state, 0, (size_t)r->div_tiles * 8, r->stream) == cudaSuccess;
+  }
   ok = ok && cudaMalloc((void**)&r->ptrs, 2 * kStateArrays * sizeof(void*)) == cudaSuccess;
   const int tiles = (r->n_cells + kScanTile - 1) / kScanTile;
   // whole scan tiles of counts: the scan loads and clears them as int4
@@ -476,6 +677,8 @@ int cbm_rods_upload(cbm_rods* r, int64_t n, const void* const* fields) {
   if (n < 0 || n > r->cfg.n_max) return rfail(r, CBM_ERR_ARG, "n must be in [0, n_max]");
   for (int q = 0; q < CBM_ROD_PRESSURE; ++q)
     if (!fields[q]) return rfail(r, CBM_ERR_ARG, "a rod field is missing");
+  if (r->grow && !fields[CBM_ROD_L_TARGET])
+    return rfail(r, CBM_ERR_ARG, "rods2dGrowth needs the lTarget field");
   ROD_TRY(r, cudaStreamSynchronize(r->stream));
   if ((int)n != r->n) drop_graphs(r);  // the graphs hold n in their launch shapes
   r->n = (int)n;
@@ -486,6 +689,19 @@ int cbm_rods_upload(cbm_rods* r, int64_t n, const void* const* fields) {
       ROD_TRY(r, cudaMemcpyAsync(field_ptr(r, 0, q), fields[q], b, cudaMemcpyHostToDevice,
                                  r->stream));
     ROD_TRY(r, cudaMemsetAsync(field_ptr(r, 0, CBM_ROD_PRESSURE), 0, b, r->stream));
+    if (r->grow)
+      ROD_TRY(r, cudaMemcpyAsync(field_ptr(r, 0, CBM_ROD_L_TARGET), fields[CBM_ROD_L_TARGET], b,
+                                 cudaMemcpyHostToDevice, r->stream));
+  }
+  ROD_TRY(r, cudaMemsetAsync(&r->ctr->err, 0, sizeof(int), r->stream));
+  if (r->grow) {
+    r->cnt_host[0] = n;
+    r->cnt_host[1] = 0;
+    r->cnt_host[2] = n;
+    r->cnt_host[3] = 0;
+    ROD_TRY(r, cudaMemcpyAsync(r->cnt, r->cnt_host, sizeof r->cnt_host, cudaMemcpyHostToDevice,
+                               r->stream));
+    ROD_TRY(r, cudaMemsetAsync(&r->div_ctr->err, 0, sizeof(int), r->stream));
   }
   const unsigned nb = (unsigned)(n > 0 ? (n + kTile - 1) / kTile : 1);
   if (r->tsize == 8) {
@@ -516,18 +732,36 @@ int cbm_rods_step(cbm_rods* r, int32_t nsteps, int32_t flags) {
   }
   for (; s < nsteps; ++s) enqueue_one(r);
   ROD_TRY(r, cudaGetLastError());
-  if (flags & CBM_SYNC) ROD_TRY(r, cudaStreamSynchronize(r->stream));
+  if (flags & CBM_SYNC) {
+    int e[2] = {0, 0};
+    ROD_TRY(r, cudaMemcpyAsync(&e[0], &r->ctr->err, sizeof(int), cudaMemcpyDeviceToHost, r->stream));
+    if (r->grow)
+      ROD_TRY(r, cudaMemcpyAsync(&e[1], &r->div_ctr->err, sizeof(int), cudaMemcpyDeviceToHost,
+                                 r->stream));
+    ROD_TRY(r, cudaStreamSynchronize(r->stream));
+    const int bits = e[0] | e[1];
+    if (bits & kErrAgentOverflow)
+      return rfail(r, CBM_ERR_AGENT_OVERFLOW, "a division found no room below n_max");
+    if (bits & kErrTimeout) return rfail(r, CBM_ERR_TIMEOUT, "a bounded wait of the cell scan gave up");
+  }
   return CBM_OK;
 }
 
 int cbm_rods_download(cbm_rods* r, void* const* fields, int64_t* n_out) {
   if (!r || !fields) return rfail(r, CBM_ERR_ARG, "null argument");
   if (!r->loaded) return rfail(r, CBM_ERR_STATE, "cbm_rods_download before cbm_rods_upload");
+  if (r->grow) {
+    ROD_TRY(r, cudaMemcpyAsync(r->cnt_host, r->cnt, sizeof r->cnt_host, cudaMemcpyDeviceToHost,
+                               r->stream));
+    ROD_TRY(r, cudaStreamSynchronize(r->stream));
+    r->n = (int)r->cnt_host[2 * r->cur];
+  }
   const size_t b = (size_t)r->n * r->tsize;
-  for (int q = 0; q < CBM_RODS_FIELDS; ++q)
-    if (fields[q] && b)
-      ROD_TRY(r, cudaMemcpyAsync(fields[q], field_ptr(r, r->cur, q), b, cudaMemcpyDeviceToHost,
-                                 r->stream));
+  for (int q = 0; q < CBM_RODS_FIELDS; ++q) {
+    void* src = field_ptr(r, r->cur, q);  // null: lTarget without rods2dGrowth
+    if (fields[q] && src && b)
+      ROD_TRY(r, cudaMemcpyAsync(fields[q], src, b, cudaMemcpyDeviceToHost, r->stream));
+  }
   ROD_TRY(r, cudaStreamSynchronize(r->stream));
   if (n_out) *n_out = r->n;
   return CBM_OK;

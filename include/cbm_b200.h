@@ -391,6 +391,19 @@ typedef struct cbm_rods_config {
   double cell_edge;
   double dt;
   double kn, gamma_n, gamma_t, mu_cc, mu_cw, beta, beta_w;
+  /* rods2dGrowth (rods.jl:123-163) when growth_model != 0:
+   *   dt(l) = growth/(1 + alpha pressure), pressure lagged like fx;
+   *   the rule, before the ODE: a rod with l > lTarget divides into two rods
+   *   at x +- (l+d)/4 (cos, sin)(theta), l = (l-d)/2, omega +- ww,
+   *   ww = uniform(-.1, .1), lTarget = uniform(l_max - sigma_l_target,
+   *   l_max + sigma_l_target) each (the other fields are the parent's), and
+   *   is removed; update! fills the holes from the tail as the reference.
+   * uniform(a, b) = (b - a) u + a with u the shared stream of cbm_rng.h
+   * (seed, step, parent index, CBM_STREAM_ROD_*). */
+  int32_t growth_model;
+  int32_t pad0;
+  double growth, alpha, sigma_l_target, l_max;
+  uint64_t seed;
 } cbm_rods_config;
 
 typedef struct cbm_rods cbm_rods;
@@ -398,16 +411,21 @@ int cbm_rods_create(cbm_rods** out, const cbm_rods_config* cfg);
 void cbm_rods_destroy(cbm_rods* r);
 const char* cbm_rods_last_error(const cbm_rods* r);
 /* The per-rod fields, each an array of n reals of the configured precision,
- * in this order (CBM_RODS_FIELDS of them; pressure is read by download only). */
-#define CBM_RODS_FIELDS 13
+ * in this order (CBM_RODS_FIELDS of them; pressure is read by download only;
+ * lTarget is used by rods2dGrowth only). */
+#define CBM_RODS_FIELDS 14
 enum {
   CBM_ROD_X = 0, CBM_ROD_Y, CBM_ROD_VX, CBM_ROD_VY, CBM_ROD_THETA, CBM_ROD_OMEGA, CBM_ROD_D,
-  CBM_ROD_L, CBM_ROD_M, CBM_ROD_FX, CBM_ROD_FY, CBM_ROD_W, CBM_ROD_PRESSURE
+  CBM_ROD_L, CBM_ROD_M, CBM_ROD_FX, CBM_ROD_FY, CBM_ROD_W, CBM_ROD_PRESSURE, CBM_ROD_L_TARGET
 };
-/* fields[k] for k < CBM_ROD_PRESSURE are read (host arrays); sets the step to 0 */
+/* fields[k] for k < CBM_ROD_PRESSURE are read (host arrays), and
+ * fields[CBM_ROD_L_TARGET] with growth_model; sets the step to 0 */
 int cbm_rods_upload(cbm_rods* r, int64_t n, const void* const* fields);
+/* With growth_model, flags & CBM_SYNC also reports CBM_ERR_AGENT_OVERFLOW when
+ * a division found no room below n_max (the state is then undefined). */
 int cbm_rods_step(cbm_rods* r, int32_t nsteps, int32_t flags);
-/* fields[k] (host arrays of at least n reals) receive every field; *n_out = n */
+/* fields[k] (host arrays of at least n reals, or NULL) receive the fields;
+ * *n_out = n (with growth_model the current count, read back from the device) */
 int cbm_rods_download(cbm_rods* r, void* const* fields, int64_t* n_out);
 void* cbm_rods_stream(cbm_rods* r);
 

@@ -44,6 +44,8 @@
 #define CBM_STREAM_DEATH 2u    /* uniform(0,1) for the death branch */
 #define CBM_STREAM_USER 3u     /* cbm_rng_fill and tests */
 #define CBM_STREAM_NOISE_FINAL 4u /* EulerHeun: the fresh draw of its final update */
+#define CBM_STREAM_ROD_TORQUE 5u  /* rods2dGrowth: uniform(-.1, .1) torque kick at division */
+#define CBM_STREAM_ROD_TARGET 6u  /* rods2dGrowth: lTarget of the first daughter (+1: second) */
 
 /* ---- exactly rounded primitives that are never fused ------------------- */
 #if defined(__CUDA_ARCH__)

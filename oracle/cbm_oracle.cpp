@@ -1433,6 +1433,8 @@ template <typename T>
 struct Rods {
   cbm_rods_config cfg;
   int64_t n = 0;
+  int64_t step = 0;
+  int err = 0;
   std::vector<T> f[CBM_RODS_FIELDS];
   std::vector<T> cosT, sinT, fx_, fy_, w_, p_;
   int64_t nc[2] = {1, 1};
@@ -1538,6 +1540,137 @@ void rodStep(Rods<T>& R) {
   rodGrid(R);
 }
 
+/* rods2dGrowth (rods.jl:123-163): step! with the reference's bookkeeping.
+ * agentStepRule! writes the daughters into the "__" copies at rows N + NAdd
+ * (@addAgent: the fields not given are the parent's committed values) and
+ * records the parent in holeFromRemoveAt (@removeAgent,
+ * functionRule.jl:9-111); agentStepDE! integrates rows < N from the committed
+ * state; update! fills the holes from the surviving tail
+ * (kernelListSurvived / kernelFillHolesParameters, update.jl:15-84) and
+ * commits.  When the births do not fit below n_max, no rod divides in that
+ * step and the overflow is reported: the device's behaviour, where the
+ * reference would add up to the capacity and raise. */
+template <typename T>
+void rodStepGrowth(Rods<T>& R) {
+  const int64_t N = R.n, nMax = R.cfg.n_max;
+  std::vector<T>* F = R.f;
+  const T kn = (T)R.cfg.kn, gn = (T)R.cfg.gamma_n, gt = (T)R.cfg.gamma_t, mucc = (T)R.cfg.mu_cc;
+  for (int64_t i = 0; i < N; ++i) rodCosSin(F[CBM_ROD_THETA][i], R.cosT[i], R.sinT[i]);
+  std::vector<T> G[CBM_RODS_FIELDS];
+  for (int q = 0; q < CBM_RODS_FIELDS; ++q) G[q] = F[q];
+  // agentStepRule!
+  int64_t D = 0;
+  for (int64_t i = 0; i < N; ++i) D += F[CBM_ROD_L][i] > F[CBM_ROD_L_TARGET][i];
+  std::vector<int64_t> holes;
+  std::vector<char> survive((size_t)nMax, 1);
+  int64_t nAdd = 0;
+  if (N + 2 * D > nMax) {
+    R.err = CBM_ERR_AGENT_OVERFLOW;
+  } else {
+    const T lo = (T)R.cfg.l_max - (T)R.cfg.sigma_l_target;
+    const T hi = (T)R.cfg.l_max + (T)R.cfg.sigma_l_target;
+    for (int64_t i = 0; i < N; ++i) {
+      const T l = F[CBM_ROD_L][i];
+      if (!(l > F[CBM_ROD_L_TARGET][i])) continue;
+      const T d = F[CBM_ROD_D][i], x = F[CBM_ROD_X][i], y = F[CBM_ROD_Y][i];
+      const T om = F[CBM_ROD_OMEGA][i];
+      // ww = CBMDistributions.uniform(-.1,.1) = (l1 - l0) rand() + l0 (random.jl:15)
+      const T ww = ((T)0.1 - (T)-0.1) *
+                       cbm_uniform<T>(R.cfg.seed, R.step, (uint32_t)i, CBM_STREAM_ROD_TORQUE, 0u) +
+                   (T)-0.1;
+      for (int h = 0; h < 2; ++h) {
+        const int64_t slot = N + nAdd;
+        nAdd += 1;
+        for (int q = 0; q < CBM_RODS_FIELDS; ++q) G[q][slot] = F[q][i];
+        const T sg = h == 0 ? (l + d) / (T)4 : -(l + d) / (T)4;
+        G[CBM_ROD_X][slot] = sg * R.cosT[i] + x;
+        G[CBM_ROD_Y][slot] = sg * R.sinT[i] + y;
+        G[CBM_ROD_L][slot] = (l - d) / (T)2;
+        G[CBM_ROD_OMEGA][slot] = h == 0 ? om + ww : om - ww;
+        G[CBM_ROD_L_TARGET][slot] =
+            (hi - lo) * cbm_uniform<T>(R.cfg.seed, R.step, (uint32_t)i,
+                                       CBM_STREAM_ROD_TARGET + (uint32_t)h, 0u) + lo;
+      }
+      holes.push_back(i);
+      survive[(size_t)i] = 0;
+    }
+  }
+  // agentStepDE!: the neighbor sums and Euler from the committed state
+  const T dt = (T)R.cfg.dt, beta = (T)R.cfg.beta, bw = (T)R.cfg.beta_w;
+  const T growth = (T)R.cfg.growth, alpha = (T)R.cfg.alpha;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < N; ++i) {
+    T sfx = 0, sfy = 0, sw = 0, sp = 0;
+    const T x = F[CBM_ROD_X][i], y = F[CBM_ROD_Y][i], d = F[CBM_ROD_D][i], l = F[CBM_ROD_L][i];
+    const T vx = F[CBM_ROD_VX][i], vy = F[CBM_ROD_VY][i], m = F[CBM_ROD_M][i];
+    auto pair = [&](int64_t j) {
+      if (j == i) return;
+      T xa, ya, xb, yb;
+      rodIntersection(x, y, l, R.cosT[i], R.sinT[i], F[CBM_ROD_X][j], F[CBM_ROD_Y][j],
+                      F[CBM_ROD_L][j], R.cosT[j], R.sinT[j], xa, ya, xb, yb);
+      T rij = std::sqrt((xa - xb) * (xa - xb) + (ya - yb) * (ya - yb));
+      if (!(rij > (T)0 && rij < (d + F[CBM_ROD_D][j]) / (T)2)) return;
+      T dl = d - rij;
+      T me = m / (T)2;
+      T nx = (xa - xb) / rij;
+      T ny = (ya - yb) / rij;
+      T wx = vx - F[CBM_ROD_VX][j];
+      T wy = vy - F[CBM_ROD_VY][j];
+      T vn = nx * wx + ny * wy;
+      T fn = kn * (dl * std::sqrt(dl)) - gn * me * dl * vn;
+      T ft = -jlMin(gt * me * std::sqrt(dl), mucc * fn);
+      T fx = fn * nx + ft * (wx - vn * nx);
+      T fy = fn * ny + ft * (wy - vn * ny);
+      sfx += fx;
+      sfy += fy;
+      sw += (xa - x) * fy - (ya - y) * fx;
+      sp += std::sqrt(fx * fx + fy * fy);
+    };
+    if (R.cfg.neighbors == CBM_NEIGH_FULL) {
+      for (int64_t j = 0; j < N; ++j) pair(j);
+    } else {
+      const int64_t c = rodCell(R, i);
+      const int64_t cx = c % R.nc[0], cy = c / R.nc[0];
+      for (int k = 0; k < 9; ++k) {
+        const int64_t qx = cx + k % 3 - 1, qy = cy + k / 3 - 1;
+        if (qx < 0 || qx >= R.nc[0] || qy < 0 || qy >= R.nc[1]) continue;
+        const int64_t cc = qx + R.nc[0] * qy;
+        for (int64_t s = R.cellStart[cc]; s < R.cellStart[cc + 1]; ++s) pair(R.cellAgents[s]);
+      }
+    }
+    const T om = F[CBM_ROD_OMEGA][i];
+    T ax = -beta * vx + F[CBM_ROD_FX][i] / m;
+    T ay = -beta * vy + F[CBM_ROD_FY][i] / m;
+    T aw = F[CBM_ROD_W][i] / (m * ((d + l) * (d + l)) / (T)12 + m * (d * d)) - bw * om;
+    T al = growth / ((T)1 + alpha * F[CBM_ROD_PRESSURE][i]);  // rods.jl:138
+    G[CBM_ROD_X][i] = x + vx * dt;
+    G[CBM_ROD_Y][i] = y + vy * dt;
+    G[CBM_ROD_VX][i] = vx + ax * dt;
+    G[CBM_ROD_VY][i] = vy + ay * dt;
+    G[CBM_ROD_THETA][i] = F[CBM_ROD_THETA][i] + om * dt;
+    G[CBM_ROD_OMEGA][i] = om + aw * dt;
+    G[CBM_ROD_L][i] = l + al * dt;
+    G[CBM_ROD_FX][i] = sfx;
+    G[CBM_ROD_FY][i] = sfy;
+    G[CBM_ROD_W][i] = sw;
+    G[CBM_ROD_PRESSURE][i] = sp;
+  }
+  // update!
+  std::vector<int64_t> repo;
+  int64_t lastPos = N + nAdd - 1;
+  while ((int64_t)holes.size() > (int64_t)repo.size() && lastPos >= 0) {
+    if (survive[(size_t)lastPos]) repo.push_back(lastPos);
+    lastPos -= 1;
+  }
+  for (int q = 0; q < CBM_RODS_FIELDS; ++q)
+    for (size_t k = 0; k < repo.size(); ++k)
+      if (holes[k] < repo[k]) G[q][(size_t)holes[k]] = G[q][(size_t)repo[k]];
+  R.n = N + nAdd - (int64_t)holes.size();
+  for (int q = 0; q < CBM_RODS_FIELDS; ++q) F[q] = G[q];
+  R.step += 1;
+  rodGrid(R);
+}
+
 struct RodHandle {
   int prec;
   void* p;
@@ -1583,11 +1716,16 @@ int oracle_rods_upload(void* vh, int64_t n, const void* const* fields) {
   auto up = [&](auto* R) {
     using T = typename std::remove_reference<decltype(R->cosT[0])>::type;
     R->n = n;
+    R->step = 0;
+    R->err = 0;
+    const bool grow = R->cfg.growth_model != 0;
+    const size_t rows = grow ? (size_t)std::max<int64_t>(n, R->cfg.n_max) : (size_t)n;
     for (int q = 0; q < CBM_RODS_FIELDS; ++q) {
-      R->f[q].assign((size_t)n, (T)0);
-      if (q < CBM_ROD_PRESSURE) std::copy((const T*)fields[q], (const T*)fields[q] + n, R->f[q].begin());
+      R->f[q].assign(rows, (T)0);
+      if (q < CBM_ROD_PRESSURE || (grow && q == CBM_ROD_L_TARGET))
+        std::copy((const T*)fields[q], (const T*)fields[q] + n, R->f[q].begin());
     }
-    for (auto* v : {&R->cosT, &R->sinT, &R->fx_, &R->fy_, &R->w_, &R->p_}) v->assign((size_t)n, (T)0);
+    for (auto* v : {&R->cosT, &R->sinT, &R->fx_, &R->fy_, &R->w_, &R->p_}) v->assign(rows, (T)0);
     rodGrid(*R);
   };
   if (h->prec == CBM_F64) up((Rods<double>*)h->p);
@@ -1598,8 +1736,15 @@ int oracle_rods_upload(void* vh, int64_t n, const void* const* fields) {
 int oracle_rods_step(void* vh, int nsteps) {
   RodHandle* h = (RodHandle*)vh;
   for (int s = 0; s < nsteps; ++s) {
-    if (h->prec == CBM_F64) rodStep(*(Rods<double>*)h->p);
-    else rodStep(*(Rods<float>*)h->p);
+    if (h->prec == CBM_F64) {
+      auto& R = *(Rods<double>*)h->p;
+      if (R.cfg.growth_model) rodStepGrowth(R);
+      else rodStep(R);
+    } else {
+      auto& R = *(Rods<float>*)h->p;
+      if (R.cfg.growth_model) rodStepGrowth(R);
+      else rodStep(R);
+    }
   }
   return CBM_OK;
 }
@@ -1609,11 +1754,30 @@ int oracle_rods_download(void* vh, void* const* fields) {
   auto down = [&](auto* R) {
     using T = typename std::remove_reference<decltype(R->cosT[0])>::type;
     for (int q = 0; q < CBM_RODS_FIELDS; ++q)
-      if (fields[q]) std::copy(R->f[q].begin(), R->f[q].end(), (T*)fields[q]);
+      if (fields[q]) std::copy(R->f[q].begin(), R->f[q].begin() + R->n, (T*)fields[q]);
   };
   if (h->prec == CBM_F64) down((Rods<double>*)h->p);
   else down((Rods<float>*)h->p);
   return CBM_OK;
+}
+
+/* one uniform u in [0, 1) of the shared stream, for transcriptions in tests */
+double oracle_uniform_f64(uint64_t seed, int64_t step, uint32_t agent, uint32_t stream,
+                          uint32_t community) {
+  return cbm_uniform_f64(seed, step, agent, stream, community);
+}
+
+/* the rod count and the error code (CBM_ERR_AGENT_OVERFLOW) of the last steps */
+int64_t oracle_rods_count(void* vh, int* err) {
+  RodHandle* h = (RodHandle*)vh;
+  if (h->prec == CBM_F64) {
+    auto& R = *(Rods<double>*)h->p;
+    if (err) *err = R.err;
+    return R.n;
+  }
+  auto& R = *(Rods<float>*)h->p;
+  if (err) *err = R.err;
+  return R.n;
 }
 
 /* rodForces of one pair, for the pin against a transcription of rods.jl */

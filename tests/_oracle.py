@@ -61,6 +61,8 @@ def load_oracle(abi):
         "oracle_rods_step": (C.c_int, [vp, C.c_int]),
         "oracle_rods_download": (C.c_int, [vp, C.POINTER(vp)]),
         "oracle_rod_pair_f64": (C.c_int, [C.POINTER(dbl)] * 4),
+        "oracle_rods_count": (i64, [vp, C.POINTER(C.c_int)]),
+        "oracle_uniform_f64": (dbl, [u64, i64, u32, u32, u32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -249,18 +251,27 @@ class OracleRods:
     __del__ = close
 
     def upload(self, state):
-        cols = [state[k] for k in self.abi.ROD_FIELDS[:12]]
-        arrs = [np.ascontiguousarray(c, dtype=self.dtype) for c in cols]
+        nf = len(self.abi.ROD_FIELDS)
+        arrs = [np.ascontiguousarray(state[k], dtype=self.dtype) for k in self.abi.ROD_FIELDS[:12]]
         self.n = len(arrs[0])
-        ptrs = (C.c_void_p * 13)(*([a.ctypes.data for a in arrs] + [None]))
+        lt = np.ascontiguousarray(state.get("l_target", np.zeros(self.n)), dtype=self.dtype)
+        self._keep = arrs + [lt]
+        ptrs = (C.c_void_p * nf)(*([a.ctypes.data for a in arrs] + [None, lt.ctypes.data]))
         self.lib.oracle_rods_upload(self.h, self.n, ptrs)
 
     def step(self, n):
         self.lib.oracle_rods_step(self.h, n)
 
+    def count(self):
+        err = C.c_int()
+        n = self.lib.oracle_rods_count(self.h, C.byref(err))
+        return int(n), int(err.value)
+
     def download(self):
-        out = np.zeros((13, self.n), self.dtype)
-        ptrs = (C.c_void_p * 13)(*[out[q].ctypes.data for q in range(13)])
+        nf = len(self.abi.ROD_FIELDS)
+        self.n = self.count()[0]
+        out = np.zeros((nf, self.n), self.dtype)
+        ptrs = (C.c_void_p * nf)(*[out[q].ctypes.data for q in range(nf)])
         self.lib.oracle_rods_download(self.h, ptrs)
         return {k: out[q] for q, k in enumerate(self.abi.ROD_FIELDS)}
 

@@ -76,3 +76,19 @@ def test_rods_create_rejects_bad_configurations():
         with pytest.raises(abi.CbmError) as e:
             abi.Rods2D(abi.make_rods_config(**kw))
         assert e.value.code == abi.CBM_ERR_ARG, change
+
+
+def test_rods_growth_config_checked():
+    import pytest
+    abi = conftest.cbm._abi
+    base = dict(n_max=8, box_lo=(-5.0, -5.0), box_hi=(5.0, 5.0), dt=1e-4, kn=1.0, gamma_n=1.0,
+                gamma_t=1.0, mu_cc=0.1, beta=0.8, beta_w=0.8, cell_edge=3.0)
+    cfg = abi.make_rods_config(**base, growth=float("nan"), l_max=3.0)
+    with pytest.raises(abi.CbmError) as e:
+        abi.Rods2D(cfg)
+    assert e.value.code == abi.CBM_ERR_ARG
+    cfg = abi.make_rods_config(**base)
+    cfg.growth_model = 2
+    with pytest.raises(abi.CbmError) as e:
+        abi.Rods2D(cfg)
+    assert e.value.code == abi.CBM_ERR_ARG

@@ -119,3 +119,68 @@ def test_rods_bacteries_constants(gpu_lib, abi, prec):
                                **bench.ROD_PARAMS)
     contacts = _compare(abi, cbm, cfg, st, [1, 9, 30])
     assert contacts > 1000
+
+
+GROW = dict(growth=0.5, alpha=50.0, sigma_l_target=0.2, l_max=3.0, seed=91)
+
+
+def _growth_colony(abi, n, seed, half):
+    st = _colony(abi, n, seed, half)
+    rng = np.random.default_rng(seed + 1)
+    st["l"] = rng.uniform(2.0, 3.0, n)
+    st["l_target"] = st["l"] + rng.uniform(-0.05, 0.3, n)
+    return st
+
+
+@pytest.mark.parametrize("graph", [True, False])
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("neighbors", ["cell_linked", "full"])
+def test_rods_growth_bitexact(gpu_lib, abi, prec, neighbors, graph):
+    """rods2dGrowth: rods grow at dt(l) = growth/(1+α pressure), divide past
+    lTarget into two daughters with drawn torque and targets, and update!
+    fills the parents' rows from the tail; the device matches the checker
+    row by row while the colony grows."""
+    from conftest import cbm
+    n0 = 400 if neighbors == "cell_linked" else 150
+    half = math.sqrt(n0) * 0.9
+    st = _growth_colony(abi, n0, 31, half)
+    cfg = abi.make_rods_config(
+        4 * n0, (-half - 30, -half - 30), (half + 30, half + 30), cell_edge=4.0,
+        neighbors=abi.NEIGH_CELL_LINKED if neighbors == "cell_linked" else abi.NEIGH_FULL,
+        precision=abi.F32 if prec == "f32" else abi.F64, **bench_rod_params(), **GROW)
+    g = cbm._abi.Rods2D(cfg)
+    o = OracleRods(abi, cfg)
+    g.upload(st)
+    o.upload(st)
+    sizes = []
+    for s in [1, 2, 5, 8]:
+        g.step(s, abi.SYNC | (0 if graph else abi.NO_GRAPH))
+        o.step(s)
+        a, b = g.download(), o.download()
+        assert len(a["x"]) == len(b["x"]) == o.count()[0]
+        for k in abi.ROD_FIELDS:
+            np.testing.assert_array_equal(a[k], b[k], err_msg=f"{k} after {s} steps")
+        sizes.append(len(a["x"]))
+    g.close()
+    o.close()
+    assert sizes[0] > n0 and sizes[-1] > sizes[0]
+
+
+def test_rods_growth_overflow(gpu_lib, abi):
+    from conftest import cbm
+    st = _growth_colony(abi, 100, 32, 9.0)
+    st["l_target"] = st["l"] - 1.0  # every rod divides: 300 rows > n_max
+    cfg = abi.make_rods_config(250, (-20.0, -20.0), (20.0, 20.0), cell_edge=4.0,
+                               **bench_rod_params(), **GROW)
+    g = cbm._abi.Rods2D(cfg)
+    g.upload(st)
+    with pytest.raises(cbm._abi.CbmError) as e:
+        g.step(1)
+    assert e.value.code == abi.CBM_ERR_AGENT_OVERFLOW
+    assert len(g.download()["x"]) == 100  # nothing divided
+    g.close()
+
+
+def bench_rod_params():
+    import bench
+    return dict(bench.ROD_PARAMS)

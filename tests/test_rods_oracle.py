@@ -286,3 +286,91 @@ def test_rods_step_matches_transcription(neighbors):
             np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
     assert np.count_nonzero(ref["pressure"]) > 10  # rods are in contact
 
+
+
+GROW = dict(growth=200.0, alpha=50.0, sigma_l_target=0.2, l_max=3.0, seed=77)
+
+
+def _uniform(step, agent, stream):
+    return load_oracle(abi).oracle_uniform_f64(GROW["seed"], step, agent, stream, 0)
+
+
+def _py_grow_step(st, step, neighbors, edge, n_max):
+    """One step! of rods2dGrowth (rods.jl:123-163), as the reference runs it:
+    agentStepRule! (@addAgent at rows N + NAdd into the new copies, fields not
+    given taken from the parent; @removeAgent), agentStepDE! (rods2D's ODE and
+    dt(l) = growth/(1+α pressure), pressure committed), update! (holes filled
+    from the surviving tail, update.jl:15-84) and the commit."""
+    f = {k: list(map(float, v)) for k, v in st.items()}
+    n = len(f["x"])
+    de = _py_step(st, neighbors, edge)  # rows < n: Euler and the neighbor sums
+    g = {k: list(map(float, v)) for k, v in de.items()}
+    for i in range(n):
+        g["l"][i] = f["l"][i] + (GROW["growth"] / (1 + GROW["alpha"] * f["pressure"][i])) * PARAMS["dt"]
+    dividers = [i for i in range(n) if f["l"][i] > f["l_target"][i]]
+    holes, survive = [], [True] * (n + 2 * len(dividers))
+    if n + 2 * len(dividers) <= n_max:
+        lo, hi = GROW["l_max"] - GROW["sigma_l_target"], GROW["l_max"] + GROW["sigma_l_target"]
+        for i in dividers:
+            c, s = _cossin(f["theta"][i])
+            ww = (0.1 - -0.1) * _uniform(step, i, 5) + -0.1
+            l, d = f["l"][i], f["d"][i]
+            for h in (0, 1):
+                for k in g:
+                    g[k].append(f[k][i])
+                sg = (l + d) / 4 if h == 0 else -(l + d) / 4
+                g["x"][-1] = sg * c + f["x"][i]
+                g["y"][-1] = sg * s + f["y"][i]
+                g["l"][-1] = (l - d) / 2
+                g["omega"][-1] = f["omega"][i] + ww if h == 0 else f["omega"][i] - ww
+                g["l_target"][-1] = (hi - lo) * _uniform(step, i, 6 + h) + lo
+            holes.append(i)
+            survive[i] = False
+    repo, last = [], len(g["x"]) - 1
+    while len(holes) > len(repo) and last >= 0:
+        if survive[last]:
+            repo.append(last)
+        last -= 1
+    for k in g:
+        for hole, src in zip(holes, repo):
+            if hole < src:
+                g[k][hole] = g[k][src]
+    n_new = len(g["x"]) - len(holes)
+    return {k: np.array(v[:n_new]) for k, v in g.items()}
+
+
+@pytest.mark.parametrize("neighbors", ["full", "cell_linked"])
+def test_rods_growth_step_matches_transcription(neighbors):
+    """rods2dGrowth in Float64: divisions in most steps, including rods that
+    divide in the same step, against the transcription, field by field."""
+    nb = abi.NEIGH_FULL if neighbors == "full" else abi.NEIGH_CELL_LINKED
+    edge = 4.0
+    st = _colony(24, 5, box=5.0)
+    rng = np.random.default_rng(6)
+    st["l_target"] = st["l"] + rng.uniform(-0.02, 0.06, 24)  # a third divide at once
+    cfg = abi.make_rods_config(200, BOX_LO, BOX_HI, cell_edge=edge, neighbors=nb,
+                               precision=abi.F64, **PARAMS, **GROW)
+    orc = OracleRods(abi, cfg)
+    orc.upload(st)
+    ref = {k: np.asarray(v, dtype=float) for k, v in st.items()}
+    sizes = []
+    for step in range(6):
+        ref = _py_grow_step(ref, step, nb, edge, 200)
+        orc.step(1)
+        got = orc.download()
+        assert orc.count() == (len(ref["x"]), 0)
+        for k in abi.ROD_FIELDS:
+            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"{k} after step {step}")
+        sizes.append(len(ref["x"]))
+    assert sizes[0] > 24 and sizes[-1] > sizes[0]
+
+
+def test_rods_growth_overflow_divides_nothing():
+    st = _colony(10, 8, box=3.0)
+    st["l_target"] = st["l"] - 0.5  # every rod divides
+    cfg = abi.make_rods_config(25, BOX_LO, BOX_HI, cell_edge=4.0, precision=abi.F64, **PARAMS,
+                               **GROW)
+    orc = OracleRods(abi, cfg)
+    orc.upload(st)
+    orc.step(1)
+    assert orc.count() == (10, abi.CBM_ERR_AGENT_OVERFLOW)
