@@ -8,14 +8,18 @@
 //      fx, fy, W;
 //   2. update!: the new copies are committed;
 //   3. computeNeighbors!: the grid is rebuilt on the new positions.
-// Rods stay in index order (rods2D has no division or death).  The force
-// arithmetic is cbm_rods_math.h.
+// In rods2D the rods stay in index order.  rods2dGrowth (rods.jl:123-163)
+// adds dt(l) = growth/(1 + alpha pressure) and, before step 1, the division
+// rule, whose births and removals update! resolves by filling holes from the
+// tail (rod_divide).  The force arithmetic is cbm_rods_math.h.
 //
 // The state is double-buffered: k_rod_step reads buffer a (committed) and
 // writes buffer b, so 1 and 2 are one launch and the commit is a swap.  The
 // same launch computes the cell of each new position and its atomic rank
 // (assignCells); the scan, scatter and stable passes of cbm_grid.cuh finish
-// the grid.  Four launches per step, replayed from a CUDA graph of two steps.
+// the grid.  Four launches per step (seven with growth: the division flags,
+// their scan and the holes come first), replayed from a CUDA graph of two
+// steps.
 //
 // A rod's candidates are spread over a group of kRodLanes lanes: lane k takes
 // candidates k, k + G, ...; after each chunk of G the group's terms are
