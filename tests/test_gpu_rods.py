@@ -1,8 +1,9 @@
-"""The device rods2D model (cbm_rods_*, src/models/rods.jl) against the
-checker, bit for bit: Float32 and Float64, CellLinked and all-pairs neighbors,
-dense colonies where most rods touch several others, rods outside the simBox
-(clamped into the border cells), several steps per call, and the empty and
-single-rod cases."""
+"""The device rods2D and rods2dGrowth models (cbm_rods_*, src/models/rods.jl)
+against the checker, bit for bit: Float32 and Float64, CellLinked and
+all-pairs neighbors, dense colonies where most rods touch several others, rods
+outside the simBox (clamped into the border cells), several steps per call,
+graph and one-by-one launches, the empty and single-rod cases, and growing
+colonies whose rods divide (rows filled from the tail as update! does)."""
 import math
 
 import numpy as np
