@@ -1549,7 +1549,8 @@ void rodStep(Rods<T>& R) {
  * (kernelListSurvived / kernelFillHolesParameters, update.jl:15-84) and
  * commits.  When the births do not fit below n_max, no rod divides in that
  * step and the overflow is reported: the device's behaviour, where the
- * reference would add up to the capacity and raise. */
+ * reference adds daughters while rows remain, silently drops the rest and
+ * still removes every parent (functionRule.jl:58-70). */
 template <typename T>
 void rodStepGrowth(Rods<T>& R) {
   const int64_t N = R.n, nMax = R.cfg.n_max;
