@@ -21,8 +21,21 @@ from _oracle import OracleRods, load_oracle, oracle_rod_pair
 abi = cbm._abi
 
 
+def _sqrt(v):
+    """sqrt in the operand's precision (np.float32 stays Float32)."""
+    return np.sqrt(v) if isinstance(v, np.float32) else math.sqrt(v)
+
+
 def _cossin(theta):
     lib = load_oracle(abi)
+    if isinstance(theta, np.float32):
+        w = theta * np.float32(0.15915494309189535)
+        w = w - np.floor(w)
+        if w >= 1:
+            w = w - np.float32(1)
+        c, s = C.c_float(), C.c_float()
+        lib.oracle_cossin_f32(float(w), C.byref(c), C.byref(s))
+        return np.float32(c.value), np.float32(s.value)
     w = theta * 0.15915494309189535
     w = w - math.floor(w)
     if w >= 1.0:
@@ -69,7 +82,7 @@ def point2line(x1, y1, x2, y2, t2):
 
 
 def point_inside_rod(x1, y1, l1, t1, px, py, sep):
-    di = jl_max(math.sqrt((x1 - px) * (x1 - px) + (y1 - py) * (y1 - py)), 0.00000001)
+    di = jl_max(_sqrt((x1 - px) * (x1 - px) + (y1 - py) * (y1 - py)), 0.00000001)
     dxi = (px - x1) / di
     dyi = (py - y1) / di
     return sep * jl_min(di, l1 / 2) * dxi + x1, sep * jl_min(di, l1 / 2) * dyi + y1
@@ -78,8 +91,8 @@ def point_inside_rod(x1, y1, l1, t1, px, py, sep):
 def rod_intersection(x1, y1, l1, t1, x2, y2, l2, t2, sep=0.99):
     x1a, y1a, x2a, y2a = x1, y1, x2, y2
     px, py = intersection2lines(x1, y1, t1, x2, y2, t2)
-    di = math.sqrt((x1 - px) * (x1 - px) + (y1 - py) * (y1 - py))
-    dj = math.sqrt((x2 - px) * (x2 - px) + (y2 - py) * (y2 - py))
+    di = _sqrt((x1 - px) * (x1 - px) + (y1 - py) * (y1 - py))
+    dj = _sqrt((x2 - px) * (x2 - px) + (y2 - py) * (y2 - py))
     c1, s1 = _cossin(t1)
     c2, s2 = _cossin(t2)
     norm = c1 * s2 - s1 * c2
@@ -100,11 +113,11 @@ def rod_intersection(x1, y1, l1, t1, x2, y2, l2, t2, sep=0.99):
     else:
         x2a, y2a = point_inside_rod(x2, y2, l2, t2, px, py, sep)
         x1a, y1a = point2line(x2a, y2a, x1, y1, t1)
-        dj = math.sqrt((x1 - x1a) * (x1 - x1a) + (y1 - y1a) * (y1 - y1a))
+        dj = _sqrt((x1 - x1a) * (x1 - x1a) + (y1 - y1a) * (y1 - y1a))
         if dj > l1 / 2:
             x1a, y1a = point_inside_rod(x1, y1, l1, t1, px, py, sep)
             x2b, y2b = point2line(x1a, y1a, x2, y2, t2)
-            dj = math.sqrt((x2 - x2b) * (x2 - x2b) + (y2 - y2b) * (y2 - y2b))
+            dj = _sqrt((x2 - x2b) * (x2 - x2b) + (y2 - y2b) * (y2 - y2b))
             if dj < l2 / 2:
                 x2a, y2a = x2b, y2b
     return x1a, y1a, x2a, y2a
@@ -112,10 +125,10 @@ def rod_intersection(x1, y1, l1, t1, x2, y2, l2, t2, sep=0.99):
 
 # --- rodForces (src/models/rods.jl:21-59) ----------------------------------------
 def rod_forces(x, y, d, l, th, vx, vy, m, x2, y2, d2, l2, th2, vx2, vy2, kn, gn, gt, mucc,
-               pow15=lambda v: v * math.sqrt(v)):
+               pow15=lambda v: v * _sqrt(v)):
     fx = fy = w = 0.0
     xi, yi, xj, yj = rod_intersection(x, y, l, th, x2, y2, l2, th2)
-    rij = math.sqrt((xi - xj) * (xi - xj) + (yi - yj) * (yi - yj))
+    rij = _sqrt((xi - xj) * (xi - xj) + (yi - yj) * (yi - yj))
     if rij > 0.0 and rij < (d + d2) / 2:
         delta = d - rij
         me = m / 2
@@ -125,7 +138,7 @@ def rod_forces(x, y, d, l, th, vx, vy, m, x2, y2, d2, l2, th2, vx2, vy2, kn, gn,
         vijy = vy - vy2
         vn = nx * vijx + ny * vijy
         fn = kn * pow15(delta) - gn * me * delta * vn
-        ft = -jl_min(gt * me * math.sqrt(delta), mucc * fn)
+        ft = -jl_min(gt * me * _sqrt(delta), mucc * fn)
         fx = fn * nx + ft * (vijx - vn * nx)
         fy = fn * ny + ft * (vijy - vn * ny)
         w = (xi - x) * fy - (yi - y) * fx
@@ -217,7 +230,7 @@ def _py_step(st, neighbors, edge):
     """One step!: agentStepDE! (Euler over rods2D's agentODE), update!,
     with neighbors walked as @loopOverNeighbors does."""
     n = len(st["x"])
-    f = {k: list(map(float, v)) for k, v in st.items()}
+    f = {k: list(np.asarray(v)) for k, v in st.items()}
     order = list(range(n))
     if neighbors == abi.NEIGH_CELL_LINKED:
         nc = [math.ceil((BOX_HI[d] - BOX_LO[d]) / edge + 2) for d in range(2)]
@@ -226,7 +239,8 @@ def _py_step(st, neighbors, edge):
         members = {}
         for i in range(n):
             members.setdefault(cell[i], []).append(i)
-    new = {k: [0.0] * n for k in ("fx", "fy", "W", "pressure")}
+    zero = f["x"][0] * 0 if n else 0.0
+    new = {k: [zero] * n for k in ("fx", "fy", "W", "pressure")}
     for i in range(n):
         if neighbors == abi.NEIGH_FULL:
             cand = order
@@ -250,7 +264,7 @@ def _py_step(st, neighbors, edge):
             fx += a
             fy += b
             w += c
-            p += math.sqrt(a * a + b * b)
+            p += _sqrt(a * a + b * b)
         new["fx"][i], new["fy"][i], new["W"][i], new["pressure"][i] = fx, fy, w, p
     dt, beta, bw = PARAMS["dt"], PARAMS["beta"], PARAMS["beta_w"]
     out = {k: list(v) for k, v in f.items()}
@@ -266,6 +280,27 @@ def _py_step(st, neighbors, edge):
     for k in new:
         out[k] = new[k]
     return {k: np.array(v) for k, v in out.items()}
+
+
+@pytest.mark.parametrize("neighbors", ["full", "cell_linked"])
+def test_rods_step_f32_matches_transcription(neighbors):
+    """The Float32 checker against the same transcription run on np.float32
+    scalars: every operation and constant in Float32."""
+    nb = abi.NEIGH_FULL if neighbors == "full" else abi.NEIGH_CELL_LINKED
+    st = {k: v.astype(np.float32) for k, v in _colony(50, 4, box=5.0).items()}
+    cfg = abi.make_rods_config(50, BOX_LO, BOX_HI, cell_edge=4.0, neighbors=nb,
+                               precision=abi.F32, **PARAMS)
+    orc = OracleRods(abi, cfg)
+    orc.upload(st)
+    ref = st
+    for _ in range(3):
+        ref = _py_step(ref, nb, 4.0)
+        orc.step(1)
+        got = orc.download()
+        for k in abi.ROD_FIELDS[:13]:
+            assert ref[k].dtype == np.float32, k
+            np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+    assert np.count_nonzero(ref["pressure"]) > 10
 
 
 @pytest.mark.parametrize("neighbors", ["full", "cell_linked"])
