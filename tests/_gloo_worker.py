@@ -112,3 +112,31 @@ def run_fit(rank, world, port, out_dir):
     finally:
         dist.barrier()
         dist.destroy_process_group()
+
+
+SWARM_SEARCH = {"k_rep": (5.0, 20.0), "sigma": (0.0, 0.1)}
+
+
+def swarm_rows(rank=0, world=1, dist=None):
+    """swarm_algorithm over the host batch; every rank runs the same driver
+    with the same seed and scores its share of each generation."""
+    cbm = load_package()
+    ev = cbm.fitting.BatchedEvaluator(None, fit_state(0, None), fit_loss, 5, (0.0,) * 3,
+                                      (1.0,) * 3, FIT_DEFAULTS, rank=rank, world=world,
+                                      dist=dist, factory=FakeBatch)
+    rows = cbm.fitting.swarm_algorithm(None, SWARM_SEARCH, population=6, stop_max_generations=3,
+                                       rng=np.random.default_rng(2), evaluate_population=ev,
+                                       return_all=True)
+    return np.array([[r["k_rep"], r["sigma"], r["_score_"]] for r in rows])
+
+
+def run_swarm(rank, world, port, out_dir):
+    """The swarm driver with each generation partitioned over two gloo ranks."""
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        np.save(os.path.join(out_dir, f"swarm{rank}.npy"), swarm_rows(rank, world, dist))
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()

@@ -179,3 +179,26 @@ def test_batched_evaluator_host_batch():
     for c, r in enumerate(rows):
         expect = float(np.mean(x0 + 5 * (c + 1) * 1e-3)) + r["sigma"]
         assert r["_score_"] == pytest.approx(expect, rel=1e-12)
+
+
+def test_swarm_generations_sharded_over_two_gloo_ranks(tmp_path):
+    """Each generation's batch is partitioned over two ranks and the scores
+    gathered; both ranks then hold the single-rank run's rows exactly."""
+    import socket
+
+    import torch.multiprocessing as mp
+    world = 2
+    ctx = mp.get_context("spawn")
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    procs = [ctx.Process(target=W.run_swarm, args=(r, world, port, str(tmp_path)))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    r0, r1 = (np.load(tmp_path / f"swarm{r}.npy") for r in range(world))
+    np.testing.assert_array_equal(r0, r1)
+    np.testing.assert_array_equal(r0, W.swarm_rows())
