@@ -1768,6 +1768,11 @@ double oracle_uniform_f64(uint64_t seed, int64_t step, uint32_t agent, uint32_t 
   return cbm_uniform_f64(seed, step, agent, stream, community);
 }
 
+float oracle_uniform_f32(uint64_t seed, int64_t step, uint32_t agent, uint32_t stream,
+                         uint32_t community) {
+  return cbm_uniform_f32(seed, step, agent, stream, community);
+}
+
 /* the rod count and the error code (CBM_ERR_AGENT_OVERFLOW) of the last steps */
 int64_t oracle_rods_count(void* vh, int* err) {
   RodHandle* h = (RodHandle*)vh;

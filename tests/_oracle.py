@@ -63,6 +63,7 @@ def load_oracle(abi):
         "oracle_rod_pair_f64": (C.c_int, [C.POINTER(dbl)] * 4),
         "oracle_rods_count": (i64, [vp, C.POINTER(C.c_int)]),
         "oracle_uniform_f64": (dbl, [u64, i64, u32, u32, u32]),
+        "oracle_uniform_f32": (C.c_float, [u64, i64, u32, u32, u32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

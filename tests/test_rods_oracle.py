@@ -252,7 +252,7 @@ def _py_step(st, neighbors, edge):
                     qx, qy = cx + dx, cy + dy
                     if 0 <= qx < nc[0] and 0 <= qy < nc[1]:
                         cand += members.get(qx + nc[0] * qy, [])
-        fx = fy = w = p = 0
+        fx = fy = w = p = zero
         for j in cand:
             if j == i:
                 continue
@@ -326,8 +326,11 @@ def test_rods_step_matches_transcription(neighbors):
 GROW = dict(growth=200.0, alpha=50.0, sigma_l_target=0.2, l_max=3.0, seed=77)
 
 
-def _uniform(step, agent, stream):
-    return load_oracle(abi).oracle_uniform_f64(GROW["seed"], step, agent, stream, 0)
+def _uniform(step, agent, stream, f32=False):
+    lib = load_oracle(abi)
+    if f32:
+        return np.float32(lib.oracle_uniform_f32(GROW["seed"], step, agent, stream, 0))
+    return lib.oracle_uniform_f64(GROW["seed"], step, agent, stream, 0)
 
 
 def _py_grow_step(st, step, neighbors, edge, n_max):
@@ -336,19 +339,23 @@ def _py_grow_step(st, step, neighbors, edge, n_max):
     given taken from the parent; @removeAgent), agentStepDE! (rods2D's ODE and
     dt(l) = growth/(1+α pressure), pressure committed), update! (holes filled
     from the surviving tail, update.jl:15-84) and the commit."""
-    f = {k: list(map(float, v)) for k, v in st.items()}
+    f32 = np.asarray(st["x"]).dtype == np.float32
+    T = np.float32 if f32 else float
+    f = {k: list(np.asarray(v)) for k, v in st.items()}
     n = len(f["x"])
     de = _py_step(st, neighbors, edge)  # rows < n: Euler and the neighbor sums
-    g = {k: list(map(float, v)) for k, v in de.items()}
+    g = {k: list(np.asarray(v)) for k, v in de.items()}
     for i in range(n):
-        g["l"][i] = f["l"][i] + (GROW["growth"] / (1 + GROW["alpha"] * f["pressure"][i])) * PARAMS["dt"]
+        g["l"][i] = f["l"][i] + (T(GROW["growth"]) / (1 + T(GROW["alpha"]) * f["pressure"][i])) * \
+            T(PARAMS["dt"])
     dividers = [i for i in range(n) if f["l"][i] > f["l_target"][i]]
     holes, survive = [], [True] * (n + 2 * len(dividers))
     if n + 2 * len(dividers) <= n_max:
-        lo, hi = GROW["l_max"] - GROW["sigma_l_target"], GROW["l_max"] + GROW["sigma_l_target"]
+        lo = T(GROW["l_max"]) - T(GROW["sigma_l_target"])
+        hi = T(GROW["l_max"]) + T(GROW["sigma_l_target"])
         for i in dividers:
             c, s = _cossin(f["theta"][i])
-            ww = (0.1 - -0.1) * _uniform(step, i, 5) + -0.1
+            ww = (T(0.1) - T(-0.1)) * _uniform(step, i, 5, f32) + T(-0.1)
             l, d = f["l"][i], f["d"][i]
             for h in (0, 1):
                 for k in g:
@@ -358,7 +365,7 @@ def _py_grow_step(st, step, neighbors, edge, n_max):
                 g["y"][-1] = sg * s + f["y"][i]
                 g["l"][-1] = (l - d) / 2
                 g["omega"][-1] = f["omega"][i] + ww if h == 0 else f["omega"][i] - ww
-                g["l_target"][-1] = (hi - lo) * _uniform(step, i, 6 + h) + lo
+                g["l_target"][-1] = (hi - lo) * _uniform(step, i, 6 + h, f32) + lo
             holes.append(i)
             survive[i] = False
     repo, last = [], len(g["x"]) - 1
@@ -374,20 +381,24 @@ def _py_grow_step(st, step, neighbors, edge, n_max):
     return {k: np.array(v[:n_new]) for k, v in g.items()}
 
 
+@pytest.mark.parametrize("prec", ["f64", "f32"])
 @pytest.mark.parametrize("neighbors", ["full", "cell_linked"])
-def test_rods_growth_step_matches_transcription(neighbors):
-    """rods2dGrowth in Float64: divisions in most steps, including rods that
-    divide in the same step, against the transcription, field by field."""
+def test_rods_growth_step_matches_transcription(neighbors, prec):
+    """rods2dGrowth: divisions in most steps, including rods that divide in
+    the same step, against the transcription, field by field (in Float32 on
+    np.float32 scalars)."""
     nb = abi.NEIGH_FULL if neighbors == "full" else abi.NEIGH_CELL_LINKED
     edge = 4.0
     st = _colony(24, 5, box=5.0)
     rng = np.random.default_rng(6)
     st["l_target"] = st["l"] + rng.uniform(-0.02, 0.06, 24)  # a third divide at once
+    if prec == "f32":
+        st = {k: v.astype(np.float32) for k, v in st.items()}
     cfg = abi.make_rods_config(200, BOX_LO, BOX_HI, cell_edge=edge, neighbors=nb,
-                               precision=abi.F64, **PARAMS, **GROW)
+                               precision=abi.F32 if prec == "f32" else abi.F64, **PARAMS, **GROW)
     orc = OracleRods(abi, cfg)
     orc.upload(st)
-    ref = {k: np.asarray(v, dtype=float) for k, v in st.items()}
+    ref = dict(st)
     sizes = []
     for step in range(6):
         ref = _py_grow_step(ref, step, nb, edge, 200)
@@ -397,6 +408,7 @@ def test_rods_growth_step_matches_transcription(neighbors):
         for k in abi.ROD_FIELDS:
             np.testing.assert_array_equal(got[k], ref[k], err_msg=f"{k} after step {step}")
         sizes.append(len(ref["x"]))
+        assert all(v.dtype == st["x"].dtype for v in ref.values())
     assert sizes[0] > 24 and sizes[-1] > sizes[0]
 
 
