@@ -53,3 +53,44 @@ def test_ctypes_mirrors_match_the_header(tmp_path):
         for fname, _ in cls._fields_:
             field = getattr(cls, fname)
             assert table[(cname, fname)] == (field.offset, field.size), (cname, fname)
+
+
+JULIA_TYPES = {"Int32": C.c_int32, "Int64": C.c_int64, "UInt32": C.c_uint32,
+               "UInt64": C.c_uint64, "Float64": C.c_double}
+
+
+def _julia_structs():
+    """name -> [(field, Julia type)] of the `struct Cbm... end` blocks of the
+    Julia stubs."""
+    import re
+    text = open(os.path.join(conftest.ROOT, "INTEGRATION.md")).read()
+    out = {}
+    for m in re.finditer(r"^(?:mutable )?struct (Cbm\w+)\n(.*?)^end", text, flags=re.S | re.M):
+        fields = []
+        for part in re.split(r"[;\n]", m.group(2)):
+            part = part.strip()
+            if part:
+                name, typ = part.split("::")
+                fields.append((name.strip(), typ.strip()))
+        out[m.group(1)] = fields
+    return out
+
+
+def _ctype_of(julia):
+    import re
+    m = re.fullmatch(r"NTuple\{(\d+),(\w+)\}", julia)
+    if m:
+        return JULIA_TYPES[m.group(2)] * int(m.group(1))
+    return JULIA_TYPES[julia]
+
+
+def test_julia_stub_structs_match_the_mirrors():
+    """The Julia mirrors in the ccall stubs list the C fields in order, with
+    types of the same size (Julia cannot run here, so the text is checked)."""
+    jl = _julia_structs()
+    for name in ("CbmConfig", "CbmCommunityDesc", "CbmBatchTuning", "CbmMediumConfig",
+                 "CbmRodsConfig"):
+        cls = getattr(abi, name)
+        assert [f for f, _ in jl[name]] == [f for f, _ in cls._fields_], name
+        for (f, jt), (_, ct) in zip(jl[name], cls._fields_):
+            assert C.sizeof(_ctype_of(jt)) == C.sizeof(ct), (name, f)
