@@ -110,17 +110,26 @@ __device__ __forceinline__ void rod_assign_cell(const RodStep<T>& R, int row, T 
   R.agent_rank[row] = atomicAdd(R.cell_count + c, 1);
 }
 
+// The rows that @addAgent keeps: A = min(2D, n_max - n) (functionRule.jl:58-70
+// drops a birth whose row would pass nMax_)
+__device__ __forceinline__ int rod_births(int n, int D, int n_max) {
+  return 2 * D < n_max - n ? 2 * D : n_max - n;
+}
+
 // rods2dGrowth's rule for a rod with l > lTarget (rods.jl:141-161), with the
 // bookkeeping of @addAgent / @removeAgent and update! folded in.  The k-th
-// dividing rod (index order) adds rows n + 2k and n + 2k + 1 and leaves a
-// hole at its own row.  update! then moves the last D of the n + 2D rows, in
-// reverse order, into the holes in ascending order
+// dividing rod (index order) asks for rows n + 2k and n + 2k + 1, of which
+// the first A exist, and leaves a hole at its own row.  update! then moves
+// the highest surviving rows, newborns first and then old rows from the top,
+// into the holes in ascending order while the hole lies below its source
 // (kernelListSurvived / kernelFillHolesParameters, update.jl:15-84).  So
-// row s >= n + D lands at holes[n + 2D - 1 - s], and every other row stays.
-// Fields not given to @addAgent are the parent's committed values.
+// newborn row s lands at holes[n + A - 1 - s] when that index is below D,
+// and stays at s otherwise.  Fields not given to @addAgent are the parent's
+// committed values.
 template <typename T>
 __device__ void rod_divide(const RodStep<T>& R, int i, int n) {
   const int D = R.div_rank[n], k = R.div_rank[i];
+  const int A = rod_births(n, D, R.n_max);
   const long long step = R.cnt_a[1];
   const T x = R.a[kSX][i], y = R.a[kSY][i], c = R.a[kSCOS][i], s = R.a[kSSIN][i];
   const T l = R.a[kSL][i], d = R.a[kSD][i], om = R.a[kSOM][i];
@@ -130,8 +139,10 @@ __device__ void rod_divide(const RodStep<T>& R, int i, int n) {
   const T q = (l + d) / (T)4;
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
-    const int slot = n + 2 * k + h;  // < n_max: the caller checked n + 2 D <= n_max
-    const int row = slot < n + D ? slot : R.holes[n + 2 * D - 1 - slot];
+    if (2 * k + h >= A) continue;  // the birth found no row below n_max
+    const int slot = n + 2 * k + h;
+    const int m = n + A - 1 - slot;  // in [0, A)
+    const int row = m < D ? R.holes[m] : slot;
     const T xs = h == 0 ? q * c + x : (-(l + d) / (T)4) * c + x;
     const T ys = h == 0 ? q * s + y : (-(l + d) / (T)4) * s + y;
     const T lt = (R.lt_hi - R.lt_lo) *
@@ -234,12 +245,18 @@ __global__ void __launch_bounds__(kRodBlock) k_rod_step(RodStep<T> R) {
     }
   }
   if (!live || lane != 0) return;
+  int row = i;  // the final row of rod i
   if constexpr (GROW) {
-    // without room for every birth the step divides nothing and reports the
-    // overflow (k_rod_holes), so the rows stay well formed
-    if (R.div_rank[i + 1] != R.div_rank[i] && n + 2 * R.div_rank[n] <= R.n_max) {
+    if (R.div_rank[i + 1] != R.div_rank[i]) {
       rod_divide<T>(R, i, n);
       return;
+    }
+    // with fewer births than parents, update! also moves old rows: rod i is
+    // the (n - 1 - i - dividers above it)-th surviving old row from the top
+    const int D = R.div_rank[n], A = rod_births(n, D, R.n_max);
+    if (A < D) {
+      const int q = A + (n - 1 - i) - (D - R.div_rank[i + 1]);
+      if (q < D && R.holes[q] < i) row = R.holes[q];
     }
   }
   // Euler: u + du dt with the committed forces, then the commit of the sums
@@ -251,28 +268,28 @@ __global__ void __launch_bounds__(kRodBlock) k_rod_step(RodStep<T> R) {
   const T den = (m * ((d + l) * (d + l))) / (T)12 + m * (d * d);
   const T dom = R.a[kSW][i] / den - R.beta_w * om;
   const T xn = g.x + vx * dt, yn = g.y + vy * dt, thn = th + om * dt;
-  R.b[kSX][i] = xn;
-  R.b[kSY][i] = yn;
-  R.b[kSVX][i] = vx + dvx * dt;
-  R.b[kSVY][i] = vy + dvy * dt;
-  R.b[kSTH][i] = thn;
-  R.b[kSOM][i] = om + dom * dt;
-  R.b[kSFX][i] = fx;
-  R.b[kSFY][i] = fy;
-  R.b[kSW][i] = w;
-  R.b[kSP][i] = p;
+  R.b[kSX][row] = xn;
+  R.b[kSY][row] = yn;
+  R.b[kSVX][row] = vx + dvx * dt;
+  R.b[kSVY][row] = vy + dvy * dt;
+  R.b[kSTH][row] = thn;
+  R.b[kSOM][row] = om + dom * dt;
+  R.b[kSFX][row] = fx;
+  R.b[kSFY][row] = fy;
+  R.b[kSW][row] = w;
+  R.b[kSP][row] = p;
   T cn, sn;
   cbm_rod_cossin<T>(thn, &cn, &sn);
-  R.b[kSCOS][i] = cn;
-  R.b[kSSIN][i] = sn;
+  R.b[kSCOS][row] = cn;
+  R.b[kSSIN][row] = sn;
   if constexpr (GROW) {
     // dt(l) = growth/(1 + alpha pressure), the committed pressure (rods.jl:137-139)
-    R.b[kSL][i] = l + (R.growth / ((T)1 + R.alpha * R.a[kSP][i])) * dt;
-    R.b[kSLT][i] = R.a[kSLT][i];
-    R.b[kSD][i] = d;
-    R.b[kSM][i] = m;
+    R.b[kSL][row] = l + (R.growth / ((T)1 + R.alpha * R.a[kSP][i])) * dt;
+    R.b[kSLT][row] = R.a[kSLT][i];
+    R.b[kSD][row] = d;
+    R.b[kSM][row] = m;
   }
-  if (!R.full) rod_assign_cell<T>(R, i, xn, yn);
+  if (!R.full) rod_assign_cell<T>(R, row, xn, yn);
 }
 
 // rods2dGrowth, before the step: the division flags l > lTarget of the
@@ -294,11 +311,10 @@ __global__ void __launch_bounds__(kTile) k_rod_holes(RodStep<T> R, int* holes, C
   const int i = blockIdx.x * kTile + threadIdx.x;
   const int n = (int)R.cnt_a[0];
   if (i == 0) {
-    const long long D = R.div_rank[n];
-    const bool room = n + 2 * D <= R.n_max;
-    R.cnt_b[0] = room ? n + D : n;
+    const int D = R.div_rank[n], A = rod_births(n, D, R.n_max);
+    R.cnt_b[0] = n + A - D;  // N + NAdd - NRemove
     R.cnt_b[1] = R.cnt_a[1] + 1;
-    if (!room) atomicOr(&ctr->err, kErrAgentOverflow);
+    if (A < 2 * D) atomicOr(&ctr->err, kErrAgentOverflow);  // births were dropped
   }
   if (i >= n) return;
   if (R.div_rank[i + 1] != R.div_rank[i]) holes[R.div_rank[i]] = i;

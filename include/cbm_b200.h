@@ -422,9 +422,8 @@ enum {
  * fields[CBM_ROD_L_TARGET] with growth_model; sets the step to 0 */
 int cbm_rods_upload(cbm_rods* r, int64_t n, const void* const* fields);
 /* With growth_model, flags & CBM_SYNC also reports CBM_ERR_AGENT_OVERFLOW when
- * the births of a step did not fit below n_max; that step divided nothing
- * (the reference instead drops the births beyond n_max and still removes
- * every parent). */
+ * births were dropped for want of rows below n_max; as in the reference, the
+ * step drops them in order and still removes every parent. */
 int cbm_rods_step(cbm_rods* r, int32_t nsteps, int32_t flags);
 /* fields[k] (host arrays of at least n reals, or NULL) receive the fields;
  * *n_out = n (with growth_model the current count, read back from the device) */

@@ -1547,10 +1547,8 @@ void rodStep(Rods<T>& R) {
  * functionRule.jl:9-111); agentStepDE! integrates rows < N from the committed
  * state; update! fills the holes from the surviving tail
  * (kernelListSurvived / kernelFillHolesParameters, update.jl:15-84) and
- * commits.  When the births do not fit below n_max, no rod divides in that
- * step and the overflow is reported: the device's behaviour, where the
- * reference adds daughters while rows remain, silently drops the rest and
- * still removes every parent (functionRule.jl:58-70). */
+ * commits.  Births beyond n_max are dropped in order and every parent is
+ * still removed (functionRule.jl:58-70); the overflow is also reported. */
 template <typename T>
 void rodStepGrowth(Rods<T>& R) {
   const int64_t N = R.n, nMax = R.cfg.n_max;
@@ -1560,14 +1558,10 @@ void rodStepGrowth(Rods<T>& R) {
   std::vector<T> G[CBM_RODS_FIELDS];
   for (int q = 0; q < CBM_RODS_FIELDS; ++q) G[q] = F[q];
   // agentStepRule!
-  int64_t D = 0;
-  for (int64_t i = 0; i < N; ++i) D += F[CBM_ROD_L][i] > F[CBM_ROD_L_TARGET][i];
   std::vector<int64_t> holes;
   std::vector<char> survive((size_t)nMax, 1);
   int64_t nAdd = 0;
-  if (N + 2 * D > nMax) {
-    R.err = CBM_ERR_AGENT_OVERFLOW;
-  } else {
+  {
     const T lo = (T)R.cfg.l_max - (T)R.cfg.sigma_l_target;
     const T hi = (T)R.cfg.l_max + (T)R.cfg.sigma_l_target;
     for (int64_t i = 0; i < N; ++i) {
@@ -1580,7 +1574,12 @@ void rodStepGrowth(Rods<T>& R) {
                        cbm_uniform<T>(R.cfg.seed, R.step, (uint32_t)i, CBM_STREAM_ROD_TORQUE, 0u) +
                    (T)-0.1;
       for (int h = 0; h < 2; ++h) {
+        // @addAgent: i1New_ = N + NAdd_ + 1 is kept only if nMax_ >= i1New_
         const int64_t slot = N + nAdd;
+        if (slot >= nMax) {
+          R.err = CBM_ERR_AGENT_OVERFLOW;
+          continue;
+        }
         nAdd += 1;
         for (int q = 0; q < CBM_RODS_FIELDS; ++q) G[q][slot] = F[q][i];
         const T sg = h == 0 ? (l + d) / (T)4 : -(l + d) / (T)4;
@@ -1592,7 +1591,7 @@ void rodStepGrowth(Rods<T>& R) {
             (hi - lo) * cbm_uniform<T>(R.cfg.seed, R.step, (uint32_t)i,
                                        CBM_STREAM_ROD_TARGET + (uint32_t)h, 0u) + lo;
       }
-      holes.push_back(i);
+      holes.push_back(i);  // @removeAgent
       survive[(size_t)i] = 0;
     }
   }

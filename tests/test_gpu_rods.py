@@ -167,19 +167,35 @@ def test_rods_growth_bitexact(gpu_lib, abi, prec, neighbors, graph):
     assert sizes[0] > n0 and sizes[-1] > sizes[0]
 
 
-def test_rods_growth_overflow(gpu_lib, abi):
+@pytest.mark.parametrize("n_max", [100, 101, 130, 160, 199, 300])
+def test_rods_growth_overflow(gpu_lib, abi, n_max):
+    """Births beyond n_max are dropped in order and every parent is still
+    removed (functionRule.jl:58-70), old rows moving into the holes when
+    fewer daughters than parents were born; the status reports the
+    overflow.  Rows match the checker bit for bit, from no room to room for
+    every birth."""
     from conftest import cbm
     st = _growth_colony(abi, 100, 32, 9.0)
-    st["l_target"] = st["l"] - 1.0  # every rod divides: 300 rows > n_max
-    cfg = abi.make_rods_config(250, (-20.0, -20.0), (20.0, 20.0), cell_edge=4.0,
+    st["l_target"] = st["l"] + np.where(np.arange(100) % 4 == 1, 1.0, -1.0)  # 75 divide
+    cfg = abi.make_rods_config(n_max, (-20.0, -20.0), (20.0, 20.0), cell_edge=4.0,
                                **bench_rod_params(), **GROW)
     g = cbm._abi.Rods2D(cfg)
+    o = OracleRods(abi, cfg)
     g.upload(st)
-    with pytest.raises(cbm._abi.CbmError) as e:
+    o.upload(st)
+    if n_max < 250:
+        with pytest.raises(cbm._abi.CbmError) as e:
+            g.step(1)
+        assert e.value.code == abi.CBM_ERR_AGENT_OVERFLOW
+    else:
         g.step(1)
-    assert e.value.code == abi.CBM_ERR_AGENT_OVERFLOW
-    assert len(g.download()["x"]) == 100  # nothing divided
+    o.step(1)
+    a, b = g.download(), o.download()
+    assert len(a["x"]) == len(b["x"]) == 100 + min(150, n_max - 100) - 75
+    for k in abi.ROD_FIELDS:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
     g.close()
+    o.close()
 
 
 def bench_rod_params():

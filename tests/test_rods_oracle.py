@@ -349,25 +349,26 @@ def _py_grow_step(st, step, neighbors, edge, n_max):
         g["l"][i] = f["l"][i] + (T(GROW["growth"]) / (1 + T(GROW["alpha"]) * f["pressure"][i])) * \
             T(PARAMS["dt"])
     dividers = [i for i in range(n) if f["l"][i] > f["l_target"][i]]
-    holes, survive = [], [True] * (n + 2 * len(dividers))
-    if n + 2 * len(dividers) <= n_max:
-        lo = T(GROW["l_max"]) - T(GROW["sigma_l_target"])
-        hi = T(GROW["l_max"]) + T(GROW["sigma_l_target"])
-        for i in dividers:
-            c, s = _cossin(f["theta"][i])
-            ww = (T(0.1) - T(-0.1)) * _uniform(step, i, 5, f32) + T(-0.1)
-            l, d = f["l"][i], f["d"][i]
-            for h in (0, 1):
-                for k in g:
-                    g[k].append(f[k][i])
-                sg = (l + d) / 4 if h == 0 else -(l + d) / 4
-                g["x"][-1] = sg * c + f["x"][i]
-                g["y"][-1] = sg * s + f["y"][i]
-                g["l"][-1] = (l - d) / 2
-                g["omega"][-1] = f["omega"][i] + ww if h == 0 else f["omega"][i] - ww
-                g["l_target"][-1] = (hi - lo) * _uniform(step, i, 6 + h, f32) + lo
-            holes.append(i)
-            survive[i] = False
+    holes, survive = [], [True] * n_max
+    lo = T(GROW["l_max"]) - T(GROW["sigma_l_target"])
+    hi = T(GROW["l_max"]) + T(GROW["sigma_l_target"])
+    for i in dividers:
+        c, s = _cossin(f["theta"][i])
+        ww = (T(0.1) - T(-0.1)) * _uniform(step, i, 5, f32) + T(-0.1)
+        l, d = f["l"][i], f["d"][i]
+        for h in (0, 1):
+            if len(g["x"]) >= n_max:  # functionRule.jl:58-70: the birth is dropped
+                continue
+            for k in g:
+                g[k].append(f[k][i])
+            sg = (l + d) / 4 if h == 0 else -(l + d) / 4
+            g["x"][-1] = sg * c + f["x"][i]
+            g["y"][-1] = sg * s + f["y"][i]
+            g["l"][-1] = (l - d) / 2
+            g["omega"][-1] = f["omega"][i] + ww if h == 0 else f["omega"][i] - ww
+            g["l_target"][-1] = (hi - lo) * _uniform(step, i, 6 + h, f32) + lo
+        holes.append(i)  # @removeAgent runs whether or not the births fitted
+        survive[i] = False
     repo, last = [], len(g["x"]) - 1
     while len(holes) > len(repo) and last >= 0:
         if survive[last]:
@@ -412,12 +413,101 @@ def test_rods_growth_step_matches_transcription(neighbors, prec):
     assert sizes[0] > 24 and sizes[-1] > sizes[0]
 
 
-def test_rods_growth_overflow_divides_nothing():
+@pytest.mark.parametrize("n_max", [10, 11, 14, 17, 25, 30])
+def test_rods_growth_overflow_matches_transcription(n_max):
+    """Births beyond n_max are dropped in order and every parent is still
+    removed; update! then also moves surviving old rows into the holes when
+    fewer daughters than parents were born.  Capacities from no room at all
+    to room for every birth."""
     st = _colony(10, 8, box=3.0)
-    st["l_target"] = st["l"] - 0.5  # every rod divides
-    cfg = abi.make_rods_config(25, BOX_LO, BOX_HI, cell_edge=4.0, precision=abi.F64, **PARAMS,
+    st["l_target"] = st["l"] + np.where(np.arange(10) % 3 == 1, 1.0, -0.5)  # 7 of 10 divide
+    cfg = abi.make_rods_config(n_max, BOX_LO, BOX_HI, cell_edge=4.0, precision=abi.F64, **PARAMS,
                                **GROW)
     orc = OracleRods(abi, cfg)
     orc.upload(st)
+    ref = _py_grow_step(dict(st), 0, abi.NEIGH_CELL_LINKED, 4.0, n_max)
     orc.step(1)
-    assert orc.count() == (10, abi.CBM_ERR_AGENT_OVERFLOW)
+    got = orc.download()
+    overflow = 10 + 2 * 7 > n_max
+    assert orc.count() == (len(ref["x"]), abi.CBM_ERR_AGENT_OVERFLOW if overflow else 0)
+    assert len(ref["x"]) == 10 + min(14, n_max - 10) - 7
+    for k in abi.ROD_FIELDS:
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+
+
+def _literal_rows(n, flags, n_max):
+    """The reference's bookkeeping on labels: rows after @addAgent /
+    @removeAgent and update!'s fill (update.jl:15-84)."""
+    rows = [("old", i) for i in range(n)]
+    survive = [True] * n_max
+    holes, k = [], 0
+    for i in range(n):
+        if not flags[i]:
+            continue
+        for h in (0, 1):
+            if len(rows) < n_max:
+                rows.append(("new", k, h))
+        holes.append(i)
+        survive[i] = False
+        k += 1
+    repo, last = [], len(rows) - 1
+    while len(holes) > len(repo) and last >= 0:
+        if survive[last]:
+            repo.append(last)
+        last -= 1
+    for hole, src in zip(holes, repo):
+        if hole < src:
+            rows[hole] = rows[src]
+    return rows[:len(rows) - len(holes)]
+
+
+def _device_rows(n, flags, n_max):
+    """The closed form of k_rod_holes / k_rod_step / rod_divide
+    (cellbasedmodels.jl_b200/csrc/cbm_rods.cu): every row written once, at
+    its final index."""
+    rank = [0] * (n + 1)
+    for i in range(n):
+        rank[i + 1] = rank[i] + flags[i]
+    D = rank[n]
+    A = min(2 * D, n_max - n)
+    holes = [i for i in range(n) if flags[i]]
+    out = [None] * (n + A - D)
+
+    def put(row, label):
+        assert 0 <= row < len(out) and out[row] is None, (row, label)
+        out[row] = label
+
+    for i in range(n):
+        if flags[i]:
+            k = rank[i]
+            for h in (0, 1):
+                e = 2 * k + h
+                if e >= A:
+                    continue
+                s = n + e
+                m = n + A - 1 - s
+                put(holes[m] if m < D else s, ("new", k, h))
+        else:
+            dest = i
+            if A < D:
+                m = A + (n - 1 - i) - (D - rank[i + 1])
+                if m < D and holes[m] < i:
+                    dest = holes[m]
+            put(dest, ("old", i))
+    assert None not in out
+    return out
+
+
+def test_device_closed_form_matches_the_bookkeeping():
+    """The device writes each row straight to its final index; on labels,
+    that gives the reference's rows for every mix of divisions and
+    capacities, overflow included."""
+    rng = np.random.default_rng(12)
+    cases = 0
+    for _ in range(3000):
+        n = int(rng.integers(0, 14))
+        flags = [int(v) for v in rng.random(n) < rng.random()]
+        n_max = n + int(rng.integers(0, 2 * sum(flags) + 3))
+        assert _device_rows(n, flags, n_max) == _literal_rows(n, flags, n_max), (n, flags, n_max)
+        cases += n_max < n + 2 * sum(flags)
+    assert cases > 500  # overflow cases covered
