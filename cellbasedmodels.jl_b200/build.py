@@ -1,7 +1,8 @@
 """Builds libcbm_b200.so, the sm_100a shared library behind include/cbm_b200.h.
 
-`python build.py` (or `build()` from Python) runs nvcc directly; the library
-is written next to this file so it travels with the source tree.  Flags:
+`python build.py` (or `build()` from Python) runs nvcc directly, one process
+per source file, and links the objects (kept in _build/) into the library,
+which is written next to this file so it travels with the source tree.  Flags:
   -gencode arch=compute_100a,code=sm_100a  B200 only
   -fmad=false   no FMA contraction: the same rounding as the Julia reference
                 and the CPU checker, which makes results bit-identical
@@ -24,13 +25,18 @@ DEPS = SOURCES + [
 ]
 
 
+OBJ_DIR = os.path.join(HERE, "_build")
+FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-fmad=false",
+         "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+
+
+def _nvcc():
+    return os.environ.get("NVCC", "nvcc")
+
+
 def nvcc_cmd(extra=()):
-    nvcc = os.environ.get("NVCC", "nvcc")
-    return [
-        nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3",
-        "-fmad=false", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-        "--expt-relaxed-constexpr", *extra, "-o", LIB, *SOURCES,
-    ]
+    """One nvcc command that compiles and links every source (serial)."""
+    return [_nvcc(), *FLAGS, "-shared", *extra, "-o", LIB, *SOURCES]
 
 
 def up_to_date():
@@ -41,9 +47,23 @@ def up_to_date():
 
 
 def build(force=False, verbose=False, extra=()):
+    """Compiles each source to an object in parallel, then links the library."""
     if not force and up_to_date():
         return LIB
-    cmd = nvcc_cmd(extra)
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    procs = []
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+        objs.append(obj)
+        cmd = [_nvcc(), *FLAGS, *extra, "-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((cmd, subprocess.Popen(cmd)))
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

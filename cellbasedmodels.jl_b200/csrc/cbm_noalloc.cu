@@ -12,6 +12,7 @@
 // file-scope array below.
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <mutex>
 #include <string>
 
@@ -41,7 +42,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void* g_scratch_ptr[kMaxDevices] = {};
-std::string g_noalloc_error;
+// The last argument error of this host thread: each thread reads the
+// message of its own failed call, and no two threads share the string.
+thread_local std::string g_noalloc_error;
 
 int nfail(int code, const char* msg) {
   g_noalloc_error = msg;
@@ -94,6 +97,28 @@ void launch(const void* const* pos, int n, const double* lo, const double* hi, d
 }  // namespace
 
 extern "C" const char* cbm_noalloc_last_error(void) { return g_noalloc_error.c_str(); }
+
+extern "C" int cbm_noalloc_status(void* stream) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+    return nfail(CBM_ERR_CUDA, "no usable CUDA device");
+  {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_scratch_ptr[dev]) return CBM_OK;  // no call has run on this device
+  }
+  // The error bits of the counter block in the static array, read after the
+  // work queued on `stream` (the last call's launches included) has finished.
+  int err = 0;
+  cudaError_t e = cudaMemcpyFromSymbolAsync(&err, g_noalloc_scratch, sizeof err,
+                                            offsetof(Counters, err), cudaMemcpyDeviceToHost,
+                                            (cudaStream_t)stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) return nfail(CBM_ERR_CUDA, cudaGetErrorString(e));
+  if (err & kErrTimeout)
+    return nfail(CBM_ERR_TIMEOUT,
+                 "the cell scan's bounded wait gave up: cell_start and cell_agents are incomplete");
+  return CBM_OK;
+}
 
 extern "C" int cbm_cell_grid_noalloc(const void* x, const void* y, const void* z, int32_t n_agents,
                                      int32_t dims, int32_t precision, const double* box_lo,

@@ -465,6 +465,14 @@ int cbm_cell_grid_noalloc(const void* x, const void* y, const void* z, int32_t n
                           const double* box_hi, double cell_edge, int32_t* agent_cell,
                           int32_t* cell_start, int32_t* cell_agents, void* stream);
 const char* cbm_noalloc_last_error(void);
+/* Status of the last cbm_cell_grid_noalloc call on the current device: waits
+ * for `stream` (the stream that call was given), then reads the error bits
+ * that its kernels left in the static scratch array.  CBM_ERR_TIMEOUT means
+ * the cell scan's bounded wait gave up and the grid it wrote is incomplete.
+ * It synchronises the stream, so call it outside any stream capture.  It
+ * allocates nothing.  The message of a failed call (of either function) is
+ * kept per host thread and read with cbm_noalloc_last_error(). */
+int cbm_noalloc_status(void* stream);
 
 #ifdef __cplusplus
 }

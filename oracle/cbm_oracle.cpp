@@ -1194,7 +1194,9 @@ void oracle_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t 
  * Manifest.toml but Julia cannot run here).  Directions 0..2 carry
  * d/d(k_rep, k_att, r_rep); further directions carry d/d of chosen initial
  * coordinates.  The cutoff r_att is a plain number (held fixed), as in the
- * adjoint.  All pairs are visited (small N).
+ * adjoint.  Pairs come from a cell grid rebuilt every step, in the
+ * reference's CellLinked order; agents are evaluated in parallel (each
+ * agent's sum is sequential, so the result does not depend on the threads).
  * ------------------------------------------------------------------------- */
 namespace {
 
@@ -1265,39 +1267,64 @@ extern "C" int oracle_adjoint_dual(const cbm_config* cfg, int64_t n, const doubl
   rho.d[2] = 1.0;
   const double ratt = cfg->r_att;
   const Dual dt = dconst(cfg->dt);
-  // The pair set is the reference's CellLinked one: j interacts with i only
-  // if their cells (cellPos, neighbors.jl:636-638, on the values) are
-  // neighbors.  Agents beyond simBox fall in the ghost layer, so the set is
-  // not every pair within the cutoff.
+  // The pair set and the order of the sums are the reference's CellLinked
+  // ones, with the grid rebuilt from the committed positions every step:
+  // agent i visits the 3^3 cells around its own (cellPosNeigh order, x
+  // fastest, neighbors.jl:658-708) and, inside a cell, the agents in
+  // ascending index (neighbors.jl:715-747).  Agents beyond simBox fall in the
+  // ghost layer (cellPos, neighbors.jl:636-638), so the set is not every pair
+  // within the cutoff.
   int64_t ncell[3];
   for (int d = 0; d < 3; ++d)
     ncell[d] = (int64_t)std::ceil((cfg->box_hi[d] - cfg->box_lo[d]) / cfg->cell_edge + 2.0);
-  std::vector<int64_t> cpos((size_t)n * 3);
+  const int64_t n_cells = ncell[0] * ncell[1] * ncell[2];
+  std::vector<int64_t> cell((size_t)n), start((size_t)n_cells + 1), order((size_t)n);
   for (int st = 0; st < nsteps; ++st) {
-    for (int64_t i = 0; i < n; ++i)
-      for (int d = 0; d < 3; ++d)
-        cpos[(size_t)i * 3 + d] = cellPos1<double>(cfg->cell_edge, x[d][(size_t)i].v, cfg->box_lo[d],
-                                                   cfg->box_hi[d], ncell[d]);
+    std::fill(start.begin(), start.end(), 0);
+    for (int64_t i = 0; i < n; ++i) {
+      int64_t lin = 0, mul = 1;
+      for (int d = 0; d < 3; ++d) {
+        lin += cellPos1<double>(cfg->cell_edge, x[d][(size_t)i].v, cfg->box_lo[d], cfg->box_hi[d],
+                                ncell[d]) * mul;
+        mul *= ncell[d];
+      }
+      cell[(size_t)i] = lin;
+      ++start[(size_t)lin + 1];
+    }
+    for (int64_t c = 0; c < n_cells; ++c) start[(size_t)c + 1] += start[(size_t)c];
+    {
+      std::vector<int64_t> fill(start.begin(), start.end() - 1);
+      for (int64_t i = 0; i < n; ++i) order[(size_t)fill[(size_t)cell[(size_t)i]]++] = i;
+    }
+#pragma omp parallel for schedule(dynamic, 64) num_threads(g_threads)
     for (int64_t i = 0; i < n; ++i) {
       Dual acc[3] = {dconst(0), dconst(0), dconst(0)};
-      for (int64_t j = 0; j < n; ++j) {
-        if (j == i) continue;
-        bool adjacent = true;
-        for (int d = 0; d < 3; ++d) {
-          int64_t dc = cpos[(size_t)i * 3 + d] - cpos[(size_t)j * 3 + d];
-          if (dc < -1 || dc > 1) adjacent = false;
+      const int64_t c = cell[(size_t)i];
+      const int64_t q[3] = {c % ncell[0], (c / ncell[0]) % ncell[1], c / (ncell[0] * ncell[1])};
+      for (int nb = 0; nb < 27; ++nb) {
+        const int64_t p[3] = {q[0] + nb % 3 - 1, q[1] + (nb / 3) % 3 - 1, q[2] + nb / 9 - 1};
+        if (p[0] < 0 || p[1] < 0 || p[2] < 0 || p[0] >= ncell[0] || p[1] >= ncell[1] ||
+            p[2] >= ncell[2])
+          continue;
+        const int64_t cn = p[0] + ncell[0] * (p[1] + ncell[1] * p[2]);
+        for (int64_t s = start[(size_t)cn]; s < start[(size_t)cn + 1]; ++s) {
+          const int64_t j = order[(size_t)s];
+          if (j == i) continue;
+          double ev[3];
+          for (int d = 0; d < 3; ++d) ev[d] = x[d][(size_t)i].v - x[d][(size_t)j].v;
+          if (!(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2] < ratt * ratt * (1.0 + 1e-9)))
+            continue;  // beyond the cutoff for certain
+          Dual e[3];
+          for (int d = 0; d < 3; ++d) e[d] = x[d][(size_t)i] - x[d][(size_t)j];
+          Dual s2 = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
+          Dual dd = dsqrt(s2);
+          Dual F;
+          if (dd.v < rho.v) F = k * (rho - dd);
+          else if (dd.v < ratt) F = dconst(0) - a * (dd - rho);
+          else continue;
+          Dual sc = F / dd;
+          for (int d = 0; d < 3; ++d) acc[d] = acc[d] + sc * e[d];
         }
-        if (!adjacent) continue;
-        Dual e[3];
-        for (int d = 0; d < 3; ++d) e[d] = x[d][(size_t)i] - x[d][(size_t)j];
-        Dual s2 = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
-        Dual dd = dsqrt(s2);
-        Dual F;
-        if (dd.v < rho.v) F = k * (rho - dd);
-        else if (dd.v < ratt) F = dconst(0) - a * (dd - rho);
-        else continue;
-        Dual sc = F / dd;
-        for (int d = 0; d < 3; ++d) acc[d] = acc[d] + sc * e[d];
       }
       for (int d = 0; d < 3; ++d) xn[d][(size_t)i] = x[d][(size_t)i] + acc[d] * dt;
     }

@@ -178,9 +178,12 @@ class OracleContext:
         return out[:n]
 
 
-def oracle_adjoint_dual(abi, cfg, x0, target, nsteps, seeds=()):
-    """Forward-mode dual numbers of the Euler trajectory: (loss, dL/dtheta, dL/dx0[seeds])."""
+def oracle_adjoint_dual(abi, cfg, x0, target, nsteps, seeds=(), threads=None):
+    """Forward-mode dual numbers of the Euler trajectory: (loss, dL/dtheta, dL/dx0[seeds]).
+    Agents are evaluated on `threads` host threads (all cores by default); the
+    result does not depend on the count."""
     lib = load_oracle(abi)
+    lib.oracle_set_threads(int(threads or os.cpu_count()))
     f = lib.oracle_adjoint_dual
     f.restype = C.c_int
     f.argtypes = [C.POINTER(abi.CbmConfig), C.c_int64, C.POINTER(C.c_void_p), C.c_int,

@@ -139,3 +139,35 @@ def adjoint_problem(abi, N=65536, L=80.0, seed=5, steps=200, precision=None, the
     x0 = [rng.uniform(0, L, N) for _ in range(3)]
     star = tuple(t * (1 + 0.1 * z) for t, z in zip(theta, rng.normal(size=3)))
     return kw, x0, star
+
+
+def profile_colony_3d(abi, r_edges, r_counts, v_edges, v_counts, g_edges, g_counts, N=None,
+                      L=400.0, seed=12, precision=None, n_max=None):
+    """A colony drawn from measured distributions instead of grown: agents at
+    the radial density of the histogram (r_edges, r_counts) around the centre
+    of [0,L]^3 (uniform in volume inside each shell), with volumes and growth
+    rates drawn from their histograms (uniform inside each bin).  N defaults
+    to the histogram's total.  The configuration is colony_3d's."""
+    rng = np.random.default_rng(seed)
+    r_counts = np.asarray(r_counts, np.float64)
+    N = int(r_counts.sum()) if N is None else int(N)
+
+    def draw(edges, counts, n):
+        edges = np.asarray(edges, np.float64)
+        p = np.asarray(counts, np.float64)
+        k = rng.choice(len(p), size=n, p=p / p.sum())
+        return k, edges[k] + (edges[k + 1] - edges[k]) * rng.uniform(size=n)
+
+    k, _ = draw(r_edges, r_counts, N)
+    r_edges = np.asarray(r_edges, np.float64)
+    lo3, hi3 = r_edges[k] ** 3, r_edges[k + 1] ** 3
+    rad = np.cbrt(lo3 + (hi3 - lo3) * rng.uniform(size=N))
+    u = rng.normal(size=(N, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    p = L / 2 + u * rad[:, None]
+    _, v = draw(v_edges, v_counts, N)
+    _, g = draw(g_edges, g_counts, N)
+    kw, _ = colony_3d(abi, N=1, R=1.0, L=L, n_max=n_max or int(1.2 * N), seed=seed,
+                      precision=precision)
+    state = dict(x=p[:, 0], y=p[:, 1], z=p[:, 2], v=v, g=g)
+    return kw, state

@@ -198,6 +198,40 @@ def test_rods_growth_overflow(gpu_lib, abi, n_max):
     o.close()
 
 
+@pytest.mark.parametrize("first,stride,n_max", [(60, 1, 110), (60, 1, 100), (60, 1, 125),
+                                                (51, 2, 112), (90, 1, 104)])
+def test_rods_growth_overflow_top_rows(gpu_lib, abi, first, stride, n_max):
+    """Dividers in the top rows with little room: rows first, first+stride,
+    ... up to 99 divide, and only n_max - 100 daughters fit.  Fewer daughters
+    than parents are born, so the fill moves surviving old rows, and some of
+    them have holes above them and stay where they are (update.jl:15-119)."""
+    from conftest import cbm
+    st = _growth_colony(abi, 100, 33, 9.0)
+    divide = np.zeros(100, bool)
+    divide[first::stride] = True
+    st["l_target"] = st["l"] + np.where(divide, -1.0, 1.0)
+    cfg = abi.make_rods_config(n_max, (-20.0, -20.0), (20.0, 20.0), cell_edge=4.0,
+                               **bench_rod_params(), **GROW)
+    g = cbm._abi.Rods2D(cfg)
+    o = OracleRods(abi, cfg)
+    g.upload(st)
+    o.upload(st)
+    n_div = int(divide.sum())
+    if 2 * n_div > n_max - 100:
+        with pytest.raises(cbm._abi.CbmError) as e:
+            g.step(1)
+        assert e.value.code == abi.CBM_ERR_AGENT_OVERFLOW
+    else:
+        g.step(1)
+    o.step(1)
+    a, b = g.download(), o.download()
+    assert len(a["x"]) == len(b["x"]) == 100 + min(2 * n_div, n_max - 100) - n_div
+    for k in abi.ROD_FIELDS:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    g.close()
+    o.close()
+
+
 def bench_rod_params():
     import bench
     return dict(bench.ROD_PARAMS)

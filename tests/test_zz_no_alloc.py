@@ -30,6 +30,8 @@ def _bind(lib):
                   C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double, C.c_void_p,
                   C.c_void_p, C.c_void_p, C.c_void_p]
     lib.cbm_noalloc_last_error.restype = C.c_char_p
+    lib.cbm_noalloc_status.restype = C.c_int
+    lib.cbm_noalloc_status.argtypes = [C.c_void_p]
     return f
 
 
@@ -57,6 +59,8 @@ def test_noalloc_grid_matches_context_grid_twice(gpu_lib, abi, prec):
                 kw["cell_edge"], agent_cell.data_ptr(), cell_start.data_ptr(),
                 cell_agents.data_ptr(), stream)
         assert rc == 0, gpu_lib.cbm_noalloc_last_error()
+        # the scan's bounded waits all ended: the status of the finished call is OK
+        assert gpu_lib.cbm_noalloc_status(stream) == 0, gpu_lib.cbm_noalloc_last_error()
         torch.cuda.synchronize()
         np.testing.assert_array_equal(agent_cell.cpu().numpy(), ref["agent_cell"], err_msg=f"call {call}")
         np.testing.assert_array_equal(cell_start.cpu().numpy()[:nc], ref["cell_start"], err_msg=f"call {call}")
