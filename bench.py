@@ -257,11 +257,10 @@ def grow_colony(cbm, args, rank):
     far denser than packed spheres (about 4 agents per unit volume in its core
     at 10^6, some 350 neighbors inside the cutoff), which is the state the
     reference's own run reaches with this model."""
-    from scenarios import colony_3d
+    from scenarios import growing_colony_3d
     abi = cbm._abi
     prec = abi.F64 if args.precision == "f64" else abi.F32
-    kw, st = colony_3d(abi, N=10_000, R=20.0, L=400.0, n_max=int(1.2 * args.n), seed=2 + rank,
-                       precision=prec)
+    kw, st = growing_colony_3d(abi, args.n, precision=prec, seed=2 + rank)
     ctx = cbm.Context(abi.make_config(**kw))
     ctx.upload(st)
     steps = 0
@@ -747,7 +746,7 @@ def run_configs(args):
     against a Float64 run of the same seeded inputs after 100 steps."""
     import torch
     from _oracle import OracleContext
-    from scenarios import aggregation_2d, chemotaxis_2d, colony_3d, packed_colony_3d
+    from scenarios import aggregation_2d, chemotaxis_2d, colony_3d, growing_colony_3d, packed_colony_3d
     cbm = load_package()
     abi = cbm._abi
     out = {}
@@ -804,7 +803,7 @@ def run_configs(args):
     # [0,400]^3, grown by division to 10^6 (n_max 1.2M), Float32, graph
     # replays in chunks of 10 steps; agent-steps counted per chunk from N at its
     # ends (trapezoid)
-    kw, st = colony_3d(abi, N=10_000, R=20.0, L=400.0, n_max=1_200_000, seed=2)
+    kw, st = growing_colony_3d(abi, 1_000_000, seed=2)
     g = cbm.Context(abi.make_config(**kw))
     g.upload(st)
     stream = torch.cuda.ExternalStream(g.stream())

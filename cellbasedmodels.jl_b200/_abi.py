@@ -52,7 +52,7 @@ class CbmConfig(C.Structure):
         ("growth", C.c_int32), ("medium", C.c_int32), ("v_div", C.c_double),
         ("div_sep", C.c_double), ("p_death", C.c_double), ("n_medium", C.c_int32 * 3),
         ("medium_sampling", C.c_int32), ("diff_D", C.c_double), ("decay", C.c_double),
-        ("secretion", C.c_double), ("chemotaxis", C.c_double),
+        ("secretion", C.c_double), ("chemotaxis", C.c_double), ("uptake", C.c_double),
     ]
 
 
@@ -77,7 +77,7 @@ def make_config(**kw):
                     wall_range=0.0, drift_linear=0.0, growth=0, medium=0, v_div=0.0,
                     div_sep=0.0, p_death=0.0, n_medium=(1, 1, 1),
                     medium_sampling=MEDIUM_NEAREST, diff_D=0.0, decay=0.0, secretion=0.0,
-                    chemotaxis=0.0)
+                    chemotaxis=0.0, uptake=0.0)
     unknown = set(kw) - set(defaults)
     if unknown:
         raise TypeError(f"unknown cbm_config fields: {sorted(unknown)}")

@@ -269,26 +269,53 @@ Params<T> params(const cbm_ctx* c, int parity) {
   P.diff_D = (T)k.diff_D;
   P.decay = (T)k.decay;
   P.secretion_amt = (T)k.secretion * (T)k.dt;
+  P.uptake_amt = (T)k.uptake * (T)k.dt;
   P.chemotaxis = (T)k.chemotaxis;
   P.seed = k.seed;
   P.community = k.community;
   return P;
 }
 
+// agents add to the medium (secretion) or take from it (uptake)
+bool exchanges(const cbm_config& k) { return k.medium && (k.secretion != 0 || k.uptake != 0); }
 bool uses_gather(const cbm_config& k) {
-  return k.medium && k.secretion != 0 && k.medium_sampling == CBM_MEDIUM_BILINEAR &&
+  return exchanges(k) && k.medium_sampling == CBM_MEDIUM_BILINEAR &&
          k.neighbors == CBM_NEIGH_CELL_LINKED;
 }
 bool rule_needed(const cbm_config& k) {
-  return k.walls == CBM_WALLS_REFLECT || (k.medium && k.secretion != 0 && !uses_gather(k)) ||
+  return k.walls == CBM_WALLS_REFLECT || (exchanges(k) && !uses_gather(k)) ||
          k.fate != CBM_FATE_NONE;
 }
+// the atomic rule path reads the committed field from a snapshot
+bool needs_snapshot(const cbm_config& k) { return k.uptake != 0 && exchanges(k) && !uses_gather(k); }
 
 // blocks of the 2D shared-memory stencils (one tile per block)
 dim3 stencil_grid(const cbm_ctx* c) {
   const int nx = c->cfg.n_medium[0] > 0 ? c->cfg.n_medium[0] : 1;
   const int ny = c->cfg.n_medium[1] > 0 ? c->cfg.n_medium[1] : 1;
   return dim3((unsigned)((nx + kStX - 1) / kStX), (unsigned)((ny + kStTileY - 1) / kStTileY));
+}
+
+// z planes per block of the 3D stencils: enough blocks to give every SM four,
+// and runs of at least 8 planes (each run also reads the two planes that
+// close it)
+int stencil_z_run(const cbm_ctx* c) {
+  const dim3 g = stencil_grid(c);
+  const long long xy = (long long)g.x * g.y;
+  const int nz = c->cfg.n_medium[2] > 0 ? c->cfg.n_medium[2] : 1;
+  const long long want = 4LL * (c->n_sm > 0 ? c->n_sm : 148);
+  long long runs = (want + xy - 1) / xy;
+  if (runs < 1) runs = 1;
+  long long z_run = (nz + runs - 1) / runs;
+  if (z_run < 8) z_run = 8;
+  return (int)z_run;
+}
+dim3 stencil_grid_3d(const cbm_ctx* c) {
+  dim3 g = stencil_grid(c);
+  const int nz = c->cfg.n_medium[2] > 0 ? c->cfg.n_medium[2] : 1;
+  const int zr = stencil_z_run(c);
+  g.z = (unsigned)((nz + zr - 1) / zr);
+  return g;
 }
 
 // ---- stage launches (enqueue only) -----------------------------------------
@@ -298,6 +325,8 @@ void enqueue_medium_rule(cbm_ctx* c, const Params<T>& P) {
     PROF("k_medium_grad");
     if (D == 2)
       k_medium_grad_2d<T><<<stencil_grid(c), dim3(kStX, kStY), 0, c->stream>>>(P);
+    else if (D == 3)
+      k_medium_grad_3d<T><<<stencil_grid_3d(c), dim3(kStX, kStY), 0, c->stream>>>(P, stencil_z_run(c));
     else
       k_medium_grad<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
   }
@@ -306,6 +335,10 @@ void enqueue_medium_rule(cbm_ctx* c, const Params<T>& P) {
 template <typename T, int D>
 void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P) {
   const cbm_config& k = c->cfg;
+  if (needs_snapshot(k)) {
+    PROF("k_medium_snapshot");
+    k_medium_snapshot<T><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
+  }
   if (uses_gather(k)) {
     PROF("k_secrete_gather");
     k_secrete_gather<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
@@ -365,6 +398,8 @@ void enqueue_medium_de(cbm_ctx* c, const Params<T>& P) {
     PROF("k_medium_de");
     if (D == 2)
       k_medium_de_2d<T><<<stencil_grid(c), dim3(kStX, kStY), 0, c->stream>>>(P);
+    else if (D == 3)
+      k_medium_de_3d<T><<<stencil_grid_3d(c), dim3(kStX, kStY), 0, c->stream>>>(P, stencil_z_run(c));
     else
       k_medium_de<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
   }
@@ -415,6 +450,7 @@ int kernels_per_step(const cbm_ctx* c) {
   const cbm_config& k = c->cfg;
   int n = 0;
   if (k.medium && k.chemotaxis != 0) n += 1;
+  if (needs_snapshot(k)) n += 1;
   if (uses_gather(k)) n += 1;
   if (rule_needed(k)) n += 1;           // rule (with births and deaths when fate is on)
   if (k.fate != CBM_FATE_NONE) n += 1;  // compaction
@@ -665,6 +701,9 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     for (int d = 0; d < k.dims; ++d)
       if (k.n_medium[d] < 1) return fail(nullptr, CBM_ERR_ARG, "n_medium[%d] must be >= 1", d);
   }
+  if (!(k.uptake >= 0) || k.uptake > 1e300)
+    return fail(nullptr, CBM_ERR_ARG, "uptake must be finite and >= 0");
+  if (k.uptake != 0 && !k.medium) return fail(nullptr, CBM_ERR_ARG, "uptake needs a medium");
 
   cbm_ctx* c = new cbm_ctx;
   c->cfg = k;

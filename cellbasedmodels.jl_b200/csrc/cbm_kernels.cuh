@@ -128,6 +128,7 @@ struct Params {
   T v_div, div_sep, p_death;
   T dx_m[3];
   T diff_D, decay, secretion_amt, chemotaxis;
+  T uptake_amt;             // uptake * dt (0: no uptake, and no clamp of the field)
   uint64_t seed;
   uint32_t community;
 };
@@ -396,10 +397,11 @@ __global__ void __launch_bounds__(kTile) k_medium_grad(Params<T> P) {
 }
 
 // ---------------------------------------------------------------------------
-// Bilinear secretion as a gather over medium nodes.  Atomic adds of unequal
-// amounts would sum in an arbitrary order; here every node adds the
-// contributions of the agents whose stencil covers it in ascending agent
-// index, the order of the reference's serial agent loop.  The agents are
+// Bilinear secretion and uptake as a gather over medium nodes.  Atomic adds
+// of unequal amounts would sum in an arbitrary order; here every node adds
+// the contributions w (secretion dt - uptake dt c0) of the agents whose
+// stencil covers it in ascending agent index, the order of the reference's
+// serial agent loop (c0: the node's committed value).  The agents are
 // found through the cell grid, which holds exactly the committed positions
 // the rule reads when the grid is rebuilt every step (CellLinked).
 // ---------------------------------------------------------------------------
@@ -419,7 +421,10 @@ __global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
   if (D > 1) q[1] = (n / P.n_medium[0]) % P.n_medium[1];
   if (D > 2) q[2] = n / (P.n_medium[0] * P.n_medium[1]);
   const T amt = P.secretion_amt;
-  T acc = P.c_cur[n];
+  const T c_com = P.c_cur[n];  // committed value: this thread is the node's only writer
+  const bool upt = P.uptake_amt != (T)0;
+  const T net = upt ? amt - P.uptake_amt * c_com : amt;  // secretion - first-order uptake
+  T acc = c_com;
   auto add = [&](int slot) {
     T x[3];
     to3<T>(P.PA[slot], x);
@@ -428,7 +433,7 @@ __global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
     bilinear<T, D>(P, x, nodes, w);
 #pragma unroll
     for (int k = 0; k < (1 << D); ++k)
-      if (nodes[k] == n) acc = acc + w[k] * amt;
+      if (nodes[k] == n) acc = acc + w[k] * net;
   };
   // The stencil of bilinear() covers node q exactly when, on every axis, one
   // of its two clamped indices is q (the same expressions, without weights).
@@ -542,8 +547,8 @@ template <typename T, int D>
 __device__ __forceinline__ int rule_agent(const Params<T>& P, int i, long long step) {
   const int s = P.inv[i];
   T x[3] = {(T)0, (T)0, (T)0};
-  if (P.walls == CBM_WALLS_REFLECT || (P.medium && P.secretion_amt != (T)0))
-    to3<T>(P.PA[s], x);
+  const bool exchange = P.medium && (P.secretion_amt != (T)0 || P.uptake_amt != (T)0);
+  if (P.walls == CBM_WALLS_REFLECT || exchange) to3<T>(P.PA[s], x);
   if (P.walls == CBM_WALLS_REFLECT) {
     T y[3] = {x[0], x[1], x[2]};
 #pragma unroll
@@ -553,15 +558,24 @@ __device__ __forceinline__ int rule_agent(const Params<T>& P, int i, long long s
     }
     P.U[s] = from3<T>(y);
   }
-  if (P.medium && P.secretion_amt != (T)0 && !secretion_by_gather(P)) {
+  if (exchange && !secretion_by_gather(P)) {
+    // c__ += w (secretion dt - uptake dt c) with c the committed value, which
+    // k_medium_snapshot copied to c_nxt before the rule (c_cur changes under
+    // the atomics).  Nearest-node terms are equal for every agent of a node,
+    // so their atomic sum does not depend on the order.
+    const bool upt = P.uptake_amt != (T)0;
     if (P.medium_sampling == CBM_MEDIUM_NEAREST) {
-      atomicAdd(P.c_cur + nearest_node<T, D>(P, x), P.secretion_amt);
+      const int nn = nearest_node<T, D>(P, x);
+      atomicAdd(P.c_cur + nn, upt ? P.secretion_amt - P.uptake_amt * P.c_nxt[nn] : P.secretion_amt);
     } else {
       int nodes[8];
       T w[8];
       bilinear<T, D>(P, x, nodes, w);
 #pragma unroll
-      for (int q = 0; q < (1 << D); ++q) atomicAdd(P.c_cur + nodes[q], w[q] * P.secretion_amt);
+      for (int q = 0; q < (1 << D); ++q)
+        atomicAdd(P.c_cur + nodes[q],
+                  upt ? w[q] * (P.secretion_amt - P.uptake_amt * P.c_nxt[nodes[q]])
+                      : w[q] * P.secretion_amt);
     }
   }
   int fate = 0;
@@ -1415,6 +1429,12 @@ __global__ void __launch_bounds__(kTile) k_stage_combine(Params<T> P, int op) {
 // mediumStepDE!: FTCS Euler step u <- u + dt (D lap(u) - lambda u) inside,
 // du = 0 on the border (macros.jl:203-258)
 // ---------------------------------------------------------------------------
+// The field as the DE step reads it: clamped at zero when uptake is on.
+template <typename T>
+__device__ __forceinline__ T medium_in(const Params<T>& P, T v) {
+  return (P.uptake_amt != (T)0 && v < (T)0) ? (T)0 : v;
+}
+
 template <typename T, int D>
 __global__ void __launch_bounds__(kTile) k_medium_de(Params<T> P) {
   int n = blockIdx.x * kTile + threadIdx.x;
@@ -1426,7 +1446,7 @@ __global__ void __launch_bounds__(kTile) k_medium_de(Params<T> P) {
   bool in = true;
 #pragma unroll
   for (int d = 0; d < D; ++d) in = in && q[d] > 0 && q[d] < P.n_medium[d] - 1;
-  T u = P.c_cur[n];
+  T u = medium_in(P, P.c_cur[n]);
   if (!in) {
     P.c_nxt[n] = u;
     return;
@@ -1435,7 +1455,8 @@ __global__ void __launch_bounds__(kTile) k_medium_de(Params<T> P) {
   T lap = (T)0;
 #pragma unroll
   for (int d = 0; d < D; ++d) {
-    T l = ((P.c_cur[n + stride[d]] - (T)2 * u) + P.c_cur[n - stride[d]]) / (P.dx_m[d] * P.dx_m[d]);
+    T l = ((medium_in(P, P.c_cur[n + stride[d]]) - (T)2 * u) + medium_in(P, P.c_cur[n - stride[d]])) /
+          (P.dx_m[d] * P.dx_m[d]);
     lap = d == 0 ? l : lap + l;
   }
   T k = P.diff_D * lap - P.decay * u;
@@ -1452,12 +1473,14 @@ constexpr int kStX = 32, kStY = 8, kStRows = 4;
 constexpr int kStTileY = kStY * kStRows;
 
 template <typename T>
-__device__ __forceinline__ void stage_tile2(const Params<T>& P, T (*tile)[kStX + 2], int x0, int y0) {
+__device__ __forceinline__ void stage_tile2(const Params<T>& P, T (*tile)[kStX + 2], int x0, int y0,
+                                            bool clamp) {
   const int nx = P.n_medium[0], ny = P.n_medium[1];
   for (int k = threadIdx.y * kStX + threadIdx.x; k < (kStTileY + 2) * (kStX + 2); k += kStX * kStY) {
     const int ty = k / (kStX + 2), tx = k % (kStX + 2);
     const int gx = x0 + tx - 1, gy = y0 + ty - 1;
-    tile[ty][tx] = (gx >= 0 && gx < nx && gy >= 0 && gy < ny) ? P.c_cur[(size_t)gy * nx + gx] : (T)0;
+    const T v = (gx >= 0 && gx < nx && gy >= 0 && gy < ny) ? P.c_cur[(size_t)gy * nx + gx] : (T)0;
+    tile[ty][tx] = clamp ? medium_in(P, v) : v;
   }
   __syncthreads();
 }
@@ -1467,7 +1490,7 @@ __global__ void __launch_bounds__(kStX * kStY) k_medium_grad_2d(Params<T> P) {
   __shared__ T tile[kStTileY + 2][kStX + 2];
   const int nx = P.n_medium[0], ny = P.n_medium[1];
   const int x0 = blockIdx.x * kStX, y0 = blockIdx.y * kStTileY;
-  stage_tile2<T>(P, tile, x0, y0);
+  stage_tile2<T>(P, tile, x0, y0, false);
   const int x = x0 + threadIdx.x;
   if (x >= nx) return;
 #pragma unroll
@@ -1487,7 +1510,7 @@ __global__ void __launch_bounds__(kStX * kStY) k_medium_de_2d(Params<T> P) {
   __shared__ T tile[kStTileY + 2][kStX + 2];
   const int nx = P.n_medium[0], ny = P.n_medium[1];
   const int x0 = blockIdx.x * kStX, y0 = blockIdx.y * kStTileY;
-  stage_tile2<T>(P, tile, x0, y0);
+  stage_tile2<T>(P, tile, x0, y0, true);
   const int x = x0 + threadIdx.x;
   if (x >= nx) return;
 #pragma unroll
@@ -1507,6 +1530,103 @@ __global__ void __launch_bounds__(kStX * kStY) k_medium_de_2d(Params<T> P) {
     const T k = P.diff_D * lap - P.decay * u;
     P.c_nxt[n] = u + P.dt * k;
   }
+}
+
+// ---------------------------------------------------------------------------
+// 3D medium stencils (7-point), marching along z: a block of kStX x kStY
+// threads owns a kStX x kStTileY column of nodes over a run of z planes.  Each
+// thread keeps its kStRows nodes of the planes z-1, z and z+1 in registers;
+// plane z is staged in shared memory with a one-node x/y halo for the
+// in-plane neighbours.  Every node of the run is read from HBM once, plus the
+// halo and the two planes that close the run.  Same expressions as
+// k_medium_grad / k_medium_de: lap = (l_x + l_y) + l_z.
+// ---------------------------------------------------------------------------
+template <typename T, bool kDE>
+__device__ __forceinline__ void stencil_3d(const Params<T>& P, int z_run) {
+  __shared__ T tile[kStTileY + 2][kStX + 2];
+  const int nx = P.n_medium[0], ny = P.n_medium[1], nz = P.n_medium[2];
+  const int x0 = blockIdx.x * kStX, y0 = blockIdx.y * kStTileY;
+  const int za = blockIdx.z * z_run;
+  const int zb = za + z_run < nz ? za + z_run : nz;
+  const size_t plane = (size_t)nx * (size_t)ny;
+  auto read = [&](int gx, int gy, int gz) -> T {
+    if (gx < 0 || gx >= nx || gy < 0 || gy >= ny || gz < 0 || gz >= nz) return (T)0;
+    const T v = P.c_cur[(size_t)gz * plane + (size_t)gy * nx + gx];
+    return kDE ? medium_in(P, v) : v;
+  };
+  const int x = x0 + threadIdx.x;
+  T lo[kStRows], mid[kStRows], hi[kStRows];
+#pragma unroll
+  for (int r = 0; r < kStRows; ++r) {
+    const int y = y0 + threadIdx.y + r * kStY;
+    lo[r] = read(x, y, za - 1);
+    mid[r] = read(x, y, za);
+  }
+  const int t = threadIdx.y * kStX + threadIdx.x;
+  for (int z = za; z < zb; ++z) {
+#pragma unroll
+    for (int r = 0; r < kStRows; ++r) hi[r] = read(x, y0 + threadIdx.y + r * kStY, z + 1);
+    __syncthreads();  // every thread is done with the previous plane's tile
+#pragma unroll
+    for (int r = 0; r < kStRows; ++r) tile[threadIdx.y + r * kStY + 1][threadIdx.x + 1] = mid[r];
+    if (t < kStTileY) {
+      tile[t + 1][0] = read(x0 - 1, y0 + t, z);
+    } else if (t < 2 * kStTileY) {
+      tile[t - kStTileY + 1][kStX + 1] = read(x0 + kStX, y0 + t - kStTileY, z);
+    } else if (t < 2 * kStTileY + kStX) {
+      tile[0][t - 2 * kStTileY + 1] = read(x0 + t - 2 * kStTileY, y0 - 1, z);
+    } else if (t < 2 * kStTileY + 2 * kStX) {
+      tile[kStTileY + 1][t - 2 * kStTileY - kStX + 1] =
+          read(x0 + t - 2 * kStTileY - kStX, y0 + kStTileY, z);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kStRows; ++r) {
+      const int ty = threadIdx.y + r * kStY, y = y0 + ty;
+      if (x < nx && y < ny) {
+        const size_t n = (size_t)z * plane + (size_t)y * nx + x;
+        const bool in = x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1;
+        const int tx = threadIdx.x + 1, tyy = ty + 1;
+        if (kDE) {
+          const T u = mid[r];
+          if (!in) {
+            P.c_nxt[n] = u;
+          } else {
+            const T l0 = ((tile[tyy][tx + 1] - (T)2 * u) + tile[tyy][tx - 1]) / (P.dx_m[0] * P.dx_m[0]);
+            const T l1 = ((tile[tyy + 1][tx] - (T)2 * u) + tile[tyy - 1][tx]) / (P.dx_m[1] * P.dx_m[1]);
+            const T l2 = ((hi[r] - (T)2 * u) + lo[r]) / (P.dx_m[2] * P.dx_m[2]);
+            const T lap = (l0 + l1) + l2;
+            const T k = P.diff_D * lap - P.decay * u;
+            P.c_nxt[n] = u + P.dt * k;
+          }
+        } else {
+          P.grad_nxt[0][n] = in ? (tile[tyy][tx + 1] - tile[tyy][tx - 1]) / ((T)2 * P.dx_m[0]) : (T)0;
+          P.grad_nxt[1][n] = in ? (tile[tyy + 1][tx] - tile[tyy - 1][tx]) / ((T)2 * P.dx_m[1]) : (T)0;
+          P.grad_nxt[2][n] = in ? (hi[r] - lo[r]) / ((T)2 * P.dx_m[2]) : (T)0;
+        }
+      }
+      lo[r] = mid[r];
+      mid[r] = hi[r];
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kStX * kStY) k_medium_grad_3d(Params<T> P, int z_run) {
+  stencil_3d<T, false>(P, z_run);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kStX * kStY) k_medium_de_3d(Params<T> P, int z_run) {
+  stencil_3d<T, true>(P, z_run);
+}
+
+// The committed field, copied before an agent rule that adds to it with
+// atomics and takes up from it: the uptake reads the value before the rule.
+template <typename T>
+__global__ void __launch_bounds__(kTile) k_medium_snapshot(Params<T> P) {
+  const int n = blockIdx.x * kTile + threadIdx.x;
+  if (n < P.n_nodes) P.c_nxt[n] = P.c_cur[n];
 }
 
 // ---------------------------------------------------------------------------

@@ -89,8 +89,18 @@ enum { CBM_WALLS_NONE = 0, CBM_WALLS_REFLECT = 1, CBM_WALLS_PUSH = 2 };
 enum { CBM_FATE_NONE = 0, CBM_FATE_VOLUME = 1, CBM_FATE_ID_PARITY = 2 };
 
 /* Where agents read and write the medium.  NEAREST is the reference's
- * cellInMesh (src/metrics.jl:18-20); BILINEAR spreads over the four (eight)
- * surrounding medium nodes. */
+ * cellInMesh (src/metrics.jl:18-20); BILINEAR spreads over the two (four,
+ * eight) surrounding medium nodes with multilinear weights w_q.
+ *
+ * Secretion and uptake happen in the agent rule, in agent order, as the
+ * reference's `c__[node] += ...` statements would (auxiliar.jl:353-365): agent
+ * i adds to each node q of its stencil
+ *     w_q * (secretion * dt - (uptake * dt) * c_q)
+ * where c_q is the committed value of node q (the field before this step's
+ * rule), so the uptake is first order in the local concentration.  With
+ * uptake = 0 the term is w_q * secretion * dt.  With uptake > 0 the medium's DE
+ * step reads the field clamped at zero, max(c, 0), on every node: an uptake
+ * larger than the node holds leaves it empty, never negative. */
 enum { CBM_MEDIUM_NEAREST = 0, CBM_MEDIUM_BILINEAR = 1 };
 
 /* cbm_step flags */
@@ -140,6 +150,7 @@ typedef struct cbm_config {
   double decay;          /* medium decay rate lambda */
   double secretion;      /* amount per unit time each agent adds to c */
   double chemotaxis;     /* dt(x) += chemotaxis * dc/dx / (1 + |grad c|) */
+  double uptake;         /* first-order uptake rate per agent (CBM_MEDIUM_* above) */
 } cbm_config;
 
 /* ---- state exchanged with the host (Community fields) ------------------- */

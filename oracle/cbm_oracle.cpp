@@ -71,7 +71,8 @@ struct Com {
   int64_t nCells[3] = {1, 1, 1};
   T edge = 0;
   std::vector<int64_t> cellAssignedToAgent, cellNumAgents, cellCumSum;
-  std::vector<int64_t> neighborN, neighborList;  // list column-major (nMax x nMaxNeighbors)
+  std::vector<int64_t> neighborN;
+  std::vector<int32_t> neighborList;  // column-major (nMax x nMaxNeighbors); indices < 2^31
   std::vector<T> posOld[3], accumulatedDistance;
   const T* ext_noise = nullptr;  // EM increments given by the caller for one step (i * D + d)
 
@@ -271,7 +272,7 @@ void appendNeighbor(Com<T>& C, int64_t i, int64_t j) {
     C.err = CBM_ERR_NEIGHBOR_OVERFLOW;
     return;
   }
-  C.neighborList[i + k * C.nMax] = j;
+  C.neighborList[i + k * C.nMax] = (int32_t)j;
   C.neighborN[i] = k + 1;
 }
 
@@ -400,6 +401,7 @@ void agentStepRule(Com<T>& C) {
   const cbm_config& k = C.cfg;
   const int D = C.dims;
   const T amt = (T)k.secretion * (T)k.dt;
+  const T upt = (T)k.uptake * (T)k.dt;
   for (int64_t i = 0; i < C.N; ++i) {
     T p[3];
     for (int d = 0; d < D; ++d) p[d] = C.x[d][i];
@@ -410,16 +412,20 @@ void agentStepRule(Com<T>& C) {
         else if (p[d] > hi) C.x_[d][i] = (T)2 * hi - p[d];
       }
     }
-    if (k.medium && k.secretion != 0) {
-      // c += secretion*dt at the agent (auxiliar.jl:353-365)
+    if (k.medium && (k.secretion != 0 || k.uptake != 0)) {
+      // c__[node] += w (secretion dt - uptake dt c[node]) at the agent, c the
+      // committed field (auxiliar.jl:353-365 writes c__ inside the rule); the
+      // uptake term is this library's first-order sink, absent when uptake = 0
       if (k.medium_sampling == CBM_MEDIUM_NEAREST) {
         int64_t n = nearestNode(C, p);
-        C.c_[n] = C.c_[n] + amt;
+        C.c_[n] = C.c_[n] + (k.uptake != 0 ? amt - upt * C.c[n] : amt);
       } else {
         int64_t nodes[8];
         T w[8];
         bilinear(C, p, nodes, w);
-        for (int q = 0; q < (1 << D); ++q) C.c_[nodes[q]] = C.c_[nodes[q]] + w[q] * amt;
+        for (int q = 0; q < (1 << D); ++q)
+          C.c_[nodes[q]] =
+              C.c_[nodes[q]] + (k.uptake != 0 ? w[q] * (amt - upt * C.c[nodes[q]]) : w[q] * amt);
       }
     }
     if (k.fate == CBM_FATE_VOLUME) {
@@ -673,6 +679,9 @@ void mediumStepDE(Com<T>& C) {
   if (!C.cfg.medium) return;
   const T D = (T)C.cfg.diff_D, lam = (T)C.cfg.decay, dt = (T)C.cfg.dt;
   int64_t stride[3] = {1, C.nm[0], C.nm[0] * C.nm[1]};
+  if (C.cfg.uptake != 0)  // with uptake the step reads the field clamped at zero
+    for (int64_t n = 0; n < C.nNodes; ++n)
+      if (C.c_[n] < (T)0) C.c_[n] = (T)0;
   std::vector<T> k(C.nNodes, (T)0);
   for (int64_t n = 0; n < C.nNodes; ++n) {
     int64_t q[3];

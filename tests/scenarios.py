@@ -29,12 +29,12 @@ def ball_radius(N, density=0.15):
 
 
 def colony_3d(abi, N=10000, R=None, L=400.0, n_max=None, seed=2, precision=None,
-              neighbors=None, p_death=1e-4, sigma=0.05):
+              neighbors=None, p_death=1e-4, sigma=0.05, n_max_neighbors=64):
     """3D colony: N agents uniform in a radius-R ball centred in [0,L]^3 (R from
     the packing density 0.15 when not given),
     v ~ U(1,2), g ~ U(0.8,1.2), EM sigma, divide at v >= 2 into daughters at
     +-0.5 r, death probability p_death, CLVD with R_list 3.3 and rebuild at 0.15,
-    dt = 0.005."""
+    dt = 0.005, Verlet rows of n_max_neighbors."""
     rng = np.random.default_rng(seed)
     R = ball_radius(N) if R is None else R
     u = rng.normal(size=(N, 3))
@@ -45,11 +45,26 @@ def colony_3d(abi, N=10000, R=None, L=400.0, n_max=None, seed=2, precision=None,
     kw = dict(dims=3, precision=abi.F32 if precision is None else precision,
               n_max=n_max or int(1.2 * N), box_lo=(0.0,) * 3, box_hi=(L,) * 3, dt=0.005,
               seed=seed, neighbors=alg, cell_edge=3.3, skin=3.3, rebuild_threshold=0.15,
-              n_max_neighbors=64, integrator=abi.INT_EM, sigma=sigma, k_rep=10.0, r_rep=2.0,
+              n_max_neighbors=n_max_neighbors, integrator=abi.INT_EM, sigma=sigma, k_rep=10.0, r_rep=2.0,
               k_att=1.0, r_att=3.0, att_form=abi.ATT_FROM_REP, growth=1, fate=abi.FATE_VOLUME,
               v_div=2.0, div_sep=0.5, p_death=p_death)
     state = dict(x=p[:, 0], y=p[:, 1], z=p[:, 2], v=rng.uniform(1, 2, N), g=rng.uniform(0.8, 1.2, N))
     return kw, state
+
+
+# Verlet row capacity of the growing colony: rows must hold every agent within
+# the list radius 3.3, for the reference's CLVD to be defined (a fuller row
+# writes past neighborList_).  The colony grown to 10^6 has up to about 820
+# such agents (about 4 agents per unit volume in its core).
+GROWN_COLONY_ROW = 1024
+
+
+def growing_colony_3d(abi, n_target, precision=None, seed=2):
+    """The configured 3D growing colony: 10^4 agents uniform in a radius-20
+    ball centred in [0,400]^3 (colony_3d's model), with capacity 1.2 n_target
+    and Verlet rows that hold the grown state's partners."""
+    return colony_3d(abi, N=10_000, R=20.0, L=400.0, n_max=int(1.2 * n_target), seed=seed,
+                     precision=precision, n_max_neighbors=GROWN_COLONY_ROW)
 
 
 def packed_colony_3d(abi, N=1_000_000, density=0.15, L=400.0, seed=2, n_max=None, precision=None,
@@ -170,4 +185,24 @@ def profile_colony_3d(abi, r_edges, r_counts, v_edges, v_counts, g_edges, g_coun
     kw, _ = colony_3d(abi, N=1, R=1.0, L=L, n_max=n_max or int(1.2 * N), seed=seed,
                       precision=precision)
     state = dict(x=p[:, 0], y=p[:, 1], z=p[:, 2], v=v, g=g)
+    return kw, state
+
+
+def medium_colony(abi, dims, N=3000, L=40.0, n_medium=40, seed=6, bilinear=True, precision=None,
+                  neighbors=None, uptake=0.05, secretion=0.1, chemotaxis=0.5, dt=0.05):
+    """Agents on a 1D/2D/3D FTCS medium (unit spacing by default): soft-sphere
+    repulsion (k=10, r=1), EM noise sigma 0.1, secretion, first-order uptake
+    and chemotactic drift, D=1, decay 0.01, CellLinked edge 2 unless another
+    neighbor algorithm is given."""
+    rng = np.random.default_rng(seed)
+    alg = abi.NEIGH_CELL_LINKED if neighbors is None else neighbors
+    kw = dict(dims=dims, precision=abi.F32 if precision is None else precision, n_max=N,
+              box_lo=(0.0,) * dims, box_hi=(L,) * dims, dt=dt, seed=seed, neighbors=alg,
+              cell_edge=2.4, skin=2.4, n_max_neighbors=64, integrator=abi.INT_EM, sigma=0.1,
+              k_rep=10.0, r_rep=2.0, k_att=0.0, r_att=2.0, medium=1,
+              n_medium=(n_medium,) * dims, diff_D=1.0, decay=0.01, secretion=secretion,
+              uptake=uptake, chemotaxis=chemotaxis,
+              medium_sampling=abi.MEDIUM_BILINEAR if bilinear else abi.MEDIUM_NEAREST)
+    p = rng.uniform(0, L, size=(dims, N))
+    state = {k: p[d] for d, k in enumerate("xyz"[:dims])}
     return kw, state

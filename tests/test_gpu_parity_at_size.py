@@ -21,8 +21,8 @@ import pytest
 
 import conftest
 from _oracle import OracleContext, oracle_adjoint_dual
-from scenarios import (adjoint_problem, aggregation_2d, batched_sweep, chemotaxis_2d, colony_3d,
-                       make_descs, plain_config_for)
+from scenarios import (adjoint_problem, aggregation_2d, batched_sweep, chemotaxis_2d,
+                       growing_colony_3d, make_descs, plain_config_for)
 from test_gpu_parity import assert_same_grid, assert_same_lists, assert_same_state
 
 cbm = conftest.cbm
@@ -36,8 +36,7 @@ def grown_colony(abi, n_target, precision):
     """The configured colony (10^4 agents uniform in a radius-20 ball centred
     in [0,400]^3, seed 2) grown on the device until N >= n_target.  Returns
     the configuration and the state with its counters."""
-    kw, st = colony_3d(abi, N=10_000, R=20.0, L=400.0, n_max=int(1.2 * n_target), seed=2,
-                       precision=precision)
+    kw, st = growing_colony_3d(abi, n_target, precision=precision)
     g = cbm.Context(abi.make_config(**kw))
     g.upload(st)
     steps = 0
@@ -73,7 +72,7 @@ def test_grown_colony_1e5_100_steps_bitexact(gpu_lib, abi, prec):
     g, o = from_snapshot(abi, kw, snap)
     for _ in range(4):
         g.step(25)
-        o.step(25)
+        assert o.step(25) == 0  # no Verlet row of the checker overflowed
         a, b = g.download(), o.download()
         assert_same_state(a, b, COLONY_KEYS)
         assert (a["id_max"], a["step"]) == (b["id_max"], b["step"])
@@ -91,7 +90,7 @@ def test_grown_colony_1e6_three_steps_bitexact(gpu_lib, abi):
     assert snap["N"] >= 1_000_000
     g, o = from_snapshot(abi, kw, snap)
     g.step(3)
-    o.step(3)
+    assert o.step(3) == 0  # no Verlet row of the checker overflowed
     a, b = g.download(), o.download()
     assert_same_state(a, b, COLONY_KEYS)
     assert a["id_max"] == b["id_max"]
