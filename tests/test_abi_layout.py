@@ -59,11 +59,20 @@ JULIA_TYPES = {"Int32": C.c_int32, "Int64": C.c_int64, "UInt32": C.c_uint32,
                "UInt64": C.c_uint64, "Float64": C.c_double}
 
 
+JULIA_SRC = os.path.join(conftest.ROOT, "julia", "CellBasedModelsB200", "src")
+
+
+def _julia_text():
+    """The Julia binding's sources (julia/CellBasedModelsB200/src/*.jl)."""
+    return "\n".join(open(os.path.join(JULIA_SRC, f)).read()
+                     for f in sorted(os.listdir(JULIA_SRC)) if f.endswith(".jl"))
+
+
 def _julia_structs():
     """name -> [(field, Julia type)] of the `struct Cbm... end` blocks of the
-    Julia stubs."""
+    Julia binding."""
     import re
-    text = open(os.path.join(conftest.ROOT, "INTEGRATION.md")).read()
+    text = _julia_text()
     out = {}
     for m in re.finditer(r"^(?:mutable )?struct (Cbm\w+)\n(.*?)^end", text, flags=re.S | re.M):
         fields = []
@@ -85,7 +94,7 @@ def _ctype_of(julia):
 
 
 def test_julia_stub_structs_match_the_mirrors():
-    """The Julia mirrors in the ccall stubs list the C fields in order, with
+    """The Julia mirrors of the binding list the C fields in order, with
     types of the same size (Julia cannot run here, so the text is checked)."""
     jl = _julia_structs()
     for name in ("CbmConfig", "CbmCommunityDesc", "CbmBatchTuning", "CbmMediumConfig",
@@ -128,13 +137,25 @@ def _header_arity():
     return arity
 
 
-def test_julia_ccalls_bind_declared_entry_points():
-    """Every ccall of the Julia stubs names an entry point of include/*.h and
-    passes as many argument types as the C prototype has parameters."""
+def _julia_ccalls(text):
     import re
-    text = open(os.path.join(conftest.ROOT, "INTEGRATION.md")).read()
+    return list(re.finditer(r"ccall\(\(:(cbm_\w+), LIBCBM\),\s*[\w{}]+,\s*\(", text))
+
+
+def test_julia_binds_every_declared_entry_point():
+    """The Julia binding has a ccall for every entry point of include/*.h."""
+    from test_abi_exports import declared_functions
+    bound = {m.group(1) for m in _julia_ccalls(_julia_text())}
+    missing = sorted(set(declared_functions()) - bound)
+    assert not missing, missing
+
+
+def test_julia_ccalls_bind_declared_entry_points():
+    """Every ccall of the Julia binding names an entry point of include/*.h and
+    passes as many argument types as the C prototype has parameters."""
+    text = _julia_text()
     arity = _header_arity()
-    calls = list(re.finditer(r"ccall\(\(:(cbm_\w+), LIBCBM\),\s*[\w{}]+,\s*\(", text))
+    calls = _julia_ccalls(text)
     assert len(calls) >= 30
     for m in calls:
         # the argument-type tuple: from the opening parenthesis to its match
