@@ -201,20 +201,27 @@ class SmiClocks:
                 "samples": len(sm), "source": "nvidia-smi -lms 200"}
 
 
-# DRAM bytes per agent of one launch, from one ncu capture each (dram__bytes_read.sum
-# + dram__bytes_write.sum) of k_agent_de in walk mode, Float32: the grown colony
-# (5.34 GB for about 1.02M agents, first timed step: the partner lists, written
-# and read back, dominate; the compulsory state is 45 B/agent) and the packed
-# snapshot (35.5 MB for about 1.01M agents, whose partners rarely leave the
-# shared-memory queue).  Traffic grows in proportion to the agents of the
-# launch, so it is scaled to the bench's agent count.
-MEASURED_TRAFFIC_PER_AGENT = {("k_agent_de", 4, True, "grown"): 5230.0,
-                              ("k_agent_de", 4, True, "packed"): 35.1}
+# Per-agent figures of one ncu capture of k_agent_de on the grown colony
+# (Float32): DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) and warp
+# instructions (smsp__inst_executed.sum) per agent of the launch.  They are
+# read from the capture's summary under profiles/, which gives the command
+# that made it; a changed kernel needs a new capture.
+KERNEL_PROFILE = os.path.join(ROOT, "profiles", "k_agent_de_grown_colony_1m_f32.md")
 
 
-def traffic_per_launch(name, s, walked, agents, workload):
-    t = MEASURED_TRAFFIC_PER_AGENT.get((name, s, bool(walked), workload))
-    return None if t is None else round(t * agents)
+def profile_per_agent(path=KERNEL_PROFILE):
+    """{"dram_bytes_per_agent": B, "warp_inst_per_agent": I} from the lines
+    `per-agent: name = value` of a profile summary (absent: {})."""
+    out = {}
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("per-agent:") and "=" in line:
+                    k, v = line[len("per-agent:"):].split("=", 1)
+                    out[k.strip()] = float(v.strip().split()[0])
+    except OSError:
+        pass
+    return out
 
 
 def alg_bytes_per_agent(name, s, d, nbar, verlet, fate):
@@ -283,9 +290,47 @@ def pinned_state(cbm, cfg, state, capacity):
     return bufs
 
 
-def run_ours(args, rank, world, local_rank):
+def e2e_through_abi(cbm, ctx, cfg, steps):
+    """loadToPlatform! + step! + bringFromPlatform! per step through the C ABI
+    (cbm_upload, cbm_step, cbm_download) from and to pinned host buffers,
+    starting from the context's current state.  The first of `steps` calls
+    also builds the step graph of its parity and is not counted.  Returns
+    (seconds, agent-steps, H2D bytes, D2H bytes) of the counted calls and the
+    state before them."""
     import ctypes as C
 
+    import torch
+    abi = cbm._abi
+    s = 8 if cfg.precision == abi.F64 else 4
+    cap = int(cfg.n_max)
+    snap = ctx.download()
+    host = pinned_state(cbm, cfg, {k: snap[k] for k in ("x", "y", "z", "v", "g", "id", "parent")},
+                        cap)
+    lib = ctx.lib
+    e2e_time, e2e_agents, h2d, d2h = 0.0, 0, 0, 0
+    nstate = snap["N"]
+    t_now, st_now, idm = snap["t"], snap["step"], snap["id_max"]
+    per_agent = 3 * s + 2 * s + 16  # x,y,z,v,g + id,parent
+    for k in range(steps):
+        view = host.view(N=nstate, t=t_now, step=st_now, id_max=idm,
+                         fields=("x", "y", "z", "v", "g", "id", "parent"))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx._check(lib.cbm_upload(ctx.h, C.byref(view)))
+        ctx._check(lib.cbm_step(ctx.h, 1, abi.SYNC))
+        view.capacity = cap
+        ctx._check(lib.cbm_download(ctx.h, C.byref(view), abi.VIEW_COMMITTED))
+        t1 = time.perf_counter()
+        if k > 0:
+            e2e_time += t1 - t0
+            e2e_agents += nstate
+            h2d += nstate * per_agent
+            d2h += view.N * per_agent
+        nstate, t_now, st_now, idm = view.N, view.t, view.step, view.id_max
+    return e2e_time, e2e_agents, h2d, d2h, snap
+
+
+def run_ours(args, rank, world, local_rank):
     import torch
     cbm = load_package()
     abi = cbm._abi
@@ -296,6 +341,16 @@ def run_ours(args, rank, world, local_rank):
     grow_steps = 0
     if args.workload == "grown":
         kw, ctx, grow_steps = grow_colony(cbm, args, rank)
+        if args.timed_neighbors == "cell_linked":
+            # the grown state in a CellLinked context: the same force walk
+            # (every step of the colony has births, so CLVD walks the cells
+            # too), without the Verlet rows' memory on the device
+            snap = ctx.download()
+            ctx.close()
+            kw = dict(kw, neighbors=abi.NEIGH_CELL_LINKED)
+            ctx = cbm.Context(abi.make_config(**kw))
+            ctx.upload({k: snap[k] for k in ("x", "y", "z", "v", "g", "id", "parent")},
+                       t=snap["t"], step=snap["step"], id_max=snap["id_max"])
         cfg = abi.make_config(**kw)
     else:
         kw, state = make_workload(abi, args, rank)
@@ -304,6 +359,9 @@ def run_ours(args, rank, world, local_rank):
         ctx.upload(state)
     stream = torch.cuda.ExternalStream(ctx.stream())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    # every kernel of the step graph bracketed by events on the library's
+    # stream, read after each timed replay
+    ctx.set_kernel_timing(True)
 
     for _ in range(args.warmup):
         ctx.step(1, abi.SYNC)
@@ -313,6 +371,7 @@ def run_ours(args, rank, world, local_rank):
     clocks = Clocks(local_rank)
     clocks.start()
     total_ms, agent_steps = 0.0, 0
+    kern = {}  # kernel -> [ms of each timed launch]
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     for _ in range(args.steps):
@@ -323,11 +382,14 @@ def run_ours(args, rank, world, local_rank):
         e1.synchronize()
         total_ms += e0.elapsed_time(e1)
         agent_steps += n_before
+        for name, ms in ctx.kernel_times():
+            kern.setdefault(name, []).append(ms)
         flush.zero_()  # evict L2 (256 MB > 126 MB) between timed steps
         torch.cuda.synchronize()
     ctx.sync()
     torch.cuda.synchronize()
     clk = clocks.stop()
+    ctx.set_kernel_timing(False)
     if dist:
         t = torch.tensor([total_ms, float(agent_steps)], dtype=torch.float64, device="cuda")
         tmax = t.clone()
@@ -340,59 +402,47 @@ def run_ours(args, rank, world, local_rank):
     value = agent_steps_job / (total_ms_job / 1e3)
     ms_per_step = total_ms_job / args.steps
 
-    # per-kernel durations of eager steps (events on the library stream)
-    prof = {}
-    for _ in range(args.profile_steps):
-        for name, ms in ctx.profile_step():
-            prof.setdefault(name, []).append(ms)
-    n_now = ctx.counters()["N"]
-    # A step that followed an add/remove walks the cells instead of reading the
-    # list (recompute-on-event), so its compulsory bytes are the cell-mode ones.
+    # roofline of the dominant kernel over the timed steps: its launches were
+    # timed inside the step graphs above, on the library's stream
     walked = ctx.counters()["flag"] == 1
     verlet = cfg.neighbors in (abi.NEIGH_CLVD, abi.NEIGH_VERLET_DISPLACEMENT) and not walked
     nbar = float(np.mean(ctx.neighbors()[0])) if verlet else 0.0
     s = 8 if cfg.precision == abi.F64 else 4
-    kern = {k: (float(np.mean(v)), float(np.sum(v))) for k, v in prof.items()}
-    top = max(kern, key=lambda k: kern[k][1])
+    stats = {k: (float(np.mean(v)), float(np.sum(v))) for k, v in kern.items()}
+    top = max(stats, key=lambda k: stats[k][1])
+    agents = agent_steps / args.steps  # agents per launch, averaged over the timed steps
     hbm, peak_kind = peaks()
     bpa = alg_bytes_per_agent(top, s, cfg.dims, nbar, verlet, cfg.fate != abi.FATE_NONE)
     roof = None
     if bpa is not None:
-        achieved = bpa * n_now / (kern[top][0] / 1e3) / 1e9
+        avg_ms = stats[top][0]
+        achieved = bpa * agents / (avg_ms / 1e3) / 1e9
+        per = profile_per_agent() if (top == "k_agent_de" and s == 4 and walked
+                                      and args.workload == "grown") else {}
+        traffic = per.get("dram_bytes_per_agent")
         roof = {"kernel": top, "bound": "hbm", "achieved": round(achieved, 1),
                 "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4),
-                "traffic": traffic_per_launch(top, s, walked, n_now, args.workload),
-                "alg_bytes_per_agent": round(bpa, 2), "agents": n_now, "nbar": round(nbar, 2),
-                "avg_ms": round(kern[top][0], 4)}
-    step_share = {k: round(v[1] / sum(x[1] for x in kern.values()), 4) for k, v in kern.items()}
+                "traffic": None if traffic is None else round(traffic * agents),
+                "traffic_source": os.path.relpath(KERNEL_PROFILE, ROOT) if traffic else None,
+                "alg_bytes_per_agent": round(bpa, 2), "agents": round(agents), "nbar": round(nbar, 2),
+                "avg_ms": round(avg_ms, 4), "launches_timed": len(kern[top])}
+        inst = per.get("warp_inst_per_agent")
+        if inst and clk and clk.get("sm_mhz"):
+            # issue-rate roofline: warp instructions per second against the
+            # issue limit of 148 SMs x 4 schedulers x one instruction a clock
+            n_sm = torch.cuda.get_device_properties(local_rank).multi_processor_count
+            issue_peak = n_sm * 4 * clk["sm_mhz"] * 1e6
+            issue = inst * agents / (avg_ms / 1e3)
+            roof["issue"] = {"achieved": round(issue / 1e9, 2), "peak": round(issue_peak / 1e9, 2),
+                             "unit": "G warp-instructions/s", "frac": round(issue / issue_peak, 4),
+                             "warp_inst_per_agent": inst,
+                             "source": os.path.relpath(KERNEL_PROFILE, ROOT)}
+    step_share = {k: round(v[1] / sum(x[1] for x in stats.values()), 4) for k, v in stats.items()}
+    kern = stats
 
     # end to end through the C ABI with pinned host buffers
-    cap = int(cfg.n_max)
-    snap = ctx.download()
-    host = pinned_state(cbm, cfg, {k: snap[k] for k in ("x", "y", "z", "v", "g", "id", "parent")},
-                        cap)
-    lib = ctx.lib
-    e2e_time, e2e_agents, h2d, d2h = 0.0, 0, 0, 0
-    nstate = snap["N"]
-    t_now, st_now, idm = snap["t"], snap["step"], snap["id_max"]
-    per_agent = 3 * s + 2 * s + 16  # x,y,z,v,g + id,parent
-    for k in range(args.e2e_steps):
-        view = host.view(N=nstate, t=t_now, step=st_now, id_max=idm,
-                         fields=("x", "y", "z", "v", "g", "id", "parent"))
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        ctx._check(lib.cbm_upload(ctx.h, C.byref(view)))
-        ctx._check(lib.cbm_step(ctx.h, 1, abi.SYNC))
-        view.capacity = cap
-        ctx._check(lib.cbm_download(ctx.h, C.byref(view), abi.VIEW_COMMITTED))
-        t1 = time.perf_counter()
-        if k > 0:  # the first call also builds the step graph of this parity
-            e2e_time += t1 - t0
-            e2e_agents += nstate
-            h2d += nstate * per_agent
-            d2h += view.N * per_agent
-        nstate, t_now, st_now, idm = view.N, view.t, view.step, view.id_max
+    e2e_time, e2e_agents, h2d, d2h, snap = e2e_through_abi(cbm, ctx, cfg, args.e2e_steps)
     n_e2e = max(args.e2e_steps - 1, 1)
     if dist:
         t = torch.tensor([e2e_time, float(e2e_agents)], dtype=torch.float64, device="cuda")
@@ -842,12 +892,18 @@ def run_configs(args):
     n0 = g.counters()["N"]
     g.step(3)
     ms = _device_steps(cbm, g, args.config_f64_steps, flush=flush)
+    # end to end through the C ABI in Float64, host copies included
+    et, ea, eh, ed, _ = e2e_through_abi(cbm, g, abi.make_config(**kw64), args.e2e_steps)
     g.close()
+    n_e2e = max(args.e2e_steps - 1, 1)
     out["colony_3d_f64"] = {"workload": "grown from 10^4 in Float64", "grow_steps": gsteps,
                             "agents": int(n0), "steps_timed": args.config_f64_steps,
                             "ms_per_step": round(ms / args.config_f64_steps, 4),
                             "value": round(n0 * args.config_f64_steps / (ms / 1e3), 1),
-                            "unit": UNIT}
+                            "unit": UNIT, "dtype": "f64",
+                            "e2e": {"value": round(ea / et, 1), "unit": UNIT,
+                                    "h2d_bytes_per_step": int(eh / n_e2e),
+                                    "d2h_bytes_per_step": int(ed / n_e2e)}}
     kw, st = packed_colony_3d(abi, N=args.n)
     g = cbm.Context(abi.make_config(**kw))
     g.upload(st)
@@ -943,6 +999,58 @@ def cpu_baseline(args, steps, threads=None, kw=None, snap=None):
                        f"every step, OpenMP over agents, from the GPU run's state")
 
 
+def run_reference(args, config):
+    """The reference arm: the CPU restatement of the reference's CPU path (the
+    oracle: Float64, CellLinked rebuilt every step, OpenMP over agents, serial
+    compaction, as src/neighbors.jl:918-979 and update.jl:15-119 run it) on
+    all host cores, W untimed and K timed steps.  The reference is Julia and
+    cannot run here.  Its input is built without the product library: growing
+    10^4 agents to 10^6 on the CPU takes hours, so for the grown workload a
+    stand-in of 10^6 agents is drawn from the grown colony's measured density,
+    volume and growth-rate histograms (tests/golden/), with the grown state's
+    partner counts.  The CPU steps it at least as fast as the grown state
+    itself, so the ratio to this arm understates the speed-up, if anything."""
+    cbm = load_package()  # the ctypes structures only: libcbm_b200.so is not loaded
+    abi = cbm._abi
+    from _oracle import OracleContext
+    if args.workload == "grown":
+        from scenarios import grown_colony_stand_in
+        kw, state = grown_colony_stand_in(abi, precision=abi.F64)
+        sample = ("the 10^6-agent grown-colony stand-in (density, volume and growth-rate "
+                  "histograms of the colony grown on the device, numbered in cell order)")
+    else:
+        kw, state = make_workload(abi, args, 0)
+        sample = f"the packed snapshot at density {args.density}"
+    kw = dict(kw, neighbors=abi.NEIGH_CELL_LINKED, precision=abi.F64)
+    threads = os.cpu_count()
+    o = OracleContext(abi, abi.make_config(**kw), threads=threads)
+    o.upload(state)
+    for _ in range(args.warmup):
+        o.step(1)
+    wall, agent_steps = 0.0, 0
+    for _ in range(args.steps):
+        n = o.counters()["N"]
+        t0 = time.perf_counter()
+        o.step(1)
+        wall += time.perf_counter() - t0
+        agent_steps += n
+    o.close()
+    value = agent_steps / wall
+    cb = {"value": round(value, 1), "unit": UNIT, "cores": threads, "kind": "port",
+          "sample": f"{args.steps} timed steps (after {args.warmup} untimed) of {sample}, "
+                    f"{agent_steps // max(args.steps, 1)} agents per step, Float64, "
+                    f"CellLinked(3.3) rebuilt every step, OpenMP over agents"}
+    return {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * wall / max(args.steps, 1), 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config, "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "the reference is Julia and cannot run here; this times its C++ restatement "
+                    "(the CPU checker) on the host cores"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -957,7 +1065,9 @@ def main():
                     help="grown: the colony grown from 10^4 to n (the configured run); "
                          "packed: a synthetic snapshot at packing density")
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
-    ap.add_argument("--profile-steps", type=int, default=5)
+    ap.add_argument("--timed-neighbors", default="clvd", choices=["clvd", "cell_linked"],
+                    help="cell_linked: time the grown state in a CellLinked context (the same "
+                         "force walk without the Verlet rows' memory; for profiler captures)")
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1006,32 +1116,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        steps = args.steps + args.warmup
-        kw = snap = None
-        if args.workload == "grown":
-            # the same input state as the GPU arm: the colony grown from 10^4
-            # (prepared through the library; the timed steps below run the CPU
-            # restatement only)
-            import torch
-            torch.cuda.set_device(local_rank)
-            cbm = load_package()
-            kw, gctx, gsteps = grow_colony(cbm, args, 0)
-            snap = gctx.download()
-            gctx.close()
-            config["grow_steps"] = gsteps
-        cb = cpu_baseline(args, max(1, min(args.steps, 5)), kw=kw, snap=snap)
-        line = {"metric": METRIC, "value": round(cb["value"], 1), "unit": UNIT,
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": round(1e3 * args.n / cb["value"], 3), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": config, "impl": "reference",
-                "cpu_baseline": cb,
-                "e2e": {"value": round(cb["value"], 1), "unit": UNIT, "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0},
-                "note": "the reference is Julia and cannot run here; this times its C++ "
-                        "restatement (the CPU checker) on the host cores; "
-                        f"{min(args.steps, 5)} of {steps} requested steps were run"}
-        print(json.dumps(line), flush=True)
+        print(json.dumps(run_reference(args, config)), flush=True)
         return
 
     if world > 1:
@@ -1057,8 +1142,8 @@ def main():
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": round(r["ms_per_step"], 4), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
-                "data": "synthetic", "config": dict(config, grow_steps=r["grow_steps"],
-                                                    agents_after_timing=r["snap"]["N"]),
+                "data": "synthetic", "config": config,
+                "state": {"grow_steps": r["grow_steps"], "agents_after_timing": r["snap"]["N"]},
                 "roofline": r["roof"],
                 "cpu_baseline": cb, "e2e": r["e2e"], "gpu_launches": r["launches"],
                 "clocks": r["clocks"], "kernel_share": r["share"],

@@ -143,6 +143,9 @@ def load_library(path=LIB_PATH):
         "cbm_kernels_per_step": (C.c_int, [vp]),
         "cbm_profile_step": (C.c_int, [vp, i32, C.POINTER(C.c_float), C.POINTER(C.c_char_p),
                                        C.POINTER(i32)]),
+        "cbm_set_kernel_timing": (C.c_int, [vp, i32]),
+        "cbm_kernel_times": (C.c_int, [vp, i32, C.POINTER(C.c_float), C.POINTER(C.c_char_p),
+                                       C.POINTER(i32)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -328,6 +331,18 @@ class Context:
         names = (C.c_char_p * 64)()
         n = C.c_int32()
         self._check(self.lib.cbm_profile_step(self.h, 64, ms, names, C.byref(n)))
+        return [(names[i].decode(), ms[i]) for i in range(min(n.value, 64))]
+
+    def set_kernel_timing(self, on=True):
+        """Event records around every kernel inside the step graphs (on), or none."""
+        self._check(self.lib.cbm_set_kernel_timing(self.h, 1 if on else 0))
+
+    def kernel_times(self):
+        """[(kernel name, ms)] of the last graph-replayed step (kernel timing on)."""
+        ms = (C.c_float * 64)()
+        names = (C.c_char_p * 64)()
+        n = C.c_int32()
+        self._check(self.lib.cbm_kernel_times(self.h, 64, ms, names, C.byref(n)))
         return [(names[i].decode(), ms[i]) for i in range(min(n.value, 64))]
 
 

@@ -87,7 +87,9 @@ struct cbm_ctx {
   bool rule_done = false, de_done = false, mrule_done = false, mde_done = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
 
-  // per-kernel event timing of eager steps (cbm_profile_step)
+  // per-kernel event timing: of eager steps (cbm_profile_step, `marks`) and,
+  // when graph timing is on, inside the step graph of each parity
+  // (`gmarks[p]`, re-recorded by every replay)
   bool prof = false;
   struct Mark {
     const char* name;
@@ -95,6 +97,11 @@ struct cbm_ctx {
   };
   std::vector<Mark> marks;
   size_t mark_used = 0;
+  bool graph_timing = false;
+  std::vector<Mark> gmarks[2];
+  size_t gmark_used[2] = {0, 0};
+  std::vector<Mark>* prof_set = nullptr;  // the set being recorded
+  size_t* prof_used = nullptr;
 };
 
 extern "C" int cbm_sync(cbm_ctx* c);
@@ -134,13 +141,15 @@ struct Prof {
   cbm_ctx::Mark* m = nullptr;
   Prof(cbm_ctx* ctx, const char* name) : c(ctx) {
     if (!c->prof) return;
-    if (c->mark_used == c->marks.size()) {
+    std::vector<cbm_ctx::Mark>& set = c->prof_set ? *c->prof_set : c->marks;
+    size_t& used = c->prof_used ? *c->prof_used : c->mark_used;
+    if (used == set.size()) {
       cbm_ctx::Mark mk{name, {nullptr, nullptr}};
       cudaEventCreate(&mk.ev[0]);
       cudaEventCreate(&mk.ev[1]);
-      c->marks.push_back(mk);
+      set.push_back(mk);
     }
-    m = &c->marks[c->mark_used++];
+    m = &set[used++];
     m->name = name;
     cudaEventRecord(m->ev[0], c->stream);
   }
@@ -606,6 +615,13 @@ void free_all(cbm_ctx* c) {
   c->marks.clear();
   for (int q = 0; q < 2; ++q)
     if (c->graph[q]) cudaGraphExecDestroy(c->graph[q]);
+  for (int q = 0; q < 2; ++q) {
+    for (auto& m : c->gmarks[q]) {
+      cudaEventDestroy(m.ev[0]);
+      cudaEventDestroy(m.ev[1]);
+    }
+    c->gmarks[q].clear();
+  }
   for (void* p : c->allocs) cudaFree(p);
   c->allocs.clear();
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1056,7 +1072,16 @@ int cbm_step(cbm_ctx* c, int32_t nsteps, int32_t flags) {
       if (!c->graph[p]) {
         cudaGraph_t g = nullptr;
         CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        if (c->graph_timing) {  // event records around each kernel become graph nodes
+          c->prof = true;
+          c->prof_set = &c->gmarks[p];
+          c->prof_used = &c->gmark_used[p];
+          c->gmark_used[p] = 0;
+        }
         dispatch<FullStep>(c, p);
+        c->prof = false;
+        c->prof_set = nullptr;
+        c->prof_used = nullptr;
         cudaError_t e = cudaStreamEndCapture(c->stream, &g);
         if (e != cudaSuccess) return fail(c, CBM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
         e = cudaGraphInstantiate(&c->graph[p], g, 0);
@@ -1261,5 +1286,38 @@ int cbm_profile_step(cbm_ctx* c, int32_t max_kernels, float* ms, const char** na
 }
 
 int cbm_kernels_per_step(cbm_ctx* c) { return c ? kernels_per_step(c) : 0; }
+
+int cbm_set_kernel_timing(cbm_ctx* c, int32_t on) {
+  if (!c) return CBM_ERR_ARG;
+  cudaSetDevice(c->device);
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if ((on != 0) != c->graph_timing) {
+    for (int q = 0; q < 2; ++q)
+      if (c->graph[q]) {
+        cudaGraphExecDestroy(c->graph[q]);
+        c->graph[q] = nullptr;
+      }
+    c->graph_timing = on != 0;
+  }
+  return CBM_OK;
+}
+
+int cbm_kernel_times(cbm_ctx* c, int32_t max_kernels, float* ms, const char** names,
+                     int32_t* n_kernels) {
+  if (!c || !n_kernels) return CBM_ERR_ARG;
+  if (!c->graph_timing) return fail(c, CBM_ERR_STATE, "kernel timing is off (cbm_set_kernel_timing)");
+  cudaSetDevice(c->device);
+  const int p = c->parity ^ 1;  // the parity of the step replayed last
+  if (!c->graph[p]) return fail(c, CBM_ERR_STATE, "no step graph has been replayed yet");
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  *n_kernels = (int32_t)c->gmark_used[p];
+  for (size_t q = 0; q < c->gmark_used[p] && (int)q < max_kernels; ++q) {
+    float t = 0.f;
+    CUDA_TRY(c, cudaEventElapsedTime(&t, c->gmarks[p][q].ev[0], c->gmarks[p][q].ev[1]));
+    if (ms) ms[q] = t;
+    if (names) names[q] = c->gmarks[p][q].name;
+  }
+  return CBM_OK;
+}
 
 }  // extern "C"

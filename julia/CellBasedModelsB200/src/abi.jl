@@ -186,6 +186,19 @@ function cbm_profile_step(ctx, max_kernels=32)
     [(unsafe_string(names[k]), ms[k]) for k in 1:n[]]
 end
 
+"""Kernel timing inside the step graphs on (true) or off; graphs are captured again."""
+cbm_set_kernel_timing(ctx, on::Bool) =
+    check(ccall((:cbm_set_kernel_timing, LIBCBM), Cint, (Ptr{Cvoid}, Int32), ctx, on ? 1 : 0), ctx)
+"""Durations (ms) and names of the kernels of the last graph-replayed step."""
+function cbm_kernel_times(ctx, max_kernels=32)
+    ms = zeros(Float32, max_kernels)
+    names = fill(Ptr{UInt8}(C_NULL), max_kernels)
+    n = Ref{Int32}(0)
+    check(ccall((:cbm_kernel_times, LIBCBM), Cint, (Ptr{Cvoid}, Int32, Ptr{Float32}, Ptr{Ptr{UInt8}}, Ref{Int32}),
+                ctx, max_kernels, ms, names, n), ctx)
+    [(unsafe_string(names[k]), ms[k]) for k in 1:min(n[], max_kernels)]
+end
+
 # ---- batched communities ------------------------------------------------------------
 cbm_batch_last_error(b) = unsafe_string(ccall((:cbm_batch_last_error, LIBCBM), Cstring, (Ptr{Cvoid},), b))
 bcheck(rc, b) = rc == CBM_OK ? nothing : throw(CbmError(rc, cbm_batch_last_error(b)))

@@ -6,6 +6,9 @@ measured on (soft-sphere aggregation, a growing 3D colony, chemotaxis on a
 medium, many small communities, a differentiable ODE trajectory); sizes are
 parameters so that tests run small cases and the bench the full ones.
 """
+import json
+import os
+
 import numpy as np
 
 
@@ -59,11 +62,11 @@ def colony_3d(abi, N=10000, R=None, L=400.0, n_max=None, seed=2, precision=None,
 GROWN_COLONY_ROW = 1024
 
 
-def growing_colony_3d(abi, n_target, precision=None, seed=2):
+def growing_colony_3d(abi, n_target, precision=None, seed=2, headroom=1.2):
     """The configured 3D growing colony: 10^4 agents uniform in a radius-20
-    ball centred in [0,400]^3 (colony_3d's model), with capacity 1.2 n_target
-    and Verlet rows that hold the grown state's partners."""
-    return colony_3d(abi, N=10_000, R=20.0, L=400.0, n_max=int(1.2 * n_target), seed=seed,
+    ball centred in [0,400]^3 (colony_3d's model), with capacity
+    headroom * n_target and Verlet rows that hold the grown state's partners."""
+    return colony_3d(abi, N=10_000, R=20.0, L=400.0, n_max=int(headroom * n_target), seed=seed,
                      precision=precision, n_max_neighbors=GROWN_COLONY_ROW)
 
 
@@ -206,3 +209,25 @@ def medium_colony(abi, dims, N=3000, L=40.0, n_medium=40, seed=6, bilinear=True,
     p = rng.uniform(0, L, size=(dims, N))
     state = {k: p[d] for d, k in enumerate("xyz"[:dims])}
     return kw, state
+
+
+def grown_colony_stand_in(abi, precision=None, seed=12):
+    """A stand-in for the colony grown to 10^6 that is built without growing
+    it: agents drawn from the grown colony's measured radial density, volume
+    and growth-rate histograms (tests/golden/grown_colony_1e6_profile.json),
+    numbered in the order of the cell grid (edge 3.3, x fastest).  Its agents
+    have the grown state's partner counts (about 354 within the cutoff), and
+    the CPU restatement steps it at least as fast as the grown state: the
+    grown colony's own numbering keeps some locality (sisters sit next to each
+    other), which a random numbering loses and the cell numbering exceeds."""
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden", "grown_colony_1e6_profile.json")) as f:
+        prof = json.load(f)
+    kw, st = profile_colony_3d(abi, prof["r_edges"], prof["r_counts"], prof["v_edges"],
+                               prof["v_counts"], prof["g_edges"], prof["g_counts"], seed=seed,
+                               precision=precision)
+    c = np.floor(np.stack([st["x"], st["y"], st["z"]]) / 3.3).astype(np.int64)
+    order = np.lexsort((c[0], c[1], c[2]))
+    st = {k: np.asarray(v)[order] for k, v in st.items()}
+    kw = dict(kw, n_max_neighbors=GROWN_COLONY_ROW)
+    return kw, st
