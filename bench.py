@@ -507,12 +507,27 @@ def run_batched(args, rank=0, world=1, dist=None):
     ms_job = cbm.sweep.max_over_ranks(dist, ms)
     total = sum(d["n"] for d in descs)
     batched = total * args.batched_steps / (ms_job / 1e3)
+    roof = None
+    if tuning is not None:
+        # compulsory bytes of a list step per agent: positions read and
+        # written (2 x 3 x 4), the row count (4) and the list row (4 n_bar),
+        # n_bar = density x (4/3) pi R^3 at the sweep's density (one agent
+        # per 2.5^3) and the tuned list radius R = cutoff + skin
+        R = 3.0 + tuning.skin
+        nbar = (1.0 / 2.5 ** 3) * 4.0 / 3.0 * math.pi * R ** 3
+        bpa = 2 * 3 * 4 + 4 + 4 * nbar
+        hbm, peak_kind = peaks()
+        achieved = bpa * batched / 1e9
+        roof = {"kernel": "k_batch", "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "alg_bytes_per_agent_step": round(bpa, 1), "nbar": round(nbar, 1),
+                "list_radius": R}
     out = {"communities": len(descs), "agents": int(total), "steps": args.batched_steps,
            "value": round(batched, 1), "unit": UNIT, "ms": round(ms_job, 3),
            "ranks": world, "scaling": "strong" if world > 1 else None,
            "rank0_communities": len(sb.mine), "rank0_agents": int(sb.n_agents),
            "tuning": tuning.as_dict() if tuning is not None else None,
-           "autotune_s": round(tune_s, 3), "clocks": clk}
+           "autotune_s": round(tune_s, 3), "clocks": clk, "roofline": roof}
     if rank != 0 or tuning is None:
         return out
     # The plain path, one community at a time, on a sample of the communities:
@@ -807,7 +822,18 @@ def run_configs(args):
     g = cbm.Context(abi.make_config(**kw))
     g.upload(st)
     g.step(3)
-    ms = _device_steps(cbm, g, args.config_steps)
+    # one cbm_step call of all the timed steps (evolve!'s saveEach steps a
+    # call): for this small fate-free community, one cooperative launch
+    stream = torch.cuda.ExternalStream(g.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    g.step(args.config_steps, 0)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    g.sync()
+    ms_graph = _device_steps(cbm, g, 20)  # one call per step, for comparison
     o = OracleContext(abi, abi.make_config(**kw), threads=threads)
     o.upload(st)
     t0 = time.perf_counter()
@@ -820,7 +846,10 @@ def run_configs(args):
         "us_per_step": round(1e3 * ms / args.config_steps, 2),
         "value": round(4096 * args.config_steps / (ms / 1e3), 1), "unit": UNIT,
         "cpu_us_per_step": round(1e6 * cpu_s, 2), "cpu_cores": threads,
-        "note": "L2-resident and launch-bound: one graph replay per step (rule, DE, update, grid)"}
+        "us_per_step_one_call_per_step": round(1e3 * ms_graph / 20, 2),
+        "note": "L2-resident: the timed steps are one cbm_step call, run by one cooperative "
+                "launch (grid barriers between the phases of a step); "
+                "us_per_step_one_call_per_step: one call (one launch) per step"}
 
     # c3: 2D chemotaxis, 2e5 agents, 1024^2 Float32 medium
     kw, st = chemotaxis_2d(abi)

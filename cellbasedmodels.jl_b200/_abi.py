@@ -357,11 +357,12 @@ class CbmCommunityDesc(C.Structure):
 class CbmBatchTuning(C.Structure):
     _fields_ = [("threads", C.c_int32), ("ctas_per_sm", C.c_int32), ("skin", C.c_double),
                 ("rebuild_threshold", C.c_double), ("tile_agents", C.c_int32),
-                ("pad", C.c_int32)]
+                ("lanes_per_agent", C.c_int32)]
 
     def as_dict(self):
         return dict(threads=self.threads, ctas_per_sm=self.ctas_per_sm, skin=self.skin,
-                    rebuild_threshold=self.rebuild_threshold, tile_agents=self.tile_agents)
+                    rebuild_threshold=self.rebuild_threshold, tile_agents=self.tile_agents,
+                    lanes_per_agent=max(self.lanes_per_agent, 1))
 
 
 def _bind_batch(lib):
@@ -438,8 +439,10 @@ class Batch:
         self._check(self.lib.cbm_batch_get_tuning(self.h, C.byref(t)))
         return t
 
-    def set_tuning(self, threads, ctas_per_sm, skin, rebuild_threshold=0.0, tile_agents=0):
-        t = CbmBatchTuning(threads, ctas_per_sm, skin, rebuild_threshold, tile_agents, 0)
+    def set_tuning(self, threads, ctas_per_sm, skin, rebuild_threshold=0.0, tile_agents=0,
+                   lanes_per_agent=1):
+        t = CbmBatchTuning(threads, ctas_per_sm, skin, rebuild_threshold, tile_agents,
+                           lanes_per_agent)
         self._check(self.lib.cbm_batch_set_tuning(self.h, C.byref(t)))
 
     def autotune(self, trial_steps=20):

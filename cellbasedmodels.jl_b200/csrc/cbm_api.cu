@@ -16,6 +16,7 @@
 
 #include "../../include/cbm_b200.h"
 #include "cbm_kernels.cuh"
+#include "cbm_small.cuh"
 
 using namespace cbm;
 
@@ -86,6 +87,9 @@ struct cbm_ctx {
   int parity = 0;
   bool rule_done = false, de_done = false, mrule_done = false, mde_done = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  // small fate-free communities: all steps of a call in one cooperative launch
+  unsigned* small_bar = nullptr;  // grid barrier words (count, generation, abort)
+  long long n_loaded = 0;         // N of the last upload (fixed without births and deaths)
 
   // per-kernel event timing: of eager steps (cbm_profile_step, `marks`) and,
   // when graph timing is on, inside the step graph of each parity
@@ -827,6 +831,7 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     }
   }
   c->ctr = (Counters*)dalloc(c, sizeof(Counters), &ok);
+  c->small_bar = (unsigned*)dalloc(c, 4 * sizeof(unsigned), &ok);
   if (!ok) {
     int rc = fail(nullptr, CBM_ERR_NOMEM, "device allocation failed for n_max=%lld", (long long)k.n_max);
     free_all(c);
@@ -922,6 +927,7 @@ int cbm_upload(cbm_ctx* c, const cbm_state_view* h) {
   c->parity = 0;
   reset_stage_flags(c);
   c->loaded = true;
+  c->n_loaded = h->N;
   dispatch<Pack>(c, (int)N);
   dispatch<FirstSort>(c);
   int rc = check_launch(c);
@@ -1058,6 +1064,42 @@ int cbm_sync(cbm_ctx* c) {
   return CBM_OK;
 }
 
+}  // extern "C"
+
+// A fate-free CellLinked community small enough for one cooperative launch
+// of all its steps (cbm_small.cuh)
+bool small_eligible(const cbm_ctx* c) {
+  const cbm_config& k = c->cfg;
+  return k.neighbors == CBM_NEIGH_CELL_LINKED && k.fate == CBM_FATE_NONE && !k.growth &&
+         !k.medium && k.force_mode == CBM_FORCE_DIRECT &&
+         (k.integrator == CBM_INT_EULER || k.integrator == CBM_INT_EM) &&
+         c->n_cells <= kSmallMaxCells && c->n_loaded > 0 && c->n_loaded <= kSmallMaxAgents;
+}
+
+template <typename T, int D>
+struct SmallSteps {
+  static void run(cbm_ctx* c, int nsteps, cudaError_t* err) {
+    Params<T> P0 = params<T>(c, c->parity), P1 = params<T>(c, c->parity ^ 1);
+    SmallBarrier bar{c->small_bar, c->small_bar + 1, (int*)(c->small_bar + 2)};
+    int n_cells = c->n_cells;
+    const size_t smem = (size_t)(n_cells + 1) * sizeof(int);
+    int bps = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_small_steps<T, D>, kSmallThreads,
+                                                      smem) != cudaSuccess || bps < 1)
+      bps = 1;
+    long long want = (c->n_loaded + kSmallThreads - 1) / kSmallThreads;
+    long long blocks = std::min<long long>(want, (long long)c->n_sm);
+    blocks = std::max<long long>(1, std::min<long long>(blocks, (long long)bps * c->n_sm));
+    *err = cudaMemsetAsync(c->small_bar, 0, 4 * sizeof(unsigned), c->stream);
+    if (*err != cudaSuccess) return;
+    void* args[] = {&P0, &P1, &bar, &nsteps, &n_cells};
+    *err = cudaLaunchCooperativeKernel((const void*)k_small_steps<T, D>, dim3((unsigned)blocks),
+                                       dim3(kSmallThreads), args, smem, c->stream);
+  }
+};
+
+extern "C" {
+
 int cbm_step(cbm_ctx* c, int32_t nsteps, int32_t flags) {
   if (!c) return CBM_ERR_ARG;
   if (!c->loaded) return fail(c, CBM_ERR_STATE, "community not uploaded");
@@ -1066,6 +1108,14 @@ int cbm_step(cbm_ctx* c, int32_t nsteps, int32_t flags) {
   if (c->rule_done || c->de_done || c->mrule_done || c->mde_done)
     return fail(c, CBM_ERR_STATE, "a step is half done through the stage calls; call cbm_update first");
   const bool use_graph = !(flags & CBM_NO_GRAPH);
+  if (use_graph && nsteps > 0 && !c->graph_timing && small_eligible(c)) {
+    cudaError_t e = cudaSuccess;
+    dispatch<SmallSteps>(c, (int)nsteps, &e);
+    if (e != cudaSuccess) return fail(c, CBM_ERR_CUDA, "small-community launch failed: %s", cudaGetErrorString(e));
+    if (nsteps & 1) c->parity ^= 1;
+    if (flags & CBM_SYNC) return cbm_sync(c);
+    return CBM_OK;
+  }
   for (int s = 0; s < nsteps; ++s) {
     const int p = c->parity;
     if (use_graph) {

@@ -189,6 +189,140 @@ __device__ __forceinline__ void pair_force(const Comm& C, const float* xi, const
   for (int d = 0; d < 3; ++d) acc[d] = acc[d] + sc * e[d];
 }
 
+// The same pair term as pair_force, returned instead of added: t = (F/d) e.
+__device__ __forceinline__ bool pair_term3(const Comm& C, const float* xi, const float* xj,
+                                           float* t) {
+  float e[3];
+  e[0] = xi[0] - xj[0];
+  float s2 = e[0] * e[0];
+  e[1] = xi[1] - xj[1];
+  s2 = s2 + e[1] * e[1];
+  e[2] = xi[2] - xj[2];
+  s2 = s2 + e[2] * e[2];
+  if (s2 >= C.cut2) return false;
+  const float dd = sqrtf(s2);
+  float F;
+  if (dd < C.r_rep) F = C.k_rep * (C.r_rep - dd);
+  else if (dd < C.r_att) F = -(C.k_att * (dd - C.r_rep));
+  else return false;
+  const float sc = F / dd;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) t[d] = sc * e[d];
+  return true;
+}
+
+// L lanes of a warp that share one agent (lanes_per_agent): the lane's place
+// in its group and the group's lanes.
+template <int L>
+struct Group {
+  int gl;
+  unsigned mask;
+  __device__ Group() {
+    const int lane = threadIdx.x & 31;
+    gl = lane & (L - 1);
+    mask = (L == 32 ? 0xffffffffu : ((1u << L) - 1u)) << (lane & ~(L - 1));
+  }
+};
+
+// The terms of the group's lanes added to acc in lane order (the list order
+// of the entries the lanes hold); every lane of the group keeps the same acc.
+template <int L>
+__device__ __forceinline__ void group_add(const Group<L>& g, bool has, const float* t, float* acc) {
+#pragma unroll
+  for (int u = 0; u < L; ++u) {
+    const int hu = __shfl_sync(g.mask, has ? 1 : 0, u, L);
+    const float t0 = __shfl_sync(g.mask, t[0], u, L);
+    const float t1 = __shfl_sync(g.mask, t[1], u, L);
+    const float t2 = __shfl_sync(g.mask, t[2], u, L);
+    if (hu) {
+      acc[0] = acc[0] + t0;
+      acc[1] = acc[1] + t1;
+      acc[2] = acc[2] + t2;
+    }
+  }
+}
+
+// Rebuild step of slot q with L lanes: lane u of the group takes candidates
+// u, u + L, ... of each run; the list row is written at the places the
+// group's ballot gives (candidate order), and the terms are added in
+// candidate order by group_add.
+template <bool SM, int L>
+__device__ __forceinline__ void build_row_group(const BatchParams& B, const Comm& C,
+                                                const float4* X, const float* sx, const float* sy,
+                                                const float* sz, int q, const float* xi, int* list,
+                                                int* nbr_n, float* acc) {
+  const Group<L> g;
+  const int n = C.n, M = B.max_nbrs;
+  const int* start = B.cell_start + C.cell_off;
+  int q3[3];
+  cell_coords<3>(C.nc, cell_of<float, 3>(B.edge, C.lo, C.hi, C.nc, xi), q3);
+  const int xa = max(q3[0] - 1, 0), xb = min(q3[0] + 1, C.nc[0] - 1);
+  const int shift = (threadIdx.x & 31) & ~(L - 1);
+  int m = 0;
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int z = q3[2] + dz;
+    if (z < 0 || z >= C.nc[2]) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int y = q3[1] + dy;
+      if (y < 0 || y >= C.nc[1]) continue;
+      const int row = (z * C.nc[1] + y) * C.nc[0];
+      const int s1 = start[row + xb + 1];
+      for (int base = start[row + xa]; base < s1; base += L) {
+        const int s = base + g.gl;
+        bool in = false, has = false;
+        float t[3] = {0.f, 0.f, 0.f};
+        if (s < s1 && s != q) {
+          float xj[3];
+          pos_of<SM>(X, sx, sy, sz, s, xj);
+          float e = xi[0] - xj[0];
+          float s2 = e * e;
+          e = xi[1] - xj[1];
+          s2 = s2 + e * e;
+          e = xi[2] - xj[2];
+          s2 = s2 + e * e;
+          in = s2 < B.skin2 && (s2 < B.skin2_lo || sqrtf(s2) < B.skin);
+          if (in) has = pair_term3(C, xi, xj, t);
+        }
+        const unsigned gb = (__ballot_sync(g.mask, in) >> shift) & ((1u << L) - 1u);
+        if (in) {
+          const int pos = m + __popc(gb & ((1u << g.gl) - 1u));
+          if (pos < M) list[(long long)pos * n + q] = s;
+        }
+        m += __popc(gb);
+        group_add<L>(g, has, t, acc);
+      }
+    }
+  }
+  if (g.gl == 0) {
+    if (m > M) atomicOr(B.err, kErrNeighborOverflow);
+    nbr_n[q] = m < M ? m : M;
+  }
+}
+
+// Non-rebuild step of slot q with L lanes: lane u takes list entries u,
+// u + L, ...; the terms are added in list order.
+template <bool SM, int L>
+__device__ __forceinline__ void list_row_group(const BatchParams& B, const Comm& C,
+                                               const float4* X, const float* sx, const float* sy,
+                                               const float* sz, int q, const float* xi,
+                                               const int* list, const int* nbr_n, float* acc) {
+  const Group<L> g;
+  const int n = C.n;
+  const int m = nbr_n[q];
+  const int* row = list + q;
+  for (int k0 = 0; k0 < m; k0 += L) {
+    const int k = k0 + g.gl;
+    bool has = false;
+    float t[3] = {0.f, 0.f, 0.f};
+    if (k < m) {
+      float xj[3];
+      pos_of<SM>(X, sx, sy, sz, row[(long long)k * n], xj);
+      has = pair_term3(C, xi, xj, t);
+    }
+    group_add<L>(g, has, t, acc);
+  }
+}
+
 // Rebuild step of slot q: the CLVD list row (verletNeighborsCLVD,
 // neighbors.jl:1071-1131 as intended: the 27 cells x fastest, d < list
 // radius) and, in the same pass and the same order, the force.  For fixed
@@ -263,7 +397,7 @@ __device__ __forceinline__ void list_row(const BatchParams& B, const Comm& C, co
 }
 
 // all requested steps of one community
-template <int NT, bool SM>
+template <int NT, bool SM, int L>
 __device__ void run_comm(const BatchParams& B, const Comm& C, int ci, int nsteps, float* sx,
                          float* sy, float* sz, int* warp_sums, int* s_flag) {
   int par = B.parity[ci];
@@ -292,12 +426,19 @@ __device__ void run_comm(const BatchParams& B, const Comm& C, int ci, int nsteps
     __syncthreads();
     // the flag of the next step: every thread has read it last step
     if (threadIdx.x == 0) s_flag[(t + 1) & 1] = 0;
-    for (int q = threadIdx.x; q < n; q += NT) {
+    // L lanes per agent: the group of lanes (threadIdx.x / L) shares slot q
+    for (int q = (int)threadIdx.x / L; q < n; q += NT / L) {
       const float4 me = Xc[q];
       const float xi[3] = {me.x, me.y, me.z};
       float acc[3] = {0.f, 0.f, 0.f};
-      if (rebuild) build_row<SM>(B, C, Xc, sx, sy, sz, q, xi, list, nbr_n, acc);
-      else list_row<SM>(B, C, Xc, sx, sy, sz, q, xi, list, nbr_n, acc);
+      if constexpr (L == 1) {
+        if (rebuild) build_row<SM>(B, C, Xc, sx, sy, sz, q, xi, list, nbr_n, acc);
+        else list_row<SM>(B, C, Xc, sx, sy, sz, q, xi, list, nbr_n, acc);
+      } else {
+        if (rebuild) build_row_group<SM, L>(B, C, Xc, sx, sy, sz, q, xi, list, nbr_n, acc);
+        else list_row_group<SM, L>(B, C, Xc, sx, sy, sz, q, xi, list, nbr_n, acc);
+        if ((threadIdx.x & (L - 1)) != 0) continue;  // the group's first lane integrates
+      }
       float z[3];
       cbm_normals(B.seed, step, (uint32_t)agent_index(me), CBM_STREAM_NOISE, C.community, 3, z);
       float xn[3];
@@ -327,7 +468,7 @@ __device__ void run_comm(const BatchParams& B, const Comm& C, int ci, int nsteps
 
 // MINB: resident CTAs per SM the register allocation must allow (the
 // tuning's ctas_per_sm when it is 1 or 2)
-template <int NT, int MINB>
+template <int NT, int MINB, int L>
 __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams B, int nsteps) {
   extern __shared__ float s_tile[];
   __shared__ int s_comm;
@@ -345,8 +486,8 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams B, int nsteps) {
     const int ci = s_comm;
     if (ci < 0) return;
     const Comm C = B.comms[ci];
-    if (C.n <= B.tile) run_comm<NT, true>(B, C, ci, nsteps, sx, sy, sz, warp_sums, s_flag);
-    else run_comm<NT, false>(B, C, ci, nsteps, sx, sy, sz, warp_sums, s_flag);
+    if (C.n <= B.tile) run_comm<NT, true, L>(B, C, ci, nsteps, sx, sy, sz, warp_sums, s_flag);
+    else run_comm<NT, false, L>(B, C, ci, nsteps, sx, sy, sz, warp_sums, s_flag);
     __syncthreads();
   }
 }
@@ -390,7 +531,7 @@ struct cbm_batch {
   int* nbr_n = nullptr;
   int* nbr_list = nullptr;
   int* d_err = nullptr;
-  cbm_batch_tuning tune{256, 2, 0.3, 0.0, 0, 0};
+  cbm_batch_tuning tune{256, 2, 0.3, 0.0, 0, 1};
   std::map<int, cudaGraphExec_t> graphs;  // per nsteps
   int n_sm = 148;
 };
@@ -448,10 +589,18 @@ double list_radius(const cbm_batch* b) { return b->cutoff + b->tune.skin; }
 using BatchKernel = void (*)(BatchParams, int);
 
 // registers limited for two resident CTAs when the tuning asks for two or more
+template <int NT, int L>
+void launch_batch_l(cbm_batch* b, const BatchParams& B, int nsteps, int grid, size_t smem) {
+  if (b->tune.ctas_per_sm >= 2) k_batch<NT, 2, L><<<grid, NT, smem, b->stream>>>(B, nsteps);
+  else k_batch<NT, 1, L><<<grid, NT, smem, b->stream>>>(B, nsteps);
+}
 template <int NT>
 void launch_batch(cbm_batch* b, const BatchParams& B, int nsteps, int grid, size_t smem) {
-  if (b->tune.ctas_per_sm >= 2) k_batch<NT, 2><<<grid, NT, smem, b->stream>>>(B, nsteps);
-  else k_batch<NT, 1><<<grid, NT, smem, b->stream>>>(B, nsteps);
+  switch (b->tune.lanes_per_agent) {
+    case 2: launch_batch_l<NT, 2>(b, B, nsteps, grid, smem); break;
+    case 4: launch_batch_l<NT, 4>(b, B, nsteps, grid, smem); break;
+    default: launch_batch_l<NT, 1>(b, B, nsteps, grid, smem); break;
+  }
 }
 
 // dynamic shared memory of a position tile (x, y, z arrays)
@@ -460,8 +609,13 @@ size_t tile_bytes(int tile_agents) { return (size_t)std::max(tile_agents, 0) * 3
 
 int set_smem_limit(cbm_batch* b) {
   const int bytes = (int)tile_bytes(b->tune.tile_agents);
-  for (const BatchKernel k : {k_batch<128, 1>, k_batch<128, 2>, k_batch<256, 1>, k_batch<256, 2>,
-                              k_batch<512, 1>, k_batch<512, 2>, k_batch<1024, 1>, k_batch<1024, 2>})
+  for (const BatchKernel k :
+       {k_batch<128, 1, 1>, k_batch<128, 2, 1>, k_batch<256, 1, 1>, k_batch<256, 2, 1>,
+        k_batch<512, 1, 1>, k_batch<512, 2, 1>, k_batch<1024, 1, 1>, k_batch<1024, 2, 1>,
+        k_batch<128, 1, 2>, k_batch<128, 2, 2>, k_batch<256, 1, 2>, k_batch<256, 2, 2>,
+        k_batch<512, 1, 2>, k_batch<512, 2, 2>, k_batch<1024, 1, 2>, k_batch<1024, 2, 2>,
+        k_batch<128, 1, 4>, k_batch<128, 2, 4>, k_batch<256, 1, 4>, k_batch<256, 2, 4>,
+        k_batch<512, 1, 4>, k_batch<512, 2, 4>, k_batch<1024, 1, 4>, k_batch<1024, 2, 4>})
     BCUDA(b, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   return CBM_OK;
 }
@@ -689,9 +843,13 @@ int cbm_batch_set_tuning(cbm_batch* b, const cbm_batch_tuning* t) {
     return bfail(b, CBM_ERR_ARG, "ctas_per_sm must be in [1, 8] and skin positive");
   if (t->tile_agents < 0 || tile_bytes(t->tile_agents) > (size_t)kMaxTileBytes)
     return bfail(b, CBM_ERR_ARG, "tile_agents must be in [0, %d]", kMaxTileBytes / 12);
+  if (t->lanes_per_agent != 0 && t->lanes_per_agent != 1 && t->lanes_per_agent != 2 &&
+      t->lanes_per_agent != 4)
+    return bfail(b, CBM_ERR_ARG, "lanes_per_agent must be 1, 2 or 4");
   cudaSetDevice(b->device);
   BCUDA(b, cudaStreamSynchronize(b->stream));
   b->tune = *t;
+  if (b->tune.lanes_per_agent == 0) b->tune.lanes_per_agent = 1;
   return apply_tuning(b);
 }
 
@@ -810,6 +968,26 @@ int cbm_batch_autotune(cbm_batch* b, int32_t trial_steps, cbm_batch_tuning* best
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  // times trial_steps of tuning t on the saved state; the fastest is kept
+  auto try_tuning = [&](const cbm_batch_tuning& t) {
+    if (cbm_batch_set_tuning(b, &t)) return;
+    if (cudaMemcpy(b->P[0], p0.data(), n * 16, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->P[1], p1.data(), n * 16, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->parity, par.data(), nc * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->step, st.data(), nc * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+      return;
+    cudaEventRecord(e0, b->stream);
+    int rc = enqueue_batch(b, trial_steps);
+    cudaEventRecord(e1, b->stream);
+    if (rc) return;
+    if (batch_sync(b)) return;  // an overflowing list disqualifies the setting
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = t;
+    }
+  };
   for (double sk : skins)
     for (int th : threads)
       for (int cp : ctas)
@@ -819,24 +997,16 @@ int cbm_batch_autotune(cbm_batch* b, int32_t trial_steps, cbm_batch_tuning* best
         const int fit = (int)std::min<long long>(kMaxTileBytes, 227 * 1024 / cp - 1024) / 12;
         const int tile = staged ? std::min(fit, largest) : 0;
         if (staged && tile < 1) continue;
-        cbm_batch_tuning t{th, cp, sk, 0.0, tile, 0};
-        if (cbm_batch_set_tuning(b, &t)) continue;
-        BCUDA(b, cudaMemcpy(b->P[0], p0.data(), n * 16, cudaMemcpyHostToDevice));
-        BCUDA(b, cudaMemcpy(b->P[1], p1.data(), n * 16, cudaMemcpyHostToDevice));
-        BCUDA(b, cudaMemcpy(b->parity, par.data(), nc * 4, cudaMemcpyHostToDevice));
-        BCUDA(b, cudaMemcpy(b->step, st.data(), nc * 8, cudaMemcpyHostToDevice));
-        cudaEventRecord(e0, b->stream);
-        int rc = enqueue_batch(b, trial_steps);
-        cudaEventRecord(e1, b->stream);
-        if (rc) continue;
-        if (batch_sync(b)) continue;  // an overflowing list disqualifies the setting
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best_ms) {
-          best_ms = ms;
-          best = t;
-        }
+        cbm_batch_tuning t{th, cp, sk, 0.0, tile, 1};
+        try_tuning(t);
       }
+  // agents per warp: the best setting with 2 and 4 lanes per agent
+  const cbm_batch_tuning one_lane = best;
+  for (int lanes : {2, 4}) {
+    cbm_batch_tuning t = one_lane;
+    t.lanes_per_agent = lanes;
+    try_tuning(t);
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   int rc = cbm_batch_set_tuning(b, &best);

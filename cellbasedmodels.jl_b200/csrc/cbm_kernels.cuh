@@ -916,6 +916,94 @@ __device__ __forceinline__ T filter_s2(const T* xi, const T* xj) {
   }
 }
 
+// The end of agentStepDE! for slot s once its pair forces are summed in acc:
+// pushing walls, the lagged force, linear drift and chemotaxis, then the
+// integrator (Euler or Euler-Maruyama), the commit of the written slot and
+// the displacement check of the Verlet algorithms.  xi: the positions the
+// step reads (the stage's, the rule's reflected ones, or the committed ones).
+template <typename T, int D>
+__device__ __forceinline__ void finish_agent(const Params<T>& P, const int s, const T* xi, T* acc) {
+  const int p = P.parity;
+  if (P.walls == CBM_WALLS_PUSH) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      if (xi[d] < P.box_lo[d] + P.wall_range) acc[d] = acc[d] + P.wall_force;
+      else if (xi[d] > P.box_hi[d] - P.wall_range) acc[d] = acc[d] - P.wall_force;
+    }
+  }
+  T dv[3];
+  if (P.force_mode == CBM_FORCE_LAGGED) {
+    T fc[3];
+    to3<T>(P.FA[s], fc);
+    P.FB[s] = from3<T>(acc);
+#pragma unroll
+    for (int d = 0; d < D; ++d) dv[d] = fc[d];
+  } else {
+#pragma unroll
+    for (int d = 0; d < D; ++d) dv[d] = acc[d];
+  }
+  if (P.drift_linear != (T)0) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) dv[d] = dv[d] + (-P.drift_linear) * xi[d];
+  }
+  if (P.medium && P.chemotaxis != (T)0) {
+    T gv[3] = {(T)0, (T)0, (T)0};
+    if (P.medium_sampling == CBM_MEDIUM_NEAREST) {
+      int nn = nearest_node<T, D>(P, xi);
+#pragma unroll
+      for (int d = 0; d < D; ++d) gv[d] = ld(P.grad_cur[d] + nn);
+    } else {
+      int nodes[8];
+      T w[8];
+      bilinear<T, D>(P, xi, nodes, w);
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        T sm = (T)0;
+#pragma unroll
+        for (int q = 0; q < (1 << D); ++q) sm = sm + w[q] * ld(P.grad_cur[d] + nodes[q]);
+        gv[d] = sm;
+      }
+    }
+    T g2 = gv[0] * gv[0];
+    if (D > 1) g2 = g2 + gv[1] * gv[1];
+    if (D > 2) g2 = g2 + gv[2] * gv[2];
+    T den = (T)1 + sqrt(g2);
+#pragma unroll
+    for (int d = 0; d < D; ++d) dv[d] = dv[d] + (P.chemotaxis * gv[d]) / den;
+  }
+  if (P.KOUT) {  // a stage of a multi-stage integrator: f(u) only
+    P.KOUT[s] = from3<T>(dv);
+    return;
+  }
+  const int i = ld(P.IA + s);  // agent index of the slot
+  T xn[3] = {(T)0, (T)0, (T)0};
+  if (P.integrator == CBM_INT_EM) {
+    T xi_n[3] = {(T)0, (T)0, (T)0};
+    if (P.noise) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) xi_n[d] = P.noise[(size_t)i * D + d];
+    } else {
+      cbm_normals(P.seed, P.ctr->step[p], (uint32_t)i, CBM_STREAM_NOISE, P.community, D, xi_n);
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) xn[d] = (xi[d] + dv[d] * P.dt) + (P.sigma * xi_n[d]) * P.sqrt_dt;
+  } else {
+#pragma unroll
+    for (int d = 0; d < D; ++d) xn[d] = xi[d] + dv[d] * P.dt;
+  }
+  P.PB[s] = from3<T>(xn);
+  P.VB[s] = P.growth ? P.VA[s] + ld(P.G + i) * P.dt : P.VA[s];
+  P.IB[s] = i;
+  if (is_verlet(P) && !P.ctr->events) {
+    // verletDisplacement (neighbors.jl:367-391) on the new positions; when
+    // agents are added or removed this step the flag is already set and the
+    // check is skipped.
+    T xo[3];
+    to3<T>(P.POLD[s], xo);
+    if (dist<T, D>(xn, xo) >= P.rebuild_thr) P.ctr->flag[p] = 1;
+  }
+}
+
 // Slot s of N; `list` is this thread's partner list (null: none); `live`
 // holds the lanes of this warp whose slot is below N.
 template <typename T, int D>
@@ -1197,84 +1285,7 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
       pair(xj);
     }
   }
-  if (P.walls == CBM_WALLS_PUSH) {
-#pragma unroll
-    for (int d = 0; d < D; ++d) {
-      if (xi[d] < P.box_lo[d] + P.wall_range) acc[d] = acc[d] + P.wall_force;
-      else if (xi[d] > P.box_hi[d] - P.wall_range) acc[d] = acc[d] - P.wall_force;
-    }
-  }
-  T dv[3];
-  if (P.force_mode == CBM_FORCE_LAGGED) {
-    T fc[3];
-    to3<T>(P.FA[s], fc);
-    P.FB[s] = from3<T>(acc);
-#pragma unroll
-    for (int d = 0; d < D; ++d) dv[d] = fc[d];
-  } else {
-#pragma unroll
-    for (int d = 0; d < D; ++d) dv[d] = acc[d];
-  }
-  if (P.drift_linear != (T)0) {
-#pragma unroll
-    for (int d = 0; d < D; ++d) dv[d] = dv[d] + (-P.drift_linear) * xi[d];
-  }
-  if (P.medium && P.chemotaxis != (T)0) {
-    T gv[3] = {(T)0, (T)0, (T)0};
-    if (P.medium_sampling == CBM_MEDIUM_NEAREST) {
-      int nn = nearest_node<T, D>(P, xi);
-#pragma unroll
-      for (int d = 0; d < D; ++d) gv[d] = ld(P.grad_cur[d] + nn);
-    } else {
-      int nodes[8];
-      T w[8];
-      bilinear<T, D>(P, xi, nodes, w);
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        T sm = (T)0;
-#pragma unroll
-        for (int q = 0; q < (1 << D); ++q) sm = sm + w[q] * ld(P.grad_cur[d] + nodes[q]);
-        gv[d] = sm;
-      }
-    }
-    T g2 = gv[0] * gv[0];
-    if (D > 1) g2 = g2 + gv[1] * gv[1];
-    if (D > 2) g2 = g2 + gv[2] * gv[2];
-    T den = (T)1 + sqrt(g2);
-#pragma unroll
-    for (int d = 0; d < D; ++d) dv[d] = dv[d] + (P.chemotaxis * gv[d]) / den;
-  }
-  if (P.KOUT) {  // a stage of a multi-stage integrator: f(u) only
-    P.KOUT[s] = from3<T>(dv);
-    return;
-  }
-  const int i = ld(P.IA + s);  // agent index of the slot
-  T xn[3] = {(T)0, (T)0, (T)0};
-  if (P.integrator == CBM_INT_EM) {
-    T xi_n[3] = {(T)0, (T)0, (T)0};
-    if (P.noise) {
-#pragma unroll
-      for (int d = 0; d < D; ++d) xi_n[d] = P.noise[(size_t)i * D + d];
-    } else {
-      cbm_normals(P.seed, P.ctr->step[p], (uint32_t)i, CBM_STREAM_NOISE, P.community, D, xi_n);
-    }
-#pragma unroll
-    for (int d = 0; d < D; ++d) xn[d] = (xi[d] + dv[d] * P.dt) + (P.sigma * xi_n[d]) * P.sqrt_dt;
-  } else {
-#pragma unroll
-    for (int d = 0; d < D; ++d) xn[d] = xi[d] + dv[d] * P.dt;
-  }
-  P.PB[s] = from3<T>(xn);
-  P.VB[s] = P.growth ? P.VA[s] + ld(P.G + i) * P.dt : P.VA[s];
-  P.IB[s] = i;
-  if (is_verlet(P) && !P.ctr->events) {
-    // verletDisplacement (neighbors.jl:367-391) on the new positions; when
-    // agents are added or removed this step the flag is already set and the
-    // check is skipped.
-    T xo[3];
-    to3<T>(P.POLD[s], xo);
-    if (dist<T, D>(xn, xo) >= P.rebuild_thr) P.ctr->flag[p] = 1;
-  }
+  finish_agent<T, D>(P, s, xi, acc);
 }
 
 // One block per resident slot of the device, so each thread owns one region

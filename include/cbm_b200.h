@@ -296,7 +296,9 @@ typedef struct cbm_batch_tuning {
   int32_t tile_agents;   /* communities of at most this many agents gather neighbor
                             positions from a shared-memory tile (12 B per agent,
                             at most 220 KiB); 0: every gather goes through L1/L2 */
-  int32_t pad;
+  int32_t lanes_per_agent; /* lanes that share one agent's list and pair terms: 1, 2 or 4
+                            (32, 16 or 8 agents a warp; 0 means 1); the terms are added
+                            in list order whatever the lanes */
 } cbm_batch_tuning;
 
 typedef struct cbm_batch cbm_batch;

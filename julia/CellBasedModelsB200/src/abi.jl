@@ -91,7 +91,7 @@ end
 """Mirror of `cbm_batch_tuning`."""
 struct CbmBatchTuning
     threads::Int32; ctas_per_sm::Int32; skin::Float64; rebuild_threshold::Float64
-    tile_agents::Int32; pad::Int32
+    tile_agents::Int32; lanes_per_agent::Int32
 end
 
 """Mirror of `cbm_medium_config` (the implicit DGADI medium)."""

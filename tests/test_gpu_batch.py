@@ -28,7 +28,14 @@ def run_plain(abi, base, desc, state, tuning, steps):
     dict(threads=256, ctas_per_sm=2, skin=0.3, rebuild_threshold=0.0, tile_agents=0),
     dict(threads=128, ctas_per_sm=4, skin=0.15, rebuild_threshold=0.0, tile_agents=1000),
     dict(threads=1024, ctas_per_sm=1, skin=0.6, rebuild_threshold=0.0, tile_agents=18000),
-    dict(threads=512, ctas_per_sm=2, skin=1.5, rebuild_threshold=0.2, tile_agents=9000)])
+    dict(threads=512, ctas_per_sm=2, skin=1.5, rebuild_threshold=0.2, tile_agents=9000),
+    # several lanes per agent (16 and 8 agents a warp): terms still added in list order
+    dict(threads=256, ctas_per_sm=2, skin=0.3, rebuild_threshold=0.0, tile_agents=0,
+         lanes_per_agent=2),
+    dict(threads=512, ctas_per_sm=1, skin=1.0, rebuild_threshold=0.0, tile_agents=1000,
+         lanes_per_agent=4),
+    dict(threads=1024, ctas_per_sm=1, skin=0.6, rebuild_threshold=0.0, tile_agents=18000,
+         lanes_per_agent=2)])
 def test_batch_matches_plain_path(gpu_lib, abi, tuning):
     base, descs, states = small_sweep(abi)
     b = cbm.Batch(abi.make_config(**base), make_descs(abi, descs))
@@ -67,7 +74,7 @@ def test_batch_autotune_restores_state(gpu_lib, abi):
     b.step(5)
     before = [b.download(c) for c in range(len(descs))]
     t = b.autotune(trial_steps=5)
-    assert t.threads in (128, 256, 512, 1024) and t.skin > 0
+    assert t.threads in (128, 256, 512, 1024) and t.skin > 0 and t.lanes_per_agent in (1, 2, 4)
     after = [b.download(c) for c in range(len(descs))]
     for a, r in zip(after, before):
         assert a["step"] == r["step"]
