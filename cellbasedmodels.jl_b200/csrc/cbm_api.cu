@@ -155,10 +155,16 @@ struct Prof {
     }
     m = &set[used++];
     m->name = name;
-    cudaEventRecord(m->ev[0], c->stream);
+    record(m->ev[0]);
   }
   ~Prof() {
-    if (m) cudaEventRecord(m->ev[1], c->stream);
+    if (m) record(m->ev[1]);
+  }
+  // inside a stream capture an event record becomes a graph node only with
+  // the external flag (a plain record there just orders the capture)
+  void record(cudaEvent_t e) {
+    if (c->prof_set) cudaEventRecordWithFlags(e, c->stream, cudaEventRecordExternal);
+    else cudaEventRecord(e, c->stream);
   }
 };
 #define PROF(name) Prof prof_scope_(c, name)

@@ -1,0 +1,35 @@
+"""Kernel timing inside the step graphs (cbm_set_kernel_timing /
+cbm_kernel_times): every kernel of a replayed step is timed by events on the
+library's stream, and the timing changes no result."""
+import numpy as np
+import pytest
+
+import conftest
+from scenarios import colony_3d
+
+cbm = conftest.cbm
+pytestmark = pytest.mark.gpu
+
+
+def test_kernel_times_of_graph_replays(gpu_lib, abi):
+    kw, st = colony_3d(abi, N=3000, L=60.0, n_max=6000, p_death=2e-3)
+    cfg = abi.make_config(**kw)
+    a, b = cbm.Context(cfg), cbm.Context(cfg)
+    a.upload(st)
+    b.upload(st)
+    a.set_kernel_timing(True)
+    for _ in range(4):
+        a.step(1)
+        times = a.kernel_times()
+        names = [n for n, _ in times]
+        assert len(times) == a.kernels_per_step()
+        assert "k_agent_de" in names and "k_sort_place" in names
+        assert all(ms > 0 for _, ms in times)
+    a.set_kernel_timing(False)
+    a.step(3)
+    b.step(7)
+    sa, sb = a.download(), b.download()
+    for k in ("x", "y", "z", "v", "id"):
+        np.testing.assert_array_equal(sa[k], sb[k], err_msg=k)
+    with pytest.raises(cbm.CbmError):
+        a.kernel_times()  # timing is off again
