@@ -264,6 +264,7 @@ Params<T> params(const cbm_ctx* c, int parity) {
   P.medium = k.medium;
   P.medium_sampling = k.medium_sampling;
   P.dt = (T)k.dt;
+  P.dt_time = k.dt;
   P.sqrt_dt = std::sqrt((T)k.dt);
   P.sigma = (T)k.sigma;
   P.edge = (T)(k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT ? k.skin : k.cell_edge);

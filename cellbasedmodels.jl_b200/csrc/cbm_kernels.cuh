@@ -114,6 +114,7 @@ struct Params {
       medium_sampling;
   T box_lo[3], box_hi[3];
   T dt, sqrt_dt, sigma;
+  double dt_time;           // the configured dt, by which the time t advances
   T edge;               // grid cell edge
   T skin, rebuild_thr;
   T k_rep, r_rep, k_att, r_att;
@@ -1741,7 +1742,7 @@ __global__ void k_commit(Params<T> P) {
   C->N[p ^ 1] = C->N[p] + C->n_add - C->n_remove;
   C->n_add = 0;
   C->n_remove = 0;
-  C->t[p ^ 1] = C->t[p] + (double)P.dt;
+  C->t[p ^ 1] = C->t[p] + P.dt_time;
   C->step[p ^ 1] = C->step[p] + 1;
   C->flag[p ^ 1] = 0;
   C->resort = (P.neighbors == CBM_NEIGH_CELL_LINKED || C->flag[p]) ? 1 : 0;

@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_steps(Params<T> P0, Par
       C->N[p ^ 1] = C->N[p];
       C->n_add = 0;
       C->n_remove = 0;
-      C->t[p ^ 1] = C->t[p] + (double)P.dt;
+      C->t[p ^ 1] = C->t[p] + P.dt_time;
       C->step[p ^ 1] = C->step[p] + 1;
       C->flag[p ^ 1] = 0;
       C->resort = 1;
