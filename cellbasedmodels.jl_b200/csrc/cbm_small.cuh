@@ -8,16 +8,17 @@
 //
 //   DE     agentStepDE! of every slot over the grid of the committed
 //          positions (the rule's wall reflection computed on the fly), the
-//          same sums in the same order as k_agent_de, into the working set B
-//   commit update!'s counters (k_commit), the histogram of the new cells
-//   scan   every block scans the cell counts into shared memory (the cell
+//          same sums in the same order as k_agent_de, into the working set B,
+//          four lanes an agent; then the histogram of the new cells
+//   scan   update!'s counters (k_commit); every block scans the cell counts
+//          into shared memory (the cell
 //          grid of these communities fits one block); block 0 stores the
 //          offsets; agent indices are scattered by (cell, arrival)
 //   place  the stable placement B -> A by (cell, agent index) of k_sort_place,
 //          and the counts are cleared for the next step
 //
-// so the state after the launch is the one the step graphs leave.  Each
-// barrier's wait is bounded: a block that gives up sets the timeout bit and
+// three grid barriers a step, and the state after the launch is the one the
+// step graphs leave.  Each barrier's wait is bounded: a block that gives up sets the timeout bit and
 // an abort flag, and every block leaves at its next barrier.
 #pragma once
 #include "cbm_kernels.cuh"
@@ -35,33 +36,46 @@ struct SmallBarrier {
   int* abort;       // a wait gave up (0 at launch)
 };
 
-// Grid barrier of the cooperative launch.  Returns false when a wait gave up
-// (here or in another block); the caller then leaves.
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void red_add_release_gpu(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid barrier of the cooperative launch.  The block's writes reach thread 0
+// through the block barrier; its arrival (acquire-release) publishes them, and
+// the last block to arrive releases the generation that the others acquire.
+// Returns false when a wait gave up (here or in another block); the caller
+// then leaves.
 __device__ __forceinline__ bool small_barrier(const SmallBarrier& B, Counters* C) {
   __shared__ int s_go;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* gen = B.gen;
-    volatile int* abort = B.abort;
-    const unsigned g = *gen;
-    __threadfence();
-    if (atomicAdd(B.count, 1u) == gridDim.x - 1) {
-      atomicExch(B.count, 0u);
-      __threadfence();
-      atomicAdd(B.gen, 1u);
+    const unsigned g = ld_acquire_gpu(B.gen);
+    if (atom_add_acq_rel_gpu(B.count, 1u) == gridDim.x - 1) {
+      *(volatile unsigned*)B.count = 0u;
+      red_add_release_gpu(B.gen, 1u);
     } else {
+      volatile int* abort = B.abort;
       unsigned polls = 0;
-      while (*gen == g && *abort == 0) {
+      while (ld_acquire_gpu(B.gen) == g && *abort == 0) {
         if (++polls == kBarrierPolls) {
           atomicOr(&C->err, kErrTimeout);
           atomicExch(B.abort, 1);
           break;
         }
-        __nanosleep(64);
+        __nanosleep(32);
       }
     }
-    __threadfence();
-    s_go = *abort == 0;
+    s_go = *(volatile int*)B.abort == 0;
   }
   __syncthreads();
   return s_go != 0;
@@ -107,13 +121,21 @@ __device__ __forceinline__ void block_scan_counts(const int* counts, int n, int*
   __syncthreads();
 }
 
-// agentStepDE! of slot s for CellLinked without a queue: the candidates of
-// the 3^D cells in the reference's order, each pair term added in that order
-// (skipping cells with no partner, as k_agent_de's pruning does, changes no
-// sum).  With reflecting walls the rule's reflected positions are computed
-// from the committed ones, here for xi and every candidate.
+// agentStepDE! of slot s for CellLinked, by the kSmallLanes lanes of a group
+// (lane gl of the group takes candidates gl, gl + kSmallLanes, ... of each
+// run): the candidates of the 3^D cells in the reference's order, the pair
+// terms of each chunk added in candidate order through the group's shuffles,
+// so the sums are those of k_agent_de (skipping cells with no partner, as its
+// pruning does, changes no sum).  With reflecting walls the rule's reflected
+// positions are computed from the committed ones, here for xi and every
+// candidate.  The group's first lane integrates.
+constexpr int kSmallLanes = 4;
+
 template <typename T, int D>
 __device__ __forceinline__ void small_de(const Params<T>& P, int s) {
+  constexpr int L = kSmallLanes;
+  const int lane = threadIdx.x & 31, gl = lane & (L - 1);
+  const unsigned gmask = ((1u << L) - 1u) << (lane & ~(L - 1));
   const bool reflect = P.walls == CBM_WALLS_REFLECT;
   auto pos = [&](int q, T* x) {
     to3<T>(P.PA[q], x);
@@ -129,17 +151,65 @@ __device__ __forceinline__ void small_de(const Params<T>& P, int s) {
   pos(s, xi);
   T acc[3] = {(T)0, (T)0, (T)0};
   const PairCoef<T> coef = pair_coef<T>(P);
-  for_cell_slots<T, D>(P, xi, [&](int q) {
-    if (q == s) return;
-    T xj[3], e[3];
-    pos(q, xj);
-    const T s2 = pair_diff<T, D>(xi, xj, e);
-    pair_term<T, D>(coef, e, s2, acc);
-  });
-  finish_agent<T, D>(P, s, xi, acc);
+  int q3[3] = {0, 0, 0};
+  cell_coords<D>(P.n_cells_d, cell_of_pos<T, D>(P, xi), q3);
+  const int nx = P.n_cells_d[0];
+  const int x0 = q3[0] > 0 ? q3[0] - 1 : 0, x1 = q3[0] < nx - 1 ? q3[0] + 1 : nx - 1;
+  constexpr int ny_rows = D > 1 ? 3 : 1, nz_rows = D > 2 ? 3 : 1;
+  for (int dz = 0; dz < nz_rows; ++dz) {
+    const int pz = D > 2 ? q3[2] + dz - 1 : 0;
+    if (D > 2 && (pz < 0 || pz >= P.n_cells_d[2])) continue;
+    for (int dy = 0; dy < ny_rows; ++dy) {
+      const int py = D > 1 ? q3[1] + dy - 1 : 0;
+      if (D > 1 && (py < 0 || py >= P.n_cells_d[1])) continue;
+      const int row = nx * (py + P.n_cells_d[1] * pz);
+      const int s0 = ld(P.cell_start + row + x0), s1 = ld(P.cell_start + row + x1 + 1);
+      for (int base = s0; base < s1; base += L) {
+        const int q = base + gl;
+        bool has = false;
+        T t[3] = {(T)0, (T)0, (T)0};
+        if (q < s1 && q != s) {
+          T xj[3], e[3];
+          pos(q, xj);
+          const T s2 = pair_diff<T, D>(xi, xj, e);
+          if (s2 < coef.cut2) {
+            const T dd = sqrt(s2);
+            T F = (T)0;
+            if (dd < coef.rrep) {
+              F = coef.krep * (coef.rrep - dd);
+              has = true;
+            } else if (dd < coef.ratt) {
+              F = coef.from_rep ? -(coef.katt * (dd - coef.rrep)) : -(coef.katt * (coef.ratt - dd));
+              has = true;
+            }
+            if (has) {
+              const T sc = F / dd;
+#pragma unroll
+              for (int d = 0; d < D; ++d) t[d] = sc * e[d];
+            }
+          }
+        }
+        // the chunk's terms, added in candidate order by every lane of the group
+#pragma unroll
+        for (int u = 0; u < L; ++u) {
+          const bool hu = __shfl_sync(gmask, has ? 1 : 0, u, L) != 0;
+          T tu[3];
+#pragma unroll
+          for (int d = 0; d < D; ++d) tu[d] = __shfl_sync(gmask, t[d], u, L);
+          if (hu) {
+#pragma unroll
+            for (int d = 0; d < D; ++d) acc[d] = acc[d] + tu[d];
+          }
+        }
+      }
+    }
+  }
+  if (gl == 0) finish_agent<T, D>(P, s, xi, acc);
 }
 
-// nsteps steps; P0 has the parity of the first step, P1 the other one.
+// nsteps steps; P0 has the parity of the first step, P1 the other one.  The
+// counts of the histogram are complete after the first barrier, the
+// counters' commit by thread 0 is read only after the next ones.
 template <typename T, int D>
 __global__ void __launch_bounds__(kSmallThreads) k_small_steps(Params<T> P0, Params<T> P1,
                                                                SmallBarrier bar, int nsteps,
@@ -153,7 +223,18 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_steps(Params<T> P0, Par
     Counters* C = P.ctr;
     const int p = P.parity;
     const int N = (int)C->N[p];
-    for (int s = tid; s < N; s += nth) small_de<T, D>(P, s);
+    // DE, kSmallLanes lanes an agent; the histogram of the new cells follows
+    // in the same phase (the agent's own written position is all it reads)
+    for (int s = tid / kSmallLanes; s < N; s += nth / kSmallLanes) {
+      small_de<T, D>(P, s);
+      if ((threadIdx.x & (kSmallLanes - 1)) == 0) {  // k_sort_hist
+        T x[3];
+        to3<T>(P.PB[s], x);
+        const int c = cell_of_pos<T, D>(P, x);
+        P.s_cell[s] = c;
+        P.s_rank[s] = atomicAdd(P.cell_count + c, 1);
+      }
+    }
     if (!small_barrier(bar, C)) return;
     if (tid == 0) {  // update!'s counters, as k_commit (no births or deaths here)
       C->slots = C->N[p];
@@ -168,14 +249,6 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_steps(Params<T> P0, Par
       if (C->list_written) C->list_valid = 1;
       C->list_written = 0;
     }
-    for (int s = tid; s < N; s += nth) {  // histogram of the new cells (k_sort_hist)
-      T x[3];
-      to3<T>(P.PB[s], x);
-      const int c = cell_of_pos<T, D>(P, x);
-      P.s_cell[s] = c;
-      P.s_rank[s] = atomicAdd(P.cell_count + c, 1);
-    }
-    if (!small_barrier(bar, C)) return;
     block_scan_counts(P.cell_count, n_cells, s_start, warp_sums);
     if (blockIdx.x == 0)
       for (int c = threadIdx.x; c <= n_cells; c += kSmallThreads) P.cell_start[c] = s_start[c];
