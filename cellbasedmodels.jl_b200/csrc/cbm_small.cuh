@@ -3,22 +3,22 @@
 // A community of a few thousand agents (the 2D aggregation of 4096 agents)
 // costs far less than the launches of its step graph: the graph's seven
 // kernels each wait for the previous one to drain.  Here one cooperative
-// launch runs all the steps of a cbm_step call.  Its blocks meet at grid
-// barriers between the phases of a step:
+// launch runs all the steps of a cbm_step call.  Its blocks meet at three
+// grid barriers a step, between the phases:
 //
 //   DE     agentStepDE! of every slot over the grid of the committed
-//          positions (the rule's wall reflection computed on the fly), the
-//          same sums in the same order as k_agent_de, into the working set B,
-//          four lanes an agent; then the histogram of the new cells
+//          positions (the rule's wall reflection computed on the fly), four
+//          lanes an agent, the same sums in the same order as k_agent_de,
+//          into the working set B; then the histogram of the new cells
 //   scan   update!'s counters (k_commit); every block scans the cell counts
-//          into shared memory (the cell
-//          grid of these communities fits one block); block 0 stores the
-//          offsets; agent indices are scattered by (cell, arrival)
-//   place  the stable placement B -> A by (cell, agent index) of k_sort_place,
-//          and the counts are cleared for the next step
+//          into shared memory (the cell grid of these communities fits one
+//          block), block 0 stores the offsets, and agent indices are
+//          scattered by (cell, arrival)
+//   place  the stable placement B -> A by (cell, agent index) of
+//          k_sort_place, and the counts are cleared for the next step
 //
-// three grid barriers a step, and the state after the launch is the one the
-// step graphs leave.  Each barrier's wait is bounded: a block that gives up sets the timeout bit and
+// The state after the launch is the one the step graphs leave.  Each
+// barrier's wait is bounded: a block that gives up sets the timeout bit and
 // an abort flag, and every block leaves at its next barrier.
 #pragma once
 #include "cbm_kernels.cuh"
