@@ -74,9 +74,6 @@ struct cbm_ctx {
   int n_sm = 148;             // multiprocessors of the device (grid of the compaction)
   int de_blocks = 1;          // persistent grid of the force kernel
   void* pair_list = nullptr;  // its partner lists (cell walks only)
-  int* sub_slots = nullptr;   // sub-cell order of the 3D force walk (k_sub_sort)
-  unsigned char* sub_off = nullptr;
-  bool sub_on = false;
   void* stage[3] = {nullptr, nullptr, nullptr};  // Heun / RK4: h, running sum, derivative
   int n_cells = 1;
   int n_cells_d[3] = {1, 1, 1};
@@ -238,9 +235,6 @@ Params<T> params(const cbm_ctx* c, int parity) {
   P.nbr_list = c->nbr_list;
   P.pair_list = (int4*)c->pair_list;
   P.pair_cap4 = kPairCap4;
-  P.sub_slots = c->sub_slots;
-  P.sub_off = c->sub_off;
-  P.sub_on = c->sub_on ? 1 : 0;
   P.c_cur = (T*)c->c[p];
   P.c_nxt = (T*)c->c[q];
   P.ctr = c->ctr;
@@ -456,14 +450,8 @@ void enqueue_update(cbm_ctx* c, const Params<T>& P) {
     PROF("k_sort_scatter");
     k_sort_scatter<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
   }
-  {
-    PROF("k_sort_place");
-    k_sort_place<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
-  }
-  if (c->sub_on) {
-    PROF("k_sub_sort");
-    k_sub_sort<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
-  }
+  PROF("k_sort_place");
+  k_sort_place<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
 }
 
 // computeNeighbors! after update!: the grid was rebuilt by the re-sort; a
@@ -489,7 +477,6 @@ int kernels_per_step(const cbm_ctx* c) {
   n += 1;                               // agent DE
   if (k.medium) n += 1;
   n += 5;                               // commit, sort hist, scan, scatter, place
-  if (c->sub_on) n += 1;                // sub-cell order of the 3D walk
   if (k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT) n += 1;
   return n;
 }
@@ -608,7 +595,6 @@ struct FirstSort {  // the re-sort half of update!, for loadToPlatform!
     k_scan_cells<<<c->n_scan_tiles, kTile, 0, c->stream>>>(A);
     k_sort_scatter<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
     k_sort_place<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
-    if (c->sub_on) k_sub_sort<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
     if (c->cfg.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT)
       k_verlet_list<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P, 0);
   }
@@ -840,14 +826,6 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     c->de_blocks = (int)(resident < c->n_blocks ? resident : c->n_blocks);
     if (cells && k.dims == 3)
       c->pair_list = dalloc(c, (size_t)c->de_blocks * kTile * kPairCap4 * sizeof(int4), &ok);
-    // the sub-cell order of the 3D cell walk: a slot list and a byte of
-    // offsets per sub-cell and cell (skipped for grids too large for it)
-    const size_t sub_bytes = (size_t)c->n_cells * (kSubCells + 1);
-    if (cells && k.dims == 3 && sub_bytes <= ((size_t)1 << 31)) {
-      c->sub_slots = (int*)dalloc(c, n * 4, &ok);
-      c->sub_off = (unsigned char*)dalloc(c, sub_bytes, &ok);
-      c->sub_on = true;
-    }
   }
   if (list) {
     c->nbr_n = (int*)dalloc(c, n * 4, &ok);
@@ -1116,7 +1094,7 @@ struct SmallSteps {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_small_steps<T, D>, kSmallThreads,
                                                       smem) != cudaSuccess || bps < 1)
       bps = 1;
-    long long want = (c->n_loaded * kSmallLanes + kSmallThreads - 1) / kSmallThreads;
+    long long want = (c->n_loaded + kSmallThreads - 1) / kSmallThreads;
     long long blocks = std::min<long long>(want, (long long)c->n_sm);
     blocks = std::max<long long>(1, std::min<long long>(blocks, (long long)bps * c->n_sm));
     *err = cudaMemsetAsync(c->small_bar, 0, 4 * sizeof(unsigned), c->stream);
@@ -1124,11 +1102,6 @@ struct SmallSteps {
     void* args[] = {&P0, &P1, &bar, &nsteps, &n_cells};
     *err = cudaLaunchCooperativeKernel((const void*)k_small_steps<T, D>, dim3((unsigned)blocks),
                                        dim3(kSmallThreads), args, smem, c->stream);
-    // the launch re-sorted the slots: the sub-cell order follows them
-    if (*err == cudaSuccess && c->sub_on) {
-      k_sub_sort<T><<<c->n_blocks, kTile, 0, c->stream>>>(params<T>(c, c->parity ^ (nsteps & 1)));
-      *err = cudaGetLastError();
-    }
   }
 };
 

@@ -92,11 +92,6 @@ struct Params {
   // blocks of four slots per thread (block j of thread t at j * kTile + t)
   int4* pair_list;
   int pair_cap4;
-  // sub-cell order of the 3D force walk (k_sub_sort): the slots of each cell
-  // by (sub-cell, slot), and per cell the first entry of each sub-cell
-  int* sub_slots;
-  unsigned char* sub_off;
-  int sub_on;
   // medium: committed / written
   T* c_cur;
   T* c_nxt;
@@ -244,13 +239,12 @@ __device__ __forceinline__ void for_cell_slots(const Params<T>& P, const T* x, F
 }
 
 // Per-thread force queue of k_agent_de, in shared memory (kQueue * 1 KB per
-// block; with the sub-cell masks, 48 KB: the static limit).  40 entries hold
-// every partner of nearly every agent of a colony at the packing density
-// (about 17 on average), whose terms then follow the walk in one converged
-// drain; in denser colonies a full queue moves to the thread's partner list
-// in global memory.
+// block, 48 KB: the static limit).  48 entries hold every partner of nearly
+// every agent of a colony at the packing density (about 17 on average), whose
+// terms then follow the walk in one converged drain; in denser colonies a
+// full queue moves to the thread's partner list in global memory.
 #ifndef CBM_FORCE_QUEUE
-#define CBM_FORCE_QUEUE 40
+#define CBM_FORCE_QUEUE 48
 #endif
 constexpr int kQueue = CBM_FORCE_QUEUE;
 
@@ -812,90 +806,6 @@ __global__ void __launch_bounds__(kTile) k_agent_fate(Params<T> P) {
 }
 
 // ---------------------------------------------------------------------------
-// Sub-cells of the 3D force walk.  A cell of the grid is split into 4^3
-// sub-cells numbered in Morton order (bit 0 x, bit 1 y, bit 2 z of the low
-// halves, bits 3-5 of the high halves), so that consecutive sub-cells lie
-// close together.  k_sub_sort lists the slots of every cell by (sub-cell,
-// slot); the force kernel's warps take their agents in that order, so the 32
-// agents of a warp lie close together, and the walk visits only the
-// sub-cells within reach of the warp.  Cells of more than kSubMax agents
-// (and the ghost layer, whose cells are unbounded) keep the slot order.
-// ---------------------------------------------------------------------------
-constexpr int kSubSplit = 4;
-constexpr int kSubCells = kSubSplit * kSubSplit * kSubSplit;
-constexpr int kSubMax = 255;  // agents of a cell whose sub-cell offsets fit a byte
-constexpr int kSubMin = 32;   // cells of fewer agents are scanned whole
-
-__device__ __forceinline__ int sub_morton(int x, int y, int z) {
-  return (x & 1) | ((y & 1) << 1) | ((z & 1) << 2) | ((x & 2) << 2) | ((y & 2) << 3) |
-         ((z & 2) << 4);
-}
-__device__ __forceinline__ void sub_unmorton(int k, int* u) {
-  u[0] = (k & 1) | ((k >> 2) & 2);
-  u[1] = ((k >> 1) & 1) | ((k >> 3) & 2);
-  u[2] = ((k >> 2) & 1) | ((k >> 4) & 2);
-}
-
-// Sub-cell of position x in interior cell q (cell coordinates): the cell
-// covers [lo + (q-1) edge, lo + q edge) on every axis (cellPos,
-// neighbors.jl:636-638).
-template <typename T>
-__device__ __forceinline__ int sub_cell_of(const Params<T>& P, const T* x, const int* q) {
-  int u[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const T lo = P.box_lo[d] + (T)(q[d] - 1) * P.edge;
-    const int v = (int)floor((x[d] - lo) / P.edge * (T)kSubSplit);
-    u[d] = v < 0 ? 0 : (v > kSubSplit - 1 ? kSubSplit - 1 : v);
-  }
-  return sub_morton(u[0], u[1], u[2]);
-}
-
-// One thread per cell (the thread of its first slot) lists the cell's slots
-// by (sub-cell, slot) in sub_slots and stores the sub-cells' first entries in
-// sub_off (relative to the cell's start; entry kSubCells is the count).  The
-// sub-cell of each slot is kept in s_rank, free once the re-sort has placed
-// the agents.
-template <typename T>
-__global__ void __launch_bounds__(kTile) k_sub_sort(Params<T> P) {
-  if (!P.ctr->resort) return;
-  const int total = P.cell_start[P.n_cells];
-  const int s = blockIdx.x * kTile + threadIdx.x;
-  if (s >= total) return;
-  const int c = P.cell_of_slot[s];
-  if (s > 0 && P.cell_of_slot[s - 1] == c) return;
-  const int n = P.cell_start[c + 1] - s;
-  int q[3];
-  q[0] = c % P.n_cells_d[0];
-  q[1] = (c / P.n_cells_d[0]) % P.n_cells_d[1];
-  q[2] = c / (P.n_cells_d[0] * P.n_cells_d[1]);
-  if (n > kSubMax) {
-    for (int j = 0; j < n; ++j) P.sub_slots[s + j] = s + j;
-    return;
-  }
-  int cnt[kSubCells];
-#pragma unroll
-  for (int k = 0; k < kSubCells; ++k) cnt[k] = 0;
-  for (int j = 0; j < n; ++j) {
-    T x[3];
-    to3<T>(P.PA[s + j], x);
-    const int k = sub_cell_of<T>(P, x, q);
-    P.s_rank[s + j] = k;
-    ++cnt[k];
-  }
-  unsigned char* off = P.sub_off + (size_t)c * (kSubCells + 1);
-  int o = 0;
-  for (int k = 0; k < kSubCells; ++k) {
-    off[k] = (unsigned char)o;
-    const int t = cnt[k];
-    cnt[k] = o;
-    o += t;
-  }
-  off[kSubCells] = (unsigned char)o;
-  for (int j = 0; j < n; ++j) P.sub_slots[s + cnt[P.s_rank[s + j]]++] = s + j;
-}
-
-// ---------------------------------------------------------------------------
 // agentStepDE!: fused neighbor force + Euler / EM update, one thread per slot
 // (src/integrators.jl:465-505,683-734, functionDE.jl:13-117)
 // ---------------------------------------------------------------------------
@@ -1263,146 +1173,10 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
           else drain();
         }
       };
-      // The walk over the sub-cells (3D, dense cells).  The warp visits, in
-      // ascending cell order, the cells around any of its agents; a lane takes
-      // the candidates of the 27 cells around its own.  In a dense cell the
-      // warp tests only the sub-cells within reach of the bounding box of its
-      // agents, in sub-cell order; a lane marks the candidates that may be
-      // inside the cutoff in a bit mask over the cell's slots and then queues
-      // them in slot order.  Since the cells around an agent, x fastest, hold
-      // ascending slots, the queue receives the candidates in the order of the
-      // reference's loop (neighbors.jl:715-747), as the run walk does.
-      auto walk_subcells = [&](int cell, auto&& scan_fn) {
-        __shared__ unsigned smask[(kSubMax + 1) / 32 * kTile];
-        const int lane = threadIdx.x & 31;
-        const int nxc = P.n_cells_d[0], nyc = P.n_cells_d[1], nzc = P.n_cells_d[2];
-        const int q3[3] = {cell % nxc, (cell / nxc) % nyc, cell / (nxc * nyc)};
-        T blo[3], bhi[3];
-        int clo[3], chi[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          blo[d] = bhi[d] = xi[d];
-          clo[d] = __reduce_min_sync(live, q3[d]);
-          chi[d] = __reduce_max_sync(live, q3[d]);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          const bool src = (live >> (lane ^ o)) & 1u;
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            const T a = __shfl_xor_sync(live, blo[d], o), b = __shfl_xor_sync(live, bhi[d], o);
-            if (src) {
-              blo[d] = a < blo[d] ? a : blo[d];
-              bhi[d] = b > bhi[d] ? b : bhi[d];
-            }
-          }
-        }
-        const T reach = P.cut_reach, r2 = reach * reach;
-        const T sub = P.edge / (T)kSubSplit;
-        // rounding of the cell and sub-cell assignments (as walk_runs)
-        T margin = (T)0;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const T m = (T)16 * Eps<T>::v * (fabs(P.box_lo[d]) + fabs(P.box_hi[d]) + P.edge);
-          margin = m > margin ? m : margin;
-        }
-        margin = margin + (T)1e-4 * reach;
-        const int zb = clo[2] > 0 ? clo[2] - 1 : 0, ze = chi[2] < nzc - 1 ? chi[2] + 1 : nzc - 1;
-        const int yb = clo[1] > 0 ? clo[1] - 1 : 0, ye = chi[1] < nyc - 1 ? chi[1] + 1 : nyc - 1;
-        const int xb = clo[0] > 0 ? clo[0] - 1 : 0, xe = chi[0] < nxc - 1 ? chi[0] + 1 : nxc - 1;
-        for (int cz = zb; cz <= ze; ++cz)
-          for (int cy = yb; cy <= ye; ++cy)
-            for (int cx = xb; cx <= xe; ++cx) {
-              const int c = cx + nxc * (cy + nyc * cz);
-              const int cs = ld(P.cell_start + c);
-              const int nc = ld(P.cell_start + c + 1) - cs;
-              if (nc == 0) continue;
-              const bool adj = abs(cx - q3[0]) <= 1 && abs(cy - q3[1]) <= 1 && abs(cz - q3[2]) <= 1;
-              if (!__any_sync(live, adj)) continue;
-              const bool ghost = cx == 0 || cx == nxc - 1 || cy == 0 || cy == nyc - 1 || cz == 0 ||
-                                 cz == nzc - 1;
-              if (ghost || nc > kSubMax || nc < kSubMin) {
-                scan_fn(cs, cs + nc, adj);
-                continue;
-              }
-              const int cq[3] = {cx, cy, cz};
-              // sub-cells within reach of the warp's box: lane l tests l and l + 32
-              unsigned long long rmask = 0ull;
-#pragma unroll
-              for (int h = 0; h < 2; ++h) {
-                int u[3];
-                sub_unmorton(lane + 32 * h, u);
-                T g2 = (T)0;
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                  const T lo = P.box_lo[d] + (T)(cq[d] - 1) * P.edge + (T)u[d] * sub - margin;
-                  const T hi = lo + sub + (T)2 * margin;
-                  T g = lo - bhi[d];
-                  const T g1 = blo[d] - hi;
-                  g = g > g1 ? g : g1;
-                  g = g > (T)0 ? g : (T)0;
-                  g2 = g2 + g * g;
-                }
-                const unsigned b = __ballot_sync(live, g2 < r2) | ~live;  // lanes out of live: keep
-                rmask |= (unsigned long long)b << (32 * h);
-              }
-              const unsigned char* off = P.sub_off + (size_t)c * (kSubCells + 1);
-              const int nw = (nc + 31) >> 5;
-              for (int w = 0; w < nw; ++w) smask[w * kTile + threadIdx.x] = 0u;
-              while (rmask) {
-                const int k0 = __ffsll((long long)rmask) - 1;
-                const unsigned long long m = ~(rmask >> k0);
-                const int k1 = m ? k0 + __ffsll((long long)m) - 1 : kSubCells;
-                rmask = k1 >= kSubCells ? 0ull : (rmask & (~0ull << k1));
-                const int e1 = cs + off[k1];
-                int e = cs + off[k0];
-                for (; e + 4 <= e1; e += 4) {
-                  int qq[4];
-                  T s2v[4];
-#pragma unroll
-                  for (int v = 0; v < 4; ++v) qq[v] = ld(P.sub_slots + e + v);
-#pragma unroll
-                  for (int v = 0; v < 4; ++v) {
-                    T xj[3];
-                    to3<T>(U[qq[v]], xj);
-                    s2v[v] = filter_s2<T, D>(xi, xj);
-                  }
-#pragma unroll
-                  for (int v = 0; v < 4; ++v)
-                    if (adj && s2v[v] < cut2f) {
-                      const int b = qq[v] - cs;
-                      smask[(b >> 5) * kTile + threadIdx.x] |= 1u << (b & 31);
-                    }
-                }
-                for (; e < e1; ++e) {
-                  const int qv = ld(P.sub_slots + e);
-                  T xj[3];
-                  to3<T>(U[qv], xj);
-                  if (adj && filter_s2<T, D>(xi, xj) < cut2f) {
-                    const int b = qv - cs;
-                    smask[(b >> 5) * kTile + threadIdx.x] |= 1u << (b & 31);
-                  }
-                }
-              }
-              // this lane's marked candidates, in slot order
-              for (int w = 0; w < nw; ++w) {
-                unsigned mw = smask[w * kTile + threadIdx.x];
-                while (mw) {
-                  const int b = __ffs((int)mw) - 1;
-                  mw &= mw - 1u;
-                  if (nq == kQueue) flush(false);
-                  queue[nq * kTile + threadIdx.x] = cs + 32 * w + b;
-                  ++nq;
-                }
-              }
-            }
-      };
       // the slot's cell is the grid's assignment of the committed position,
       // which the walk starts from unless the rule reflected it off a wall
       const int own_cell = (reflect || P.XS) ? -1 : ld(P.cell_of_slot + s);
-      // the candidates of slots [s0, s1) in slot order; lanes that `take`
-      // them queue those that may be inside the cutoff
-      auto scan = [&](int s0, int s1, bool take) {
+      walk_runs<T, D>(P, xi, P.cut_reach, [&](int s0, int s1) {
         int q = s0;
         for (; q + 4 <= s1; q += 4) {
           room(4);
@@ -1419,28 +1193,16 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             queue[nq * kTile + threadIdx.x] = q + u;
-            nq += (take && s2v[u] < cut2f) ? 1 : 0;
+            nq += s2v[u] < cut2f ? 1 : 0;
           }
         }
         for (; q < s1; ++q) {
           room(1);
           T xj[3];
           to3<T>(U[q], xj);
-          if (take && filter_s2<T, D>(xi, xj) < cut2f) push(q);
+          if (filter_s2<T, D>(xi, xj) < cut2f) push(q);
         }
-      };
-      bool walked = false;
-      if constexpr (D == 3) {
-        // dense cells only: in sparse ones a warp's agents span many cells
-        if (P.sub_on && own_cell >= 0 && !P.no_prune &&
-            __all_sync(live, ld(P.cell_start + own_cell + 1) - ld(P.cell_start + own_cell) >=
-                                 kSubMin)) {
-          walk_subcells(own_cell, scan);
-          walked = true;
-        }
-      }
-      if (!walked) walk_runs<T, D>(P, xi, P.cut_reach, [&](int s0, int s1) { scan(s0, s1, true); },
-                                   own_cell);
+      }, own_cell);
       // a warp with a stored list evaluates from the list, every entry of the
       // queue appended first; otherwise the queue is drained below
       if constexpr (kPartnerLists<D>) {
@@ -1548,10 +1310,8 @@ __global__ void __launch_bounds__(kTile, sizeof(T) == 4 ? 4 : 3) k_agent_de(Para
       P.pair_list ? P.pair_list + (size_t)blockIdx.x * P.pair_cap4 * kTile + threadIdx.x : nullptr;
   int run = (int)blockIdx.x * (kTile / 32) + (int)(threadIdx.x >> 5);
   while (run < n_runs) {
-    // with the sub-cell order, run r is entries 32r.. of it: agents close together
-    const int idx = (run << 5) + lane;
-    const int slot = (P.sub_on && idx < N) ? ld(P.sub_slots + idx) : idx;
-    agent_de<T, D>(P, N, slot, list, __ballot_sync(kFull, idx < N));
+    const int slot = (run << 5) + lane;
+    agent_de<T, D>(P, N, slot, list, __ballot_sync(kFull, slot < N));
     __syncwarp();
     int t = 0;
     if (lane == 0) t = (int)atomicAdd(&C->de_ticket, 1u);
