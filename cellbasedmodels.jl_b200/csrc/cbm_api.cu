@@ -87,8 +87,7 @@ struct cbm_ctx {
   int parity = 0;
   bool rule_done = false, de_done = false, mrule_done = false, mde_done = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  // small fate-free communities: all steps of a call in one cooperative launch
-  unsigned* small_bar = nullptr;  // grid barrier words (count, generation, abort)
+  // small fate-free communities: all steps of a call in one cluster launch
   long long n_loaded = 0;         // N of the last upload (fixed without births and deaths)
 
   // per-kernel event timing: of eager steps (cbm_profile_step, `marks`) and,
@@ -838,7 +837,6 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     }
   }
   c->ctr = (Counters*)dalloc(c, sizeof(Counters), &ok);
-  c->small_bar = (unsigned*)dalloc(c, 4 * sizeof(unsigned), &ok);
   if (!ok) {
     int rc = fail(nullptr, CBM_ERR_NOMEM, "device allocation failed for n_max=%lld", (long long)k.n_max);
     free_all(c);
@@ -1073,8 +1071,8 @@ int cbm_sync(cbm_ctx* c) {
 
 }  // extern "C"
 
-// A fate-free CellLinked community small enough for one cooperative launch
-// of all its steps (cbm_small.cuh)
+// A fate-free CellLinked community small enough for one cluster launch of all
+// its steps (cbm_small.cuh)
 bool small_eligible(const cbm_ctx* c) {
   const cbm_config& k = c->cfg;
   return k.neighbors == CBM_NEIGH_CELL_LINKED && k.fate == CBM_FATE_NONE && !k.growth &&
@@ -1087,21 +1085,33 @@ template <typename T, int D>
 struct SmallSteps {
   static void run(cbm_ctx* c, int nsteps, cudaError_t* err) {
     Params<T> P0 = params<T>(c, c->parity), P1 = params<T>(c, c->parity ^ 1);
-    SmallBarrier bar{c->small_bar, c->small_bar + 1, (int*)(c->small_bar + 2)};
     int n_cells = c->n_cells;
     const size_t smem = (size_t)(n_cells + 1) * sizeof(int);
-    int bps = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_small_steps<T, D>, kSmallThreads,
-                                                      smem) != cudaSuccess || bps < 1)
-      bps = 1;
-    long long want = (c->n_loaded + kSmallThreads - 1) / kSmallThreads;
-    long long blocks = std::min<long long>(want, (long long)c->n_sm);
-    blocks = std::max<long long>(1, std::min<long long>(blocks, (long long)bps * c->n_sm));
-    *err = cudaMemsetAsync(c->small_bar, 0, 4 * sizeof(unsigned), c->stream);
+    auto kern = k_small_steps<T, D>;
+    // one cluster: as many blocks as four lanes an agent need, up to 16
+    long long want = (c->n_loaded * kSmallLanes + kSmallThreads - 1) / kSmallThreads;
+    int blocks = (int)std::max<long long>(1, std::min<long long>(want, kSmallMaxBlocks));
+    *err = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (*err != cudaSuccess) return;
-    void* args[] = {&P0, &P1, &bar, &nsteps, &n_cells};
-    *err = cudaLaunchCooperativeKernel((const void*)k_small_steps<T, D>, dim3((unsigned)blocks),
-                                       dim3(kSmallThreads), args, smem, c->stream);
+    cudaLaunchConfig_t lc = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    lc.blockDim = dim3(kSmallThreads);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = c->stream;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    for (;; blocks /= 2) {  // the largest cluster the device can schedule
+      attr[0].val.clusterDim.x = (unsigned)blocks;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      lc.gridDim = dim3((unsigned)blocks);
+      int clusters = 0;
+      if ((cudaOccupancyMaxActiveClusters(&clusters, kern, &lc) == cudaSuccess && clusters > 0) ||
+          blocks == 1)
+        break;
+    }
+    *err = cudaLaunchKernelEx(&lc, kern, P0, P1, nsteps, n_cells);
   }
 };
 

@@ -2,9 +2,11 @@
 //
 // A community of a few thousand agents (the 2D aggregation of 4096 agents)
 // costs far less than the launches of its step graph: the graph's seven
-// kernels each wait for the previous one to drain.  Here one cooperative
-// launch runs all the steps of a cbm_step call.  Its blocks meet at three
-// grid barriers a step, between the phases:
+// kernels each wait for the previous one to drain.  Here one launch of a
+// single thread-block cluster (up to 16 blocks of 1024 threads, scheduled
+// together on one GPC) runs all the steps of a cbm_step call.  Its blocks
+// meet at three hardware cluster barriers a step (barrier.cluster with
+// release / acquire), between the phases:
 //
 //   DE     agentStepDE! of every slot over the grid of the committed
 //          positions (the rule's wall reflection computed on the fly), four
@@ -17,68 +19,25 @@
 //   place  the stable placement B -> A by (cell, agent index) of
 //          k_sort_place, and the counts are cleared for the next step
 //
-// The state after the launch is the one the step graphs leave.  Each
-// barrier's wait is bounded: a block that gives up sets the timeout bit and
-// an abort flag, and every block leaves at its next barrier.
+// The state after the launch is the one the step graphs leave.  Every block
+// takes every barrier (the loops are uniform), so no wait depends on a
+// condition that could fail to arrive.
 #pragma once
 #include "cbm_kernels.cuh"
 
 namespace cbm {
 
-constexpr int kSmallThreads = 256;
+constexpr int kSmallThreads = 1024;
+constexpr int kSmallMaxBlocks = 16;     // blocks of the cluster (16 needs the non-portable size)
 constexpr int kSmallMaxAgents = 32768;  // communities stepped by one launch (fate-free CellLinked)
 constexpr int kSmallMaxCells = 8192;    // cell grids a block scans in shared memory
-constexpr unsigned kBarrierPolls = 1u << 23;  // polls (about 0.1 us each) before a wait gives up
 
-struct SmallBarrier {
-  unsigned* count;  // blocks arrived at the current barrier (0 at launch)
-  unsigned* gen;    // barriers passed
-  int* abort;       // a wait gave up (0 at launch)
-};
-
-__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v) {
-  unsigned old;
-  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-  return old;
-}
-__device__ __forceinline__ void red_add_release_gpu(unsigned* p, unsigned v) {
-  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Grid barrier of the cooperative launch.  The block's writes reach thread 0
-// through the block barrier; its arrival (acquire-release) publishes them, and
-// the last block to arrive releases the generation that the others acquire.
-// Returns false when a wait gave up (here or in another block); the caller
-// then leaves.
-__device__ __forceinline__ bool small_barrier(const SmallBarrier& B, Counters* C) {
-  __shared__ int s_go;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned g = ld_acquire_gpu(B.gen);
-    if (atom_add_acq_rel_gpu(B.count, 1u) == gridDim.x - 1) {
-      *(volatile unsigned*)B.count = 0u;
-      red_add_release_gpu(B.gen, 1u);
-    } else {
-      volatile int* abort = B.abort;
-      unsigned polls = 0;
-      while (ld_acquire_gpu(B.gen) == g && *abort == 0) {
-        if (++polls == kBarrierPolls) {
-          atomicOr(&C->err, kErrTimeout);
-          atomicExch(B.abort, 1);
-          break;
-        }
-        __nanosleep(32);
-      }
-    }
-    s_go = *(volatile int*)B.abort == 0;
-  }
-  __syncthreads();
-  return s_go != 0;
+// Barrier of the cluster's blocks: every thread arrives with release and
+// waits with acquire, so the global writes before it are visible after it.
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile(
+      "barrier.cluster.arrive.release;\n\t"
+      "barrier.cluster.wait.acquire;" ::: "memory");
 }
 
 // Exclusive scan of counts[0, n) by one block into out[0, n]; out[n] = total.
@@ -212,8 +171,7 @@ __device__ __forceinline__ void small_de(const Params<T>& P, int s) {
 // counters' commit by thread 0 is read only after the next ones.
 template <typename T, int D>
 __global__ void __launch_bounds__(kSmallThreads) k_small_steps(Params<T> P0, Params<T> P1,
-                                                               SmallBarrier bar, int nsteps,
-                                                               int n_cells) {
+                                                               int nsteps, int n_cells) {
   extern __shared__ int s_start[];  // n_cells + 1 offsets of the grid being built
   __shared__ int warp_sums[kSmallThreads / 32];
   const int tid = (int)(blockIdx.x * kSmallThreads + threadIdx.x);
@@ -235,7 +193,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_steps(Params<T> P0, Par
         P.s_rank[s] = atomicAdd(P.cell_count + c, 1);
       }
     }
-    if (!small_barrier(bar, C)) return;
+    cluster_barrier();
     if (tid == 0) {  // update!'s counters, as k_commit (no births or deaths here)
       C->slots = C->N[p];
       C->N[p ^ 1] = C->N[p];
@@ -253,7 +211,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_steps(Params<T> P0, Par
     if (blockIdx.x == 0)
       for (int c = threadIdx.x; c <= n_cells; c += kSmallThreads) P.cell_start[c] = s_start[c];
     for (int s = tid; s < N; s += nth) P.s_key[s_start[P.s_cell[s]] + P.s_rank[s]] = P.IB[s];
-    if (!small_barrier(bar, C)) return;
+    cluster_barrier();
     for (int s = tid; s < N; s += nth) {  // stable placement by agent index (k_sort_place)
       const int c = P.s_cell[s];
       const int key = P.IB[s];
@@ -269,7 +227,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_steps(Params<T> P0, Par
     }
     for (int c = tid; c < n_cells; c += nth) P.cell_count[c] = 0;
     if (tid == 0) C->list_valid = 0;
-    if (!small_barrier(bar, C)) return;
+    cluster_barrier();
   }
 }
 
