@@ -1230,7 +1230,22 @@ def main():
                 "cpu_baseline": cb, "e2e": r["e2e"], "gpu_launches": r["launches"],
                 "clocks": r["clocks"], "kernel_share": r["share"],
                 "kernel_avg_ms": {k: round(v[0], 4) for k, v in r["kern"].items()},
-                "batched": batched, "adjoint": adjoint, "configs": configs}
+                "configs": configs, "batched": batched, "adjoint": adjoint}
+        # the key figures once more at the end of the line (a reader that keeps
+        # only its tail still sees them)
+        summ = {"value": line["value"], "e2e": r["e2e"]["value"],
+                "k_agent_de_ms": r["roof"]["avg_ms"] if r["roof"] else None,
+                "issue_frac": (r["roof"] or {}).get("issue", {}).get("frac"),
+                "cpu_baseline": round(cb["value"], 1) if cb else None}
+        if batched:
+            summ.update(batched=batched.get("value"), batched_vs_plain=batched.get("speedup_vs_plain"))
+        if adjoint:
+            summ["adjoint_cost_ratio"] = adjoint.get("cost_ratio")
+        if configs:
+            summ["aggregation_2d_us_per_step"] = configs["aggregation_2d"]["us_per_step"]
+            summ["colony_3d_f64"] = configs["colony_3d_f64"]["value"]
+            summ["colony_3d_f64_e2e"] = configs["colony_3d_f64"]["e2e"]["value"]
+        line["summary"] = summ
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -1549,13 +1549,16 @@ __global__ void __launch_bounds__(kStX * kStY) k_medium_de_2d(Params<T> P) {
 // threads owns a kStX x kStTileY column of nodes over a run of z planes.  Each
 // thread keeps its kStRows nodes of the planes z-1, z and z+1 in registers;
 // plane z is staged in shared memory with a one-node x/y halo for the
-// in-plane neighbours.  Every node of the run is read from HBM once, plus the
-// halo and the two planes that close the run.  Same expressions as
-// k_medium_grad / k_medium_de: lap = (l_x + l_y) + l_z.
+// in-plane neighbours.  The march is pipelined: while plane z is computed,
+// the values of plane z+2 and the halo of plane z+1 are already in flight,
+// and the staged tiles alternate between two buffers, so a plane costs one
+// block barrier and no exposed load latency.  Every node of the run is read
+// from HBM once, plus the halo and the two planes that close the run.  Same
+// expressions as k_medium_grad / k_medium_de: lap = (l_x + l_y) + l_z.
 // ---------------------------------------------------------------------------
 template <typename T, bool kDE>
 __device__ __forceinline__ void stencil_3d(const Params<T>& P, int z_run) {
-  __shared__ T tile[kStTileY + 2][kStX + 2];
+  __shared__ T tile[2][kStTileY + 2][kStX + 2];
   const int nx = P.n_medium[0], ny = P.n_medium[1], nz = P.n_medium[2];
   const int x0 = blockIdx.x * kStX, y0 = blockIdx.y * kStTileY;
   const int za = blockIdx.z * z_run;
@@ -1567,31 +1570,37 @@ __device__ __forceinline__ void stencil_3d(const Params<T>& P, int z_run) {
     return kDE ? medium_in(P, v) : v;
   };
   const int x = x0 + threadIdx.x;
-  T lo[kStRows], mid[kStRows], hi[kStRows];
+  const int t = threadIdx.y * kStX + threadIdx.x;
+  // the halo node this thread stages: x-halo columns, then y-halo rows
+  int hx = 0, hy = 0, hr = 0, hc = 0;
+  const bool halo = t < 2 * kStTileY + 2 * kStX;
+  if (t < kStTileY) {
+    hx = x0 - 1, hy = y0 + t, hr = t + 1, hc = 0;
+  } else if (t < 2 * kStTileY) {
+    hx = x0 + kStX, hy = y0 + t - kStTileY, hr = t - kStTileY + 1, hc = kStX + 1;
+  } else if (t < 2 * kStTileY + kStX) {
+    hx = x0 + t - 2 * kStTileY, hy = y0 - 1, hr = 0, hc = t - 2 * kStTileY + 1;
+  } else if (halo) {
+    hx = x0 + t - 2 * kStTileY - kStX, hy = y0 + kStTileY, hr = kStTileY + 1,
+    hc = t - 2 * kStTileY - kStX + 1;
+  }
+  T lo[kStRows], mid[kStRows], hi[kStRows], nxt[kStRows];
 #pragma unroll
   for (int r = 0; r < kStRows; ++r) {
     const int y = y0 + threadIdx.y + r * kStY;
     lo[r] = read(x, y, za - 1);
     mid[r] = read(x, y, za);
+    hi[r] = read(x, y, za + 1);
+    tile[0][threadIdx.y + r * kStY + 1][threadIdx.x + 1] = mid[r];
   }
-  const int t = threadIdx.y * kStX + threadIdx.x;
+  if (halo) tile[0][hr][hc] = read(hx, hy, za);
+  int buf = 0;
   for (int z = za; z < zb; ++z) {
+    // in flight during this plane: plane z + 2 and the halo of plane z + 1
 #pragma unroll
-    for (int r = 0; r < kStRows; ++r) hi[r] = read(x, y0 + threadIdx.y + r * kStY, z + 1);
-    __syncthreads();  // every thread is done with the previous plane's tile
-#pragma unroll
-    for (int r = 0; r < kStRows; ++r) tile[threadIdx.y + r * kStY + 1][threadIdx.x + 1] = mid[r];
-    if (t < kStTileY) {
-      tile[t + 1][0] = read(x0 - 1, y0 + t, z);
-    } else if (t < 2 * kStTileY) {
-      tile[t - kStTileY + 1][kStX + 1] = read(x0 + kStX, y0 + t - kStTileY, z);
-    } else if (t < 2 * kStTileY + kStX) {
-      tile[0][t - 2 * kStTileY + 1] = read(x0 + t - 2 * kStTileY, y0 - 1, z);
-    } else if (t < 2 * kStTileY + 2 * kStX) {
-      tile[kStTileY + 1][t - 2 * kStTileY - kStX + 1] =
-          read(x0 + t - 2 * kStTileY - kStX, y0 + kStTileY, z);
-    }
-    __syncthreads();
+    for (int r = 0; r < kStRows; ++r) nxt[r] = read(x, y0 + threadIdx.y + r * kStY, z + 2);
+    const T hnext = halo ? read(hx, hy, z + 1) : (T)0;
+    __syncthreads();  // tile[buf] complete; tile[buf ^ 1] no longer read
 #pragma unroll
     for (int r = 0; r < kStRows; ++r) {
       const int ty = threadIdx.y + r * kStY, y = y0 + ty;
@@ -1604,22 +1613,31 @@ __device__ __forceinline__ void stencil_3d(const Params<T>& P, int z_run) {
           if (!in) {
             P.c_nxt[n] = u;
           } else {
-            const T l0 = ((tile[tyy][tx + 1] - (T)2 * u) + tile[tyy][tx - 1]) / (P.dx_m[0] * P.dx_m[0]);
-            const T l1 = ((tile[tyy + 1][tx] - (T)2 * u) + tile[tyy - 1][tx]) / (P.dx_m[1] * P.dx_m[1]);
+            const T l0 = ((tile[buf][tyy][tx + 1] - (T)2 * u) + tile[buf][tyy][tx - 1]) /
+                         (P.dx_m[0] * P.dx_m[0]);
+            const T l1 = ((tile[buf][tyy + 1][tx] - (T)2 * u) + tile[buf][tyy - 1][tx]) /
+                         (P.dx_m[1] * P.dx_m[1]);
             const T l2 = ((hi[r] - (T)2 * u) + lo[r]) / (P.dx_m[2] * P.dx_m[2]);
             const T lap = (l0 + l1) + l2;
             const T k = P.diff_D * lap - P.decay * u;
             P.c_nxt[n] = u + P.dt * k;
           }
         } else {
-          P.grad_nxt[0][n] = in ? (tile[tyy][tx + 1] - tile[tyy][tx - 1]) / ((T)2 * P.dx_m[0]) : (T)0;
-          P.grad_nxt[1][n] = in ? (tile[tyy + 1][tx] - tile[tyy - 1][tx]) / ((T)2 * P.dx_m[1]) : (T)0;
+          P.grad_nxt[0][n] =
+              in ? (tile[buf][tyy][tx + 1] - tile[buf][tyy][tx - 1]) / ((T)2 * P.dx_m[0]) : (T)0;
+          P.grad_nxt[1][n] =
+              in ? (tile[buf][tyy + 1][tx] - tile[buf][tyy - 1][tx]) / ((T)2 * P.dx_m[1]) : (T)0;
           P.grad_nxt[2][n] = in ? (hi[r] - lo[r]) / ((T)2 * P.dx_m[2]) : (T)0;
         }
       }
+      // plane z + 1 into the other buffer, then shift the column
+      tile[buf ^ 1][ty + 1][threadIdx.x + 1] = hi[r];
       lo[r] = mid[r];
       mid[r] = hi[r];
+      hi[r] = nxt[r];
     }
+    if (halo) tile[buf ^ 1][hr][hc] = hnext;
+    buf ^= 1;
   }
 }
 
