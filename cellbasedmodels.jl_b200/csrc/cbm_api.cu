@@ -17,6 +17,7 @@
 #include "../../include/cbm_b200.h"
 #include "cbm_kernels.cuh"
 #include "cbm_small.cuh"
+#include "cbm_stencil_tma.cuh"
 
 using namespace cbm;
 
@@ -65,6 +66,9 @@ struct cbm_ctx {
   // medium
   void* c[2] = {};
   void* grad[2][3] = {};
+  // 3D medium: tensor maps of c[0] and c[1] for the TMA-fed stencils
+  CUtensorMap tmap_c[2];
+  bool tma_medium = false;
   Counters* ctr = nullptr;
   int* scratch_int = nullptr;  // n_max ints for inspection calls
   void* ext_noise = nullptr;   // EM increments of cbm_step_noise (n_max * dims reals, lazy)
@@ -188,6 +192,17 @@ T bound2_lo(double r) {
   return (double)t > v ? std::nextafter(t, (T)0) : t;
 }
 
+// 1 / v when v > 0 is a power of two whose reciprocal is representable
+// (exactly), else 0.
+template <typename T>
+T exact_reciprocal(T v) {
+  if (!(v > (T)0) || !std::isfinite(v)) return (T)0;
+  int e = 0;
+  if (std::frexp(v, &e) != (T)0.5) return (T)0;
+  const T r = std::ldexp((T)1, 1 - e);
+  return (r > (T)0 && std::isfinite(r) && r * v == (T)1) ? r : (T)0;
+}
+
 template <typename T>
 Params<T> params(const cbm_ctx* c, int parity) {
   using V4 = typename V4T<T>::type;
@@ -248,6 +263,16 @@ Params<T> params(const cbm_ctx* c, int parity) {
     // dx = (hi - lo) / NMedium in Float64 (communityStructure.jl:274)
     P.dx_m[d] = d < k.dims && k.medium ? (T)((k.box_hi[d] - k.box_lo[d]) / (double)k.n_medium[d])
                                        : (T)1;
+  }
+  P.exact_scale = k.medium ? 1 : 0;
+  for (int d = 0; d < 3; ++d) {
+    P.inv_dx[d] = P.inv_dx2[d] = P.inv_2dx[d] = (T)0;
+    if (d < k.dims && k.medium) {
+      P.inv_dx[d] = exact_reciprocal<T>(P.dx_m[d]);
+      P.inv_dx2[d] = exact_reciprocal<T>(P.dx_m[d] * P.dx_m[d]);
+      P.inv_2dx[d] = exact_reciprocal<T>((T)2 * P.dx_m[d]);
+      if (P.inv_dx2[d] == (T)0 || P.inv_2dx[d] == (T)0) P.exact_scale = 0;
+    }
   }
   P.n_scan_tiles = c->n_scan_tiles;
   P.n_nodes = c->n_nodes;
@@ -337,6 +362,53 @@ dim3 stencil_grid_3d(const cbm_ctx* c) {
   return g;
 }
 
+// Tensor maps of the two medium buffers for the TMA-fed 3D stencils: the
+// field as an (nx, ny, nz) array of reals, boxes of one plane of a column
+// tile (TmaPlane), zeros outside.  Needs rows of a multiple of 16 bytes (the
+// strides of a tensor map); other shapes keep the register-pipelined
+// stencils.  cuTensorMapEncodeTiled is reached through the runtime's driver
+// entry point, so the library does not link the driver library itself.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled_fn() {
+  static EncodeTiledFn fn = []() -> EncodeTiledFn {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<EncodeTiledFn>(f);
+  }();
+  return fn;
+}
+
+template <typename T>
+bool encode_medium_maps(cbm_ctx* c) {
+  using G = TmaPlane<T>;
+  const cbm_config& k = c->cfg;
+  if (!k.medium || k.dims != 3) return false;
+  const unsigned long long nx = k.n_medium[0], ny = k.n_medium[1], nz = k.n_medium[2];
+  if ((nx * sizeof(T)) % 16 != 0) return false;
+  EncodeTiledFn enc = encode_tiled_fn();
+  if (!enc) return false;
+  const cuuint64_t dim[3] = {nx, ny, nz};
+  const cuuint64_t stride[2] = {nx * sizeof(T), nx * ny * sizeof(T)};
+  const cuuint32_t box[3] = {(cuuint32_t)G::kBX, (cuuint32_t)G::kBY, 1};
+  const cuuint32_t estride[3] = {1, 1, 1};
+  for (int q = 0; q < 2; ++q)
+    if (enc(&c->tmap_c[q],
+            sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+            c->c[q], dim, stride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  return true;
+}
+
 // ---- stage launches (enqueue only) -----------------------------------------
 template <typename T, int D>
 void enqueue_medium_rule(cbm_ctx* c, const Params<T>& P) {
@@ -345,7 +417,11 @@ void enqueue_medium_rule(cbm_ctx* c, const Params<T>& P) {
     if (D == 2)
       k_medium_grad_2d<T><<<stencil_grid(c), dim3(kStX, kStY), 0, c->stream>>>(P);
     else if (D == 3)
-      k_medium_grad_3d<T><<<stencil_grid_3d(c), dim3(kStX, kStY), 0, c->stream>>>(P, stencil_z_run(c));
+      if (c->tma_medium)
+        k_medium_grad_3d_tma<T><<<stencil_grid_3d(c), dim3(kStX, kStY), TmaPlane<T>::kSmem,
+                                  c->stream>>>(P, c->tmap_c[P.parity], stencil_z_run(c));
+      else
+        k_medium_grad_3d<T><<<stencil_grid_3d(c), dim3(kStX, kStY), 0, c->stream>>>(P, stencil_z_run(c));
     else
       k_medium_grad<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
   }
@@ -359,8 +435,14 @@ void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P) {
     k_medium_snapshot<T><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
   }
   if (uses_gather(k)) {
-    PROF("k_secrete_gather");
-    k_secrete_gather<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
+    PROF("k_secrete_rows");
+    const int nm[3] = {c->cfg.n_medium[0], D > 1 ? c->cfg.n_medium[1] : 1,
+                       D > 2 ? c->cfg.n_medium[2] : 1};
+    const long long patches = (long long)((nm[0] + 31) / 32) *
+                              ((nm[1] + GatherPatch<D>::kY - 1) / GatherPatch<D>::kY) *
+                              ((nm[2] + GatherPatch<D>::kZ - 1) / GatherPatch<D>::kZ);
+    k_secrete_rows<T, D><<<(unsigned)((patches + kRowWarps - 1) / kRowWarps), kRowWarps * 32, 0,
+                           c->stream>>>(P);
   }
   if (!rule_needed(k)) return;
   if (k.fate != CBM_FATE_NONE) {
@@ -418,7 +500,11 @@ void enqueue_medium_de(cbm_ctx* c, const Params<T>& P) {
     if (D == 2)
       k_medium_de_2d<T><<<stencil_grid(c), dim3(kStX, kStY), 0, c->stream>>>(P);
     else if (D == 3)
-      k_medium_de_3d<T><<<stencil_grid_3d(c), dim3(kStX, kStY), 0, c->stream>>>(P, stencil_z_run(c));
+      if (c->tma_medium)
+        k_medium_de_3d_tma<T><<<stencil_grid_3d(c), dim3(kStX, kStY), TmaPlane<T>::kSmem,
+                                c->stream>>>(P, c->tmap_c[P.parity], stencil_z_run(c));
+      else
+        k_medium_de_3d<T><<<stencil_grid_3d(c), dim3(kStX, kStY), 0, c->stream>>>(P, stencil_z_run(c));
     else
       k_medium_de<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
   }
@@ -843,6 +929,7 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     delete c;
     return rc;
   }
+  c->tma_medium = c->tsize == 8 ? encode_medium_maps<double>(c) : encode_medium_maps<float>(c);
   cudaMemsetAsync(c->cell_count, 0, (size_t)c->n_cells * 4, c->stream);
   cudaMemsetAsync(c->scan_state, 0, (size_t)c->n_scan_tiles * 8, c->stream);
   cudaMemsetAsync(c->fate_state, 0, (size_t)c->n_blocks * 8, c->stream);

@@ -128,6 +128,8 @@ struct Params {
   T wall_force, wall_range, drift_linear;
   T v_div, div_sep, p_death;
   T dx_m[3];
+  T inv_dx[3], inv_dx2[3], inv_2dx[3];  // 1 / dx, 1 / dx^2, 1 / (2 dx) when powers of two, else 0
+  int exact_scale;           // every axis of the medium has both reciprocals
   T diff_D, decay, secretion_amt, chemotaxis;
   T uptake_amt;             // uptake * dt (0: no uptake, and no clamp of the field)
   uint64_t seed;
@@ -171,15 +173,22 @@ __device__ __forceinline__ int nearest_node(const Params<T>& P, const T* x) {
   return lin;
 }
 
-// Nodes and weights of the multilinear stencil around x (nodes at the cell
-// centres lo + (i + 1/2) dx, indices clamped to the grid).
+// v / dx on axis d: the product with the exact reciprocal when dx is a power
+// of two (the same correctly rounded value), else the quotient.
+template <typename T>
+__device__ __forceinline__ T over_dx(const Params<T>& P, int d, T v) {
+  return P.inv_dx[d] != (T)0 ? v * P.inv_dx[d] : v / P.dx_m[d];
+}
+
+// Clamped node indices i0 <= i1 of the multilinear stencil around x on each
+// axis (nodes at the cell centres lo + (i + 1/2) dx) and the fractional
+// offsets tt.
 template <typename T, int D>
-__device__ __forceinline__ void bilinear(const Params<T>& P, const T* x, int* node, T* w) {
-  int i0[3], i1[3];
-  T tt[3];
+__device__ __forceinline__ void bilinear_axes(const Params<T>& P, const T* x, int* i0, int* i1,
+                                              T* tt) {
 #pragma unroll
   for (int d = 0; d < D; ++d) {
-    T s = (x[d] - P.box_lo[d]) / P.dx_m[d] - (T)0.5;
+    T s = over_dx(P, d, x[d] - P.box_lo[d]) - (T)0.5;
     T fl = floor(s);
     tt[d] = s - fl;
     int a = (int)fl, b = a + 1;
@@ -187,19 +196,34 @@ __device__ __forceinline__ void bilinear(const Params<T>& P, const T* x, int* no
     i0[d] = a < 0 ? 0 : (a > hi ? hi : a);
     i1[d] = b < 0 ? 0 : (b > hi ? hi : b);
   }
+}
+
+// Weight of stencil node q (bit d of q: i1 rather than i0 on axis d).
+template <typename T, int D>
+__device__ __forceinline__ T bilinear_weight(const T* tt, int q) {
+  T wq = (T)1;
+#pragma unroll
+  for (int d = 0; d < D; ++d) wq = wq * (((q >> d) & 1) ? tt[d] : (T)1 - tt[d]);
+  return wq;
+}
+
+// Nodes and weights of the multilinear stencil around x (indices clamped to
+// the grid).
+template <typename T, int D>
+__device__ __forceinline__ void bilinear(const Params<T>& P, const T* x, int* node, T* w) {
+  int i0[3], i1[3];
+  T tt[3];
+  bilinear_axes<T, D>(P, x, i0, i1, tt);
 #pragma unroll
   for (int q = 0; q < (1 << D); ++q) {
     int lin = 0, mul = 1;
-    T wq = (T)1;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-      bool h = (q >> d) & 1;
-      lin += (h ? i1[d] : i0[d]) * mul;
+      lin += (((q >> d) & 1) ? i1[d] : i0[d]) * mul;
       mul *= P.n_medium[d];
-      wq = wq * (h ? tt[d] : (T)1 - tt[d]);
     }
     node[q] = lin;
-    w[q] = wq;
+    w[q] = bilinear_weight<T, D>(tt, q);
   }
 }
 
@@ -411,12 +435,35 @@ __device__ __forceinline__ bool secretion_by_gather(const Params<T>& P) {
   return P.medium_sampling == CBM_MEDIUM_BILINEAR && P.neighbors == CBM_NEIGH_CELL_LINKED;
 }
 
+// Cell range on axis d of the agents whose stencil can cover node q: such
+// agents lie in [lo + (q - 1/2) dx, lo + (q + 3/2) dx) (unbounded below for
+// q = 0, above for the last node), widened by a rounding margin.  Both ends
+// are non-decreasing in q.
+template <typename T>
+__device__ __forceinline__ T gather_margin(const Params<T>& P, int d) {
+  return (T)1e-3 * P.dx_m[d] + (T)64 * Eps<T>::v * (fabs(P.box_lo[d]) + fabs(P.box_hi[d]));
+}
+template <typename T>
+__device__ __forceinline__ int gather_cell_lo(const Params<T>& P, int d, int q) {
+  return q == 0 ? 0
+                : cell_pos1<T>(P.edge, P.box_lo[d] + ((T)q - (T)0.5) * P.dx_m[d] - gather_margin(P, d),
+                               P.box_lo[d], P.box_hi[d], P.n_cells_d[d]);
+}
+template <typename T>
+__device__ __forceinline__ int gather_cell_hi(const Params<T>& P, int d, int q) {
+  return q == P.n_medium[d] - 1
+             ? P.n_cells_d[d] - 1
+             : cell_pos1<T>(P.edge, P.box_lo[d] + ((T)q + (T)1.5) * P.dx_m[d] + gather_margin(P, d),
+                            P.box_lo[d], P.box_hi[d], P.n_cells_d[d]);
+}
+
+// The gather of one node n by one thread: the agents of its cell box that
+// touch it, sorted by index (or a k-way merge over the cells when more than
+// kTouch touch it).  The path of crowded runs of k_secrete_rows.
 template <typename T, int D>
-__global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
+__device__ __forceinline__ void secrete_node(const Params<T>& P, int n) {
   constexpr int kMaxCells = D == 1 ? 4 : (D == 2 ? 16 : 64);
   constexpr int kTouch = 32;  // agents collected per node before the merge fallback
-  const int n = blockIdx.x * kTile + threadIdx.x;
-  if (n >= P.n_nodes) return;
   int q[3] = {0, 0, 0};
   q[0] = n % P.n_medium[0];
   if (D > 1) q[1] = (n / P.n_medium[0]) % P.n_medium[1];
@@ -444,7 +491,7 @@ __global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
     bool t = true;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-      const T sd = (x[d] - P.box_lo[d]) / P.dx_m[d] - (T)0.5;
+      const T sd = over_dx(P, d, x[d] - P.box_lo[d]) - (T)0.5;
       const int a = (int)floor(sd), b = a + 1;
       const int hi = P.n_medium[d] - 1;
       const int i0 = a < 0 ? 0 : (a > hi ? hi : a);
@@ -453,25 +500,12 @@ __global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
     }
     return t;
   };
-  // Agents whose stencil covers node q along an axis lie in x in
-  // [lo+(q-1/2)dx, lo+(q+3/2)dx) (unbounded below for q = 0, above for the
-  // last node).  The cells of that box, widened by a rounding margin, are
-  // scanned; the agents that touch the node are kept sorted by index and
-  // added in that order, the order of the reference's serial agent loop.
   int c0[3] = {0, 0, 0}, c1[3] = {0, 0, 0};
   int ncell = 1;
 #pragma unroll
   for (int d = 0; d < D; ++d) {
-    const int nc = P.n_cells_d[d];
-    const T dx = P.dx_m[d];
-    const T margin = (T)1e-3 * dx + (T)64 * Eps<T>::v * (fabs(P.box_lo[d]) + fabs(P.box_hi[d]));
-    c0[d] = q[d] == 0 ? 0
-                      : cell_pos1<T>(P.edge, P.box_lo[d] + ((T)q[d] - (T)0.5) * dx - margin,
-                                     P.box_lo[d], P.box_hi[d], nc);
-    c1[d] = q[d] == P.n_medium[d] - 1
-                ? nc - 1
-                : cell_pos1<T>(P.edge, P.box_lo[d] + ((T)q[d] + (T)1.5) * dx + margin,
-                               P.box_lo[d], P.box_hi[d], nc);
+    c0[d] = gather_cell_lo(P, d, q[d]);
+    c1[d] = gather_cell_hi(P, d, q[d]);
     ncell *= c1[d] - c0[d] + 1;
   }
   int tj[kTouch], ts[kTouch];
@@ -537,6 +571,171 @@ __global__ void __launch_bounds__(kTile) k_secrete_gather(Params<T> P) {
     for (int j = 0; j < N; ++j) add(P.inv[j]);
   }
   P.c_cur[n] = acc;
+}
+
+// The gather by patches: one warp takes the runs of 32 nodes along x of a
+// 2 x 2 patch of (y, z) rows (2 rows in 2D, 1 in 1D), four nodes a lane in
+// 3D.  The union of the patch nodes' cell boxes is read at once: each lane
+// takes one row of cells (one (y, z) pair of the box; its agents are
+// contiguous slots), a warp scan numbers the candidates, and every lane takes
+// one candidate of a chunk, computes its stencil (bilinear_axes, the
+// expressions of bilinear()) and the patch nodes it falls on.  The agents
+// that touch the patch are appended to a warp list, the list is ranked by
+// agent index, and each lane adds the terms of its nodes in that order (and
+// in stencil order within an agent), the sums of secrete_node.  A patch whose
+// box has more than 32 rows, or that more than 32 agents touch, falls back to
+// secrete_node for each of its nodes.  A node that no agent touches keeps its
+// value and is not written.
+constexpr int kRowWarps = 8;  // warps (patches) per block of k_secrete_rows
+
+template <int D>
+struct GatherPatch {
+  static constexpr int kY = D > 1 ? 2 : 1, kZ = D > 2 ? 2 : 1, kRuns = kY * kZ;
+};
+
+template <typename T, int D>
+__global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P) {
+  constexpr int K = 1 << D;
+  constexpr int PY = GatherPatch<D>::kY, PZ = GatherPatch<D>::kZ, NP = GatherPatch<D>::kRuns;
+  __shared__ int s_j[kRowWarps][32];
+  __shared__ unsigned char s_code[kRowWarps][32][K];  // run * 32 + lane of stencil node k, or 0xff
+  __shared__ T s_w[kRowWarps][32][K];
+  __shared__ unsigned char s_perm[kRowWarps][32];
+  const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+  const int nx = P.n_medium[0];
+  const int ny = D > 1 ? P.n_medium[1] : 1, nz = D > 2 ? P.n_medium[2] : 1;
+  const int px = (nx + 31) >> 5, py = (ny + PY - 1) / PY, pz = (nz + PZ - 1) / PZ;
+  const int patch = blockIdx.x * kRowWarps + wb;
+  if (patch >= px * py * pz) return;  // the whole warp
+  const int rx = patch % px, ryz = patch / px;
+  const int x0 = rx * 32, y0 = (ryz % py) * PY, z0 = (ryz / py) * PZ;
+  const int xl = min(x0 + 31, nx - 1), yl = min(y0 + PY - 1, ny - 1), zl = min(z0 + PZ - 1, nz - 1);
+  const int qx = x0 + lane;
+  // the lane's nodes (run p: y0 + p % PY, z0 + p / PY) and their committed
+  // values (this lane is their only writer; read early, used last)
+  int node[NP];
+  bool mine[NP];
+  T c_com[NP];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    const int y = y0 + p % PY, z = z0 + p / PY;
+    mine[p] = qx < nx && y < ny && z < nz;
+    node[p] = qx + nx * (y + ny * z);
+    c_com[p] = mine[p] ? P.c_cur[node[p]] : (T)0;
+  }
+  const int cx0 = gather_cell_lo(P, 0, x0), cx1 = gather_cell_hi(P, 0, xl);
+  const int cy0 = D > 1 ? gather_cell_lo(P, 1, y0) : 0, cy1 = D > 1 ? gather_cell_hi(P, 1, yl) : 0;
+  const int cz0 = D > 2 ? gather_cell_lo(P, 2, z0) : 0, cz1 = D > 2 ? gather_cell_hi(P, 2, zl) : 0;
+  const int nry = cy1 - cy0 + 1, nrows = nry * (cz1 - cz0 + 1);
+  bool crowded = nrows > 32;
+  int ne = 0;  // entries of the warp list
+  if (!crowded) {
+    int s0 = 0, cnt = 0;
+    if (lane < nrows) {
+      const int row = P.n_cells_d[0] * ((cy0 + lane % nry) + P.n_cells_d[1] * (cz0 + lane / nry));
+      s0 = ld(P.cell_start + row + cx0);
+      cnt = ld(P.cell_start + row + cx1 + 1) - s0;
+    }
+    int inc = cnt;  // inclusive scan of the rows' counts
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, inc, o);
+      if (lane >= o) inc += y;
+    }
+    const int m_all = __shfl_sync(kFull, inc, 31);
+    const unsigned below = (1u << lane) - 1u;
+    for (int base = 0; base < m_all; base += 32) {
+      const int m = base + lane;
+      int r = 0;  // row of candidate m: the rows that end at or before it
+      for (int k = 0; k < nrows; ++k) r += __shfl_sync(kFull, inc, k) <= m;
+      const int rr = r < 31 ? r : 31;
+      const int sl = __shfl_sync(kFull, s0, rr) + m - (__shfl_sync(kFull, inc, rr) -
+                                                       __shfl_sync(kFull, cnt, rr));
+      bool hit = false;
+      unsigned char code[K];
+      T w[K];
+      int j = 0;
+      if (m < m_all) {
+        T x[3];
+        to3<T>(P.PA[sl], x);
+        j = P.IA[sl];
+        int i0[3] = {0, 0, 0}, i1[3] = {0, 0, 0};
+        T tt[3];
+        bilinear_axes<T, D>(P, x, i0, i1, tt);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const int ix = (k & 1) ? i1[0] : i0[0];
+          const int iy = ((k >> 1) & 1) ? i1[1] : i0[1];
+          const int iz = ((k >> 2) & 1) ? i1[2] : i0[2];
+          bool on = ix >= x0 && ix <= xl;
+          if (D > 1) on = on && iy >= y0 && iy <= yl;
+          if (D > 2) on = on && iz >= z0 && iz <= zl;
+          const int run = (D > 2 ? (iz - z0) * PY : 0) + (D > 1 ? iy - y0 : 0);
+          code[k] = on ? (unsigned char)(run * 32 + ix - x0) : (unsigned char)0xff;
+          w[k] = bilinear_weight<T, D>(tt, k);
+          hit = hit || on;
+        }
+      }
+      const unsigned hits = __ballot_sync(kFull, hit);
+      if (ne + __popc(hits) > 32) {
+        crowded = true;
+        break;
+      }
+      if (hit) {
+        const int e = ne + __popc(hits & below);
+        s_j[wb][e] = j;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          s_code[wb][e][k] = code[k];
+          s_w[wb][e][k] = w[k];
+        }
+      }
+      ne += __popc(hits);
+    }
+  }
+  if (crowded) {
+#pragma unroll 1
+    for (int p = 0; p < NP; ++p) {
+      const int y = y0 + p % PY, z = z0 + p / PY;
+      if (qx < nx && y < ny && z < nz) secrete_node<T, D>(P, qx + nx * (y + ny * z));
+    }
+    return;
+  }
+  if (ne == 0) return;
+  __syncwarp();
+  if (lane < ne) {  // rank by agent index (the indices are distinct)
+    const int j = s_j[wb][lane];
+    int r = 0;
+    for (int e = 0; e < ne; ++e) r += s_j[wb][e] < j;
+    s_perm[wb][r] = (unsigned char)lane;
+  }
+  __syncwarp();
+  const T amt = P.secretion_amt;
+  const bool upt = P.uptake_amt != (T)0;
+  T acc[NP], net[NP];
+  bool touched[NP];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    net[p] = upt ? amt - P.uptake_amt * c_com[p] : amt;  // secretion - first-order uptake
+    acc[p] = c_com[p];
+    touched[p] = false;
+  }
+  for (int r = 0; r < ne; ++r) {
+    const int e = s_perm[wb][r];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int c = s_code[wb][e][k];
+#pragma unroll
+      for (int p = 0; p < NP; ++p)
+        if (c == p * 32 + lane) {
+          acc[p] = acc[p] + s_w[wb][e][k] * net[p];
+          touched[p] = true;
+        }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < NP; ++p)
+    if (mine[p] && touched[p]) P.c_cur[node[p]] = acc[p];
 }
 
 // ---------------------------------------------------------------------------
@@ -1447,6 +1646,19 @@ __device__ __forceinline__ T medium_in(const Params<T>& P, T v) {
   return (P.uptake_amt != (T)0 && v < (T)0) ? (T)0 : v;
 }
 
+// v / (dx dx) and v / (2 dx) on axis d.  With kScale the divisor is a power
+// of two, and the product with its exact reciprocal is the same correctly
+// rounded value as the quotient (subnormal results, zeros and infinities
+// included), without a division.
+template <bool kScale, typename T>
+__device__ __forceinline__ T over_dx2(const Params<T>& P, int d, T v) {
+  return kScale ? v * P.inv_dx2[d] : v / (P.dx_m[d] * P.dx_m[d]);
+}
+template <bool kScale, typename T>
+__device__ __forceinline__ T over_2dx(const Params<T>& P, int d, T v) {
+  return kScale ? v * P.inv_2dx[d] : v / ((T)2 * P.dx_m[d]);
+}
+
 template <typename T, int D>
 __global__ void __launch_bounds__(kTile) k_medium_de(Params<T> P) {
   int n = blockIdx.x * kTile + threadIdx.x;
@@ -1497,8 +1709,8 @@ __device__ __forceinline__ void stage_tile2(const Params<T>& P, T (*tile)[kStX +
   __syncthreads();
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kStX * kStY) k_medium_grad_2d(Params<T> P) {
+template <typename T, bool kScale>
+__device__ __forceinline__ void medium_grad_2d(const Params<T>& P) {
   __shared__ T tile[kStTileY + 2][kStX + 2];
   const int nx = P.n_medium[0], ny = P.n_medium[1];
   const int x0 = blockIdx.x * kStX, y0 = blockIdx.y * kStTileY;
@@ -1512,13 +1724,19 @@ __global__ void __launch_bounds__(kStX * kStY) k_medium_grad_2d(Params<T> P) {
     const size_t n = (size_t)y * nx + x;
     const bool in = x > 0 && x < nx - 1 && y > 0 && y < ny - 1;
     const int tx = threadIdx.x + 1, tyy = ty + 1;
-    P.grad_nxt[0][n] = in ? (tile[tyy][tx + 1] - tile[tyy][tx - 1]) / ((T)2 * P.dx_m[0]) : (T)0;
-    P.grad_nxt[1][n] = in ? (tile[tyy + 1][tx] - tile[tyy - 1][tx]) / ((T)2 * P.dx_m[1]) : (T)0;
+    P.grad_nxt[0][n] = in ? over_2dx<kScale>(P, 0, tile[tyy][tx + 1] - tile[tyy][tx - 1]) : (T)0;
+    P.grad_nxt[1][n] = in ? over_2dx<kScale>(P, 1, tile[tyy + 1][tx] - tile[tyy - 1][tx]) : (T)0;
   }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kStX * kStY) k_medium_de_2d(Params<T> P) {
+__global__ void __launch_bounds__(kStX * kStY) k_medium_grad_2d(Params<T> P) {
+  if (P.exact_scale) medium_grad_2d<T, true>(P);
+  else medium_grad_2d<T, false>(P);
+}
+
+template <typename T, bool kScale>
+__device__ __forceinline__ void medium_de_2d(const Params<T>& P) {
   __shared__ T tile[kStTileY + 2][kStX + 2];
   const int nx = P.n_medium[0], ny = P.n_medium[1];
   const int x0 = blockIdx.x * kStX, y0 = blockIdx.y * kStTileY;
@@ -1536,12 +1754,18 @@ __global__ void __launch_bounds__(kStX * kStY) k_medium_de_2d(Params<T> P) {
       P.c_nxt[n] = u;
       continue;
     }
-    const T l0 = ((tile[tyy][tx + 1] - (T)2 * u) + tile[tyy][tx - 1]) / (P.dx_m[0] * P.dx_m[0]);
-    const T l1 = ((tile[tyy + 1][tx] - (T)2 * u) + tile[tyy - 1][tx]) / (P.dx_m[1] * P.dx_m[1]);
+    const T l0 = over_dx2<kScale>(P, 0, (tile[tyy][tx + 1] - (T)2 * u) + tile[tyy][tx - 1]);
+    const T l1 = over_dx2<kScale>(P, 1, (tile[tyy + 1][tx] - (T)2 * u) + tile[tyy - 1][tx]);
     const T lap = l0 + l1;
     const T k = P.diff_D * lap - P.decay * u;
     P.c_nxt[n] = u + P.dt * k;
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kStX * kStY) k_medium_de_2d(Params<T> P) {
+  if (P.exact_scale) medium_de_2d<T, true>(P);
+  else medium_de_2d<T, false>(P);
 }
 
 // ---------------------------------------------------------------------------

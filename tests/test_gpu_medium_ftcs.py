@@ -110,3 +110,56 @@ def test_chemotaxis_2d_with_uptake(gpu_lib, abi):
         g.step(25)
         o.step(25)
         assert_same_state(g.download(), o.download(), ["x", "y", "c", "gx", "gy"])
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("dims", [2, 3])
+def test_secretion_runs_sparse_and_crowded(gpu_lib, abi, dims, prec):
+    """The gather by runs of 32 nodes: a crowded clump (runs that more than 32
+    agents touch take the per-node path), sparse agents (runs of a few
+    agents, untouched runs left as they are), agents beyond the box (clamped
+    stencils that put two terms on one node) and a medium width that is not
+    a multiple of 32."""
+    nm = {2: (150, 70), 3: (75, 30, 26)}[dims]
+    L = tuple(float(v) for v in nm)
+    kw, _ = medium_colony(abi, dims, N=4500, L=L[0], n_medium=1,
+                          precision=abi.F32 if prec == "f32" else abi.F64)
+    kw.update(box_hi=L, n_medium=nm)
+    rng = np.random.default_rng(17)
+    n_clump, n_sparse, n_out = 1500, 2500, 500
+    lo = np.array([0.2 * v for v in L])
+    clump = lo[:, None] + rng.uniform(0, 10.0, (dims, n_clump))
+    sparse = rng.uniform(0, 1, (dims, n_sparse)) * np.array(L)[:, None]
+    out = rng.uniform(-1.5, 1.5, (dims, n_out)) + np.where(
+        rng.uniform(0, 1, (dims, n_out)) < 0.5, 0.0, np.array(L)[:, None])
+    p = np.concatenate([clump, sparse, out], axis=1)
+    p = p[:, rng.permutation(p.shape[1])]
+    st = {k: p[d] for d, k in enumerate("xyz"[:dims])}
+    st["c"] = rng.uniform(0, 1, int(np.prod(nm)))
+    g, o = both(abi, kw, st)
+    for _ in range(2):
+        g.step(6)
+        o.step(6)
+        assert_same_state(g.download(), o.download(), keys(dims))
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("dx", [0.5, 0.75, 1.5625])
+@pytest.mark.parametrize("dims", [2, 3])
+def test_medium_spacings(gpu_lib, abi, dims, dx, prec):
+    """Spacings other than 1: powers of two (dx^2 and 2 dx applied through
+    their exact reciprocals) and others (divided), on medium widths whose rows
+    are a multiple of 16 bytes (the TMA-fed 3D stencils) and widths that are
+    not (the register-pipelined ones)."""
+    for nm in {2: [(40, 30), (37, 29)], 3: [(24, 14, 12), (21, 14, 12)]}[dims]:
+        L = tuple(v * dx for v in nm)
+        kw, _ = medium_colony(abi, dims, N=1500, L=L[0], n_medium=1, dt=0.02,
+                              precision=abi.F32 if prec == "f32" else abi.F64)
+        kw.update(box_hi=L, n_medium=nm)
+        rng = np.random.default_rng(23)
+        st = {k: rng.uniform(0, L[d], 1500) for d, k in enumerate("xyz"[:dims])}
+        st["c"] = rng.uniform(0, 1, int(np.prod(nm)))
+        g, o = both(abi, kw, st)
+        g.step(8)
+        o.step(8)
+        assert_same_state(g.download(), o.download(), keys(dims))
