@@ -66,6 +66,7 @@ struct cbm_ctx {
   // medium
   void* c[2] = {};
   void* grad[2][3] = {};
+  int* gather_box = nullptr;  // cell-box tables of the secretion gather (k_gather_box)
   // 3D medium: tensor maps of c[0] and c[1] for the TMA-fed stencils
   CUtensorMap tmap_c[2];
   bool tma_medium = false;
@@ -244,6 +245,7 @@ Params<T> params(const cbm_ctx* c, int parity) {
   P.s_key = c->s_key;
   P.cell_count = c->cell_count;
   P.cell_start = c->cell_start;
+  P.gather_box = c->gather_box;
   P.scan_state = c->scan_state;
   P.nbr_n = c->nbr_n;
   P.nbr_list = c->nbr_list;
@@ -438,11 +440,10 @@ void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P) {
     PROF("k_secrete_rows");
     const int nm[3] = {c->cfg.n_medium[0], D > 1 ? c->cfg.n_medium[1] : 1,
                        D > 2 ? c->cfg.n_medium[2] : 1};
-    const long long patches = (long long)((nm[0] + 31) / 32) *
-                              ((nm[1] + GatherPatch<D>::kY - 1) / GatherPatch<D>::kY) *
-                              ((nm[2] + GatherPatch<D>::kZ - 1) / GatherPatch<D>::kZ);
-    k_secrete_rows<T, D><<<(unsigned)((patches + kRowWarps - 1) / kRowWarps), kRowWarps * 32, 0,
-                           c->stream>>>(P);
+    const int py = (nm[1] + GatherPatch<D>::kY - 1) / GatherPatch<D>::kY;
+    const dim3 grid((unsigned)((nm[0] + 31) / 32), (unsigned)((py + kRowWarps - 1) / kRowWarps),
+                    (unsigned)((nm[2] + GatherPatch<D>::kZ - 1) / GatherPatch<D>::kZ));
+    k_secrete_rows<T, D><<<grid, kRowWarps * 32, 0, c->stream>>>(P);
   }
   if (!rule_needed(k)) return;
   if (k.fate != CBM_FATE_NONE) {
@@ -921,6 +922,9 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
       c->c[q] = dalloc(c, (size_t)c->n_nodes * S, &ok);
       for (int d = 0; d < 3; ++d) c->grad[q][d] = dalloc(c, (size_t)c->n_nodes * S, &ok);
     }
+    size_t nb = 0;
+    for (int d = 0; d < k.dims; ++d) nb += 2 * (size_t)k.n_medium[d];
+    c->gather_box = (int*)dalloc(c, nb * 4, &ok);
   }
   c->ctr = (Counters*)dalloc(c, sizeof(Counters), &ok);
   if (!ok) {
@@ -930,6 +934,15 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     return rc;
   }
   c->tma_medium = c->tsize == 8 ? encode_medium_maps<double>(c) : encode_medium_maps<float>(c);
+  if (k.medium) {
+    int nmax = 1;
+    for (int d = 0; d < k.dims; ++d) nmax = k.n_medium[d] > nmax ? (int)k.n_medium[d] : nmax;
+    const unsigned blocks = (unsigned)((nmax + 255) / 256);
+    if (c->tsize == 8)
+      k_gather_box<double><<<blocks, 256, 0, c->stream>>>(params<double>(c, 0), c->gather_box, k.dims);
+    else
+      k_gather_box<float><<<blocks, 256, 0, c->stream>>>(params<float>(c, 0), c->gather_box, k.dims);
+  }
   cudaMemsetAsync(c->cell_count, 0, (size_t)c->n_cells * 4, c->stream);
   cudaMemsetAsync(c->scan_state, 0, (size_t)c->n_scan_tiles * 8, c->stream);
   cudaMemsetAsync(c->fate_state, 0, (size_t)c->n_blocks * 8, c->stream);

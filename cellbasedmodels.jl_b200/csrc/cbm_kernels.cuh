@@ -84,6 +84,7 @@ struct Params {
   int* s_key;           // agent index at each sorted position
   int* cell_count;
   int* cell_start;      // n_cells + 1
+  const int* gather_box;  // per medium axis d, per node q: gather_cell_lo, then gather_cell_hi
   unsigned long long* scan_state;
   // Verlet list in slot space: entry k of the row of slot s at k * n_max + s
   int* nbr_n;
@@ -457,6 +458,23 @@ __device__ __forceinline__ int gather_cell_hi(const Params<T>& P, int d, int q) 
                             P.box_lo[d], P.box_hi[d], P.n_cells_d[d]);
 }
 
+// The tables of gather_cell_lo / gather_cell_hi: for axis d (offset
+// off[d] = 2 * (n_medium[0] + ... + n_medium[d-1])), entries q and
+// n_medium[d] + q.  Filled once per context.
+template <typename T>
+__global__ void k_gather_box(Params<T> P, int* box, int dims) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  int off = 0;
+  for (int d = 0; d < dims; ++d) {
+    const int n = P.n_medium[d];
+    if (q < n) {
+      box[off + q] = gather_cell_lo(P, d, q);
+      box[off + n + q] = gather_cell_hi(P, d, q);
+    }
+    off += 2 * n;
+  }
+}
+
 // The gather of one node n by one thread: the agents of its cell box that
 // touch it, sorted by index (or a k-way merge over the cells when more than
 // kTouch touch it).  The path of crowded runs of k_secrete_rows.
@@ -604,11 +622,10 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
   const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
   const int nx = P.n_medium[0];
   const int ny = D > 1 ? P.n_medium[1] : 1, nz = D > 2 ? P.n_medium[2] : 1;
-  const int px = (nx + 31) >> 5, py = (ny + PY - 1) / PY, pz = (nz + PZ - 1) / PZ;
-  const int patch = blockIdx.x * kRowWarps + wb;
-  if (patch >= px * py * pz) return;  // the whole warp
-  const int rx = patch % px, ryz = patch / px;
-  const int x0 = rx * 32, y0 = (ryz % py) * PY, z0 = (ryz / py) * PZ;
+  // grid: x runs, y patches (a block's warps), z patches
+  const int x0 = blockIdx.x * 32;
+  const int y0 = (blockIdx.y * kRowWarps + wb) * PY, z0 = blockIdx.z * PZ;
+  if (y0 >= ny) return;  // the whole warp
   const int xl = min(x0 + 31, nx - 1), yl = min(y0 + PY - 1, ny - 1), zl = min(z0 + PZ - 1, nz - 1);
   const int qx = x0 + lane;
   // the lane's nodes (run p: y0 + p % PY, z0 + p / PY) and their committed
@@ -623,9 +640,12 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
     node[p] = qx + nx * (y + ny * z);
     c_com[p] = mine[p] ? P.c_cur[node[p]] : (T)0;
   }
-  const int cx0 = gather_cell_lo(P, 0, x0), cx1 = gather_cell_hi(P, 0, xl);
-  const int cy0 = D > 1 ? gather_cell_lo(P, 1, y0) : 0, cy1 = D > 1 ? gather_cell_hi(P, 1, yl) : 0;
-  const int cz0 = D > 2 ? gather_cell_lo(P, 2, z0) : 0, cz1 = D > 2 ? gather_cell_hi(P, 2, zl) : 0;
+  const int* bx = P.gather_box;
+  const int* by = bx + 2 * nx;
+  const int* bz = by + 2 * ny;
+  const int cx0 = ld(bx + x0), cx1 = ld(bx + nx + xl);
+  const int cy0 = D > 1 ? ld(by + y0) : 0, cy1 = D > 1 ? ld(by + ny + yl) : 0;
+  const int cz0 = D > 2 ? ld(bz + z0) : 0, cz1 = D > 2 ? ld(bz + nz + zl) : 0;
   const int nry = cy1 - cy0 + 1, nrows = nry * (cz1 - cz0 + 1);
   bool crowded = nrows > 32;
   int ne = 0;  // entries of the warp list
