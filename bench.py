@@ -1166,6 +1166,11 @@ def main():
                     help="print only the implicit-medium (DGADI) lines, without the CPU checker")
     ap.add_argument("--rods-only", action="store_true",
                     help="print only the rods2D line, without the CPU checker")
+    ap.add_argument("--medium-only", action="store_true",
+                    help="print only the 3D explicit-medium line")
+    ap.add_argument("--medium-n", type=int, default=256, help="nodes per axis of the 3D medium")
+    ap.add_argument("--medium-agents", type=int, default=200_000)
+    ap.add_argument("--medium-steps", type=int, default=50)
     ap.add_argument("--config-steps", type=int, default=200)
     ap.add_argument("--config-cpu-steps", type=int, default=5)
     ap.add_argument("--config-f64-steps", type=int, default=10)
@@ -1178,6 +1183,12 @@ def main():
         return
     if args.rods_only:
         print(json.dumps({"rods": run_rods(cpu=False), "rods_growth": run_rods_growth()}))
+        return
+    if args.medium_only:
+        cbm = load_package()
+        print(json.dumps({"medium_3d_ftcs": run_medium_3d(
+            cbm, cbm._abi, n_medium=args.medium_n, agents=args.medium_agents,
+            steps=args.medium_steps)}))
         return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

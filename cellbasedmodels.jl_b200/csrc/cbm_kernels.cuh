@@ -592,33 +592,41 @@ __device__ __forceinline__ void secrete_node(const Params<T>& P, int n) {
 }
 
 // The gather by patches: one warp takes the runs of 32 nodes along x of a
-// 2 x 2 patch of (y, z) rows (2 rows in 2D, 1 in 1D), four nodes a lane in
-// 3D.  The union of the patch nodes' cell boxes is read at once: each lane
+// patch of rows (2 x 2 (y, z) rows in 3D, 4 rows in 2D, 1 in 1D), four nodes a
+// lane.  The union of the patch nodes' cell boxes is read at once: each lane
 // takes one row of cells (one (y, z) pair of the box; its agents are
 // contiguous slots), a warp scan numbers the candidates, and every lane takes
 // one candidate of a chunk, computes its stencil (bilinear_axes, the
 // expressions of bilinear()) and the patch nodes it falls on.  The agents
-// that touch the patch are appended to a warp list, the list is ranked by
-// agent index, and each lane adds the terms of its nodes in that order (and
-// in stencil order within an agent), the sums of secrete_node.  A patch whose
-// box has more than 32 rows, or that more than 32 agents touch, falls back to
-// secrete_node for each of its nodes.  A node that no agent touches keeps its
-// value and is not written.
+// that touch the patch are appended to a warp list, and the list is ranked
+// by agent index.  The patch's values and net rates sit in shared memory;
+// entry by entry in rank order, the lanes of the entry's stencil nodes add
+// their terms (one lane in stencil order when a clamped stencil repeats a
+// node), so each node sums its terms in agent order and, within an agent, in
+// stencil order: the sums of secrete_node.  A patch whose box has more than
+// 32 rows, or that more than kCap agents touch, falls back to secrete_node
+// for each of its nodes.  A node that no agent touches keeps its value and is
+// not written.
 constexpr int kRowWarps = 8;  // warps (patches) per block of k_secrete_rows
 
 template <int D>
 struct GatherPatch {
-  static constexpr int kY = D > 1 ? 2 : 1, kZ = D > 2 ? 2 : 1, kRuns = kY * kZ;
+  static constexpr int kY = D == 2 ? 4 : (D == 3 ? 2 : 1), kZ = D > 2 ? 2 : 1;
+  static constexpr int kRuns = kY * kZ;
+  static constexpr int kCap = D == 3 ? 32 : 64;  // entries of the warp list
 };
 
 template <typename T, int D>
 __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P) {
   constexpr int K = 1 << D;
   constexpr int PY = GatherPatch<D>::kY, PZ = GatherPatch<D>::kZ, NP = GatherPatch<D>::kRuns;
-  __shared__ int s_j[kRowWarps][32];
-  __shared__ unsigned char s_code[kRowWarps][32][K];  // run * 32 + lane of stencil node k, or 0xff
-  __shared__ T s_w[kRowWarps][32][K];
-  __shared__ unsigned char s_perm[kRowWarps][32];
+  constexpr int CAP = GatherPatch<D>::kCap;
+  __shared__ int s_j[kRowWarps][CAP];                  // agent index of entry e (+ repeat flag)
+  __shared__ unsigned char s_code[kRowWarps][CAP][K];  // run * 32 + lane of stencil node k, or 0xff
+  __shared__ T s_w[kRowWarps][CAP][K];
+  __shared__ unsigned char s_perm[kRowWarps][CAP];
+  __shared__ T s_acc[kRowWarps][NP * 32], s_net[kRowWarps][NP * 32];
+  __shared__ unsigned char s_tch[kRowWarps][NP * 32];
   const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
   const int nx = P.n_medium[0];
   const int ny = D > 1 ? P.n_medium[1] : 1, nz = D > 2 ? P.n_medium[2] : 1;
@@ -671,7 +679,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
       const int rr = r < 31 ? r : 31;
       const int sl = __shfl_sync(kFull, s0, rr) + m - (__shfl_sync(kFull, inc, rr) -
                                                        __shfl_sync(kFull, cnt, rr));
-      bool hit = false;
+      bool hit = false, repeat = false;
       unsigned char code[K];
       T w[K];
       int j = 0;
@@ -682,6 +690,8 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
         int i0[3] = {0, 0, 0}, i1[3] = {0, 0, 0};
         T tt[3];
         bilinear_axes<T, D>(P, x, i0, i1, tt);
+#pragma unroll
+        for (int d = 0; d < D; ++d) repeat = repeat || i0[d] == i1[d];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
           const int ix = (k & 1) ? i1[0] : i0[0];
@@ -697,13 +707,14 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
         }
       }
       const unsigned hits = __ballot_sync(kFull, hit);
-      if (ne + __popc(hits) > 32) {
+      if (ne + __popc(hits) > CAP) {
         crowded = true;
         break;
       }
       if (hit) {
         const int e = ne + __popc(hits & below);
         s_j[wb][e] = j;
+        s_perm[wb][e] = repeat ? 1 : 0;  // the repeat flag until the ranks are in
 #pragma unroll
         for (int k = 0; k < K; ++k) {
           s_code[wb][e][k] = code[k];
@@ -722,40 +733,59 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
     return;
   }
   if (ne == 0) return;
-  __syncwarp();
-  if (lane < ne) {  // rank by agent index (the indices are distinct)
-    const int j = s_j[wb][lane];
-    int r = 0;
-    for (int e = 0; e < ne; ++e) r += s_j[wb][e] < j;
-    s_perm[wb][r] = (unsigned char)lane;
-  }
-  __syncwarp();
   const T amt = P.secretion_amt;
   const bool upt = P.uptake_amt != (T)0;
-  T acc[NP], net[NP];
-  bool touched[NP];
 #pragma unroll
   for (int p = 0; p < NP; ++p) {
-    net[p] = upt ? amt - P.uptake_amt * c_com[p] : amt;  // secretion - first-order uptake
-    acc[p] = c_com[p];
-    touched[p] = false;
+    s_acc[wb][p * 32 + lane] = c_com[p];
+    s_net[wb][p * 32 + lane] = upt ? amt - P.uptake_amt * c_com[p] : amt;  // secretion - uptake
+    s_tch[wb][p * 32 + lane] = 0;
   }
-  for (int r = 0; r < ne; ++r) {
-    const int e = s_perm[wb][r];
+  __syncwarp();
+  // rank by agent index (the indices are distinct); the order is kept as
+  // (rank -> entry) with the entry's repeat flag in bit 7
+  int rank[CAP / 32], flag[CAP / 32];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int c = s_code[wb][e][k];
-#pragma unroll
-      for (int p = 0; p < NP; ++p)
-        if (c == p * 32 + lane) {
-          acc[p] = acc[p] + s_w[wb][e][k] * net[p];
-          touched[p] = true;
-        }
+  for (int h = 0; h < CAP / 32; ++h) {
+    const int e = h * 32 + lane;
+    rank[h] = -1;
+    if (e < ne) {
+      const int j = s_j[wb][e];
+      int r = 0;
+      for (int f = 0; f < ne; ++f) r += s_j[wb][f] < j;
+      rank[h] = r;
+      flag[h] = s_perm[wb][e];
     }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int h = 0; h < CAP / 32; ++h)
+    if (rank[h] >= 0) s_perm[wb][rank[h]] = (unsigned char)((h * 32 + lane) | (flag[h] << 7));
+  __syncwarp();
+  for (int r = 0; r < ne; ++r) {
+    const int pe = s_perm[wb][r];
+    const int e = pe & 0x7f;
+    if (pe & 0x80) {  // a clamped stencil: its nodes in stencil order by one lane
+      if (lane == 0)
+        for (int k = 0; k < K; ++k) {
+          const int c = s_code[wb][e][k];
+          if (c != 0xff) {
+            s_acc[wb][c] = s_acc[wb][c] + s_w[wb][e][k] * s_net[wb][c];
+            s_tch[wb][c] = 1;
+          }
+        }
+    } else if (lane < K) {  // distinct nodes: one lane each
+      const int c = s_code[wb][e][lane];
+      if (c != 0xff) {
+        s_acc[wb][c] = s_acc[wb][c] + s_w[wb][e][lane] * s_net[wb][c];
+        s_tch[wb][c] = 1;
+      }
+    }
+    __syncwarp();
   }
 #pragma unroll
   for (int p = 0; p < NP; ++p)
-    if (mine[p] && touched[p]) P.c_cur[node[p]] = acc[p];
+    if (mine[p] && s_tch[wb][p * 32 + lane]) P.c_cur[node[p]] = s_acc[wb][p * 32 + lane];
 }
 
 // ---------------------------------------------------------------------------
