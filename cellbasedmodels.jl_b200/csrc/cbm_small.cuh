@@ -182,8 +182,13 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_steps(Params<T> P0, Par
     const int p = P.parity;
     const int N = (int)C->N[p];
     // DE, kSmallLanes lanes an agent; the histogram of the new cells follows
-    // in the same phase (the agent's own written position is all it reads)
-    for (int s = tid / kSmallLanes; s < N; s += nth / kSmallLanes) {
+    // in the same phase (the agent's own written position is all it reads).
+    // Slots are dealt to the blocks in turn (slot s to block s mod blocks),
+    // so every block holds agents from all over the community and the dense
+    // clumps do not all fall to the same block.
+    const int groups = kSmallThreads / kSmallLanes;
+    for (int s = (int)(threadIdx.x / kSmallLanes) * (int)gridDim.x + (int)blockIdx.x; s < N;
+         s += groups * (int)gridDim.x) {
       small_de<T, D>(P, s);
       if ((threadIdx.x & (kSmallLanes - 1)) == 0) {  // k_sort_hist
         T x[3];
