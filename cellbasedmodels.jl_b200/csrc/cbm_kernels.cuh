@@ -600,10 +600,10 @@ __device__ __forceinline__ void secrete_node(const Params<T>& P, int n) {
 // expressions of bilinear()) and the patch nodes it falls on.  The agents
 // that touch the patch are appended to a warp list, and the list is ranked
 // by agent index.  The patch's values and net rates sit in shared memory;
-// entry by entry in rank order, the lanes of the entry's stencil nodes add
-// their terms (one lane in stencil order when a clamped stencil repeats a
-// node), so each node sums its terms in agent order and, within an agent, in
-// stencil order: the sums of secrete_node.  A patch whose box has more than
+// groups of ranked entries add their terms with one lane per (entry, stencil
+// node), in rounds that order the lanes sharing a node, so each node sums its
+// terms in agent order and, within an agent, in stencil order: the sums of
+// secrete_node.  A patch whose box has more than
 // 32 rows, or that more than kCap agents touch, falls back to secrete_node
 // for each of its nodes.  A node that no agent touches keeps its value and is
 // not written.
@@ -621,7 +621,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
   constexpr int K = 1 << D;
   constexpr int PY = GatherPatch<D>::kY, PZ = GatherPatch<D>::kZ, NP = GatherPatch<D>::kRuns;
   constexpr int CAP = GatherPatch<D>::kCap;
-  __shared__ int s_j[kRowWarps][CAP];                  // agent index of entry e (+ repeat flag)
+  __shared__ int s_j[kRowWarps][CAP];                  // agent index of entry e
   __shared__ unsigned char s_code[kRowWarps][CAP][K];  // run * 32 + lane of stencil node k, or 0xff
   __shared__ T s_w[kRowWarps][CAP][K];
   __shared__ unsigned char s_perm[kRowWarps][CAP];
@@ -679,7 +679,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
       const int rr = r < 31 ? r : 31;
       const int sl = __shfl_sync(kFull, s0, rr) + m - (__shfl_sync(kFull, inc, rr) -
                                                        __shfl_sync(kFull, cnt, rr));
-      bool hit = false, repeat = false;
+      bool hit = false;
       unsigned char code[K];
       T w[K];
       int j = 0;
@@ -690,8 +690,6 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
         int i0[3] = {0, 0, 0}, i1[3] = {0, 0, 0};
         T tt[3];
         bilinear_axes<T, D>(P, x, i0, i1, tt);
-#pragma unroll
-        for (int d = 0; d < D; ++d) repeat = repeat || i0[d] == i1[d];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
           const int ix = (k & 1) ? i1[0] : i0[0];
@@ -714,7 +712,6 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
       if (hit) {
         const int e = ne + __popc(hits & below);
         s_j[wb][e] = j;
-        s_perm[wb][e] = repeat ? 1 : 0;  // the repeat flag until the ranks are in
 #pragma unroll
         for (int k = 0; k < K; ++k) {
           s_code[wb][e][k] = code[k];
@@ -742,46 +739,51 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
     s_tch[wb][p * 32 + lane] = 0;
   }
   __syncwarp();
-  // rank by agent index (the indices are distinct); the order is kept as
-  // (rank -> entry) with the entry's repeat flag in bit 7
-  int rank[CAP / 32], flag[CAP / 32];
+  // rank by agent index (the indices are distinct): s_perm[rank] = entry
 #pragma unroll
   for (int h = 0; h < CAP / 32; ++h) {
     const int e = h * 32 + lane;
-    rank[h] = -1;
+    int r = -1;
     if (e < ne) {
       const int j = s_j[wb][e];
-      int r = 0;
+      r = 0;
       for (int f = 0; f < ne; ++f) r += s_j[wb][f] < j;
-      rank[h] = r;
-      flag[h] = s_perm[wb][e];
-    }
-  }
-  __syncwarp();
-#pragma unroll
-  for (int h = 0; h < CAP / 32; ++h)
-    if (rank[h] >= 0) s_perm[wb][rank[h]] = (unsigned char)((h * 32 + lane) | (flag[h] << 7));
-  __syncwarp();
-  for (int r = 0; r < ne; ++r) {
-    const int pe = s_perm[wb][r];
-    const int e = pe & 0x7f;
-    if (pe & 0x80) {  // a clamped stencil: its nodes in stencil order by one lane
-      if (lane == 0)
-        for (int k = 0; k < K; ++k) {
-          const int c = s_code[wb][e][k];
-          if (c != 0xff) {
-            s_acc[wb][c] = s_acc[wb][c] + s_w[wb][e][k] * s_net[wb][c];
-            s_tch[wb][c] = 1;
-          }
-        }
-    } else if (lane < K) {  // distinct nodes: one lane each
-      const int c = s_code[wb][e][lane];
-      if (c != 0xff) {
-        s_acc[wb][c] = s_acc[wb][c] + s_w[wb][e][lane] * s_net[wb][c];
-        s_tch[wb][c] = 1;
-      }
     }
     __syncwarp();
+    if (r >= 0) s_perm[wb][r] = (unsigned char)e;
+  }
+  __syncwarp();
+  // The ranked entries in groups of 32 / K, one lane per (entry, stencil
+  // node), lanes in rank order and, within an entry, in stencil order.  Lanes
+  // whose nodes coincide (a later entry on the same node, or a clamped
+  // stencil that repeats a node) are ordered by lane: a lane's round is the
+  // number of lower lanes with its node, and the rounds are applied in turn,
+  // so every node takes its terms in rank and stencil order.
+  constexpr int G = 32 / K;
+  const int ge = lane / K, gk = lane % K;
+  const unsigned lower = (1u << lane) - 1u;
+  for (int base = 0; base < ne; base += G) {
+    const int r = base + ge;
+    int c = -1;
+    T t = (T)0;
+    if (r < ne) {
+      const int e = s_perm[wb][r];
+      const int code = s_code[wb][e][gk];
+      if (code != 0xff) {
+        c = code;
+        t = s_w[wb][e][gk];
+      }
+    }
+    const unsigned same = __match_any_sync(kFull, c >= 0 ? c : 256 + lane);
+    const int round = c >= 0 ? __popc(same & lower) : 0;
+    const int rounds = __reduce_max_sync(kFull, (unsigned)round) + 1;
+    for (int q = 0; q < rounds; ++q) {
+      if (c >= 0 && round == q) {
+        s_acc[wb][c] = s_acc[wb][c] + t * s_net[wb][c];
+        s_tch[wb][c] = 1;
+      }
+      __syncwarp();
+    }
   }
 #pragma unroll
   for (int p = 0; p < NP; ++p)
