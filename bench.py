@@ -359,20 +359,38 @@ def run_ours(args, rank, world, local_rank):
         ctx.upload(state)
     stream = torch.cuda.ExternalStream(ctx.stream())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    # every kernel of the step graph bracketed by events on the library's
-    # stream, read after each timed replay
-    ctx.set_kernel_timing(True)
-    kernel_timing = "events inside the timed graph replays"
-
-    for _ in range(args.warmup):
+    # Warm-up: the first steps build the step graphs of both parities; the
+    # last k of them (k = min(5, W - 2)) carry an event pair around every
+    # kernel (graphs of their own), read after each replay, for the per-kernel
+    # times.  Event nodes cost a few microseconds a kernel, so the K timed
+    # steps that follow carry none.
+    n_kern = max(1, min(5, args.warmup - 2))
+    kern = {}  # kernel -> [ms of each launch]
+    kern_agent_steps = 0
+    kernel_timing = "events inside the graph replays of the last warm-up steps"
+    for w in range(args.warmup):
+        timed_kernels = w >= args.warmup - n_kern
+        if timed_kernels and w == args.warmup - n_kern:
+            ctx.set_kernel_timing(True)
+        n_before = ctx.counters()["N"]
         ctx.step(1, abi.SYNC)
+        if timed_kernels and kernel_timing.startswith("events"):
+            try:
+                for name, ms in ctx.kernel_times():
+                    kern.setdefault(name, []).append(ms)
+                kern_agent_steps += n_before
+            except cbm.CbmError as err:
+                kernel_timing = f"eager steps after the timed region ({err})"
+                kern = {}
+        flush.zero_()
+        torch.cuda.synchronize()
+    ctx.set_kernel_timing(False)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(local_rank)
     clocks.start()
     total_ms, agent_steps = 0.0, 0
-    kern = {}  # kernel -> [ms of each timed launch]
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     for _ in range(args.steps):
@@ -383,21 +401,15 @@ def run_ours(args, rank, world, local_rank):
         e1.synchronize()
         total_ms += e0.elapsed_time(e1)
         agent_steps += n_before
-        if kernel_timing.startswith("events inside"):
-            try:
-                for name, ms in ctx.kernel_times():
-                    kern.setdefault(name, []).append(ms)
-            except cbm.CbmError as err:
-                kernel_timing = f"eager steps after the timed region ({err})"
-                kern = {}
         flush.zero_()  # evict L2 (256 MB > 126 MB) between timed steps
         torch.cuda.synchronize()
     ctx.sync()
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ctx.set_kernel_timing(False)
     if not kern:  # the graph's event nodes could not be read: time eager steps instead
+        kern_agent_steps = 0
         for _ in range(5):
+            kern_agent_steps += ctx.counters()["N"]
             for name, ms in ctx.profile_step():
                 kern.setdefault(name, []).append(ms)
     if dist:
@@ -412,15 +424,15 @@ def run_ours(args, rank, world, local_rank):
     value = agent_steps_job / (total_ms_job / 1e3)
     ms_per_step = total_ms_job / args.steps
 
-    # roofline of the dominant kernel over the timed steps: its launches were
-    # timed inside the step graphs above, on the library's stream
+    # roofline of the dominant kernel: its launches were timed inside the
+    # step graphs above, on the library's stream
     walked = ctx.counters()["flag"] == 1
     verlet = cfg.neighbors in (abi.NEIGH_CLVD, abi.NEIGH_VERLET_DISPLACEMENT) and not walked
     nbar = float(np.mean(ctx.neighbors()[0])) if verlet else 0.0
     s = 8 if cfg.precision == abi.F64 else 4
     stats = {k: (float(np.mean(v)), float(np.sum(v))) for k, v in kern.items()}
     top = max(stats, key=lambda k: stats[k][1])
-    agents = agent_steps / args.steps  # agents per launch, averaged over the timed steps
+    agents = kern_agent_steps / len(kern[top])  # agents per launch of the kernel-timed steps
     hbm, peak_kind = peaks()
     bpa = alg_bytes_per_agent(top, s, cfg.dims, nbar, verlet, cfg.fate != abi.FATE_NONE)
     roof = None

@@ -91,7 +91,8 @@ struct cbm_ctx {
   bool loaded = false;
   int parity = 0;
   bool rule_done = false, de_done = false, mrule_done = false, mde_done = false;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};   // step graphs of each parity
+  cudaGraphExec_t tgraph[2] = {nullptr, nullptr};  // the same with kernel timing events
   // small fate-free communities: all steps of a call in one cluster launch
   long long n_loaded = 0;         // N of the last upload (fixed without births and deaths)
 
@@ -710,8 +711,10 @@ void free_all(cbm_ctx* c) {
     cudaEventDestroy(m.ev[1]);
   }
   c->marks.clear();
-  for (int q = 0; q < 2; ++q)
+  for (int q = 0; q < 2; ++q) {
     if (c->graph[q]) cudaGraphExecDestroy(c->graph[q]);
+    if (c->tgraph[q]) cudaGraphExecDestroy(c->tgraph[q]);
+  }
   for (int q = 0; q < 2; ++q) {
     for (auto& m : c->gmarks[q]) {
       cudaEventDestroy(m.ev[0]);
@@ -1236,7 +1239,8 @@ int cbm_step(cbm_ctx* c, int32_t nsteps, int32_t flags) {
   for (int s = 0; s < nsteps; ++s) {
     const int p = c->parity;
     if (use_graph) {
-      if (!c->graph[p]) {
+      cudaGraphExec_t* graphs = c->graph_timing ? c->tgraph : c->graph;
+      if (!graphs[p]) {
         cudaGraph_t g = nullptr;
         CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         if (c->graph_timing) {  // event records around each kernel become graph nodes
@@ -1251,11 +1255,11 @@ int cbm_step(cbm_ctx* c, int32_t nsteps, int32_t flags) {
         c->prof_used = nullptr;
         cudaError_t e = cudaStreamEndCapture(c->stream, &g);
         if (e != cudaSuccess) return fail(c, CBM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&c->graph[p], g, 0);
+        e = cudaGraphInstantiate(&graphs[p], g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return fail(c, CBM_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
       }
-      CUDA_TRY(c, cudaGraphLaunch(c->graph[p], c->stream));
+      CUDA_TRY(c, cudaGraphLaunch(graphs[p], c->stream));
     } else {
       dispatch<FullStep>(c, p);
       int rc = check_launch(c);
@@ -1458,14 +1462,7 @@ int cbm_set_kernel_timing(cbm_ctx* c, int32_t on) {
   if (!c) return CBM_ERR_ARG;
   cudaSetDevice(c->device);
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  if ((on != 0) != c->graph_timing) {
-    for (int q = 0; q < 2; ++q)
-      if (c->graph[q]) {
-        cudaGraphExecDestroy(c->graph[q]);
-        c->graph[q] = nullptr;
-      }
-    c->graph_timing = on != 0;
-  }
+  c->graph_timing = on != 0;  // the two sets of step graphs are kept apart
   return CBM_OK;
 }
 
@@ -1475,7 +1472,7 @@ int cbm_kernel_times(cbm_ctx* c, int32_t max_kernels, float* ms, const char** na
   if (!c->graph_timing) return fail(c, CBM_ERR_STATE, "kernel timing is off (cbm_set_kernel_timing)");
   cudaSetDevice(c->device);
   const int p = c->parity ^ 1;  // the parity of the step replayed last
-  if (!c->graph[p]) return fail(c, CBM_ERR_STATE, "no step graph has been replayed yet");
+  if (!c->tgraph[p]) return fail(c, CBM_ERR_STATE, "no step graph has been replayed yet");
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   *n_kernels = (int32_t)c->gmark_used[p];
   for (size_t q = 0; q < c->gmark_used[p] && (int)q < max_kernels; ++q) {

@@ -255,10 +255,12 @@ int cbm_kernels_per_step(cbm_ctx* ctx);
 int cbm_profile_step(cbm_ctx* ctx, int32_t max_kernels, float* ms, const char** names,
                      int32_t* n_kernels);
 /* Kernel timing inside the step graphs (no reference counterpart; the
- * reference has no stage timers).  With on != 0 the next cbm_step captures
- * its graphs with a CUDA event recorded before and after every kernel, and
- * every replay records them again; on = 0 drops them.  Either way the graphs
- * are captured again at the next step.  Synchronises the stream. */
+ * reference has no stage timers).  With on != 0, cbm_step replays a second
+ * set of step graphs (captured at first use) with a CUDA event recorded
+ * before and after every kernel, which every replay records again; on = 0
+ * goes back to the plain graphs, which stay as they were.  The small
+ * communities' single launch is not used while timing is on.  Synchronises
+ * the stream. */
 int cbm_set_kernel_timing(cbm_ctx* ctx, int32_t on);
 /* After a graph-replayed cbm_step with kernel timing on: the durations (ms)
  * and static names of the kernels of the last step replayed, up to

@@ -1,6 +1,7 @@
 """Kernel timing inside the step graphs (cbm_set_kernel_timing /
 cbm_kernel_times): every kernel of a replayed step is timed by events on the
-library's stream, and the timing changes no result."""
+library's stream, the timing changes no result, and the plain step graphs
+captured before it are replayed again after it."""
 import numpy as np
 import pytest
 
@@ -17,6 +18,7 @@ def test_kernel_times_of_graph_replays(gpu_lib, abi):
     a, b = cbm.Context(cfg), cbm.Context(cfg)
     a.upload(st)
     b.upload(st)
+    a.step(2)  # the plain graphs of both parities
     a.set_kernel_timing(True)
     for _ in range(4):
         a.step(1)
@@ -27,7 +29,7 @@ def test_kernel_times_of_graph_replays(gpu_lib, abi):
         assert all(ms > 0 for _, ms in times)
     a.set_kernel_timing(False)
     a.step(3)
-    b.step(7)
+    b.step(9)
     sa, sb = a.download(), b.download()
     for k in ("x", "y", "z", "v", "id"):
         np.testing.assert_array_equal(sa[k], sb[k], err_msg=k)
