@@ -79,6 +79,7 @@ struct cbm_ctx {
   int n_sm = 148;             // multiprocessors of the device (grid of the compaction)
   int de_blocks = 1;          // persistent grid of the force kernel
   void* pair_list = nullptr;  // its partner lists (cell walks only)
+  void* pos32 = nullptr;      // Float64 3D cell walks: positions rounded to Float32
   void* stage[3] = {nullptr, nullptr, nullptr};  // Heun / RK4: h, running sum, derivative
   int n_cells = 1;
   int n_cells_d[3] = {1, 1, 1};
@@ -252,6 +253,7 @@ Params<T> params(const cbm_ctx* c, int parity) {
   P.nbr_list = c->nbr_list;
   P.pair_list = (int4*)c->pair_list;
   P.pair_cap4 = kPairCap4;
+  P.PA32 = (float4*)c->pos32;
   P.c_cur = (T*)c->c[p];
   P.c_nxt = (T*)c->c[q];
   P.ctr = c->ctr;
@@ -460,6 +462,10 @@ template <typename T, int D>
 void enqueue_agent_de(cbm_ctx* c, const Params<T>& P) {
   const unsigned grid = kPartnerLists<D> ? c->de_blocks : c->n_blocks;
   const int integ = c->cfg.integrator;
+  if (c->pos32) {
+    PROF("k_pos32");
+    k_pos32<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+  }
   if (integ != CBM_INT_HEUN && integ != CBM_INT_RK4 && integ != CBM_INT_EULER_HEUN) {
     PROF("k_agent_de");
     k_agent_de<T, D><<<grid, kTile, 0, c->stream>>>(P);
@@ -562,6 +568,7 @@ int kernels_per_step(const cbm_ctx* c) {
   if (rule_needed(k)) n += 1;           // rule (with births and deaths when fate is on)
   if (k.fate != CBM_FATE_NONE) n += 1;  // compaction
   n += 1;                               // agent DE
+  if (c->pos32) n += 1;                 // its Float32 positions (Float64 3D walks)
   if (k.medium) n += 1;
   n += 5;                               // commit, sort hist, scan, scatter, place
   if (k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT) n += 1;
@@ -915,6 +922,7 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     c->de_blocks = (int)(resident < c->n_blocks ? resident : c->n_blocks);
     if (cells && k.dims == 3)
       c->pair_list = dalloc(c, (size_t)c->de_blocks * kTile * kPairCap4 * sizeof(int4), &ok);
+    if (cells && k.dims == 3 && c->tsize == 8) c->pos32 = dalloc(c, n * sizeof(float4), &ok);
   }
   if (list) {
     c->nbr_n = (int*)dalloc(c, n * 4, &ok);

@@ -93,6 +93,9 @@ struct Params {
   // blocks of four slots per thread (block j of thread t at j * kTile + t)
   int4* pair_list;
   int pair_cap4;
+  // Float64 3D cell walks: the committed positions rounded to Float32, in
+  // slot order, for the walk's filter (k_pos32); null otherwise
+  float4* PA32;
   // medium: committed / written
   T* c_cur;
   T* c_nxt;
@@ -1168,6 +1171,45 @@ __device__ __forceinline__ T filter_s2(const T* xi, const T* xj) {
   }
 }
 
+// Float32 squared distance of the filter from a rounded Float64 position
+// (the packed form of filter_s2<float, 3>).
+__device__ __forceinline__ float filter_s2_f32(const float* xi, const float4 v) {
+  const float2 d = f2_sub(make_float2(xi[0], xi[1]), make_float2(v.x, v.y));
+  const float2 q = f2_mul(d, d);
+  const float dz = xi[2] - v.z;
+  return __fmaf_rn(dz, dz, q.x + q.y);
+}
+
+// Bound of the Float32 filter of a Float64 walk for an agent at xi: every
+// pair whose Float64 squared distance passes the evaluation's test s2 < cut2
+// has a Float32 one (positions rounded to nearest, filter_s2_f32) below it.
+// With u = 2^-24, X = max_k |xi_k| and c = sqrt(cut2) (1 + 1e-15) the exact
+// distance is below c, so |xj_k| <= X + c and each Float32 difference is
+// within E = u (2X + 2c)(1 + u) of the exact one; three roundings of the
+// squares and sums give s2_32 < (1 + u)^3 (c + sqrt(3) E)^2 (Minkowski).  The
+// bound is formed in Float64 with a relative margin of 1e-12 for its own
+// roundings and rounded up to Float32.
+__device__ __forceinline__ float f32_filter_bound(const double* xi, double cut2) {
+  const double u = 5.9604644775390625e-08;
+  double X = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) X = fmax(X, fabs(xi[d]));
+  const double c = sqrt(cut2) * (1.0 + 1e-15);
+  const double E = u * (2.0 * X + 2.0 * c) * (1.0 + u);
+  const double r = c + 1.7320508075688775 * E;
+  return __double2float_ru(r * r * (1.0 + 4.0 * u) * (1.0 + 1e-12));
+}
+
+// PA32 = the committed positions rounded to Float32 (slots below N).
+template <typename T>
+__global__ void __launch_bounds__(kTile) k_pos32(Params<T> P) {
+  const int N = (int)P.ctr->N[P.parity];
+  for (int s = blockIdx.x * kTile + threadIdx.x; s < N; s += gridDim.x * kTile) {
+    const typename V4T<T>::type v = P.PA[s];
+    P.PA32[s] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.f);
+  }
+}
+
 // The end of agentStepDE! for slot s once its pair forces are summed in acc:
 // pushing walls, the lagged force, linear drift and chemotaxis, then the
 // integrator (Euler or Euler-Maruyama), the commit of the written slot and
@@ -1427,8 +1469,42 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
       // the slot's cell is the grid's assignment of the committed position,
       // which the walk starts from unless the rule reflected it off a wall
       const int own_cell = (reflect || P.XS) ? -1 : ld(P.cell_of_slot + s);
+      // Float64 walks filter in Float32 on the rounded copy of the positions,
+      // with the bound widened for the rounding; the evaluation's exact test
+      // decides every queued pair
+      const float4* U32 = nullptr;
+      float xi32[3] = {0.f, 0.f, 0.f};
+      float cut2f32 = 0.f;
+      if constexpr (std::is_same<T, double>::value && D == 3) {
+        if (P.PA32 && U == P.PA) {
+          U32 = P.PA32;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) xi32[d] = (float)xi[d];
+          cut2f32 = f32_filter_bound(xi, (double)cut2);
+        }
+      }
       walk_runs<T, D>(P, xi, P.cut_reach, [&](int s0, int s1) {
         int q = s0;
+        if constexpr (std::is_same<T, double>::value && D == 3) {
+          if (U32) {
+            for (; q + 4 <= s1; q += 4) {
+              room(4);
+              float s2v[4];
+#pragma unroll
+              for (int u = 0; u < 4; ++u) s2v[u] = filter_s2_f32(xi32, U32[q + u]);
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                queue[nq * kTile + threadIdx.x] = q + u;
+                nq += s2v[u] < cut2f32 ? 1 : 0;
+              }
+            }
+            for (; q < s1; ++q) {
+              room(1);
+              if (filter_s2_f32(xi32, U32[q]) < cut2f32) push(q);
+            }
+            return;
+          }
+        }
         for (; q + 4 <= s1; q += 4) {
           room(4);
           T s2v[4];
