@@ -6,6 +6,9 @@ at their configured sizes.
   10^6 agents in Float32;
 - the 2D aggregation as configured: 4096 agents, Float64, 1000 steps;
 - the 2D chemotaxis as configured: 2x10^5 agents on a 1024^2 medium, 100 steps;
+- the 3D medium line as benched: 2x10^5 agents on a 256^3 medium with
+  secretion, uptake and chemotaxis, 20 steps (TMA-fed stencils, gather by
+  patches);
 - communities of the batched sweep, compared with the checker directly;
 - trajectory gradients of the 65536-agent adjoint problem (200 steps,
   checkpoint every 20) against the checker's forward-mode dual numbers.
@@ -22,7 +25,7 @@ import pytest
 import conftest
 from _oracle import OracleContext, oracle_adjoint_dual
 from scenarios import (adjoint_problem, aggregation_2d, batched_sweep, chemotaxis_2d,
-                       growing_colony_3d, make_descs, plain_config_for)
+                       growing_colony_3d, make_descs, medium_colony, plain_config_for)
 from test_gpu_parity import assert_same_grid, assert_same_lists, assert_same_state
 
 cbm = conftest.cbm
@@ -131,6 +134,26 @@ def test_chemotaxis_2d_as_configured(gpu_lib, abi):
         g.step(50)
         o.step(50)
         assert_same_state(g.download(), o.download(), ["x", "y", "c", "gx", "gy"])
+    assert_same_grid(g, o)
+
+
+def test_medium_3d_as_benched(gpu_lib, abi):
+    """The 3D medium line: 2x10^5 agents on a 256^3 Float32 field (unit
+    spacing, secretion, first-order uptake, chemotaxis, EM noise), the field
+    drawn from U(0, 1) with seed 9: 20 steps, bit-exact, field and gradient
+    included."""
+    n = 256
+    kw, st = medium_colony(abi, 3, N=200_000, L=float(n), n_medium=n)
+    st["c"] = np.random.default_rng(9).uniform(0.0, 1.0, n ** 3).astype(np.float32)
+    cfg = abi.make_config(**kw)
+    g = cbm.Context(cfg)
+    o = OracleContext(abi, cfg, threads=THREADS)
+    g.upload(st)
+    o.upload(st)
+    for _ in range(2):
+        g.step(10)
+        o.step(10)
+        assert_same_state(g.download(), o.download(), ["x", "y", "z", "c", "gx", "gy", "gz"])
     assert_same_grid(g, o)
 
 
