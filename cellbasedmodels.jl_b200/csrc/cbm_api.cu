@@ -444,9 +444,10 @@ void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P) {
     const int nm[3] = {c->cfg.n_medium[0], D > 1 ? c->cfg.n_medium[1] : 1,
                        D > 2 ? c->cfg.n_medium[2] : 1};
     const int py = (nm[1] + GatherPatch<D>::kY - 1) / GatherPatch<D>::kY;
-    const dim3 grid((unsigned)((nm[0] + 31) / 32), (unsigned)((py + kRowWarps - 1) / kRowWarps),
+    constexpr int W = GatherPatch<D>::kWarps;
+    const dim3 grid((unsigned)((nm[0] + 31) / 32), (unsigned)((py + W - 1) / W),
                     (unsigned)((nm[2] + GatherPatch<D>::kZ - 1) / GatherPatch<D>::kZ));
-    k_secrete_rows<T, D><<<grid, kRowWarps * 32, 0, c->stream>>>(P);
+    k_secrete_rows<T, D><<<grid, W * 32, 0, c->stream>>>(P);
   }
   if (!rule_needed(k)) return;
   if (k.fate != CBM_FATE_NONE) {

@@ -595,61 +595,62 @@ __device__ __forceinline__ void secrete_node(const Params<T>& P, int n) {
 }
 
 // The gather by patches: one warp takes the runs of 32 nodes along x of a
-// patch of rows (2 x 2 (y, z) rows in 3D, 4 rows in 2D, 1 in 1D), four nodes a
-// lane.  The union of the patch nodes' cell boxes is read at once: each lane
-// takes one row of cells (one (y, z) pair of the box; its agents are
-// contiguous slots), a warp scan numbers the candidates, and every lane takes
-// one candidate of a chunk, computes its stencil (bilinear_axes, the
-// expressions of bilinear()) and the patch nodes it falls on.  The agents
-// that touch the patch are appended to a warp list, and the list is ranked
-// by agent index.  The patch's values and net rates sit in shared memory;
-// groups of ranked entries add their terms with one lane per (entry, stencil
-// node), in rounds that order the lanes sharing a node, so each node sums its
-// terms in agent order and, within an agent, in stencil order: the sums of
-// secrete_node.  A patch whose box has more than
-// 32 rows, or that more than kCap agents touch, falls back to secrete_node
-// for each of its nodes.  A node that no agent touches keeps its value and is
-// not written.
-constexpr int kRowWarps = 8;  // warps (patches) per block of k_secrete_rows
-
+// patch of rows (4 x 4 (y, z) rows in 3D, 4 rows in 2D, 1 in 1D).  The
+// patch's committed values and net rates are loaded into shared memory.  The
+// union of the patch nodes' cell boxes is read at once: each lane takes one
+// row of cells (one (y, z) pair of the box; its agents are contiguous slots),
+// a warp scan numbers the candidates, and every lane takes one candidate of a
+// chunk, computes its stencil (bilinear_axes, the expressions of bilinear())
+// and the patch nodes it falls on.  The agents that touch the patch are
+// appended to a warp list, and the list is ranked by agent index.  Groups of
+// ranked entries add their terms with one lane per (entry, stencil node), in
+// rounds that order the lanes sharing a node, so each node sums its terms in
+// agent order and, within an agent, in stencil order: the sums of
+// secrete_node.  A patch whose box has more than 32 rows, or that more than
+// kCap agents touch, falls back to secrete_node for each of its nodes.  A
+// node that no agent touches keeps its value and is not written.
 template <int D>
 struct GatherPatch {
-  static constexpr int kY = D == 2 ? 4 : (D == 3 ? 2 : 1), kZ = D > 2 ? 2 : 1;
-  static constexpr int kRuns = kY * kZ;
-  static constexpr int kCap = D == 3 ? 32 : 64;  // entries of the warp list
+  static constexpr int kY = D >= 2 ? 4 : 1, kZ = D > 2 ? 4 : 1;
+  static constexpr int kRuns = kY * kZ;                // runs of 32 nodes a patch
+  static constexpr int kCap = D == 3 ? 32 : 64;       // entries of the warp list
+  static constexpr int kWarps = D == 3 ? 4 : 8;       // patches a block
 };
+constexpr unsigned short kNoNode = 0xffff;
 
 template <typename T, int D>
-__global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P) {
+__global__ void __launch_bounds__(GatherPatch<D>::kWarps * 32) k_secrete_rows(Params<T> P) {
   constexpr int K = 1 << D;
   constexpr int PY = GatherPatch<D>::kY, PZ = GatherPatch<D>::kZ, NP = GatherPatch<D>::kRuns;
-  constexpr int CAP = GatherPatch<D>::kCap;
-  __shared__ int s_j[kRowWarps][CAP];                  // agent index of entry e
-  __shared__ unsigned char s_code[kRowWarps][CAP][K];  // run * 32 + lane of stencil node k, or 0xff
-  __shared__ T s_w[kRowWarps][CAP][K];
-  __shared__ unsigned char s_perm[kRowWarps][CAP];
-  __shared__ T s_acc[kRowWarps][NP * 32], s_net[kRowWarps][NP * 32];
-  __shared__ unsigned char s_tch[kRowWarps][NP * 32];
+  constexpr int CAP = GatherPatch<D>::kCap, W = GatherPatch<D>::kWarps;
+  __shared__ int s_j[W][CAP];                   // agent index of entry e
+  __shared__ unsigned short s_code[W][CAP][K];  // run * 32 + lane of stencil node k, or kNoNode
+  __shared__ T s_w[W][CAP][K];
+  __shared__ unsigned char s_perm[W][CAP];
+  __shared__ T s_acc[W][NP * 32], s_net[W][NP * 32];
+  __shared__ unsigned char s_tch[W][NP * 32];
   const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
   const int nx = P.n_medium[0];
   const int ny = D > 1 ? P.n_medium[1] : 1, nz = D > 2 ? P.n_medium[2] : 1;
   // grid: x runs, y patches (a block's warps), z patches
   const int x0 = blockIdx.x * 32;
-  const int y0 = (blockIdx.y * kRowWarps + wb) * PY, z0 = blockIdx.z * PZ;
+  const int y0 = (blockIdx.y * W + wb) * PY, z0 = blockIdx.z * PZ;
   if (y0 >= ny) return;  // the whole warp
   const int xl = min(x0 + 31, nx - 1), yl = min(y0 + PY - 1, ny - 1), zl = min(z0 + PZ - 1, nz - 1);
   const int qx = x0 + lane;
-  // the lane's nodes (run p: y0 + p % PY, z0 + p / PY) and their committed
-  // values (this lane is their only writer; read early, used last)
-  int node[NP];
-  bool mine[NP];
-  T c_com[NP];
+  // the lane's nodes (run p: y0 + p % PY, z0 + p / PY): committed values
+  // (this lane is their only writer) and net rates, secretion - uptake
+  {
+    const T amt = P.secretion_amt;
+    const bool upt = P.uptake_amt != (T)0;
 #pragma unroll
-  for (int p = 0; p < NP; ++p) {
-    const int y = y0 + p % PY, z = z0 + p / PY;
-    mine[p] = qx < nx && y < ny && z < nz;
-    node[p] = qx + nx * (y + ny * z);
-    c_com[p] = mine[p] ? P.c_cur[node[p]] : (T)0;
+    for (int p = 0; p < NP; ++p) {
+      const int y = y0 + p % PY, z = z0 + p / PY;
+      const T v = (qx < nx && y < ny && z < nz) ? P.c_cur[qx + nx * (y + ny * z)] : (T)0;
+      s_acc[wb][p * 32 + lane] = v;
+      s_net[wb][p * 32 + lane] = upt ? amt - P.uptake_amt * v : amt;
+      s_tch[wb][p * 32 + lane] = 0;
+    }
   }
   const int* bx = P.gather_box;
   const int* by = bx + 2 * nx;
@@ -683,7 +684,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
       const int sl = __shfl_sync(kFull, s0, rr) + m - (__shfl_sync(kFull, inc, rr) -
                                                        __shfl_sync(kFull, cnt, rr));
       bool hit = false;
-      unsigned char code[K];
+      unsigned short code[K];
       T w[K];
       int j = 0;
       if (m < m_all) {
@@ -702,7 +703,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
           if (D > 1) on = on && iy >= y0 && iy <= yl;
           if (D > 2) on = on && iz >= z0 && iz <= zl;
           const int run = (D > 2 ? (iz - z0) * PY : 0) + (D > 1 ? iy - y0 : 0);
-          code[k] = on ? (unsigned char)(run * 32 + ix - x0) : (unsigned char)0xff;
+          code[k] = on ? (unsigned short)(run * 32 + ix - x0) : kNoNode;
           w[k] = bilinear_weight<T, D>(tt, k);
           hit = hit || on;
         }
@@ -733,14 +734,6 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
     return;
   }
   if (ne == 0) return;
-  const T amt = P.secretion_amt;
-  const bool upt = P.uptake_amt != (T)0;
-#pragma unroll
-  for (int p = 0; p < NP; ++p) {
-    s_acc[wb][p * 32 + lane] = c_com[p];
-    s_net[wb][p * 32 + lane] = upt ? amt - P.uptake_amt * c_com[p] : amt;  // secretion - uptake
-    s_tch[wb][p * 32 + lane] = 0;
-  }
   __syncwarp();
   // rank by agent index (the indices are distinct): s_perm[rank] = entry
 #pragma unroll
@@ -772,12 +765,12 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
     if (r < ne) {
       const int e = s_perm[wb][r];
       const int code = s_code[wb][e][gk];
-      if (code != 0xff) {
+      if (code != kNoNode) {
         c = code;
         t = s_w[wb][e][gk];
       }
     }
-    const unsigned same = __match_any_sync(kFull, c >= 0 ? c : 256 + lane);
+    const unsigned same = __match_any_sync(kFull, c >= 0 ? c : 65536 + lane);
     const int round = c >= 0 ? __popc(same & lower) : 0;
     const int rounds = __reduce_max_sync(kFull, (unsigned)round) + 1;
     for (int q = 0; q < rounds; ++q) {
@@ -789,8 +782,11 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4) k_secrete_rows(Params<T> P)
     }
   }
 #pragma unroll
-  for (int p = 0; p < NP; ++p)
-    if (mine[p] && s_tch[wb][p * 32 + lane]) P.c_cur[node[p]] = s_acc[wb][p * 32 + lane];
+  for (int p = 0; p < NP; ++p) {
+    const int y = y0 + p % PY, z = z0 + p / PY;
+    if (qx < nx && y < ny && z < nz && s_tch[wb][p * 32 + lane])
+      P.c_cur[qx + nx * (y + ny * z)] = s_acc[wb][p * 32 + lane];
+  }
 }
 
 // ---------------------------------------------------------------------------
