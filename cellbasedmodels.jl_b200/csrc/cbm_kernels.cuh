@@ -480,7 +480,7 @@ __global__ void k_gather_box(Params<T> P, int* box, int dims) {
 
 // The gather of one node n by one thread: the agents of its cell box that
 // touch it, sorted by index (or a k-way merge over the cells when more than
-// kTouch touch it).  The path of crowded runs of k_secrete_rows.
+// kTouch touch it).  The path of crowded patches of k_secrete_rows.
 template <typename T, int D>
 __device__ __forceinline__ void secrete_node(const Params<T>& P, int n) {
   constexpr int kMaxCells = D == 1 ? 4 : (D == 2 ? 16 : 64);
@@ -614,7 +614,7 @@ struct GatherPatch {
   static constexpr int kY = D >= 2 ? 4 : 1, kZ = D > 2 ? 4 : 1;
   static constexpr int kRuns = kY * kZ;                // runs of 32 nodes a patch
   static constexpr int kCap = D == 3 ? 32 : 64;       // entries of the warp list
-  static constexpr int kWarps = D == 3 ? 4 : 8;       // patches a block
+  static constexpr int kWarps = D == 3 ? 4 : (D == 2 ? 8 : 1);  // patches a block (along y)
 };
 constexpr unsigned short kNoNode = 0xffff;
 
