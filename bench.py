@@ -868,27 +868,18 @@ def run_rods_growth(n=32768, steps=200):
             "value": round(0.5 * (n0 + n1) * steps / (dev_ms / 1e3), 1), "unit": "rod-steps/s"}
 
 
-def run_configs(args):
-    """The other configurations of the path: the 2D aggregation (Float64,
-    L2-resident, launch-bound: us/step) and 2D chemotaxis on a 1024^2 medium
-    (agent-steps/s and medium cell-updates/s), each with the CPU checker
-    beside it; the 3D colony in Float64; and the error of every Float32 result
-    against a Float64 run of the same seeded inputs after 100 steps."""
+def run_aggregation_2d(args, cbm, abi, cpu=True):
+    """c1: the 2D aggregation, 4096 agents, Float64: the timed steps as one
+    cbm_step call (one launch of the small-community kernel), one call a step
+    for comparison, and the CPU checker beside it when `cpu`."""
     import torch
     from _oracle import OracleContext
-    from scenarios import aggregation_2d, chemotaxis_2d, colony_3d, growing_colony_3d, packed_colony_3d
-    cbm = load_package()
-    abi = cbm._abi
-    out = {}
+    from scenarios import aggregation_2d
     threads = os.cpu_count()
-
-    # c1: 2D aggregation, N=4096, Float64, 1000 steps
     kw, st = aggregation_2d(abi)
     g = cbm.Context(abi.make_config(**kw))
     g.upload(st)
     g.step(3)
-    # one cbm_step call of all the timed steps (evolve!'s saveEach steps a
-    # call): for this small fate-free community, one cooperative launch
     stream = torch.cuda.ExternalStream(g.stream())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -899,24 +890,31 @@ def run_configs(args):
     ms = e0.elapsed_time(e1)
     g.sync()
     ms_graph = _device_steps(cbm, g, 20)  # one call per step, for comparison
-    o = OracleContext(abi, abi.make_config(**kw), threads=threads)
-    o.upload(st)
-    t0 = time.perf_counter()
-    o.step(args.config_cpu_steps)
-    cpu_s = (time.perf_counter() - t0) / args.config_cpu_steps
-    o.close()
     g.close()
-    out["aggregation_2d"] = {
-        "agents": 4096, "dtype": "f64", "steps_timed": args.config_steps,
-        "us_per_step": round(1e3 * ms / args.config_steps, 2),
-        "value": round(4096 * args.config_steps / (ms / 1e3), 1), "unit": UNIT,
-        "cpu_us_per_step": round(1e6 * cpu_s, 2), "cpu_cores": threads,
-        "us_per_step_one_call_per_step": round(1e3 * ms_graph / 20, 2),
-        "note": "L2-resident: the timed steps are one cbm_step call, run by one cooperative "
-                "launch (grid barriers between the phases of a step); "
-                "us_per_step_one_call_per_step: one call (one launch) per step"}
+    rec = {"agents": 4096, "dtype": "f64", "steps_timed": args.config_steps,
+           "us_per_step": round(1e3 * ms / args.config_steps, 2),
+           "value": round(4096 * args.config_steps / (ms / 1e3), 1), "unit": UNIT,
+           "us_per_step_one_call_per_step": round(1e3 * ms_graph / 20, 2),
+           "note": "L2-resident: the timed steps are one cbm_step call, run by one launch of "
+                   "a thread-block cluster (hardware cluster barriers between the phases of a "
+                   "step); us_per_step_one_call_per_step: one call (one launch) per step"}
+    if cpu:
+        o = OracleContext(abi, abi.make_config(**kw), threads=threads)
+        o.upload(st)
+        t0 = time.perf_counter()
+        o.step(args.config_cpu_steps)
+        cpu_s = (time.perf_counter() - t0) / args.config_cpu_steps
+        o.close()
+        rec.update(cpu_us_per_step=round(1e6 * cpu_s, 2), cpu_cores=threads)
+    return rec
 
-    # c3: 2D chemotaxis, 2e5 agents, 1024^2 Float32 medium
+
+def run_chemotaxis_2d(args, cbm, abi, cpu=True):
+    """c3: 2D chemotaxis, 2x10^5 agents on a 1024^2 Float32 medium: graph
+    replays, eager per-kernel times, and the CPU checker beside it when `cpu`."""
+    from _oracle import OracleContext
+    from scenarios import chemotaxis_2d
+    threads = os.cpu_count()
     kw, st = chemotaxis_2d(abi)
     g = cbm.Context(abi.make_config(**kw))
     g.upload(st)
@@ -926,22 +924,39 @@ def run_configs(args):
     for _ in range(3):
         for name, kms in g.profile_step():
             prof.setdefault(name, []).append(kms)
-    nodes = 1024 * 1024
-    o = OracleContext(abi, abi.make_config(**kw), threads=threads)
-    o.upload(st)
-    t0 = time.perf_counter()
-    o.step(args.config_cpu_steps)
-    cpu_s = (time.perf_counter() - t0) / args.config_cpu_steps
-    o.close()
     g.close()
-    out["chemotaxis_2d"] = {
-        "agents": 200000, "medium": "1024x1024", "dtype": "f32", "steps_timed": args.config_steps,
-        "us_per_step": round(1e3 * ms / args.config_steps, 2),
-        "value": round(200000 * args.config_steps / (ms / 1e3), 1), "unit": UNIT,
-        "cell_updates_per_s": round(nodes * args.config_steps / (ms / 1e3), 1),
-        "cpu_value": round(200000 / cpu_s, 1), "cpu_cores": threads,
-        "kernel_avg_ms": {k: round(float(np.mean(v)), 4) for k, v in prof.items()},
-        "note": "bilinear secretion as an ordered gather, FTCS, chemotactic drift"}
+    nodes = 1024 * 1024
+    rec = {"agents": 200000, "medium": "1024x1024", "dtype": "f32", "steps_timed": args.config_steps,
+           "us_per_step": round(1e3 * ms / args.config_steps, 2),
+           "value": round(200000 * args.config_steps / (ms / 1e3), 1), "unit": UNIT,
+           "cell_updates_per_s": round(nodes * args.config_steps / (ms / 1e3), 1),
+           "kernel_avg_ms": {k: round(float(np.mean(v)), 4) for k, v in prof.items()},
+           "note": "bilinear secretion and uptake as an ordered gather, FTCS, chemotactic drift"}
+    if cpu:
+        o = OracleContext(abi, abi.make_config(**kw), threads=threads)
+        o.upload(st)
+        t0 = time.perf_counter()
+        o.step(args.config_cpu_steps)
+        cpu_s = (time.perf_counter() - t0) / args.config_cpu_steps
+        o.close()
+        rec.update(cpu_value=round(200000 / cpu_s, 1), cpu_cores=threads)
+    return rec
+
+
+def run_configs(args):
+    """The other configurations of the path: the 2D aggregation (Float64,
+    L2-resident, launch-bound: us/step) and 2D chemotaxis on a 1024^2 medium
+    (agent-steps/s and medium cell-updates/s), each with the CPU checker
+    beside it; the 3D colony in Float64; and the error of every Float32 result
+    against a Float64 run of the same seeded inputs after 100 steps."""
+    import torch
+    from scenarios import aggregation_2d, chemotaxis_2d, colony_3d, growing_colony_3d, packed_colony_3d
+    cbm = load_package()
+    abi = cbm._abi
+    out = {}
+
+    out["aggregation_2d"] = run_aggregation_2d(args, cbm, abi, cpu=True)
+    out["chemotaxis_2d"] = run_chemotaxis_2d(args, cbm, abi, cpu=True)
 
     # c2 as a whole run: 10^4 agents uniform in a radius-20 ball centred in
     # [0,400]^3, grown by division to 10^6 (n_max 1.2M), Float32, graph
@@ -1176,6 +1191,8 @@ def main():
                     help="print only the implicit-medium (DGADI) lines, without the CPU checker")
     ap.add_argument("--rods-only", action="store_true",
                     help="print only the rods2D line, without the CPU checker")
+    ap.add_argument("--config-only", choices=["aggregation_2d", "chemotaxis_2d"],
+                    help="print only that configuration's line, without the CPU checker")
     ap.add_argument("--medium-only", action="store_true",
                     help="print only the 3D explicit-medium line")
     ap.add_argument("--medium-n", type=int, default=256, help="nodes per axis of the 3D medium")
@@ -1193,6 +1210,11 @@ def main():
         return
     if args.rods_only:
         print(json.dumps({"rods": run_rods(cpu=False), "rods_growth": run_rods_growth()}))
+        return
+    if args.config_only:
+        cbm = load_package()
+        fn = {"aggregation_2d": run_aggregation_2d, "chemotaxis_2d": run_chemotaxis_2d}
+        print(json.dumps({args.config_only: fn[args.config_only](args, cbm, cbm._abi, cpu=False)}))
         return
     if args.medium_only:
         cbm = load_package()
