@@ -167,8 +167,10 @@ __device__ __forceinline__ void small_de(const Params<T>& P, int s) {
 }
 
 // nsteps steps; P0 has the parity of the first step, P1 the other one.  The
-// counts of the histogram are complete after the first barrier, the
-// counters' commit by thread 0 is read only after the next ones.
+// counts of the histogram are complete after the first barrier.  The
+// counters' commit is made by the cluster's last thread in the placement
+// phase (no thread reads those counters before the next step) so that it
+// stays off the scan's path.
 template <typename T, int D>
 __global__ void __launch_bounds__(kSmallThreads) k_small_steps(Params<T> P0, Params<T> P1,
                                                                int nsteps, int n_cells) {
@@ -199,19 +201,6 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_steps(Params<T> P0, Par
       }
     }
     cluster_barrier();
-    if (tid == 0) {  // update!'s counters, as k_commit (no births or deaths here)
-      C->slots = C->N[p];
-      C->N[p ^ 1] = C->N[p];
-      C->n_add = 0;
-      C->n_remove = 0;
-      C->t[p ^ 1] = C->t[p] + P.dt_time;
-      C->step[p ^ 1] = C->step[p] + 1;
-      C->flag[p ^ 1] = 0;
-      C->resort = 1;
-      C->events = 0;
-      if (C->list_written) C->list_valid = 1;
-      C->list_written = 0;
-    }
     block_scan_counts(P.cell_count, n_cells, s_start, warp_sums);
     if (blockIdx.x == 0)
       for (int c = threadIdx.x; c <= n_cells; c += kSmallThreads) P.cell_start[c] = s_start[c];
@@ -231,7 +220,19 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_steps(Params<T> P0, Par
       P.cell_of_slot[ns] = c;
     }
     for (int c = tid; c < n_cells; c += nth) P.cell_count[c] = 0;
-    if (tid == 0) C->list_valid = 0;
+    if (tid == nth - 1) {  // update!'s counters, as k_commit (no births or deaths here)
+      C->slots = C->N[p];
+      C->N[p ^ 1] = C->N[p];
+      C->n_add = 0;
+      C->n_remove = 0;
+      C->t[p ^ 1] = C->t[p] + P.dt_time;
+      C->step[p ^ 1] = C->step[p] + 1;
+      C->flag[p ^ 1] = 0;
+      C->resort = 1;
+      C->events = 0;
+      C->list_written = 0;
+      C->list_valid = 0;  // the grid was rebuilt (computeNeighbors!)
+    }
     cluster_barrier();
   }
 }
