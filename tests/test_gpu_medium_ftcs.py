@@ -163,3 +163,20 @@ def test_medium_spacings(gpu_lib, abi, dims, dx, prec):
         g.step(8)
         o.step(8)
         assert_same_state(g.download(), o.download(), keys(dims))
+
+
+@pytest.mark.parametrize("shape", [(32, 5, 3), (8, 40, 2), (16, 3, 1), (40, 1, 6)])
+def test_medium_3d_thin_shapes(gpu_lib, abi, shape):
+    """3D media thinner than a tile (and a single plane or row): rows of a
+    multiple of 16 bytes take the TMA-fed stencils, whose plane boxes then
+    reach far beyond the field and read zeros there."""
+    nx, ny, nz = shape
+    kw, _ = medium_colony(abi, 3, N=400, L=float(max(shape)), n_medium=1)
+    kw.update(box_hi=(float(nx), float(ny), float(nz)), n_medium=(nx, ny, nz))
+    rng = np.random.default_rng(31)
+    st = dict(x=rng.uniform(0, nx, 400), y=rng.uniform(0, ny, 400), z=rng.uniform(0, nz, 400),
+              c=rng.uniform(0, 1, nx * ny * nz))
+    g, o = both(abi, kw, st)
+    g.step(9)
+    o.step(9)
+    assert_same_state(g.download(), o.download(), keys(3))

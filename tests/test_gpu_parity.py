@@ -395,3 +395,32 @@ def test_host_api_evolve(gpu_lib, abi):
     assert com.N == b["N"]
     np.testing.assert_array_equal(com.x, b["x"])
     np.testing.assert_array_equal(com.id, b["id"])
+
+
+@pytest.mark.parametrize("offset", [1.0e5, -3.0e4])
+@pytest.mark.parametrize("alg", ["CLVD", "CellLinked"])
+def test_colony_3d_f64_far_from_origin(gpu_lib, abi, alg, offset):
+    """A dividing Float64 colony whose box lies far from the origin: at
+    |x| ~ 1e5 rounding a coordinate to Float32 moves it by up to ~0.004, so
+    the Float32 filter of the Float64 walk works with a bound widened well
+    past the cutoff, and the exact Float64 test decides every pair.
+    Bit-exact with the checker, grid and lists included."""
+    neigh = dict(CLVD=abi.NEIGH_CLVD, CellLinked=abi.NEIGH_CELL_LINKED)[alg]
+    N = 3000
+    kw, st = colony_3d(abi, N=N, L=60.0, n_max=4 * N, p_death=2e-3, precision=abi.F64,
+                       neighbors=neigh)
+    kw.update(box_lo=(offset,) * 3, box_hi=(offset + 60.0,) * 3)
+    for k in "xyz":
+        st[k] = st[k] + offset
+    g, o = both(abi, kw, st)
+    for _ in range(3):
+        g.step(20)
+        o.step(20)
+        a, b = g.download(), o.download()
+        assert_same_state(a, b, ["x", "y", "z", "v", "g", "id", "parent"])
+        assert a["id_max"] == b["id_max"]
+    assert a["id_max"] > N  # divisions happened
+    if alg == "CellLinked":
+        assert_same_grid(g, o)
+    else:
+        assert_same_lists(g, o)
