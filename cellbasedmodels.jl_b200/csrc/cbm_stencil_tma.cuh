@@ -6,9 +6,10 @@
 // each with a one-node y halo and a 16-byte x halo, stream from HBM into a
 // ring of shared-memory stages by cp.async.bulk.tensor, one copy per plane
 // issued by one thread and completed on the stage's mbarrier.  While plane z
-// is computed from the stages of z - 1, z and z + 1, the next kTmaStages - 3
-// planes are in flight, so the loads never wait on registers and each block
-// keeps several planes of bytes outstanding.  The x start of every copy is a
+// is computed from the stages of z - 1, z and z + 1, the next planes are in
+// flight, so the loads never wait on registers and each block keeps several
+// planes of bytes outstanding; in Float32 two planes are computed between
+// barriers.  The x start of every copy is a
 // multiple of 16 bytes (x0 - 16 / sizeof(T)); copies that reach beyond the
 // field (the planes below 0 and above nz - 1, the halo of border tiles) read
 // zeros, which only border nodes, whose values do not use them, would see.
@@ -84,6 +85,7 @@ struct TmaPlane {
   static constexpr int kBytes = kBX * kBY * (int)sizeof(T);
   static constexpr int kStride = (kBytes + 127) / 128 * 128;
   static constexpr int kStages = sizeof(T) == 4 ? 6 : 4;
+  static constexpr int kPlanes = sizeof(T) == 4 ? 2 : 1;  // planes computed between barriers
   static constexpr int kSmem = kStages * kStride + 128;  // + alignment slack
 };
 
@@ -136,11 +138,9 @@ __device__ __forceinline__ void stencil_3d_tma(const Params<T>& P, const CUtenso
     inxy[r] = x > 0 && x < nx - 1 && y > 0 && y < ny - 1;
   }
   const size_t plane = (size_t)nx * ny;
-  wait(0);
-  wait(1);
-  for (int z = za; z < zb; ++z) {
-    const int i = z - za + 1;
-    wait(i + 1);
+  // plane i of the run (z = za - 1 + i) from the stages of i - 1, i, i + 1
+  auto compute = [&](int i) {
+    const int z = za - 1 + i;
     const T* Sm = stage(i - 1);
     const T* Sc = stage(i);
     const T* Sp = stage(i + 1);
@@ -172,8 +172,23 @@ __device__ __forceinline__ void stencil_3d_tma(const Params<T>& P, const CUtenso
         }
       }
     }
-    __syncthreads();  // stage (i - 1) % S is read by no one any more
-    if (lead && i - 1 + S < nplanes) issue(i - 1 + S);
+  };
+  wait(0);
+  wait(1);
+  // G::kPlanes planes a barrier: planes i .. i + kPlanes - 1 need the stages
+  // of i - 1 .. i + kPlanes, which the ring holds (kStages >= kPlanes + 3)
+  for (int i = 1; i <= nplanes - 2; i += G::kPlanes) {
+#pragma unroll
+    for (int q = 0; q < G::kPlanes; ++q)
+      if (i + q <= nplanes - 2) {
+        wait(i + q + 1);
+        compute(i + q);
+      }
+    __syncthreads();  // the stages of i - 1 .. i + kPlanes - 2 are read by no one any more
+    if (lead)
+#pragma unroll
+      for (int q = 0; q < G::kPlanes; ++q)
+        if (i - 1 + q + S < nplanes) issue(i - 1 + q + S);
   }
   // Every issued plane has been waited for on the normal path; after a wait
   // that ran out, the lead thread waits (bounded) for the copies still in
