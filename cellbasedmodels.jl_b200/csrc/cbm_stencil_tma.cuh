@@ -87,6 +87,9 @@ struct TmaPlane {
   static constexpr int kStages = sizeof(T) == 4 ? 6 : 4;
   static constexpr int kPlanes = sizeof(T) == 4 ? 2 : 1;  // planes computed between barriers
   static constexpr int kSmem = kStages * kStride + 128;  // + alignment slack
+  // the planes read between two barriers (kPlanes + 2) and the next one in
+  // flight fit the ring
+  static_assert(kStages >= kPlanes + 3, "plane ring too short");
 };
 
 template <typename T, bool kDE, bool kScale>
@@ -176,7 +179,7 @@ __device__ __forceinline__ void stencil_3d_tma(const Params<T>& P, const CUtenso
   wait(0);
   wait(1);
   // G::kPlanes planes a barrier: planes i .. i + kPlanes - 1 need the stages
-  // of i - 1 .. i + kPlanes, which the ring holds (kStages >= kPlanes + 3)
+  // of i - 1 .. i + kPlanes, which the ring holds
   for (int i = 1; i <= nplanes - 2; i += G::kPlanes) {
 #pragma unroll
     for (int q = 0; q < G::kPlanes; ++q)
