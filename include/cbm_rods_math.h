@@ -97,55 +97,70 @@ CBM_HD void cbm_intersection2lines(const CbmRodGeom<T>& a, const CbmRodGeom<T>& 
 }
 
 /* rodIntersection(x1, y1, l1, theta1, x2, y2, l2, theta2; separation = 0.99):
- * the closest virtual spheres of the two rods */
+ * the closest virtual spheres of the two rods.  The four cases of rods that
+ * are not parallel use four projections of the lines' intersection p:
+ * P1 = pointInsideRod(rod 1, p), P2 = pointInsideRod(rod 2, p),
+ * S1 = point2line(P2 onto rod 1) and S2 = point2line(P1 onto rod 2).  They
+ * are computed once, with the reference's expressions, and each case takes
+ * its own (so lanes of one warp in different cases share the work instead of
+ * running each case's projections in turn); the values are those of the
+ * reference's case-by-case statements. */
 template <typename T>
 CBM_HD void cbm_rod_intersection(const CbmRodGeom<T>& a, const CbmRodGeom<T>& b, T* x1a, T* y1a,
                                  T* x2a, T* y2a) {
   const T sep = (T)0.99;
-  *x1a = a.x;
-  *y1a = a.y;
-  *x2a = b.x;
-  *y2a = b.y;
   T px, py;
   cbm_intersection2lines(a, b, &px, &py);
   T ex = a.x - px, ey = a.y - py;
   const T di = sqrt(ex * ex + ey * ey);
   ex = b.x - px;
   ey = b.y - py;
-  T dj = sqrt(ex * ex + ey * ey);
+  const T dj = sqrt(ex * ex + ey * ey);
   const T norm = a.c * b.s - a.s * b.c;
   const T h1 = a.l / (T)2, h2 = b.l / (T)2;
-  if (fabs(norm) < (T)0.000001) {
+  if (fabs(norm) < (T)0.000001) {  // parallel: projections of p onto each line
     T qx, qy;
     cbm_point2line(px, py, a, &qx, &qy);
     cbm_point_inside_rod(a, qx, qy, sep, x1a, y1a);
     cbm_point2line(px, py, b, &qx, &qy);
     cbm_point_inside_rod(b, qx, qy, sep, x2a, y2a);
-  } else if (di <= h1 && dj <= h2) {
-    cbm_point_inside_rod(a, px, py, sep, x1a, y1a);
-    cbm_point_inside_rod(b, px, py, sep, x2a, y2a);
-  } else if (di <= h1 && dj > h2) {
-    cbm_point_inside_rod(b, px, py, sep, x2a, y2a);
-    cbm_point2line(*x2a, *y2a, a, x1a, y1a);
-  } else if (di > h1 && dj <= h2) {
-    cbm_point_inside_rod(a, px, py, sep, x1a, y1a);
-    cbm_point2line(*x1a, *y1a, b, x2a, y2a);
-  } else {
-    cbm_point_inside_rod(b, px, py, sep, x2a, y2a);
-    cbm_point2line(*x2a, *y2a, a, x1a, y1a);
-    ex = a.x - *x1a;
-    ey = a.y - *y1a;
-    dj = sqrt(ex * ex + ey * ey);
-    if (dj > h1) {
-      cbm_point_inside_rod(a, px, py, sep, x1a, y1a);
-      T qx, qy;
-      cbm_point2line(*x1a, *y1a, b, &qx, &qy);
-      ex = b.x - qx;
-      ey = b.y - qy;
-      dj = sqrt(ex * ex + ey * ey);
-      if (dj < h2) {
-        *x2a = qx;
-        *y2a = qy;
+    return;
+  }
+  T p1x, p1y, p2x, p2y, s1x, s1y, s2x, s2y;
+  cbm_point_inside_rod(a, px, py, sep, &p1x, &p1y);
+  cbm_point_inside_rod(b, px, py, sep, &p2x, &p2y);
+  cbm_point2line(p2x, p2y, a, &s1x, &s1y);
+  cbm_point2line(p1x, p1y, b, &s2x, &s2y);
+  if (di <= h1 && dj <= h2) {  // p inside both rods
+    *x1a = p1x;
+    *y1a = p1y;
+    *x2a = p2x;
+    *y2a = p2y;
+  } else if (di <= h1 && dj > h2) {  // p inside rod 1 only
+    *x2a = p2x;
+    *y2a = p2y;
+    *x1a = s1x;
+    *y1a = s1y;
+  } else if (di > h1 && dj <= h2) {  // p inside rod 2 only
+    *x1a = p1x;
+    *y1a = p1y;
+    *x2a = s2x;
+    *y2a = s2y;
+  } else {  // inside neither (or a comparison with NaN)
+    *x2a = p2x;
+    *y2a = p2y;
+    *x1a = s1x;
+    *y1a = s1y;
+    ex = a.x - s1x;
+    ey = a.y - s1y;
+    if (sqrt(ex * ex + ey * ey) > h1) {
+      *x1a = p1x;
+      *y1a = p1y;
+      ex = b.x - s2x;
+      ey = b.y - s2y;
+      if (sqrt(ex * ex + ey * ey) < h2) {
+        *x2a = s2x;
+        *y2a = s2y;
       }
     }
   }
