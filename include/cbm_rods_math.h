@@ -4,8 +4,9 @@
  *
  * rodForces (src/models/rods.jl:21-59) and its geometry in CBMMetrics
  * (src/metrics.jl: intersection2lines :137-152, point2line :162-170,
- * pointInsideRod :182-190, rodIntersection :202-246), statement by
- * statement.  Definitions of this build where Julia's arithmetic is not
+ * pointInsideRod :182-190, rodIntersection :202-246), expression by
+ * expression (rodIntersection computes the projections its cases share once;
+ * see there).  Definitions of this build where Julia's arithmetic is not
  * reproduced:
  *  - cos and sin: the library's own series of cbm_rng.h, on theta/(2 pi)
  *    reduced to [0, 1), so host and device give the same bits;
