@@ -25,6 +25,11 @@ struct cbm_ctx {
   cbm_config cfg{};
   int device = 0;
   cudaStream_t stream = nullptr;
+  // with a medium: the force kernel's branch of a step, forked from and
+  // joined to `stream` by events (the kernel shares no buffer with the
+  // medium kernels it overlaps)
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   size_t tsize = 4;
   std::string err;
   std::vector<void*> allocs;
@@ -582,10 +587,32 @@ int kernels_per_step(const cbm_ctx* c) {
 template <typename T, int D>
 void enqueue_full_step(cbm_ctx* c, int parity) {
   Params<T> P = params<T>(c, parity);
+  // The force kernel reads the committed positions and gradient and writes
+  // the next state; the medium kernels read and write only the field and
+  // its gradient.  With a medium the two run as parallel branches: the
+  // force kernel on `side`, forked after the last kernel it depends on (the
+  // agents' rule when there is one, else at the start of the step) and
+  // joined before the update.  Per-kernel timing keeps them in series.  A
+  // failed event call is seen like a failed launch (by the capture, or by
+  // cudaGetLastError after an eager step).
+  const bool fork = c->side && !c->prof;
+  const bool early = fork && !rule_needed(c->cfg);
+  auto agent_de = [&] {
+    cudaEventRecord(c->fork_ev, c->stream);
+    cudaStreamWaitEvent(c->side, c->fork_ev, 0);
+    cudaStream_t main = c->stream;
+    c->stream = c->side;
+    enqueue_agent_de<T, D>(c, P);
+    c->stream = main;
+    cudaEventRecord(c->join_ev, c->side);
+  };
+  if (early) agent_de();
   enqueue_medium_rule<T, D>(c, P);  // reads only committed c: may precede the secretion
   enqueue_agent_rule<T, D>(c, P);
-  enqueue_agent_de<T, D>(c, P);
+  if (!fork) enqueue_agent_de<T, D>(c, P);
+  else if (!early) agent_de();
   enqueue_medium_de<T, D>(c, P);
+  if (fork) cudaStreamWaitEvent(c->stream, c->join_ev, 0);
   enqueue_update<T, D>(c, P);
   enqueue_neighbors<T, D>(c, params<T>(c, parity ^ 1));
 }
@@ -735,6 +762,11 @@ void free_all(cbm_ctx* c) {
   }
   for (void* p : c->allocs) cudaFree(p);
   c->allocs.clear();
+  if (c->side) cudaStreamDestroy(c->side);
+  if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+  if (c->join_ev) cudaEventDestroy(c->join_ev);
+  c->side = nullptr;
+  c->fork_ev = c->join_ev = nullptr;
   if (c->stream) cudaStreamDestroy(c->stream);
   c->stream = nullptr;
 }
@@ -839,6 +871,14 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
   cudaDeviceGetAttribute(&c->n_sm, cudaDevAttrMultiProcessorCount, c->device);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
     int rc = fail(nullptr, CBM_ERR_CUDA, "cudaStreamCreate failed (is a CUDA device present?)");
+    delete c;
+    return rc;
+  }
+  if (k.medium && (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+                   cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+                   cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess)) {
+    int rc = fail(nullptr, CBM_ERR_CUDA, "creating the force kernel's stream failed");
+    free_all(c);
     delete c;
     return rc;
   }

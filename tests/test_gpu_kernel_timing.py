@@ -35,3 +35,31 @@ def test_kernel_times_of_graph_replays(gpu_lib, abi):
         np.testing.assert_array_equal(sa[k], sb[k], err_msg=k)
     with pytest.raises(cbm.CbmError):
         a.kernel_times()  # timing is off again
+
+
+@pytest.mark.parametrize("walls", [False, True])
+def test_medium_branches_match_series(gpu_lib, abi, walls):
+    """With a medium the force kernel runs on a branch of its own, in
+    parallel with the medium kernels (forked at the start of the step, or
+    after the agents' rule when reflecting walls need one); with kernel
+    timing on, and in profiled steps, the kernels run in series.  The three
+    give the same bits, in graph replays and in eager steps."""
+    from scenarios import medium_colony
+    kw, st = medium_colony(abi, 3, N=4000, L=48.0, n_medium=48)
+    if walls:
+        kw["walls"] = abi.WALLS_REFLECT
+    cfg = abi.make_config(**kw)
+    ctxs = [cbm.Context(cfg) for _ in range(4)]
+    for x in ctxs:
+        x.upload(st)
+    ctxs[0].step(8)                                   # forked graphs
+    ctxs[1].step(8, flags=abi.SYNC | abi.NO_GRAPH)    # forked eager steps
+    ctxs[2].set_kernel_timing(True)                   # graphs in series
+    ctxs[2].step(8)
+    for _ in range(8):                                # eager steps in series
+        ctxs[3].profile_step()
+    ref = ctxs[0].download()
+    for x in ctxs[1:]:
+        s = x.download()
+        for k in ("x", "y", "z", "id", "c", "gx", "gy", "gz"):
+            np.testing.assert_array_equal(s[k], ref[k], err_msg=k)
