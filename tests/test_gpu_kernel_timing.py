@@ -41,9 +41,11 @@ def test_kernel_times_of_graph_replays(gpu_lib, abi):
 def test_medium_branches_match_series(gpu_lib, abi, walls):
     """With a medium the force kernel runs on a branch of its own, in
     parallel with the medium kernels (forked at the start of the step, or
-    after the agents' rule when reflecting walls need one); with kernel
-    timing on, and in profiled steps, the kernels run in series.  The three
-    give the same bits, in graph replays and in eager steps."""
+    after the agents' rule when reflecting walls need one), and a call of
+    eight steps or more replays chained graphs in which the next step's
+    gradient runs beside each update; with kernel timing on, and in profiled
+    steps, the kernels run in series.  All give the same bits, in graph
+    replays (two chains and four single steps here) and in eager steps."""
     from scenarios import medium_colony
     kw, st = medium_colony(abi, 3, N=4000, L=48.0, n_medium=48)
     if walls:
@@ -52,11 +54,11 @@ def test_medium_branches_match_series(gpu_lib, abi, walls):
     ctxs = [cbm.Context(cfg) for _ in range(4)]
     for x in ctxs:
         x.upload(st)
-    ctxs[0].step(8)                                   # forked graphs
-    ctxs[1].step(8, flags=abi.SYNC | abi.NO_GRAPH)    # forked eager steps
+    ctxs[0].step(20)                                  # chained and forked graphs
+    ctxs[1].step(20, flags=abi.SYNC | abi.NO_GRAPH)   # forked eager steps
     ctxs[2].set_kernel_timing(True)                   # graphs in series
-    ctxs[2].step(8)
-    for _ in range(8):                                # eager steps in series
+    ctxs[2].step(20)
+    for _ in range(20):                               # eager steps in series
         ctxs[3].profile_step()
     ref = ctxs[0].download()
     for x in ctxs[1:]:
