@@ -18,6 +18,7 @@
 #include "cbm_kernels.cuh"
 #include "cbm_small.cuh"
 #include "cbm_stencil_tma.cuh"
+#include <utility>
 
 using namespace cbm;
 
@@ -193,6 +194,28 @@ struct Prof {
   }
 };
 #define PROF(name) Prof prof_scope_(c, name)
+
+// Launch on the context's stream with programmatic stream serialization,
+// where the kernel before it on the stream is a kernel (no event between):
+// the launch follows that kernel's completion without the full gap between
+// launches, and the kernel's pdl_wait() orders its memory accesses after
+// it.  A plain launch while kernels are timed (the event records sit
+// between).
+template <typename... KP, typename... A>
+void launch_pdl(cbm_ctx* c, bool pdl, void (*kern)(KP...), dim3 grid, dim3 block, size_t smem,
+                A&&... args) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = grid;
+  lc.blockDim = block;
+  lc.dynamicSmemBytes = smem;
+  lc.stream = c->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = (pdl && !c->prof) ? 1 : 0;
+  cudaLaunchKernelEx(&lc, kern, std::forward<A>(args)...);
+}
 
 // r^2 (1 + 1e-5) rounded up to T: a squared distance at or above it has a
 // correctly rounded sqrt >= (T)r, so the exact `d < r` test can be skipped
@@ -455,7 +478,7 @@ void enqueue_medium_rule(cbm_ctx* c, const Params<T>& P) {
 }
 
 template <typename T, int D>
-void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P) {
+void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P, bool pdl_gather = false) {
   const cbm_config& k = c->cfg;
   if (needs_snapshot(k)) {
     PROF("k_medium_snapshot");
@@ -469,7 +492,7 @@ void enqueue_agent_rule(cbm_ctx* c, const Params<T>& P) {
     constexpr int W = GatherPatch<D>::kWarps;
     const dim3 grid((unsigned)((nm[0] + 31) / 32), (unsigned)((py + W - 1) / W),
                     (unsigned)((nm[2] + GatherPatch<D>::kZ - 1) / GatherPatch<D>::kZ));
-    k_secrete_rows<T, D><<<grid, W * 32, 0, c->stream>>>(P);
+    launch_pdl(c, pdl_gather, k_secrete_rows<T, D>, grid, dim3(W * 32), 0, P);
   }
   if (!rule_needed(k)) return;
   if (k.fate != CBM_FATE_NONE) {
@@ -525,19 +548,20 @@ void enqueue_agent_de(cbm_ctx* c, const Params<T>& P) {
 }
 
 template <typename T, int D>
-void enqueue_medium_de(cbm_ctx* c, const Params<T>& P) {
+void enqueue_medium_de(cbm_ctx* c, const Params<T>& P, bool pdl = false) {
   if (c->cfg.medium) {
     PROF("k_medium_de");
     if (D == 2)
-      k_medium_de_2d<T><<<stencil_grid(c), dim3(kStX, kStY), 0, c->stream>>>(P);
+      launch_pdl(c, pdl, k_medium_de_2d<T>, stencil_grid(c), dim3(kStX, kStY), 0, P);
     else if (D == 3)
       if (c->tma_medium)
-        k_medium_de_3d_tma<T><<<stencil_grid_3d(c), dim3(kStX, kStY), TmaPlane<T>::kSmem,
-                                c->stream>>>(P, c->tmap_c[P.parity], stencil_z_run(c));
+        launch_pdl(c, pdl, k_medium_de_3d_tma<T>, stencil_grid_3d(c), dim3(kStX, kStY),
+                   (size_t)TmaPlane<T>::kSmem, P, c->tmap_c[P.parity], stencil_z_run(c));
       else
-        k_medium_de_3d<T><<<stencil_grid_3d(c), dim3(kStX, kStY), 0, c->stream>>>(P, stencil_z_run(c));
+        launch_pdl(c, pdl, k_medium_de_3d<T>, stencil_grid_3d(c), dim3(kStX, kStY), 0, P,
+                   stencil_z_run(c));
     else
-      k_medium_de<T, D><<<grid_blocks(c->n_nodes), kTile, 0, c->stream>>>(P);
+      launch_pdl(c, pdl, k_medium_de<T, D>, dim3(grid_blocks(c->n_nodes)), dim3(kTile), 0, P);
   }
 }
 
@@ -552,22 +576,23 @@ void enqueue_update(cbm_ctx* c, const Params<T>& P) {
     PROF("k_commit");
     k_commit<T><<<1, 1, 0, c->stream>>>(P);
   }
+  // the four sort kernels follow one another on the stream
   {
     PROF("k_sort_hist");
-    k_sort_hist<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+    launch_pdl(c, true, k_sort_hist<T, D>, dim3(c->n_blocks), dim3(kTile), 0, P);
   }
   {
     PROF("k_scan_cells");
     ScanArgs A{c->cell_count, c->cell_start, c->scan_state, c->n_cells, c->n_scan_tiles, c->ctr,
                resort_flag(c)};
-    k_scan_cells<<<c->n_scan_tiles, kTile, 0, c->stream>>>(A);
+    launch_pdl(c, true, k_scan_cells, dim3(c->n_scan_tiles), dim3(kTile), 0, A);
   }
   {
     PROF("k_sort_scatter");
-    k_sort_scatter<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+    launch_pdl(c, true, k_sort_scatter<T>, dim3(c->n_blocks), dim3(kTile), 0, P);
   }
   PROF("k_sort_place");
-  k_sort_place<T, D><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+  launch_pdl(c, true, k_sort_place<T, D>, dim3(c->n_blocks), dim3(kTile), 0, P);
 }
 
 // computeNeighbors! after update!: the grid was rebuilt by the re-sort; a
@@ -625,10 +650,13 @@ void enqueue_full_step(cbm_ctx* c, int parity, bool grad_ahead = false, bool nex
   // and in a chained graph the previous step enqueued it beside its update
   if (grad_ahead) cudaStreamWaitEvent(c->stream, c->grad_ev, 0);
   else enqueue_medium_rule<T, D>(c, P);
-  enqueue_agent_rule<T, D>(c, P);
+  // programmatic launches where the kernel before is one on this stream:
+  // the secretion after the gradient, the FTCS after the secretion
+  const bool grad_before = !grad_ahead && c->cfg.medium && c->cfg.chemotaxis != 0;
+  enqueue_agent_rule<T, D>(c, P, grad_before && !needs_snapshot(c->cfg));
   if (!fork) enqueue_agent_de<T, D>(c, P);
   else if (!early) agent_de();
-  enqueue_medium_de<T, D>(c, P);
+  enqueue_medium_de<T, D>(c, P, early && uses_gather(c->cfg) && !rule_needed(c->cfg));
   if (fork) cudaStreamWaitEvent(c->stream, c->join_ev, 0);
   if (next_grad) {
     // The next step's gradient reads the field just written and writes the

@@ -21,6 +21,16 @@ constexpr int kScanItems = 32;      // cells per thread in the cell scan (8192 p
 constexpr int kScanTile = kTile * kScanItems;
 constexpr long long kSpinLimit = 1ll << 20;  // bounded look-back wait
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream
+// serialization is launched as the kernel before it on the stream completes,
+// without the full gap between two launches; pdl_wait() returns once that
+// kernel has completed and its writes are visible (at once for a plain
+// launch), so a dependent kernel calls it before its first access to global
+// memory.  No kernel here triggers its dependents early: blocks that wait
+// resident for their predecessor would hold the SMs the concurrent branches
+// of the step graph need.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // device error bits (cbm_sync reports the first as a status code)
 enum : int {
   kErrAgentOverflow = 1 << 0,
@@ -188,6 +198,7 @@ static __global__ void __launch_bounds__(kTile) k_scan_cells(ScanArgs A) {
   __shared__ unsigned s_tile;
   __shared__ int s_prefix;
   __shared__ int s_cells[kScanTile + kScanTile / 32];
+  pdl_wait();
   if (A.due && *A.due == 0) return;
   Counters* C = A.ctr;
   const unsigned epoch = C->scan_epoch;

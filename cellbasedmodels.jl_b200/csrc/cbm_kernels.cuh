@@ -629,6 +629,7 @@ __global__ void __launch_bounds__(GatherPatch<D>::kWarps * 32) k_secrete_rows(Pa
   __shared__ unsigned char s_perm[W][CAP];
   __shared__ T s_acc[W][NP * 32], s_net[W][NP * 32];
   __shared__ unsigned char s_tch[W][NP * 32];
+  pdl_wait();
   const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
   const int nx = P.n_medium[0];
   const int ny = D > 1 ? P.n_medium[1] : 1, nz = D > 2 ? P.n_medium[2] : 1;
@@ -1785,6 +1786,7 @@ __device__ __forceinline__ T over_2dx(const Params<T>& P, int d, T v) {
 
 template <typename T, int D>
 __global__ void __launch_bounds__(kTile) k_medium_de(Params<T> P) {
+  pdl_wait();
   int n = blockIdx.x * kTile + threadIdx.x;
   if (n >= P.n_nodes) return;
   int q[3] = {0, 0, 0};
@@ -1888,6 +1890,7 @@ __device__ __forceinline__ void medium_de_2d(const Params<T>& P) {
 
 template <typename T>
 __global__ void __launch_bounds__(kStX * kStY) k_medium_de_2d(Params<T> P) {
+  pdl_wait();
   if (P.exact_scale) medium_de_2d<T, true>(P);
   else medium_de_2d<T, false>(P);
 }
@@ -1996,6 +1999,7 @@ __global__ void __launch_bounds__(kStX * kStY) k_medium_grad_3d(Params<T> P, int
 
 template <typename T>
 __global__ void __launch_bounds__(kStX * kStY) k_medium_de_3d(Params<T> P, int z_run) {
+  pdl_wait();
   stencil_3d<T, true>(P, z_run);
 }
 
@@ -2125,6 +2129,7 @@ __global__ void k_commit(Params<T> P) {
 // ---------------------------------------------------------------------------
 template <typename T, int D>
 __global__ void __launch_bounds__(kTile) k_sort_hist(Params<T> P) {
+  pdl_wait();
   const Counters* C = P.ctr;
   const int s = blockIdx.x * kTile + threadIdx.x;
   const long long slots = C->slots;
@@ -2154,6 +2159,7 @@ __global__ void __launch_bounds__(kTile) k_sort_hist(Params<T> P) {
 
 template <typename T>
 __global__ void __launch_bounds__(kTile) k_sort_scatter(Params<T> P) {
+  pdl_wait();
   const Counters* C = P.ctr;
   if (!C->resort) return;
   const int s = blockIdx.x * kTile + threadIdx.x;
@@ -2165,6 +2171,7 @@ __global__ void __launch_bounds__(kTile) k_sort_scatter(Params<T> P) {
 
 template <typename T, int D>
 __global__ void __launch_bounds__(kTile) k_sort_place(Params<T> P) {
+  pdl_wait();
   const Counters* C = P.ctr;
   if (!C->resort) return;
   const int s = blockIdx.x * kTile + threadIdx.x;

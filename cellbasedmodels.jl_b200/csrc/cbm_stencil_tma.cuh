@@ -214,6 +214,7 @@ template <typename T>
 __global__ void __launch_bounds__(kStX * kStY) k_medium_de_3d_tma(Params<T> P,
                                                                  const __grid_constant__ CUtensorMap map,
                                                                  int z_run) {
+  pdl_wait();
   if (P.exact_scale) stencil_3d_tma<T, true, true>(P, &map, z_run);
   else stencil_3d_tma<T, true, false>(P, &map, z_run);
 }
