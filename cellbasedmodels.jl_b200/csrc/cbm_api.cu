@@ -204,17 +204,7 @@ struct Prof {
 template <typename... KP, typename... A>
 void launch_pdl(cbm_ctx* c, bool pdl, void (*kern)(KP...), dim3 grid, dim3 block, size_t smem,
                 A&&... args) {
-  cudaLaunchConfig_t lc = {};
-  lc.gridDim = grid;
-  lc.blockDim = block;
-  lc.dynamicSmemBytes = smem;
-  lc.stream = c->stream;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  lc.attrs = at;
-  lc.numAttrs = (pdl && !c->prof) ? 1 : 0;
-  cudaLaunchKernelEx(&lc, kern, std::forward<A>(args)...);
+  launch_serial(c->stream, pdl && !c->prof, kern, grid, block, smem, std::forward<A>(args)...);
 }
 
 // r^2 (1 + 1e-5) rounded up to T: a squared distance at or above it has a

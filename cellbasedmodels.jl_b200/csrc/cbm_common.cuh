@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 #include "../../include/cbm_b200.h"
 #include "../../include/cbm_rng.h"
 
@@ -30,6 +32,26 @@ constexpr long long kSpinLimit = 1ll << 20;  // bounded look-back wait
 // resident for their predecessor would hold the SMs the concurrent branches
 // of the step graph need.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Host side: launch kern on stream st, with programmatic stream
+// serialization when `pdl` (then the operation before it on st must be a
+// kernel launch, and kern calls pdl_wait() before its first global access).
+// Errors are seen like those of <<<>>> launches, by cudaGetLastError.
+template <typename... KP, typename... A>
+inline void launch_serial(cudaStream_t st, bool pdl, void (*kern)(KP...), dim3 grid, dim3 block,
+                          size_t smem, A&&... args) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = grid;
+  lc.blockDim = block;
+  lc.dynamicSmemBytes = smem;
+  lc.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&lc, kern, std::forward<A>(args)...);
+}
 
 // device error bits (cbm_sync reports the first as a status code)
 enum : int {

@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(kTile) k_grid_hist(GridParams<T> G) {
 // sortAgentsInCells (neighbors.jl:837-899), first pass: scatter by atomic rank
 template <typename T>
 __global__ void __launch_bounds__(kTile) k_grid_scatter(GridParams<T> G) {
+  pdl_wait();
   const int i = blockIdx.x * kTile + threadIdx.x;
   if (i >= G.n) return;
   G.cell_tmp[G.cell_start[G.agent_cell[i]] + G.agent_rank[i]] = i;
@@ -56,6 +57,7 @@ __global__ void __launch_bounds__(kTile) k_grid_scatter(GridParams<T> G) {
 // are ascending inside each cell as in the serial CPU reference (:851-862)
 template <typename T>
 __global__ void __launch_bounds__(kTile) k_grid_stable(GridParams<T> G) {
+  pdl_wait();
   const int i = blockIdx.x * kTile + threadIdx.x;
   if (i >= G.n) return;
   const int c = G.agent_cell[i];

@@ -172,6 +172,7 @@ __device__ void rod_divide(const RodStep<T>& R, int i, int n) {
 // cell assignment of step 3 (assignCells, neighbors.jl:763-821)
 template <typename T, bool GROW>
 __global__ void __launch_bounds__(kRodBlock) k_rod_step(RodStep<T> R) {
+  pdl_wait();
   const int t = blockIdx.x * kRodBlock + threadIdx.x;
   const int i = t / kRodLanes, lane = t % kRodLanes;
   const int n = GROW ? (int)R.cnt_a[0] : R.n;
@@ -308,6 +309,7 @@ __global__ void __launch_bounds__(kTile) k_rod_flags(RodStep<T> R, int* flags, C
 // holes[k] = index of the k-th dividing rod; the step's count and counter
 template <typename T>
 __global__ void __launch_bounds__(kTile) k_rod_holes(RodStep<T> R, int* holes, Counters* ctr) {
+  pdl_wait();
   const int i = blockIdx.x * kTile + threadIdx.x;
   const int n = (int)R.cnt_a[0];
   if (i == 0) {
@@ -323,6 +325,7 @@ __global__ void __launch_bounds__(kTile) k_rod_holes(RodStep<T> R, int* holes, C
 // k_grid_scatter / k_grid_stable of cbm_grid.cuh with the rod count on the device
 template <typename T>
 __global__ void __launch_bounds__(kTile) k_rod_scatter(GridParams<T> G, const long long* cnt) {
+  pdl_wait();
   const int i = blockIdx.x * kTile + threadIdx.x;
   if (i >= (int)cnt[0]) return;
   G.cell_tmp[G.cell_start[G.agent_cell[i]] + G.agent_rank[i]] = i;
@@ -330,6 +333,7 @@ __global__ void __launch_bounds__(kTile) k_rod_scatter(GridParams<T> G, const lo
 
 template <typename T>
 __global__ void __launch_bounds__(kTile) k_rod_stable(GridParams<T> G, const long long* cnt) {
+  pdl_wait();
   const int i = blockIdx.x * kTile + threadIdx.x;
   if (i >= (int)cnt[0]) return;
   const int c = G.agent_cell[i];
@@ -513,9 +517,11 @@ void enqueue_rod_step(cbm_rods* r) {
       // the rest of computeNeighbors! on the new positions
       const GridParams<T> G = grid_params<T>(r);
       const unsigned ng = (unsigned)(r->n > 0 ? (r->n + kTile - 1) / kTile : 1);
-      k_scan_cells<<<G.n_scan_tiles, kTile, 0, r->stream>>>(grid_scan_args(G));
-      k_grid_scatter<T><<<ng, kTile, 0, r->stream>>>(G);
-      k_grid_stable<T><<<ng, kTile, 0, r->stream>>>(G);
+      // each kernel follows a kernel on the stream: programmatic launches
+      launch_serial(r->stream, true, k_scan_cells, dim3(G.n_scan_tiles), dim3(kTile), 0,
+                    grid_scan_args(G));
+      launch_serial(r->stream, true, k_grid_scatter<T>, dim3(ng), dim3(kTile), 0, G);
+      launch_serial(r->stream, true, k_grid_stable<T>, dim3(ng), dim3(kTile), 0, G);
     }
     return;
   }
@@ -540,18 +546,20 @@ void enqueue_rod_step(cbm_rods* r) {
   A.n_tiles = r->div_tiles;
   A.ctr = r->div_ctr;
   A.due = nullptr;
-  k_scan_cells<<<A.n_tiles, kTile, 0, r->stream>>>(A);
-  k_rod_holes<T><<<nt, kTile, 0, r->stream>>>(R, r->holes, r->ctr);
+  // from here each kernel follows a kernel on the stream: programmatic launches
+  launch_serial(r->stream, true, k_scan_cells, dim3(A.n_tiles), dim3(kTile), 0, A);
+  launch_serial(r->stream, true, k_rod_holes<T>, dim3(nt), dim3(kTile), 0, R, r->holes, r->ctr);
   const long long threads = (long long)k.n_max * kRodLanes;
   const unsigned nb = (unsigned)((threads + kRodBlock - 1) / kRodBlock);
-  k_rod_step<T, true><<<nb, kRodBlock, 0, r->stream>>>(R);
+  launch_serial(r->stream, true, k_rod_step<T, true>, dim3(nb), dim3(kRodBlock), 0, R);
   r->cur = 1 - r->cur;
   if (!R.full) {
     const GridParams<T> G = grid_params<T>(r);
     const long long* cnt = r->cnt + 2 * r->cur;
-    k_scan_cells<<<G.n_scan_tiles, kTile, 0, r->stream>>>(grid_scan_args(G));
-    k_rod_scatter<T><<<nt, kTile, 0, r->stream>>>(G, cnt);
-    k_rod_stable<T><<<nt, kTile, 0, r->stream>>>(G, cnt);
+    launch_serial(r->stream, true, k_scan_cells, dim3(G.n_scan_tiles), dim3(kTile), 0,
+                  grid_scan_args(G));
+    launch_serial(r->stream, true, k_rod_scatter<T>, dim3(nt), dim3(kTile), 0, G, cnt);
+    launch_serial(r->stream, true, k_rod_stable<T>, dim3(nt), dim3(kTile), 0, G, cnt);
   }
 }
 
