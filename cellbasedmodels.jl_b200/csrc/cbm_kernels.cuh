@@ -2145,16 +2145,26 @@ __global__ void __launch_bounds__(kTile) k_sort_hist(Params<T> P) {
     P.ctr->scan_ticket = 0u;  // fresh tickets and tile-state generation for the scan
     P.ctr->scan_epoch = C->scan_epoch + 1u;
   }
-  if (s >= slots) return;
-  if (P.IB[s] < 0) {
-    P.s_cell[s] = -1;
-    return;
+  // The lanes of a warp hold consecutive slots, mostly of one cell in a
+  // dense community: the lanes of each cell take their ranks with one atomic
+  // add (any ranks 0 .. count-1 of a cell do, since the placement orders
+  // the cell's agents by index).  Every lane of the warp gets here.
+  int c = -1;
+  if (s < slots && P.IB[s] >= 0) {
+    T x[3];
+    to3<T>(P.PB[s], x);
+    c = cell_of_pos<T, D>(P, x);
   }
-  T x[3];
-  to3<T>(P.PB[s], x);
-  int c = cell_of_pos<T, D>(P, x);
-  P.s_cell[s] = c;
-  P.s_rank[s] = atomicAdd(P.cell_count + c, 1);
+  if (s < slots) P.s_cell[s] = c;
+  const unsigned peers = __match_any_sync(kFull, c);
+  if (c >= 0) {
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(P.cell_count + c, __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    P.s_rank[s] = base + __popc(peers & ((1u << lane) - 1u));
+  }
 }
 
 template <typename T>
@@ -2181,8 +2191,15 @@ __global__ void __launch_bounds__(kTile) k_sort_place(Params<T> P) {
   if (c < 0) return;
   const int key = P.IB[s];
   const int s0 = P.cell_start[c], s1 = P.cell_start[c + 1];
-  int r = 0;
-  for (int q = s0; q < s1; ++q) r += ld(P.s_key + q) < key;
+  // rank among the cell's keys (the cells of a dense colony hold a hundred
+  // and more): four keys a load between the aligned ends
+  int r = 0, q = s0;
+  for (const int qa = min(s1, (s0 + 3) & ~3); q < qa; ++q) r += ld(P.s_key + q) < key;
+  for (; q + 4 <= s1; q += 4) {
+    const int4 k4 = ld(reinterpret_cast<const int4*>(P.s_key + q));
+    r += (int)(k4.x < key) + (int)(k4.y < key) + (int)(k4.z < key) + (int)(k4.w < key);
+  }
+  for (; q < s1; ++q) r += ld(P.s_key + q) < key;
   const int ns = s0 + r;
   const typename V4T<T>::type x = P.PB[s];
   P.PA[ns] = x;
