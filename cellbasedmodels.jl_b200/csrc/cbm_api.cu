@@ -90,6 +90,7 @@ struct cbm_ctx {
   CUtensorMap tmap_c[2];
   bool tma_medium = false;
   Counters* ctr = nullptr;
+  Counters* h_ctr = nullptr;   // pinned staging of the counters an upload writes
   int* scratch_int = nullptr;  // n_max ints for inspection calls
   void* ext_noise = nullptr;   // EM increments of cbm_step_noise (n_max * dims reals, lazy)
   bool ext_noise_on = false;   // the step being enqueued reads ext_noise
@@ -818,6 +819,8 @@ void free_all(cbm_ctx* c) {
     c->gmarks[q].clear();
   }
   for (void* p : c->allocs) cudaFree(p);
+  if (c->h_ctr) cudaFreeHost(c->h_ctr);
+  c->h_ctr = nullptr;
   c->allocs.clear();
   if (c->side) cudaStreamDestroy(c->side);
   if (c->side2) cudaStreamDestroy(c->side2);
@@ -1058,6 +1061,10 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     c->gather_box = (int*)dalloc(c, nb * 4, &ok);
   }
   c->ctr = (Counters*)dalloc(c, sizeof(Counters), &ok);
+  if (ok && cudaMallocHost((void**)&c->h_ctr, sizeof(Counters)) != cudaSuccess) {
+    c->h_ctr = nullptr;
+    ok = false;
+  }
   if (!ok) {
     int rc = fail(nullptr, CBM_ERR_NOMEM, "device allocation failed for n_max=%lld", (long long)k.n_max);
     free_all(c);
@@ -1114,6 +1121,11 @@ int cbm_upload(cbm_ctx* c, const cbm_state_view* h) {
   if (k.growth && N && (!h->v || !h->g)) return fail(c, CBM_ERR_ARG, "growth needs v and g");
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   cudaStream_t st = c->stream;
+  // the epochs of the counters being replaced, read before anything is
+  // enqueued, so that the copies, the counters and the first sort follow one
+  // another with one synchronisation at the end
+  Counters old;
+  CUDA_TRY(c, cudaMemcpy(&old, c->ctr, sizeof old, cudaMemcpyDeviceToHost));
   // staging: index order; absent fields are zeros (loadToPlatform! pads with zeros)
   for (int d = 0; d < 3; ++d) {
     CUDA_TRY(c, cudaMemsetAsync(c->hx[d], 0, nm * S, st));
@@ -1146,9 +1158,6 @@ int cbm_upload(cbm_ctx* c, const cbm_state_view* h) {
     }
   }
   CUDA_TRY(c, cudaMemsetAsync(c->cell_count, 0, (size_t)c->n_cells * 4, st));
-  Counters old;
-  CUDA_TRY(c, cudaMemcpyAsync(&old, c->ctr, sizeof old, cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(c, cudaStreamSynchronize(st));
   Counters hc;
   memset(&hc, 0, sizeof hc);
   hc.N[0] = hc.N[1] = h->N;
@@ -1159,7 +1168,8 @@ int cbm_upload(cbm_ctx* c, const cbm_state_view* h) {
   hc.resort = 1;  // flagRecomputeNeighbors_ = [1] and computeNeighbors! at load (communityStructure.jl:480,648)
   hc.scan_epoch = old.scan_epoch + 1;  // keep the epoch monotonic so stale tile states never match
   hc.fate_epoch = old.fate_epoch + 1;
-  CUDA_TRY(c, cudaMemcpyAsync(c->ctr, &hc, sizeof hc, cudaMemcpyHostToDevice, st));
+  *c->h_ctr = hc;  // pinned: the copy is ordered on the stream, without a wait
+  CUDA_TRY(c, cudaMemcpyAsync(c->ctr, c->h_ctr, sizeof hc, cudaMemcpyHostToDevice, st));
   c->parity = 0;
   reset_stage_flags(c);
   c->loaded = true;
@@ -1194,25 +1204,29 @@ int cbm_download(cbm_ctx* c, cbm_state_view* h, int32_t which) {
     dispatch<Gather>(c, (int)N, src);
     rc = check_launch(c);
     if (rc) return rc;
-    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   }
+  // the copies follow the gather on the context's stream, one
+  // synchronisation for all of them
+  cudaStream_t st = c->stream;
   for (int d = 0; d < k.dims; ++d) {
-    if (h->pos[d] && N) CUDA_TRY(c, cudaMemcpy(h->pos[d], c->hx[d], nb, cudaMemcpyDeviceToHost));
-    if (h->f[d] && N) CUDA_TRY(c, cudaMemcpy(h->f[d], c->hf[d], nb, cudaMemcpyDeviceToHost));
+    if (h->pos[d] && N) CUDA_TRY(c, cudaMemcpyAsync(h->pos[d], c->hx[d], nb, cudaMemcpyDeviceToHost, st));
+    if (h->f[d] && N) CUDA_TRY(c, cudaMemcpyAsync(h->f[d], c->hf[d], nb, cudaMemcpyDeviceToHost, st));
   }
-  if (h->v && N) CUDA_TRY(c, cudaMemcpy(h->v, c->hv, nb, cudaMemcpyDeviceToHost));
-  if (h->g && N) CUDA_TRY(c, cudaMemcpy(h->g, c->G, nb, cudaMemcpyDeviceToHost));
-  if (h->id && N) CUDA_TRY(c, cudaMemcpy(h->id, c->ID, (size_t)N * 8, cudaMemcpyDeviceToHost));
-  if (h->parent && N) CUDA_TRY(c, cudaMemcpy(h->parent, c->PAR, (size_t)N * 8, cudaMemcpyDeviceToHost));
+  if (h->v && N) CUDA_TRY(c, cudaMemcpyAsync(h->v, c->hv, nb, cudaMemcpyDeviceToHost, st));
+  if (h->g && N) CUDA_TRY(c, cudaMemcpyAsync(h->g, c->G, nb, cudaMemcpyDeviceToHost, st));
+  if (h->id && N) CUDA_TRY(c, cudaMemcpyAsync(h->id, c->ID, (size_t)N * 8, cudaMemcpyDeviceToHost, st));
+  if (h->parent && N)
+    CUDA_TRY(c, cudaMemcpyAsync(h->parent, c->PAR, (size_t)N * 8, cudaMemcpyDeviceToHost, st));
   if (k.medium) {
     const size_t mb = (size_t)c->n_nodes * S;
     const int qc = nw && c->mde_done ? p ^ 1 : p;
     const int qg = nw && c->mrule_done ? p ^ 1 : p;
-    if (h->medium_c) CUDA_TRY(c, cudaMemcpy(h->medium_c, c->c[qc], mb, cudaMemcpyDeviceToHost));
+    if (h->medium_c) CUDA_TRY(c, cudaMemcpyAsync(h->medium_c, c->c[qc], mb, cudaMemcpyDeviceToHost, st));
     for (int d = 0; d < k.dims; ++d)
       if (h->medium_grad[d])
-        CUDA_TRY(c, cudaMemcpy(h->medium_grad[d], c->grad[qg][d], mb, cudaMemcpyDeviceToHost));
+        CUDA_TRY(c, cudaMemcpyAsync(h->medium_grad[d], c->grad[qg][d], mb, cudaMemcpyDeviceToHost, st));
   }
+  CUDA_TRY(c, cudaStreamSynchronize(st));
   return CBM_OK;
 }
 
