@@ -1126,25 +1126,27 @@ int cbm_upload(cbm_ctx* c, const cbm_state_view* h) {
   // another with one synchronisation at the end
   Counters old;
   CUDA_TRY(c, cudaMemcpy(&old, c->ctr, sizeof old, cudaMemcpyDeviceToHost));
-  // staging: index order; absent fields are zeros (loadToPlatform! pads with zeros)
+  // staging: index order; absent fields are zeros (loadToPlatform! pads with
+  // zeros), and so is every field beyond N.  A field given by the caller is
+  // copied into [0, N) and cleared beyond it only.
+  auto stage = [&](void* dst, const void* src, size_t elem) -> cudaError_t {
+    const size_t from = (src && N) ? N : 0;
+    cudaError_t e = cudaSuccess;
+    if (from) e = cudaMemcpyAsync(dst, src, N * elem, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && nm > from)
+      e = cudaMemsetAsync((char*)dst + from * elem, 0, (nm - from) * elem, st);
+    return e;
+  };
   for (int d = 0; d < 3; ++d) {
-    CUDA_TRY(c, cudaMemsetAsync(c->hx[d], 0, nm * S, st));
-    CUDA_TRY(c, cudaMemsetAsync(c->hf[d], 0, nm * S, st));
-    if (d < k.dims && N) CUDA_TRY(c, cudaMemcpyAsync(c->hx[d], h->pos[d], N * S, cudaMemcpyHostToDevice, st));
-    if (d < k.dims && N && h->f[d])
-      CUDA_TRY(c, cudaMemcpyAsync(c->hf[d], h->f[d], N * S, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(c, stage(c->hx[d], d < k.dims ? h->pos[d] : nullptr, S));
+    CUDA_TRY(c, stage(c->hf[d], d < k.dims ? h->f[d] : nullptr, S));
   }
-  CUDA_TRY(c, cudaMemsetAsync(c->hv, 0, nm * S, st));
-  if (N && h->v) CUDA_TRY(c, cudaMemcpyAsync(c->hv, h->v, N * S, cudaMemcpyHostToDevice, st));
-  CUDA_TRY(c, cudaMemsetAsync(c->G, 0, nm * S, st));
-  if (N && h->g) CUDA_TRY(c, cudaMemcpyAsync(c->G, h->g, N * S, cudaMemcpyHostToDevice, st));
-  CUDA_TRY(c, cudaMemsetAsync(c->PAR, 0, nm * 8, st));
-  if (N && h->parent)
-    CUDA_TRY(c, cudaMemcpyAsync(c->PAR, h->parent, N * 8, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(c, stage(c->hv, h->v, S));
+  CUDA_TRY(c, stage(c->G, h->g, S));
+  CUDA_TRY(c, stage(c->PAR, h->parent, 8));
   // ids: the caller's (copied straight from its array), else 1..N; zero beyond N
-  CUDA_TRY(c, cudaMemsetAsync(c->ID, 0, (nm > 0 ? nm : 1) * 8, st));
-  if (N && h->id) CUDA_TRY(c, cudaMemcpyAsync(c->ID, h->id, N * 8, cudaMemcpyHostToDevice, st));
-  else if (N) k_default_ids<<<grid_blocks((long long)N), kTile, 0, st>>>(c->ID, (int)N);
+  CUDA_TRY(c, stage(c->ID, h->id, 8));
+  if (N && !h->id) k_default_ids<<<grid_blocks((long long)N), kTile, 0, st>>>(c->ID, (int)N);
   if (k.medium) {
     const size_t nb = (size_t)c->n_nodes * S;
     for (int q = 0; q < 2; ++q) {
