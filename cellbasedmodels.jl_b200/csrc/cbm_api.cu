@@ -100,6 +100,8 @@ struct cbm_ctx {
   int de_blocks = 1;          // persistent grid of the force kernel
   void* pair_list = nullptr;  // its partner lists (cell walks only)
   void* pos32 = nullptr;      // Float64 3D cell walks: positions rounded to Float32
+  void* pos_rows = nullptr;   // Float32 3D cell walks: positions as rows x | y | z
+  int rows_stride = 0;
   void* stage[3] = {nullptr, nullptr, nullptr};  // Heun / RK4: h, running sum, derivative
   int n_cells = 1;
   int n_cells_d[3] = {1, 1, 1};
@@ -287,6 +289,8 @@ Params<T> params(const cbm_ctx* c, int parity) {
   P.pair_list = (int4*)c->pair_list;
   P.pair_cap4 = kPairCap4;
   P.PA32 = (float4*)c->pos32;
+  P.PS = (float*)c->pos_rows;
+  P.ps_stride = c->rows_stride;
   P.c_cur = (T*)c->c[p];
   P.c_nxt = (T*)c->c[q];
   P.ctr = c->ctr;
@@ -503,6 +507,10 @@ void enqueue_agent_de(cbm_ctx* c, const Params<T>& P) {
     PROF("k_pos32");
     k_pos32<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
   }
+  if (c->pos_rows) {
+    PROF("k_pos_rows");
+    k_pos_rows<T><<<c->n_blocks, kTile, 0, c->stream>>>(P);
+  }
   if (integ != CBM_INT_HEUN && integ != CBM_INT_RK4 && integ != CBM_INT_EULER_HEUN) {
     PROF("k_agent_de");
     k_agent_de<T, D><<<grid, kTile, 0, c->stream>>>(P);
@@ -608,6 +616,7 @@ int kernels_per_step(const cbm_ctx* c) {
   if (k.fate != CBM_FATE_NONE) n += 1;  // compaction
   n += 1;                               // agent DE
   if (c->pos32) n += 1;                 // its Float32 positions (Float64 3D walks)
+  if (c->pos_rows) n += 1;              // its position rows (Float32 3D walks)
   if (k.medium) n += 1;
   n += 5;                               // commit, sort hist, scan, scatter, place
   if (k.neighbors == CBM_NEIGH_VERLET_DISPLACEMENT) n += 1;
@@ -1046,6 +1055,10 @@ int cbm_create(cbm_ctx** out, const cbm_config* cfg) {
     if (cells && k.dims == 3)
       c->pair_list = dalloc(c, (size_t)c->de_blocks * kTile * kPairCap4 * sizeof(int4), &ok);
     if (cells && k.dims == 3 && c->tsize == 8) c->pos32 = dalloc(c, n * sizeof(float4), &ok);
+    if (cells && k.dims == 3 && c->tsize == 4) {
+      c->rows_stride = (int)((n + 3) & ~(size_t)3);  // rows start on 16 bytes
+      c->pos_rows = dalloc(c, 3 * (size_t)c->rows_stride * sizeof(float), &ok);
+    }
   }
   if (list) {
     c->nbr_n = (int*)dalloc(c, n * 4, &ok);

@@ -96,6 +96,11 @@ struct Params {
   // Float64 3D cell walks: the committed positions rounded to Float32, in
   // slot order, for the walk's filter (k_pos32); null otherwise
   float4* PA32;
+  // Float32 3D cell walks: the committed positions as three rows x | y | z
+  // of ps_stride floats (a multiple of four), for the walk's filter
+  // (k_pos_rows); null otherwise
+  float* PS;
+  int ps_stride;
   // medium: committed / written
   T* c_cur;
   T* c_nxt;
@@ -1079,6 +1084,16 @@ __device__ __forceinline__ float2 f2_mul(float2 a, float2 b) {
   return *reinterpret_cast<float2*>(&r);
 }
 
+__device__ __forceinline__ float2 f2_fma(float2 a, float2 b, float2 c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;"
+      : "=l"(r)
+      : "l"(*reinterpret_cast<unsigned long long*>(&a)),
+        "l"(*reinterpret_cast<unsigned long long*>(&b)),
+        "l"(*reinterpret_cast<unsigned long long*>(&c)));
+  return *reinterpret_cast<float2*>(&r);
+}
+
 // e = xi - xj and its squared norm, in the reference's order
 // ((e0 e0 + e1 e1) + e2 e2); in Float32 the x and y halves are packed pairs.
 template <typename T, int D>
@@ -1195,6 +1210,19 @@ __device__ __forceinline__ float f32_filter_bound(const double* xi, double cut2)
   const double E = u * (2.0 * X + 2.0 * c) * (1.0 + u);
   const double r = c + 1.7320508075688775 * E;
   return __double2float_ru(r * r * (1.0 + 4.0 * u) * (1.0 + 1e-12));
+}
+
+// PS = the committed Float32 positions as rows x | y | z (slots below N).
+template <typename T>
+__global__ void __launch_bounds__(kTile) k_pos_rows(Params<T> P) {
+  const int N = (int)P.ctr->N[P.parity];
+  const int st = P.ps_stride;
+  for (int s = blockIdx.x * kTile + threadIdx.x; s < N; s += gridDim.x * kTile) {
+    const typename V4T<T>::type v = P.PA[s];
+    P.PS[s] = (float)v.x;
+    P.PS[st + s] = (float)v.y;
+    P.PS[2 * st + s] = (float)v.z;
+  }
 }
 
 // PA32 = the committed positions rounded to Float32 (slots below N).
@@ -1480,8 +1508,57 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
           cut2f32 = f32_filter_bound(xi, (double)cut2);
         }
       }
+      // Float32 walks over the position rows: four candidates a step from
+      // three 16-byte loads, their squared distances as packed pairs
+      // (fl(dx dx), then two fused terms: three roundings, as the scalar
+      // filter's, inside the widened cutoff)
+      const float* PS = nullptr;
+      float2 xx = make_float2(0.f, 0.f), yy = xx, zz = xx;
+      if constexpr (std::is_same<T, float>::value && D == 3) {
+        if (P.PS && U == P.PA) {
+          PS = P.PS;
+          xx = make_float2(xi[0], xi[0]);
+          yy = make_float2(xi[1], xi[1]);
+          zz = make_float2(xi[2], xi[2]);
+        }
+      }
       walk_runs<T, D>(P, xi, P.cut_reach, [&](int s0, int s1) {
         int q = s0;
+        if constexpr (std::is_same<T, float>::value && D == 3) {
+          if (PS) {
+            for (; q < s1 && (q & 3); ++q) {  // to a multiple of four
+              room(1);
+              T xj[3];
+              to3<T>(U[q], xj);
+              if (filter_s2<T, D>(xi, xj) < cut2f) push(q);
+            }
+            const int st = P.ps_stride;
+            for (; q + 4 <= s1; q += 4) {
+              room(4);
+              const float4 a = ld(reinterpret_cast<const float4*>(PS + q));
+              const float4 b = ld(reinterpret_cast<const float4*>(PS + st + q));
+              const float4 c = ld(reinterpret_cast<const float4*>(PS + 2 * st + q));
+              const float2 dx0 = f2_sub(xx, make_float2(a.x, a.y)), dx1 = f2_sub(xx, make_float2(a.z, a.w));
+              const float2 dy0 = f2_sub(yy, make_float2(b.x, b.y)), dy1 = f2_sub(yy, make_float2(b.z, b.w));
+              const float2 dz0 = f2_sub(zz, make_float2(c.x, c.y)), dz1 = f2_sub(zz, make_float2(c.z, c.w));
+              const float2 q0 = f2_fma(dz0, dz0, f2_fma(dy0, dy0, f2_mul(dx0, dx0)));
+              const float2 q1 = f2_fma(dz1, dz1, f2_fma(dy1, dy1, f2_mul(dx1, dx1)));
+              const float s2v[4] = {q0.x, q0.y, q1.x, q1.y};
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                queue[nq * kTile + threadIdx.x] = q + u;
+                nq += s2v[u] < cut2f ? 1 : 0;
+              }
+            }
+            for (; q < s1; ++q) {
+              room(1);
+              T xj[3];
+              to3<T>(U[q], xj);
+              if (filter_s2<T, D>(xi, xj) < cut2f) push(q);
+            }
+            return;
+          }
+        }
         if constexpr (std::is_same<T, double>::value && D == 3) {
           if (U32) {
             for (; q + 4 <= s1; q += 4) {
