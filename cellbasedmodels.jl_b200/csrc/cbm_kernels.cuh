@@ -1526,18 +1526,19 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
         int q = s0;
         if constexpr (std::is_same<T, float>::value && D == 3) {
           if (PS) {
+            // one check for room a group of eight candidates (a warp vote),
+            // and one for a run's unaligned head and tail of up to three
+            if (q & 3) room(4);
             for (; q < s1 && (q & 3); ++q) {  // to a multiple of four
-              room(1);
               T xj[3];
               to3<T>(U[q], xj);
               if (filter_s2<T, D>(xi, xj) < cut2f) push(q);
             }
             const int st = P.ps_stride;
-            for (; q + 4 <= s1; q += 4) {
-              room(4);
-              const float4 a = ld(reinterpret_cast<const float4*>(PS + q));
-              const float4 b = ld(reinterpret_cast<const float4*>(PS + st + q));
-              const float4 c = ld(reinterpret_cast<const float4*>(PS + 2 * st + q));
+            auto four = [&](int r) {
+              const float4 a = ld(reinterpret_cast<const float4*>(PS + r));
+              const float4 b = ld(reinterpret_cast<const float4*>(PS + st + r));
+              const float4 c = ld(reinterpret_cast<const float4*>(PS + 2 * st + r));
               const float2 dx0 = f2_sub(xx, make_float2(a.x, a.y)), dx1 = f2_sub(xx, make_float2(a.z, a.w));
               const float2 dy0 = f2_sub(yy, make_float2(b.x, b.y)), dy1 = f2_sub(yy, make_float2(b.z, b.w));
               const float2 dz0 = f2_sub(zz, make_float2(c.x, c.y)), dz1 = f2_sub(zz, make_float2(c.z, c.w));
@@ -1546,12 +1547,22 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
               const float s2v[4] = {q0.x, q0.y, q1.x, q1.y};
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
-                queue[nq * kTile + threadIdx.x] = q + u;
+                queue[nq * kTile + threadIdx.x] = r + u;
                 nq += s2v[u] < cut2f ? 1 : 0;
               }
+            };
+            for (; q + 8 <= s1; q += 8) {
+              room(8);
+              four(q);
+              four(q + 4);
             }
+            if (q + 4 <= s1) {
+              room(4);
+              four(q);
+              q += 4;
+            }
+            if (q < s1) room(4);
             for (; q < s1; ++q) {
-              room(1);
               T xj[3];
               to3<T>(U[q], xj);
               if (filter_s2<T, D>(xi, xj) < cut2f) push(q);
@@ -1561,44 +1572,65 @@ __device__ __forceinline__ void agent_de(const Params<T>& P, const int N, const 
         }
         if constexpr (std::is_same<T, double>::value && D == 3) {
           if (U32) {
-            for (; q + 4 <= s1; q += 4) {
-              room(4);
+            auto four = [&](int r) {
               float s2v[4];
 #pragma unroll
-              for (int u = 0; u < 4; ++u) s2v[u] = filter_s2_f32(xi32, U32[q + u]);
+              for (int u = 0; u < 4; ++u) s2v[u] = filter_s2_f32(xi32, U32[r + u]);
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
-                queue[nq * kTile + threadIdx.x] = q + u;
+                queue[nq * kTile + threadIdx.x] = r + u;
                 nq += s2v[u] < cut2f32 ? 1 : 0;
               }
+            };
+            for (; q + 8 <= s1; q += 8) {
+              room(8);
+              four(q);
+              four(q + 4);
             }
-            for (; q < s1; ++q) {
-              room(1);
+            if (q + 4 <= s1) {
+              room(4);
+              four(q);
+              q += 4;
+            }
+            if (q < s1) room(4);
+            for (; q < s1; ++q)
               if (filter_s2_f32(xi32, U32[q]) < cut2f32) push(q);
-            }
             return;
           }
         }
-        for (; q + 4 <= s1; q += 4) {
-          room(4);
+        // every candidate is written at the queue's end and kept only when it
+        // may be inside the cutoff (room() left space for the group); the
+        // agent itself is skipped in the drain
+        auto four = [&](int r) {
           T s2v[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             T xj[3];
-            to3<T>(U[q + u], xj);
+            to3<T>(U[r + u], xj);
             s2v[u] = filter_s2<T, D>(xi, xj);
           }
-          // every candidate is written at the queue's end and kept only when it
-          // may be inside the cutoff (room() left space for four); the agent
-          // itself is skipped in the drain
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            queue[nq * kTile + threadIdx.x] = q + u;
+            queue[nq * kTile + threadIdx.x] = r + u;
             nq += s2v[u] < cut2f ? 1 : 0;
           }
+        };
+        // candidates a check for room: eight in 1D and 2D; four in 3D, whose
+        // main walks take the paths above and where a longer loop here would
+        // cost the kernel registers
+        constexpr int kGroup = D == 3 ? 4 : 8;
+        for (; q + kGroup <= s1; q += kGroup) {
+          room(kGroup);
+#pragma unroll
+          for (int g = 0; g < kGroup; g += 4) four(q + g);
         }
+        if (kGroup == 8 && q + 4 <= s1) {
+          room(4);
+          four(q);
+          q += 4;
+        }
+        if (q < s1) room(4);
         for (; q < s1; ++q) {
-          room(1);
           T xj[3];
           to3<T>(U[q], xj);
           if (filter_s2<T, D>(xi, xj) < cut2f) push(q);
