@@ -200,9 +200,10 @@ int cbm_download(cbm_ctx* ctx, cbm_state_view* host, int32_t which);
 /* step! x nsteps (step.jl:96-107).  Enqueues the steps (as CUDA graph replays
  * unless CBM_NO_GRAPH) and returns; CBM_SYNC waits and reports device flags.
  * With a medium, the force kernel of a step runs beside the medium kernels,
- * and with a medium gradient a call of 8 steps or more replays graphs of 8
- * chained steps, in which each step's update runs beside the next step's
- * gradient; the results are those of the steps made one by one. */
+ * and with a medium gradient on at most 2^22 nodes a call of 8 steps or more
+ * replays graphs of 8 chained steps, in which each step's update runs beside
+ * the next step's gradient; the results are those of the steps made one by
+ * one. */
 int cbm_step(cbm_ctx* ctx, int32_t nsteps, int32_t flags);
 /* One step! whose Euler–Maruyama increments are given instead of drawn:
  * noise[i * dims + d] ~ N(0,1) for the N agents in index order, in the
